@@ -1,0 +1,226 @@
+/*
+ * vbd_b200.h -- C ABI of the B200 (sm_100a) Vertex Block Descent cloth library.
+ *
+ * This is the drop-in boundary for Newton's particle VBD cloth step.  Every entry point is
+ * plain C: integers, floats, and host or device pointers.  No torch, Warp or CUDA types
+ * appear in a signature; a CUDA stream is passed as `void*` (a `cudaStream_t`, NULL for the
+ * legacy default stream).
+ *
+ * Reference interfaces that each entry point replaces (paths inside the Newton source tree):
+ *
+ *   vbd_model_create      ModelBuilder.finalize -> Model particle/tri/edge/adjacency/coloring
+ *                         arrays (newton/_src/sim/builder.py:10962, :11033-11070, :11796-11832)
+ *                         and MeshAdjacency.init_vertex_adjacency (newton/_src/utils/mesh.py:595)
+ *   vbd_collide           CollisionPipeline.collide soft-contact branch
+ *                         (newton/_src/sim/collide.py:1553-1590) -> create_soft_contacts
+ *                         (newton/_src/geometry/kernels.py:1020-1184)
+ *   vbd_solver_create     SolverVBD.__init__ particle part
+ *                         (newton/_src/solvers/vbd/solver_vbd.py:221-618)
+ *   vbd_step              SolverVBD.step (newton/_src/solvers/vbd/solver_vbd.py:1774-1825),
+ *                         i.e. SolverBase.step(state_in, state_out, control, contacts, dt)
+ *                         (newton/_src/solvers/solver.py:358-373)
+ *   vbd_forward           SolverVBD._initialize_particles (solver_vbd.py:2065-2100):
+ *                         forward_step + apply_truncation_ts
+ *   vbd_sweep_color       one color of SolverVBD._solve_particle_iteration (solver_vbd.py:2552-2702):
+ *                         accumulate_particle_body_contact_force_and_hessian +
+ *                         solve_elasticity(_tile) + apply_truncation_ts
+ *   vbd_finalize          end of _solve_particle_iteration (copy, solver_vbd.py:2704) +
+ *                         SolverVBD._finalize_particles / update_velocity (solver_vbd.py:3158-3169)
+ *   vbd_residual          no reference counterpart: the per-vertex force residual used to gate
+ *                         iterations (Jacobi evaluation of the same force the sweep solves)
+ *   vbd_color_graph       ModelBuilder.color -> color_graph (newton/_src/sim/graph_coloring.py:243-311),
+ *                         whose assignment in the reference is done by Warp's native
+ *                         graph_coloring_assign / graph_coloring_balance
+ *
+ * Status: every function returns 0 (VBD_OK) on success or a VBD_ERR_* code; the message of
+ * the last failure on the calling thread is returned by vbd_last_error().
+ *
+ * Memory: vbd_model_create and vbd_solver_create allocate all device memory the solver will
+ * ever use.  vbd_step, vbd_forward, vbd_sweep_color, vbd_finalize, vbd_residual and
+ * vbd_collide allocate nothing.
+ *
+ * Threading: a solver is not thread-safe (its scratch is mutable), exactly like the reference.
+ */
+#ifndef VBD_B200_H
+#define VBD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------- */
+#define VBD_OK 0
+#define VBD_ERR_INVALID_ARGUMENT 1
+#define VBD_ERR_CUDA 2
+#define VBD_ERR_OUT_OF_MEMORY 3
+#define VBD_ERR_TIMEOUT 4
+#define VBD_ERR_UNSUPPORTED 5
+
+/* ---- reference enumerations (values kept identical) ---------------------------------- */
+/* ParticleFlags (newton/_src/geometry/flags.py:8) */
+#define VBD_PARTICLE_ACTIVE 1
+/* ShapeFlags.COLLIDE_PARTICLES (newton/_src/geometry/flags.py:38) */
+#define VBD_SHAPE_COLLIDE_PARTICLES 4
+/* GeoType (newton/_src/geometry/types.py:70) -- the static primitives this path supports */
+#define VBD_GEO_PLANE 1
+#define VBD_GEO_SPHERE 3
+#define VBD_GEO_BOX 7
+
+/* A static collision shape (Model.shape_* arrays with shape_body == -1). */
+typedef struct VbdShape {
+    int32_t geo_type;      /* VBD_GEO_* */
+    int32_t flags;         /* ShapeFlags bits; VBD_SHAPE_COLLIDE_PARTICLES enables particle contact */
+    int32_t world;         /* shape_world, -1 = global */
+    int32_t reserved;
+    float xform[7];        /* shape_transform: position xyz, quaternion xyzw */
+    float scale[3];        /* shape_scale: plane (width, length, 0); sphere (r, -, -); box (hx, hy, hz) */
+    float margin;          /* shape_margin [m] */
+    float material_ke;     /* shape_material_ke */
+    float material_kd;     /* shape_material_kd */
+    float material_mu;     /* shape_material_mu */
+} VbdShape;
+
+/* Finalized cloth model.  All pointers are HOST pointers, read only during vbd_model_create.
+ * Array layouts are those of newton.Model. */
+typedef struct VbdModelDesc {
+    int32_t particle_count;
+    int32_t tri_count;
+    int32_t edge_count;
+    int32_t shape_count;
+    int32_t color_count;
+    int32_t reserved;
+    const float* particle_mass;            /* [V] */
+    const float* particle_inv_mass;        /* [V] */
+    const float* particle_radius;          /* [V] */
+    const int32_t* particle_flags;         /* [V] */
+    const int32_t* particle_world;         /* [V] or NULL (all global) */
+    const int32_t* tri_indices;            /* [T,3] */
+    const float* tri_poses;                /* [T,2,2] row-major DmInv */
+    const float* tri_materials;            /* [T,5] (ke=mu, ka=lambda, kd, drag, lift) */
+    const float* tri_areas;                /* [T] */
+    const int32_t* edge_indices;           /* [E,4] (o0, o1, v0, v1) */
+    const float* edge_rest_angle;          /* [E] */
+    const float* edge_rest_length;         /* [E] */
+    const float* edge_bending_properties;  /* [E,2] (ke, kd) */
+    const int32_t* v_adj_tris_offsets;     /* [V+1], counts int32 values (2 per record) */
+    const int32_t* v_adj_tris;             /* (tri, slot) pairs */
+    const int32_t* v_adj_edges_offsets;    /* [V+1] */
+    const int32_t* v_adj_edges;            /* (edge, slot) pairs */
+    const int32_t* color_group_offsets;    /* [C+1] offsets into color_group_particles */
+    const int32_t* color_group_particles;  /* concatenated Model.particle_color_groups */
+    float gravity[3];                      /* Model.gravity[0] (the reference applies world 0's) */
+    float soft_contact_ke;                 /* Model.soft_contact_ke */
+    float soft_contact_kd;                 /* Model.soft_contact_kd */
+    float soft_contact_mu;                 /* Model.soft_contact_mu */
+    const VbdShape* shapes;                /* [S] */
+} VbdModelDesc;
+
+/* Solver options (SolverVBD keyword arguments that touch the particle path, plus launch shape). */
+typedef struct VbdSolverOptions {
+    int32_t iterations;           /* default VBD iterations per step (reference default 10) */
+    float friction_epsilon;       /* reference default 1e-2 */
+    int32_t lanes_per_vertex;     /* 1,2,4,8,16 or 0 = pick from the mesh (autotuner may override) */
+    int32_t block_size;           /* threads per block of the sweep, 0 = default 128 */
+    int32_t contacts_per_vertex;  /* capacity of the per-vertex contact table, 0 = default 4 */
+    int32_t use_graph;            /* 1: replay vbd_step from a cached CUDA graph */
+} VbdSolverOptions;
+
+/* Soft-contact records in the reference layout (newton.Contacts soft_contact_*; DEVICE pointers). */
+typedef struct VbdContacts {
+    int32_t soft_contact_max;
+    int32_t reserved;
+    int32_t* soft_contact_count;        /* [1] */
+    int32_t* soft_contact_particle;     /* [max] */
+    int32_t* soft_contact_indices;      /* [max,3]  (p, -1, -1) */
+    float* soft_contact_barycentric;    /* [max,3]  (1, 0, 0) */
+    int32_t* soft_contact_shape;        /* [max] */
+    float* soft_contact_body_pos;       /* [max,3] */
+    float* soft_contact_body_vel;       /* [max,3] */
+    float* soft_contact_normal;         /* [max,3] */
+} VbdContacts;
+
+/* Device status counters since the solver was created (or last reset). */
+typedef struct VbdStatus {
+    int64_t steps;
+    int32_t nonfinite_updates;    /* vertex updates whose displacement was NaN/Inf (update skipped) */
+    int32_t singular_blocks;      /* |det H| <= 1e-8: update skipped, as in the reference */
+    int32_t contact_overflow;     /* contacts dropped because a vertex had more than the table holds */
+    int32_t timeouts;             /* bounded grid-barrier waits that gave up */
+} VbdStatus;
+
+typedef struct VbdModel VbdModel;
+typedef struct VbdSolver VbdSolver;
+
+/* Message of the last error on this thread ("" if none). */
+const char* vbd_last_error(void);
+
+/* Library version string. */
+const char* vbd_version(void);
+
+/* Build the device-resident model on the current CUDA device (copies and re-lays-out all arrays).
+ * Replaces ModelBuilder.finalize's uploads (builder.py:11033-11070, :11796-11832). */
+int vbd_model_create(const VbdModelDesc* desc, VbdModel** out);
+int vbd_model_destroy(VbdModel* model);
+
+/* Particle-vs-static-shape contact generation: CollisionPipeline.collide soft branch
+ * (collide.py:1553-1590) / create_soft_contacts (geometry/kernels.py:1020-1184).
+ * particle_q: DEVICE [V,3] float32.  Resets and fills `contacts` (count included). */
+int vbd_collide(const VbdModel* model, const float* particle_q, float soft_contact_margin,
+                const VbdContacts* contacts, void* stream);
+
+/* SolverVBD(model, iterations=..., friction_epsilon=...) particle part (solver_vbd.py:221-618). */
+int vbd_solver_create(const VbdModel* model, const VbdSolverOptions* options, VbdSolver** out);
+int vbd_solver_destroy(VbdSolver* solver);
+
+/* SolverVBD.step(state_in, state_out, control, contacts, dt) (solver_vbd.py:1774-1825).
+ * All arrays DEVICE [V,3] float32 in the model's particle order.
+ *   q_in   : state_in.particle_q   -- read, then OVERWRITTEN with the solved positions
+ *            (the reference keeps its Gauss-Seidel iterate in state_in.particle_q)
+ *   qd_in  : state_in.particle_qd  -- read
+ *   f_ext  : state_in.particle_f   -- read (may be NULL = zero external force)
+ *   q_out  : state_out.particle_q  -- written
+ *   qd_out : state_out.particle_qd -- written
+ * contacts may be NULL (no particle-shape contact).  iterations < 0 uses the solver default. */
+int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, const float* f_ext, float* q_out,
+             float* qd_out, const VbdContacts* contacts, float dt, int32_t iterations, void* stream);
+
+/* Staged pieces of vbd_step, for parity tests against a staged oracle. */
+int vbd_forward(VbdSolver* solver, const float* q_in, const float* qd_in, const float* f_ext,
+                const VbdContacts* contacts, float dt, void* stream);
+int vbd_sweep_color(VbdSolver* solver, int32_t color, const VbdContacts* contacts, float dt, void* stream);
+int vbd_finalize(VbdSolver* solver, float* q_in, float* q_out, float* qd_out, float dt, void* stream);
+
+/* Copy the solver's current Gauss-Seidel iterate (model particle order) into q_out [V,3] (DEVICE). */
+int vbd_get_positions(const VbdSolver* solver, float* q_out, void* stream);
+
+/* Force residual at the current iterate, evaluated for every vertex at the same positions
+ * (Jacobi): r_i = |m_i (y_i - x_i)/dt^2 + f_i^elastic + f_i^contact| / (m_i |g|) for active
+ * vertices with m_i > 0, 0 otherwise.  per_vertex_out [V] (DEVICE, may be NULL) and
+ * max_out [1] (DEVICE, may be NULL). */
+int vbd_residual(VbdSolver* solver, const VbdContacts* contacts, float dt, float* per_vertex_out,
+                 float* max_out, void* stream);
+
+/* Read (synchronously) and optionally reset the device status counters. */
+int vbd_status(VbdSolver* solver, VbdStatus* out, int32_t reset);
+
+/* Number of colors and vertex count of each color as laid out on the device (host out arrays). */
+int vbd_solver_info(const VbdSolver* solver, int32_t* color_count, int32_t* lanes_per_vertex,
+                    int32_t* block_size);
+
+/* Override the sweep launch shape (used by the autotuner).  lanes in {1,2,4,8,16}. */
+int vbd_set_launch(VbdSolver* solver, int32_t lanes_per_vertex, int32_t block_size);
+
+/* Graph coloring of an undirected graph (host arrays): ModelBuilder.color -> color_graph
+ * (graph_coloring.py:243-311).  algorithm 0 = maximum cardinality search (MCS), 1 = degree-ordered
+ * greedy.  edges: [num_edges,2].  colors_out: [num_nodes].  With balance != 0, vertices are moved
+ * out of the largest color until max/min color size <= target_ratio or no move is possible. */
+int vbd_color_graph(int32_t num_nodes, int64_t num_edges, const int32_t* edges, int32_t algorithm,
+                    int32_t balance, float target_ratio, int32_t* colors_out, int32_t* num_colors_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VBD_B200_H */

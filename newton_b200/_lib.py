@@ -1,0 +1,218 @@
+"""ctypes binding of ``libvbd_b200.so`` (declared in ``include/vbd_b200.h``).
+
+The library is the only compute path: if it is missing or cannot be loaded, every solver call
+raises -- there is no CPU or eager fallback.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libvbd_b200.so"
+
+VBD_OK = 0
+VBD_ERR_INVALID_ARGUMENT = 1
+VBD_ERR_CUDA = 2
+VBD_ERR_OUT_OF_MEMORY = 3
+VBD_ERR_TIMEOUT = 4
+VBD_ERR_UNSUPPORTED = 5
+
+c_int32_p = ctypes.POINTER(ctypes.c_int32)
+c_float_p = ctypes.POINTER(ctypes.c_float)
+
+
+class VbdShape(ctypes.Structure):
+    _fields_ = [
+        ("geo_type", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
+        ("world", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("xform", ctypes.c_float * 7),
+        ("scale", ctypes.c_float * 3),
+        ("margin", ctypes.c_float),
+        ("material_ke", ctypes.c_float),
+        ("material_kd", ctypes.c_float),
+        ("material_mu", ctypes.c_float),
+    ]
+
+
+class VbdModelDesc(ctypes.Structure):
+    _fields_ = [
+        ("particle_count", ctypes.c_int32),
+        ("tri_count", ctypes.c_int32),
+        ("edge_count", ctypes.c_int32),
+        ("shape_count", ctypes.c_int32),
+        ("color_count", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("particle_mass", c_float_p),
+        ("particle_inv_mass", c_float_p),
+        ("particle_radius", c_float_p),
+        ("particle_flags", c_int32_p),
+        ("particle_world", c_int32_p),
+        ("tri_indices", c_int32_p),
+        ("tri_poses", c_float_p),
+        ("tri_materials", c_float_p),
+        ("tri_areas", c_float_p),
+        ("edge_indices", c_int32_p),
+        ("edge_rest_angle", c_float_p),
+        ("edge_rest_length", c_float_p),
+        ("edge_bending_properties", c_float_p),
+        ("v_adj_tris_offsets", c_int32_p),
+        ("v_adj_tris", c_int32_p),
+        ("v_adj_edges_offsets", c_int32_p),
+        ("v_adj_edges", c_int32_p),
+        ("color_group_offsets", c_int32_p),
+        ("color_group_particles", c_int32_p),
+        ("gravity", ctypes.c_float * 3),
+        ("soft_contact_ke", ctypes.c_float),
+        ("soft_contact_kd", ctypes.c_float),
+        ("soft_contact_mu", ctypes.c_float),
+        ("shapes", ctypes.POINTER(VbdShape)),
+    ]
+
+
+class VbdSolverOptions(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int32),
+        ("friction_epsilon", ctypes.c_float),
+        ("lanes_per_vertex", ctypes.c_int32),
+        ("block_size", ctypes.c_int32),
+        ("contacts_per_vertex", ctypes.c_int32),
+        ("use_graph", ctypes.c_int32),
+    ]
+
+
+class VbdContacts(ctypes.Structure):
+    _fields_ = [
+        ("soft_contact_max", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("soft_contact_count", ctypes.c_void_p),
+        ("soft_contact_particle", ctypes.c_void_p),
+        ("soft_contact_indices", ctypes.c_void_p),
+        ("soft_contact_barycentric", ctypes.c_void_p),
+        ("soft_contact_shape", ctypes.c_void_p),
+        ("soft_contact_body_pos", ctypes.c_void_p),
+        ("soft_contact_body_vel", ctypes.c_void_p),
+        ("soft_contact_normal", ctypes.c_void_p),
+    ]
+
+
+class VbdStatus(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_int64),
+        ("nonfinite_updates", ctypes.c_int32),
+        ("singular_blocks", ctypes.c_int32),
+        ("contact_overflow", ctypes.c_int32),
+        ("timeouts", ctypes.c_int32),
+    ]
+
+
+# (name, restype, argtypes) of every exported entry point declared in include/vbd_b200.h
+_VP = ctypes.c_void_p
+SIGNATURES = {
+    "vbd_last_error": (ctypes.c_char_p, []),
+    "vbd_version": (ctypes.c_char_p, []),
+    "vbd_model_create": (ctypes.c_int, [ctypes.POINTER(VbdModelDesc), ctypes.POINTER(_VP)]),
+    "vbd_model_destroy": (ctypes.c_int, [_VP]),
+    "vbd_collide": (ctypes.c_int, [_VP, _VP, ctypes.c_float, ctypes.POINTER(VbdContacts), _VP]),
+    "vbd_solver_create": (ctypes.c_int, [_VP, ctypes.POINTER(VbdSolverOptions), ctypes.POINTER(_VP)]),
+    "vbd_solver_destroy": (ctypes.c_int, [_VP]),
+    "vbd_step": (
+        ctypes.c_int,
+        [_VP, _VP, _VP, _VP, _VP, _VP, ctypes.POINTER(VbdContacts), ctypes.c_float, ctypes.c_int32, _VP],
+    ),
+    "vbd_forward": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.POINTER(VbdContacts), ctypes.c_float, _VP]),
+    "vbd_sweep_color": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(VbdContacts), ctypes.c_float, _VP]),
+    "vbd_finalize": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_float, _VP]),
+    "vbd_get_positions": (ctypes.c_int, [_VP, _VP, _VP]),
+    "vbd_residual": (ctypes.c_int, [_VP, ctypes.POINTER(VbdContacts), ctypes.c_float, _VP, _VP, _VP]),
+    "vbd_status": (ctypes.c_int, [_VP, ctypes.POINTER(VbdStatus), ctypes.c_int32]),
+    "vbd_solver_info": (ctypes.c_int, [_VP, c_int32_p, c_int32_p, c_int32_p]),
+    "vbd_set_launch": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),
+    "vbd_color_graph": (
+        ctypes.c_int,
+        [ctypes.c_int32, ctypes.c_int64, c_int32_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, c_int32_p, c_int32_p],
+    ),
+}
+
+_lib = None
+
+
+def load(build_if_missing: bool = True) -> ctypes.CDLL:
+    """Load (building in-tree first if needed) the CUDA library; raises if it cannot."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists() and build_if_missing and os.environ.get("VBD_NO_BUILD") != "1":
+        from . import build as _build
+
+        _build.build()
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m newton_b200.build`")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+class VbdError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[vbd error {code}] {message}")
+        self.code = code
+
+
+def check(code: int) -> None:
+    if code != VBD_OK:
+        msg = load().vbd_last_error()
+        raise VbdError(code, msg.decode() if msg else "")
+
+
+def ptr(arr) -> ctypes.c_void_p | None:
+    """Address of a torch tensor / numpy array (None -> NULL)."""
+    if arr is None:
+        return None
+    if isinstance(arr, np.ndarray):
+        return ctypes.c_void_p(arr.ctypes.data)
+    return ctypes.c_void_p(arr.data_ptr())
+
+
+def as_i32p(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(c_int32_p)
+
+
+def as_f32p(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(c_float_p)
+
+
+def color_graph(num_nodes: int, edges: np.ndarray, algorithm: int = 0, balance: bool = True, target_ratio: float = 1.1):
+    """Color an undirected graph with the library's host coloring (vbd_color_graph)."""
+    lib = load()
+    edges = np.ascontiguousarray(np.asarray(edges, dtype=np.int32).reshape(-1, 2))
+    colors = np.empty(num_nodes, dtype=np.int32)
+    nc = ctypes.c_int32(0)
+    check(
+        lib.vbd_color_graph(
+            num_nodes,
+            edges.shape[0],
+            as_i32p(edges) if edges.size else None,
+            algorithm,
+            1 if balance else 0,
+            float(target_ratio),
+            as_i32p(colors) if num_nodes else None,
+            ctypes.byref(nc),
+        )
+    )
+    return colors, int(nc.value)

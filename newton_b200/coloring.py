@@ -1,0 +1,110 @@
+"""Particle conflict graph and color groups for the Gauss-Seidel sweep.
+
+* ``construct_trimesh_graph_edges`` restates ``graph_coloring.py:99-197``: every active triangle
+  contributes its three sides; with bending, every active hinge contributes all six pairs of its
+  four vertices (negative ids skipped); pairs are canonicalised (sorted, unique).
+* ``color_graph`` restates ``graph_coloring.py:243-311`` on top of the library's host coloring
+  (``vbd_color_graph``: MCS or degree-ordered greedy, then balancing).
+* ``combine_independent_coloring_plan`` restates ``graph_coloring.py:382-410``: the colorings of
+  independent worlds are merged by pairing the smallest groups of one with the largest of the
+  other.
+"""
+
+from __future__ import annotations
+
+from enum import Enum
+
+import numpy as np
+
+from . import _lib
+
+
+class ColoringAlgorithm(Enum):
+    MCS = 0
+    GREEDY = 1
+
+
+def _canonicalize_edges(edges: np.ndarray) -> np.ndarray:
+    if edges.size == 0:
+        return np.empty((0, 2), dtype=np.int32)
+    e = np.sort(edges.astype(np.int64), axis=1)
+    e = e[e[:, 0] != e[:, 1]]
+    return np.unique(e, axis=0).astype(np.int32)
+
+
+def construct_trimesh_graph_edges(tri_indices, tri_active_mask=None, bending_edge_indices=None,
+                                  bending_edge_active_mask=None) -> np.ndarray:
+    parts = []
+    if tri_indices is not None:
+        tris = np.asarray(tri_indices, dtype=np.int32).reshape(-1, 3)
+        if tri_active_mask is not None:
+            m = np.asarray(tri_active_mask).astype(bool)
+            tris = tris if m.ndim == 0 and m else (tris[:0] if m.ndim == 0 else tris[m])
+        if tris.size:
+            parts.append(np.concatenate([tris[:, [0, 1]], tris[:, [0, 2]], tris[:, [1, 2]]], axis=0))
+    if bending_edge_indices is not None:
+        bend = np.asarray(bending_edge_indices, dtype=np.int32).reshape(-1, 4)
+        if bending_edge_active_mask is not None:
+            m = np.asarray(bending_edge_active_mask).astype(bool)
+            bend = bend if m.ndim == 0 and m else (bend[:0] if m.ndim == 0 else bend[m])
+        if bend.size:
+            pairs = np.concatenate(
+                [bend[:, [0, 1]], bend[:, [0, 2]], bend[:, [0, 3]], bend[:, [1, 2]], bend[:, [1, 3]], bend[:, [2, 3]]],
+                axis=0,
+            )
+            pairs = pairs[np.all(pairs >= 0, axis=1)]
+            if pairs.size:
+                parts.append(pairs)
+    if not parts:
+        return np.empty((0, 2), dtype=np.int32)
+    return _canonicalize_edges(np.concatenate(parts, axis=0))
+
+
+def convert_to_color_groups(num_colors: int, particle_colors: np.ndarray) -> list[np.ndarray]:
+    order = np.argsort(particle_colors, kind="stable")
+    counts = np.bincount(particle_colors, minlength=num_colors)
+    splits = np.cumsum(counts)[:-1]
+    return [g.astype(np.int32) for g in np.split(order, splits)]
+
+
+def color_graph(num_nodes: int, graph_edge_indices: np.ndarray, balance_colors: bool = True,
+                target_max_min_color_ratio: float = 1.1,
+                algorithm: ColoringAlgorithm = ColoringAlgorithm.MCS) -> list[np.ndarray]:
+    if num_nodes == 0:
+        return []
+    edges = np.asarray(graph_edge_indices)
+    if edges.ndim != 2:
+        raise ValueError(f"graph_edge_indices must be a 2 dimensional array! The provided one is {edges.ndim} dimensional.")
+    colors, nc = _lib.color_graph(num_nodes, edges, algorithm.value, balance_colors, target_max_min_color_ratio)
+    return convert_to_color_groups(nc, colors)
+
+
+def validate_coloring(graph_edges: np.ndarray, color_groups: list[np.ndarray], num_nodes: int) -> bool:
+    """True when no graph edge joins two vertices of the same color (and every vertex has one)."""
+    colors = np.full(num_nodes, -1, dtype=np.int64)
+    for c, g in enumerate(color_groups):
+        colors[np.asarray(g)] = c
+    if np.any(colors < 0):
+        return False
+    e = np.asarray(graph_edges).reshape(-1, 2)
+    return bool(np.all(colors[e[:, 0]] != colors[e[:, 1]])) if e.size else True
+
+
+def combine_independent_coloring_plan(sized_groups_1: list, sized_groups_2: list) -> list:
+    """Pair (size, chunks) groups of two independent colorings, smallest with largest."""
+    if len(sized_groups_1) == 0:
+        return sized_groups_2
+    if len(sized_groups_2) == 0:
+        return sized_groups_1
+    if len(sized_groups_1) < len(sized_groups_2):
+        sized_groups_1, sized_groups_2 = sized_groups_2, sized_groups_1
+    g1 = sorted(sized_groups_1, key=lambda g: g[0])
+    g2 = sorted(sized_groups_2, key=lambda g: -g[0])
+    out = []
+    for i, (s1, c1) in enumerate(g1):
+        if i < len(g2):
+            s2, c2 = g2[i]
+            out.append((s1 + s2, c1 + c2))
+        else:
+            out.append((s1, c1))
+    return out

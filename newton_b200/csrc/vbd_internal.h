@@ -1,0 +1,73 @@
+// vbd_internal.h -- host-side structures shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/vbd_b200.h"
+
+namespace vbd {
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t err, const char* what);
+
+#define VBD_CUDA_TRY(expr)                                       \
+    do {                                                         \
+        cudaError_t _e = (expr);                                 \
+        if (_e != cudaSuccess) return ::vbd::cuda_fail(_e, #expr); \
+    } while (0)
+
+// Per-shape data the device needs (16-byte members first).
+struct DevShape {
+    float4 mat;        // mixed contact (ke, kd, mu) and the shape margin
+    float4 pos;        // xyz + geo type (as float)
+    float4 rot;        // quaternion xyzw
+    float4 scale;      // xyz + flags (as float)
+    int world;
+    int pad[3];
+};
+
+// Device-resident model in the B200 layout:
+//  * vertices are renumbered color-major (color c occupies [color_start[c], color_start[c+1]) of
+//    the internal order, ascending original index inside a color), so each per-color launch
+//    reads its vertices' own data contiguously;
+//  * each vertex owns a contiguous run of element records (triangles first, then hinges): the
+//    element's vertex ids in internal numbering plus its rest data, replicated per incident
+//    vertex, so the sweep streams records instead of chasing CSR -> element -> data.
+struct VbdModelImpl {
+    int device = 0;
+    int V = 0, T = 0, E = 0, S = 0, C = 0;
+    int swept = 0;                    // vertices covered by a color (the rest are never solved)
+    int n_tri_rec = 0, n_edge_rec = 0;
+    bool fused_commit = true;         // colors are conflict-free for every element stencil
+    bool any_tri_damping = false, any_edge_damping = false;
+    float gravity[3] = {0, 0, 0};
+    float gravity_norm = 0.f;
+    std::vector<int> color_start;     // [C+1] internal offsets
+    std::vector<int> perm_host;       // internal -> original
+    // device arrays
+    int* perm = nullptr;              // [V] internal -> original
+    int* inv_perm = nullptr;          // [V] original -> internal
+    float4* pinfo = nullptr;          // [V] (mass, inv_mass, radius, flags as float bits)
+    int4* vadj = nullptr;             // [V] (tri_begin, tri_end, edge_begin, edge_end)
+    int4* tri_idx = nullptr;          // [n_tri_rec] internal vertex ids (order packed in bits 30-31 of .w)
+    float4* tri_D = nullptr;          // [n_tri_rec] DmInv 00, 01, 10, 11
+    float4* tri_mat = nullptr;        // [n_tri_rec] area, mu, lambda, kd
+    int4* edge_idx = nullptr;         // [n_edge_rec] o0, o1, v0, v1 (internal ids); order in bits 30-31 of .x
+    float4* edge_mat = nullptr;       // [n_edge_rec] rest angle, rest length, ke, kd
+    DevShape* shapes = nullptr;       // [S]
+    int* particle_world = nullptr;    // [V] original order (collide)
+    int* particle_flags_orig = nullptr;   // [V] original order (collide)
+    float* particle_radius_orig = nullptr;  // [V] original order (collide)
+    std::vector<DevShape> shapes_host;
+};
+
+}  // namespace vbd
+
+struct VbdModel {
+    vbd::VbdModelImpl m;
+};

@@ -1,0 +1,768 @@
+// vbd_solver.cu -- the VBD particle step on B200: forward (inertia) kernel, per-color
+// Gauss-Seidel sweep, finalize (velocity) kernel, residual kernel, CUDA-graph replay of a step.
+//
+// Step structure (SolverVBD.step, solver_vbd.py:1774-1825, particle part only):
+//   forward   : _initialize_particles (solver_vbd.py:2065-2100) = forward_step
+//               (particle_vbd_kernels.py:1350-1375) + apply_truncation_ts (:2266-2286) with t = 1,
+//               max_displacement = inf; also scatters this step's soft-contact records into a
+//               per-vertex table (replaces accumulate_particle_body_contact_force_and_hessian's
+//               per-color scan over all records, :2289-2401).
+//   sweep(c)  : one color of _solve_particle_iteration (solver_vbd.py:2552-2702): contact
+//               accumulation, solve_elasticity_tile (:2404-2565) and apply_truncation_ts,
+//               fused into one launch over the color's vertices only.
+//   finalize  : wp.copy(state_out.q, state_in.q) (solver_vbd.py:2704) + update_velocity
+//               (particle_vbd_kernels.py:1468-1471).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "vbd_internal.h"
+#include "vbd_math.cuh"
+
+namespace vbd {
+
+enum StatusSlot { kNonfinite = 0, kSingular = 1, kOverflow = 2, kTimeout = 3, kStatusSlots = 4 };
+
+struct GraphEntry {
+    float* q_in;
+    const float* qd_in;
+    const float* f_ext;
+    float* q_out;
+    float* qd_out;
+    VbdContacts contacts;
+    bool has_contacts;
+    float dt;
+    int iterations;
+    int lanes, block;
+    cudaGraphExec_t exec;
+};
+
+struct SolverImpl {
+    const VbdModelImpl* m = nullptr;
+    int iterations = 10;
+    float friction_epsilon = 1e-2f;
+    int lanes = 4;
+    int block = 128;
+    int K = 4;
+    bool use_graph = true;
+    long long steps = 0;
+    // scratch (allocated once at create)
+    float4* pos = nullptr;    // Gauss-Seidel iterate (state_in.particle_q in the reference)
+    float4* prev = nullptr;   // particle_q_prev == pos_prev_collision_detection (step start)
+    float4* y = nullptr;      // inertia target, .w = mass
+    float4* disp = nullptr;   // particle_displacements
+    int* ccount = nullptr;    // [V] contacts per vertex (internal order)
+    int* cslot = nullptr;     // [V*K] record ids
+    unsigned* status = nullptr;  // [kStatusSlots]
+    float* resid_max = nullptr;  // [1] scratch for vbd_residual
+    cudaStream_t capture_stream = nullptr;
+    std::vector<GraphEntry> graphs;
+};
+
+}  // namespace vbd
+
+struct VbdSolver {
+    vbd::SolverImpl s;
+};
+
+namespace vbd {
+
+// ---------------------------------------------------------------------------------------------
+// kernels
+// ---------------------------------------------------------------------------------------------
+struct ForwardArgs {
+    const int* perm;
+    const int* inv_perm;
+    const float4* pinfo;
+    const float* q_in;
+    const float* qd_in;
+    const float* f_ext;
+    float4* pos;
+    float4* prev;
+    float4* y;
+    float4* disp;
+    int V;
+    float3 g;
+    float dt;
+    // contact scatter
+    const int* c_count;
+    const int* c_particle;
+    int c_max;
+    int* ccount;
+    int* cslot;
+    int K;
+    unsigned* status;
+};
+
+__global__ void forward_kernel(ForwardArgs a) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid < a.V) {
+        const int i = tid;
+        const int o = a.perm[i];
+        const float4 pi = a.pinfo[i];
+        const int flags = __float_as_int(pi.w);
+        const float3 q = f3(a.q_in[3 * o], a.q_in[3 * o + 1], a.q_in[3 * o + 2]);
+        float3 yv = q, dv = f3(0.f, 0.f, 0.f);
+        if ((flags & VBD_PARTICLE_ACTIVE) && pi.y != 0.0f) {
+            const float3 v = f3(a.qd_in[3 * o], a.qd_in[3 * o + 1], a.qd_in[3 * o + 2]);
+            float3 fe = f3(0.f, 0.f, 0.f);
+            if (a.f_ext) fe = f3(a.f_ext[3 * o], a.f_ext[3 * o + 1], a.f_ext[3 * o + 2]);
+            const float3 vn = v + (a.g + fe * pi.y) * a.dt;
+            yv = q + vn * a.dt;
+            dv = vn * a.dt;
+        }
+        a.prev[i] = make_float4(q.x, q.y, q.z, 0.f);
+        a.y[i] = make_float4(yv.x, yv.y, yv.z, pi.x);
+        a.disp[i] = make_float4(dv.x, dv.y, dv.z, 0.f);
+        const float3 p = q + dv;
+        a.pos[i] = make_float4(p.x, p.y, p.z, 0.f);
+    }
+    if (a.c_count) {
+        const int n = min(*a.c_count, a.c_max);
+        if (tid < n) {
+            const int ip = a.inv_perm[a.c_particle[tid]];
+            const int k = atomicAdd(&a.ccount[ip], 1);
+            if (k < a.K) {
+                a.cslot[ip * a.K + k] = tid;
+            } else {
+                atomicAdd(&a.status[kOverflow], 1u);
+            }
+        }
+    }
+}
+
+struct SweepArgs {
+    float4* pos;
+    const float4* prev;
+    const float4* y;
+    float4* disp;
+    const int4* vadj;
+    const float4* pinfo;
+    const int4* tri_idx;
+    const float4* tri_D;
+    const float4* tri_mat;
+    const int4* edge_idx;
+    const float4* edge_mat;
+    // contacts
+    const int* ccount;
+    const int* cslot;
+    int K;
+    const int* c_shape;
+    const float* c_body_pos;
+    const float* c_body_vel;
+    const float* c_normal;
+    const DevShape* shapes;
+    // constants
+    float dt, inv_dt, dt_sqr_recip, eps_u;
+    unsigned* status;
+    int v_begin, v_end;
+    int write_pos;           // 1: commit q = prev + disp in place (conflict-free coloring)
+    float* resid_out;        // residual mode: per-vertex residual (original order) or NULL
+    float* resid_max;        // residual mode: max residual (float bits, atomicMax)
+    const int* perm;
+    float inv_g;             // 1/|g| (0 when g = 0)
+};
+
+template <bool kDamp>
+__device__ __forceinline__ void accumulate_elements(const SweepArgs& a, int i, int lane, int L, int4 adj, float3& f,
+                                                    Sym3& h) {
+    for (int r = adj.x + lane; r < adj.y; r += L) {
+        const int4 ti = __ldg(&a.tri_idx[r]);
+        const float4 D = __ldg(&a.tri_D[r]);
+        const float4 mt = __ldg(&a.tri_mat[r]);
+        const float3 x0 = xyz(a.pos[ti.x]), x1 = xyz(a.pos[ti.y]), x2 = xyz(a.pos[ti.z]);
+        float3 p0 = x0, p1 = x1, p2 = x2;
+        if (kDamp && mt.w > 0.0f) {
+            p0 = xyz(__ldg(&a.prev[ti.x]));
+            p1 = xyz(__ldg(&a.prev[ti.y]));
+            p2 = xyz(__ldg(&a.prev[ti.z]));
+        }
+        membrane_eval<kDamp>(ti.w, x0, x1, x2, p0, p1, p2, D, mt, a.inv_dt, f, h);
+    }
+    for (int r = adj.z + lane; r < adj.w; r += L) {
+        const int4 ei = __ldg(&a.edge_idx[r]);
+        const float4 em = __ldg(&a.edge_mat[r]);
+        const int order = static_cast<int>(static_cast<unsigned>(ei.x) >> 30);
+        const int o0 = ei.x & 0x3fffffff;
+        const float3 x0 = xyz(a.pos[o0]), x1 = xyz(a.pos[ei.y]), x2 = xyz(a.pos[ei.z]), x3 = xyz(a.pos[ei.w]);
+        float3 p0 = x0, p1 = x1, p2 = x2, p3 = x3;
+        if (kDamp && em.w > 0.0f) {
+            p0 = xyz(__ldg(&a.prev[o0]));
+            p1 = xyz(__ldg(&a.prev[ei.y]));
+            p2 = xyz(__ldg(&a.prev[ei.z]));
+            p3 = xyz(__ldg(&a.prev[ei.w]));
+        }
+        bending_eval<kDamp>(order, x0, x1, x2, x3, p0, p1, p2, p3, em, a.inv_dt, f, h);
+    }
+}
+
+__device__ __forceinline__ void accumulate_contacts(const SweepArgs& a, int i, float3 x, float3 xp, float radius,
+                                                    float3& f, Sym3& h) {
+    const int n = min(a.ccount[i], a.K);
+    if (n <= 0) return;
+    int ids[8];
+    const int nn = min(n, 8);
+    for (int k = 0; k < nn; ++k) ids[k] = a.cslot[i * a.K + k];
+    // records of one particle are summed in record order (the order the reference's serial
+    // launch adds them); the scatter in forward_kernel is unordered, so sort the few ids here
+    for (int p = 1; p < nn; ++p) {
+        const int v = ids[p];
+        int q = p - 1;
+        while (q >= 0 && ids[q] > v) {
+            ids[q + 1] = ids[q];
+            --q;
+        }
+        ids[q + 1] = v;
+    }
+    for (int k = 0; k < nn; ++k) {
+        const int r = ids[k];
+        const DevShape& sh = a.shapes[a.c_shape[r]];
+        const float3 bx = f3(a.c_body_pos[3 * r], a.c_body_pos[3 * r + 1], a.c_body_pos[3 * r + 2]);
+        const float3 bv = f3(a.c_body_vel[3 * r], a.c_body_vel[3 * r + 1], a.c_body_vel[3 * r + 2]);
+        const float3 nrm = f3(a.c_normal[3 * r], a.c_normal[3 * r + 1], a.c_normal[3 * r + 2]);
+        contact_eval(x, xp, bx, bv, nrm, radius, sh.mat, a.dt, a.eps_u, f, h);
+    }
+}
+
+__device__ __forceinline__ float warp_sum(float v, int L) {
+    for (int off = L >> 1; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+// One Gauss-Seidel color (kResidual = false) or a Jacobi residual evaluation over a vertex range
+// (kResidual = true).  L lanes cooperate on one vertex: each lane takes every L-th element record
+// (triangles, then hinges, as the reference's 16-thread tile does), then the partial force and
+// Hessian are summed across the L lanes with xor shuffles.
+template <int L, bool kDamp, bool kResidual>
+__global__ void __launch_bounds__(256) sweep_kernel(SweepArgs a) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = a.v_begin + tid / L;
+    const int lane = tid & (L - 1);
+    const bool valid = i < a.v_end;
+    float3 f = f3(0.f, 0.f, 0.f);
+    Sym3 h = zero_sym();
+    bool solve = false;
+    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) {
+        pi = __ldg(&a.pinfo[i]);
+        solve = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
+        if (solve) accumulate_elements<kDamp>(a, i, lane, L, __ldg(&a.vadj[i]), f, h);
+    }
+    if (L > 1) {
+        f.x = warp_sum(f.x, L);
+        f.y = warp_sum(f.y, L);
+        f.z = warp_sum(f.z, L);
+        h.xx = warp_sum(h.xx, L);
+        h.xy = warp_sum(h.xy, L);
+        h.xz = warp_sum(h.xz, L);
+        h.yy = warp_sum(h.yy, L);
+        h.yz = warp_sum(h.yz, L);
+        h.zz = warp_sum(h.zz, L);
+    }
+    if (!valid || lane != 0) return;
+    const float4 pv = a.prev[i];
+    if (!solve) {
+        if (kResidual) {
+            if (a.resid_out) a.resid_out[a.perm[i]] = 0.0f;
+        } else {
+            a.disp[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (a.write_pos) a.pos[i] = pv;
+        }
+        return;
+    }
+    const float4 xv = a.pos[i];
+    const float3 x = xyz(xv);
+    const float4 yv = a.y[i];
+    const float mass = yv.w;
+    float3 fc = f3(0.f, 0.f, 0.f);
+    Sym3 hc = zero_sym();
+    if (a.ccount) accumulate_contacts(a, i, x, xyz(pv), pi.z, fc, hc);
+    // h_total = h_elastic + m/dt^2 I + h_contact ; f_total = f_elastic + m (y - x)/dt^2 + f_contact
+    add_diag(h, mass * a.dt_sqr_recip);
+    add(h, hc);
+    const float3 fi = (mass * (xyz(yv) - x)) * a.dt_sqr_recip;
+    f = f + fi + fc;
+    if (kResidual) {
+        const float r = length(f) / mass * a.inv_g;
+        if (a.resid_out) a.resid_out[a.perm[i]] = r;
+        if (a.resid_max) atomicMax(reinterpret_cast<int*>(a.resid_max), __float_as_int(r));
+        return;
+    }
+    float3 dx;
+    float4 d = a.disp[i];
+    if (solve3(h, f, dx)) {
+        if (isfinite(dx.x) && isfinite(dx.y) && isfinite(dx.z)) {
+            d = make_float4(d.x + dx.x, d.y + dx.y, d.z + dx.z, 0.f);
+            a.disp[i] = d;
+        } else {
+            atomicAdd(&a.status[kNonfinite], 1u);
+        }
+    } else {
+        atomicAdd(&a.status[kSingular], 1u);
+    }
+    if (a.write_pos) a.pos[i] = make_float4(pv.x + d.x, pv.y + d.y, pv.z + d.z, 0.f);
+}
+
+// Commit of a color when the coloring is not conflict-free for every element stencil: the
+// sweep then leaves positions untouched (Jacobi within the color, as the reference's separate
+// apply_truncation_ts launch does) and this pass writes q = prev + disp.
+__global__ void commit_kernel(float4* pos, const float4* prev, const float4* disp, int b, int e) {
+    const int i = b + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= e) return;
+    const float4 p = prev[i], d = disp[i];
+    pos[i] = make_float4(p.x + d.x, p.y + d.y, p.z + d.z, 0.f);
+}
+
+struct FinalizeArgs {
+    const int* perm;
+    const float4* pos;
+    const float4* prev;
+    float* q_in;
+    float* q_out;
+    float* qd_out;
+    int* ccount;
+    int V;
+    float dt;
+};
+
+__global__ void finalize_kernel(FinalizeArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.V) return;
+    const int o = a.perm[i];
+    const float4 p = a.pos[i], pv = a.prev[i];
+    if (a.q_in) {
+        a.q_in[3 * o] = p.x;
+        a.q_in[3 * o + 1] = p.y;
+        a.q_in[3 * o + 2] = p.z;
+    }
+    if (a.q_out) {
+        a.q_out[3 * o] = p.x;
+        a.q_out[3 * o + 1] = p.y;
+        a.q_out[3 * o + 2] = p.z;
+    }
+    if (a.qd_out) {
+        a.qd_out[3 * o] = (p.x - pv.x) / a.dt;
+        a.qd_out[3 * o + 1] = (p.y - pv.y) / a.dt;
+        a.qd_out[3 * o + 2] = (p.z - pv.z) / a.dt;
+    }
+    if (a.ccount) a.ccount[i] = 0;
+}
+
+__global__ void gather_positions_kernel(const int* perm, const float4* pos, float* q, int V) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V) return;
+    const int o = perm[i];
+    const float4 p = pos[i];
+    q[3 * o] = p.x;
+    q[3 * o + 1] = p.y;
+    q[3 * o + 2] = p.z;
+}
+
+// ---------------------------------------------------------------------------------------------
+// host orchestration
+// ---------------------------------------------------------------------------------------------
+static SweepArgs make_sweep_args(const SolverImpl& s, const VbdContacts* c, float dt) {
+    const VbdModelImpl& m = *s.m;
+    SweepArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.pos = s.pos;
+    a.prev = s.prev;
+    a.y = s.y;
+    a.disp = s.disp;
+    a.vadj = m.vadj;
+    a.pinfo = m.pinfo;
+    a.tri_idx = m.tri_idx;
+    a.tri_D = m.tri_D;
+    a.tri_mat = m.tri_mat;
+    a.edge_idx = m.edge_idx;
+    a.edge_mat = m.edge_mat;
+    a.K = s.K;
+    if (c && m.S > 0) {
+        a.ccount = s.ccount;
+        a.cslot = s.cslot;
+        a.c_shape = c->soft_contact_shape;
+        a.c_body_pos = c->soft_contact_body_pos;
+        a.c_body_vel = c->soft_contact_body_vel;
+        a.c_normal = c->soft_contact_normal;
+        a.shapes = m.shapes;
+    }
+    a.dt = dt;
+    a.inv_dt = 1.0f / dt;
+    a.dt_sqr_recip = 1.0f / (dt * dt);
+    a.eps_u = s.friction_epsilon * dt;
+    a.status = s.status;
+    a.write_pos = m.fused_commit ? 1 : 0;
+    a.perm = m.perm;
+    a.inv_g = m.gravity_norm > 0.f ? 1.0f / m.gravity_norm : 0.f;
+    return a;
+}
+
+template <int L>
+static void launch_sweep_L(const SweepArgs& a, bool damp, bool residual, int block, cudaStream_t st) {
+    const long long threads = static_cast<long long>(a.v_end - a.v_begin) * L;
+    const int grid = static_cast<int>((threads + block - 1) / block);
+    if (grid <= 0) return;
+    if (residual) {
+        if (damp) sweep_kernel<L, true, true><<<grid, block, 0, st>>>(a);
+        else sweep_kernel<L, false, true><<<grid, block, 0, st>>>(a);
+    } else {
+        if (damp) sweep_kernel<L, true, false><<<grid, block, 0, st>>>(a);
+        else sweep_kernel<L, false, false><<<grid, block, 0, st>>>(a);
+    }
+}
+
+static void launch_sweep(const SweepArgs& a, int lanes, bool damp, bool residual, int block, cudaStream_t st) {
+    switch (lanes) {
+        case 1: launch_sweep_L<1>(a, damp, residual, block, st); break;
+        case 2: launch_sweep_L<2>(a, damp, residual, block, st); break;
+        case 8: launch_sweep_L<8>(a, damp, residual, block, st); break;
+        case 16: launch_sweep_L<16>(a, damp, residual, block, st); break;
+        default: launch_sweep_L<4>(a, damp, residual, block, st); break;
+    }
+}
+
+static int enqueue_forward(SolverImpl& s, const float* q_in, const float* qd_in, const float* f_ext,
+                           const VbdContacts* c, float dt, cudaStream_t st) {
+    const VbdModelImpl& m = *s.m;
+    ForwardArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.perm = m.perm;
+    a.inv_perm = m.inv_perm;
+    a.pinfo = m.pinfo;
+    a.q_in = q_in;
+    a.qd_in = qd_in;
+    a.f_ext = f_ext;
+    a.pos = s.pos;
+    a.prev = s.prev;
+    a.y = s.y;
+    a.disp = s.disp;
+    a.V = m.V;
+    a.g = make_float3(m.gravity[0], m.gravity[1], m.gravity[2]);
+    a.dt = dt;
+    a.K = s.K;
+    a.ccount = s.ccount;
+    a.cslot = s.cslot;
+    a.status = s.status;
+    int n = m.V;
+    if (c && m.S > 0 && c->soft_contact_count) {
+        a.c_count = c->soft_contact_count;
+        a.c_particle = c->soft_contact_particle;
+        a.c_max = c->soft_contact_max;
+        n = std::max(n, c->soft_contact_max);
+    }
+    const int block = 256;
+    if (n > 0) forward_kernel<<<(n + block - 1) / block, block, 0, st>>>(a);
+    return VBD_OK;
+}
+
+static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float dt, cudaStream_t st) {
+    const VbdModelImpl& m = *s.m;
+    SweepArgs a = make_sweep_args(s, c, dt);
+    a.v_begin = m.color_start[color];
+    a.v_end = m.color_start[color + 1];
+    if (a.v_end <= a.v_begin) return;
+    launch_sweep(a, s.lanes, m.any_tri_damping || m.any_edge_damping, false, s.block, st);
+    if (!m.fused_commit) {
+        const int n = a.v_end - a.v_begin;
+        commit_kernel<<<(n + 255) / 256, 256, 0, st>>>(s.pos, s.prev, s.disp, a.v_begin, a.v_end);
+    }
+}
+
+static void enqueue_finalize(SolverImpl& s, float* q_in, float* q_out, float* qd_out, float dt, cudaStream_t st) {
+    const VbdModelImpl& m = *s.m;
+    FinalizeArgs a;
+    a.perm = m.perm;
+    a.pos = s.pos;
+    a.prev = s.prev;
+    a.q_in = q_in;
+    a.q_out = q_out;
+    a.qd_out = qd_out;
+    a.ccount = s.ccount;
+    a.V = m.V;
+    a.dt = dt;
+    if (m.V > 0) finalize_kernel<<<(m.V + 255) / 256, 256, 0, st>>>(a);
+}
+
+static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const float* f_ext, float* q_out,
+                        float* qd_out, const VbdContacts* c, float dt, int iterations, cudaStream_t st) {
+    enqueue_forward(s, q_in, qd_in, f_ext, c, dt, st);
+    for (int it = 0; it < iterations; ++it)
+        for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st);
+    enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
+    return VBD_OK;
+}
+
+static void free_solver(SolverImpl& s) {
+    for (auto& g : s.graphs) cudaGraphExecDestroy(g.exec);
+    s.graphs.clear();
+    void* ptrs[] = {s.pos, s.prev, s.y, s.disp, s.ccount, s.cslot, s.status, s.resid_max};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (s.capture_stream) cudaStreamDestroy(s.capture_stream);
+    s.pos = s.prev = s.y = s.disp = nullptr;
+    s.ccount = s.cslot = nullptr;
+    s.status = nullptr;
+    s.resid_max = nullptr;
+    s.capture_stream = nullptr;
+}
+
+static bool same_contacts(const VbdContacts& a, const VbdContacts& b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
+
+static int check_state_args(const char* fn, const float* a, const float* b) {
+    if (!a || !b) return fail(VBD_ERR_INVALID_ARGUMENT, std::string(fn) + ": required state array is NULL");
+    return VBD_OK;
+}
+
+}  // namespace vbd
+
+using namespace vbd;
+
+extern "C" int vbd_solver_create(const VbdModel* model, const VbdSolverOptions* options, VbdSolver** out) {
+    if (!out) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_solver_create: out is NULL");
+    *out = nullptr;
+    if (!model) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_solver_create: model is NULL");
+    const VbdModelImpl& m = model->m;
+    VbdSolver* h = new VbdSolver();
+    SolverImpl& s = h->s;
+    s.m = &m;
+    if (options) {
+        if (options->iterations < 0) {
+            delete h;
+            return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_solver_create: iterations must be >= 0");
+        }
+        s.iterations = options->iterations;
+        s.friction_epsilon = options->friction_epsilon;
+        if (options->lanes_per_vertex) s.lanes = options->lanes_per_vertex;
+        if (options->block_size) s.block = options->block_size;
+        if (options->contacts_per_vertex) s.K = options->contacts_per_vertex;
+        s.use_graph = options->use_graph != 0;
+    }
+    if (s.lanes != 1 && s.lanes != 2 && s.lanes != 4 && s.lanes != 8 && s.lanes != 16) {
+        delete h;
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_solver_create: lanes_per_vertex must be 1, 2, 4, 8 or 16");
+    }
+    if (s.block < 32 || s.block > 256 || (s.block % 32) != 0) {
+        delete h;
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_solver_create: block_size must be a multiple of 32 in [32, 256]");
+    }
+    if (s.K < 1 || s.K > 8) {
+        delete h;
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_solver_create: contacts_per_vertex must be in [1, 8]");
+    }
+    auto alloc = [&](void** p, size_t bytes) -> int {
+        if (bytes == 0) bytes = 16;
+        VBD_CUDA_TRY(cudaMalloc(p, bytes));
+        VBD_CUDA_TRY(cudaMemset(*p, 0, bytes));
+        return VBD_OK;
+    };
+    const size_t V = static_cast<size_t>(m.V);
+    int rc = VBD_OK;
+    if (!rc) rc = alloc(reinterpret_cast<void**>(&s.pos), V * sizeof(float4));
+    if (!rc) rc = alloc(reinterpret_cast<void**>(&s.prev), V * sizeof(float4));
+    if (!rc) rc = alloc(reinterpret_cast<void**>(&s.y), V * sizeof(float4));
+    if (!rc) rc = alloc(reinterpret_cast<void**>(&s.disp), V * sizeof(float4));
+    if (!rc) rc = alloc(reinterpret_cast<void**>(&s.ccount), V * sizeof(int));
+    if (!rc) rc = alloc(reinterpret_cast<void**>(&s.cslot), V * s.K * sizeof(int));
+    if (!rc) rc = alloc(reinterpret_cast<void**>(&s.status), kStatusSlots * sizeof(unsigned));
+    if (!rc) rc = alloc(reinterpret_cast<void**>(&s.resid_max), sizeof(float));
+    if (!rc) {
+        cudaError_t e = cudaStreamCreateWithFlags(&s.capture_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamCreateWithFlags");
+    }
+    if (rc) {
+        free_solver(s);
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return VBD_OK;
+}
+
+extern "C" int vbd_solver_destroy(VbdSolver* solver) {
+    if (!solver) return VBD_OK;
+    free_solver(solver->s);
+    delete solver;
+    return VBD_OK;
+}
+
+extern "C" int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, const float* f_ext, float* q_out,
+                        float* qd_out, const VbdContacts* contacts, float dt, int32_t iterations, void* stream) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_step: solver is NULL");
+    SolverImpl& s = solver->s;
+    if (s.m->V == 0) return VBD_OK;
+    int rc = check_state_args("vbd_step", q_in, qd_in);
+    if (rc) return rc;
+    if (!q_out || !qd_out) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_step: state_out arrays are NULL");
+    if (!(dt > 0.0f)) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_step: dt must be > 0");
+    const int iters = iterations < 0 ? s.iterations : iterations;
+    if (contacts && !contacts->soft_contact_count) contacts = nullptr;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    s.steps++;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    VBD_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+    if (!s.use_graph || cs != cudaStreamCaptureStatusNone) {
+        // plain launches (also the path taken inside a caller's own stream capture)
+        enqueue_step(s, q_in, qd_in, f_ext, q_out, qd_out, contacts, dt, iters, st);
+        VBD_CUDA_TRY(cudaGetLastError());
+        return VBD_OK;
+    }
+    VbdContacts ckey;
+    std::memset(&ckey, 0, sizeof(ckey));
+    if (contacts) ckey = *contacts;
+    for (auto& g : s.graphs) {
+        if (g.q_in == q_in && g.qd_in == qd_in && g.f_ext == f_ext && g.q_out == q_out && g.qd_out == qd_out &&
+            g.has_contacts == (contacts != nullptr) && same_contacts(g.contacts, ckey) && g.dt == dt &&
+            g.iterations == iters && g.lanes == s.lanes && g.block == s.block) {
+            VBD_CUDA_TRY(cudaGraphLaunch(g.exec, st));
+            return VBD_OK;
+        }
+    }
+    // capture the step on the private stream, instantiate, replay on the caller's stream
+    VBD_CUDA_TRY(cudaStreamBeginCapture(s.capture_stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_step(s, q_in, qd_in, f_ext, q_out, qd_out, contacts, dt, iters, s.capture_stream);
+    cudaGraph_t graph = nullptr;
+    cudaError_t e1 = cudaGetLastError();
+    cudaError_t e2 = cudaStreamEndCapture(s.capture_stream, &graph);
+    if (e1 != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return cuda_fail(e1, "vbd_step capture");
+    }
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e3 = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e3 != cudaSuccess) return cuda_fail(e3, "cudaGraphInstantiate");
+    if (s.graphs.size() >= 8) {
+        cudaGraphExecDestroy(s.graphs.front().exec);
+        s.graphs.erase(s.graphs.begin());
+    }
+    GraphEntry g;
+    g.q_in = q_in;
+    g.qd_in = qd_in;
+    g.f_ext = f_ext;
+    g.q_out = q_out;
+    g.qd_out = qd_out;
+    g.contacts = ckey;
+    g.has_contacts = contacts != nullptr;
+    g.dt = dt;
+    g.iterations = iters;
+    g.lanes = s.lanes;
+    g.block = s.block;
+    g.exec = exec;
+    s.graphs.push_back(g);
+    VBD_CUDA_TRY(cudaGraphLaunch(exec, st));
+    return VBD_OK;
+}
+
+extern "C" int vbd_forward(VbdSolver* solver, const float* q_in, const float* qd_in, const float* f_ext,
+                           const VbdContacts* contacts, float dt, void* stream) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_forward: solver is NULL");
+    SolverImpl& s = solver->s;
+    if (s.m->V == 0) return VBD_OK;
+    int rc = check_state_args("vbd_forward", q_in, qd_in);
+    if (rc) return rc;
+    if (!(dt > 0.0f)) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_forward: dt must be > 0");
+    if (contacts && !contacts->soft_contact_count) contacts = nullptr;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // a staged sequence starts from an empty contact table
+    VBD_CUDA_TRY(cudaMemsetAsync(s.ccount, 0, sizeof(int) * static_cast<size_t>(s.m->V), st));
+    enqueue_forward(s, q_in, qd_in, f_ext, contacts, dt, st);
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+extern "C" int vbd_sweep_color(VbdSolver* solver, int32_t color, const VbdContacts* contacts, float dt,
+                               void* stream) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_sweep_color: solver is NULL");
+    SolverImpl& s = solver->s;
+    if (color < 0 || color >= s.m->C) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_sweep_color: color out of range");
+    if (!(dt > 0.0f)) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_sweep_color: dt must be > 0");
+    if (contacts && !contacts->soft_contact_count) contacts = nullptr;
+    enqueue_color(s, color, contacts, dt, static_cast<cudaStream_t>(stream));
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+extern "C" int vbd_finalize(VbdSolver* solver, float* q_in, float* q_out, float* qd_out, float dt, void* stream) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_finalize: solver is NULL");
+    if (!(dt > 0.0f)) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_finalize: dt must be > 0");
+    enqueue_finalize(solver->s, q_in, q_out, qd_out, dt, static_cast<cudaStream_t>(stream));
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+extern "C" int vbd_get_positions(const VbdSolver* solver, float* q_out, void* stream) {
+    if (!solver || !q_out) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_get_positions: NULL argument");
+    const SolverImpl& s = solver->s;
+    if (s.m->V == 0) return VBD_OK;
+    gather_positions_kernel<<<(s.m->V + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(s.m->perm, s.pos,
+                                                                                                   q_out, s.m->V);
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+extern "C" int vbd_residual(VbdSolver* solver, const VbdContacts* contacts, float dt, float* per_vertex_out,
+                            float* max_out, void* stream) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_residual: solver is NULL");
+    if (!(dt > 0.0f)) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_residual: dt must be > 0");
+    SolverImpl& s = solver->s;
+    const VbdModelImpl& m = *s.m;
+    if (contacts && !contacts->soft_contact_count) contacts = nullptr;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    float* mx = max_out ? max_out : s.resid_max;
+    VBD_CUDA_TRY(cudaMemsetAsync(mx, 0, sizeof(float), st));
+    if (per_vertex_out && m.V > m.swept) VBD_CUDA_TRY(cudaMemsetAsync(per_vertex_out, 0, sizeof(float) * m.V, st));
+    SweepArgs a = make_sweep_args(s, contacts, dt);
+    a.v_begin = 0;
+    a.v_end = m.swept;
+    a.resid_out = per_vertex_out;
+    a.resid_max = mx;
+    launch_sweep(a, s.lanes, m.any_tri_damping || m.any_edge_damping, true, s.block, st);
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+extern "C" int vbd_status(VbdSolver* solver, VbdStatus* out, int32_t reset) {
+    if (!solver || !out) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_status: NULL argument");
+    SolverImpl& s = solver->s;
+    unsigned h[kStatusSlots];
+    VBD_CUDA_TRY(cudaDeviceSynchronize());
+    VBD_CUDA_TRY(cudaMemcpy(h, s.status, sizeof(h), cudaMemcpyDeviceToHost));
+    out->steps = s.steps;
+    out->nonfinite_updates = static_cast<int32_t>(h[kNonfinite]);
+    out->singular_blocks = static_cast<int32_t>(h[kSingular]);
+    out->contact_overflow = static_cast<int32_t>(h[kOverflow]);
+    out->timeouts = static_cast<int32_t>(h[kTimeout]);
+    if (reset) {
+        VBD_CUDA_TRY(cudaMemset(s.status, 0, sizeof(h)));
+        s.steps = 0;
+    }
+    return VBD_OK;
+}
+
+extern "C" int vbd_solver_info(const VbdSolver* solver, int32_t* color_count, int32_t* lanes_per_vertex,
+                               int32_t* block_size) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_solver_info: solver is NULL");
+    if (color_count) *color_count = solver->s.m->C;
+    if (lanes_per_vertex) *lanes_per_vertex = solver->s.lanes;
+    if (block_size) *block_size = solver->s.block;
+    return VBD_OK;
+}
+
+extern "C" int vbd_set_launch(VbdSolver* solver, int32_t lanes_per_vertex, int32_t block_size) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_launch: solver is NULL");
+    const int L = lanes_per_vertex;
+    if (L != 1 && L != 2 && L != 4 && L != 8 && L != 16)
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_launch: lanes_per_vertex must be 1, 2, 4, 8 or 16");
+    if (block_size < 32 || block_size > 256 || (block_size % 32) != 0)
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_launch: block_size must be a multiple of 32 in [32, 256]");
+    solver->s.lanes = L;
+    solver->s.block = block_size;
+    return VBD_OK;
+}
+
+extern "C" const char* vbd_version(void) { return "vbd_b200 0.1 (sm_100a)"; }

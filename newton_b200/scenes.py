@@ -1,0 +1,102 @@
+"""Seeded synthetic cloth scenes with the shapes, sizes and materials of the VBD cloth workloads.
+
+* ``single_cloth``   one square cloth, horizontal (XY plane, Z up) with U(-1 mm, 1 mm) z-noise
+                     on the initial positions (rest shape flat), optional pinned corners, ground
+                     plane and sphere collider.  Materials default to the cloth workload:
+                     tri_ke = tri_ka = 1e4, tri_kd = 1e-3, edge_ke = 1e-2, edge_kd = 0,
+                     density 0.1 kg/m^2, gravity -9.81 m/s^2.
+* ``hanging_cloth``  32 x 32 vertices, 1 m side, two top corners pinned, ground at z = -1.
+* ``draped_cloth``   256 x 256 vertices, 2 m side, falling onto a static sphere (r = 0.4 m) and
+                     the ground; contact ke = 1e4 (particle and shape side), margin 5 mm.
+* ``batched_worlds`` independent cloth worlds of uneven size (N ~ U{16..96}, side ~ U[0.5, 2] m,
+                     tri_ke ~ logU[1e3, 1e5] with ka = ke, edge_ke ~ logU[1e-3, 1e-1], 0-4 random
+                     boundary pins, a ground plane per world), merged into one model whose color
+                     groups pair small with large groups across worlds.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from .builder import ModelBuilder
+from .model import ParticleFlags
+
+CLOTH_MATERIAL = dict(tri_ke=1.0e4, tri_ka=1.0e4, tri_kd=1.0e-3, edge_ke=1.0e-2, edge_kd=0.0)
+
+
+def _cloth(builder: ModelBuilder, n: int, side: float, height: float, density: float, particle_radius: float,
+           material: dict, center=(0.0, 0.0)) -> int:
+    verts, tris = ModelBuilder.grid_mesh(n - 1, n - 1, side / (n - 1), side / (n - 1))
+    start = builder.particle_count
+    builder.add_cloth_mesh(pos=(center[0] - 0.5 * side, center[1] - 0.5 * side, height), rot=(0.0, 0.0, 0.0, 1.0),
+                           scale=1.0, vel=(0.0, 0.0, 0.0), vertices=verts, indices=tris, density=density,
+                           particle_radius=particle_radius, **material)
+    return start
+
+
+def _pin(builder: ModelBuilder, indices) -> None:
+    idx = np.asarray(indices, dtype=np.int64)
+    builder.set_particle_mass(idx, 0.0)
+    flags = builder.particle_flags[idx] & ~ParticleFlags.ACTIVE
+    builder.set_particle_flags(idx, flags)
+
+
+def single_cloth(n: int = 32, side: float = 1.0, seed: int = 0, pin_top_corners: bool = True, ground: float | None = -1.0,
+                 sphere: tuple | None = None, height: float = 0.0, particle_radius: float = 5.0e-3,
+                 density: float = 0.1, material: dict | None = None, contact_ke: float = 1.0e4,
+                 include_bending: bool = True, device="cuda:0"):
+    """Returns (model, initial particle_q float32 [V,3] with z-noise)."""
+    material = dict(CLOTH_MATERIAL if material is None else material)
+    b = ModelBuilder()
+    start = _cloth(b, n, side, height, density, particle_radius, material)
+    if pin_top_corners:
+        _pin(b, [start + (n - 1) * n, start + n * n - 1])
+    cfg = ModelBuilder.ShapeConfig(ke=contact_ke)
+    if ground is not None:
+        b.add_ground_plane(height=ground, cfg=cfg)
+    if sphere is not None:
+        center, radius = sphere
+        b.add_shape_sphere(-1, xform=(tuple(center), (0.0, 0.0, 0.0, 1.0)), radius=radius, cfg=cfg)
+    b.color(include_bending=include_bending)
+    m = b.finalize(device=device)
+    m.soft_contact_ke = contact_ke
+    rng = np.random.default_rng(seed)
+    q0 = m.particle_q.copy()
+    q0[:, 2] += rng.uniform(-1.0e-3, 1.0e-3, size=m.particle_count).astype(np.float32)
+    return m, q0
+
+
+def hanging_cloth(seed: int = 0, device="cuda:0"):
+    """32 x 32 vertices (1,922 triangles), 1 m side, two top corners pinned, ground at z = -1."""
+    return single_cloth(n=32, side=1.0, seed=seed, pin_top_corners=True, ground=-1.0, device=device)
+
+
+def draped_cloth(n: int = 256, seed: int = 0, device="cuda:0"):
+    """256 x 256 vertices (130,050 triangles), 2 m side, 0.2 m above a static sphere of radius 0.4 m."""
+    return single_cloth(n=n, side=2.0, seed=seed, pin_top_corners=False, ground=0.0,
+                        sphere=((0.0, 0.0, 0.5), 0.4), height=1.1, device=device)
+
+
+def batched_worlds(num_worlds: int = 512, seed: int = 0, n_range=(16, 96), device="cuda:0", include_bending=True):
+    """Independent cloth worlds of uneven size merged into one model (colors combined per world)."""
+    rng = np.random.default_rng(seed)
+    top = ModelBuilder()
+    for w in range(num_worlds):
+        n = int(rng.integers(n_range[0], n_range[1] + 1))
+        side = float(rng.uniform(0.5, 2.0))
+        ke = float(10.0 ** rng.uniform(3.0, 5.0))
+        eke = float(10.0 ** rng.uniform(-3.0, -1.0))
+        npin = int(rng.integers(0, 5))
+        b = ModelBuilder()
+        mat = dict(tri_ke=ke, tri_ka=ke, tri_kd=1.0e-3, edge_ke=eke, edge_kd=0.0)
+        _cloth(b, n, side, 0.5, 0.1, 5.0e-3, mat)
+        if npin:
+            ring = np.concatenate([np.arange(n), np.arange(n) + (n - 1) * n, np.arange(1, n - 1) * n,
+                                   np.arange(1, n - 1) * n + n - 1])
+            _pin(b, rng.choice(ring, size=npin, replace=False))
+        b.add_ground_plane(height=0.0, cfg=ModelBuilder.ShapeConfig(ke=1.0e4))
+        b.color(include_bending=include_bending)
+        top.add_builder(b, world=w)
+    m = top.finalize(device=device)
+    m.soft_contact_ke = 1.0e4
+    return m, m.particle_q.copy()

@@ -1,0 +1,210 @@
+"""``SolverVBD`` for particles/cloth on B200, behind the reference's solver interface.
+
+Drop-in for the particle path of ``newton.solvers.SolverVBD``
+(``newton/_src/solvers/vbd/solver_vbd.py:92``): same constructor keywords for the particle path,
+same ``step(state_in, state_out, control, contacts, dt)`` contract, same state aliasing --
+``state_in.particle_q`` is overwritten with the solved positions (the reference keeps its
+Gauss-Seidel iterate there, ``solver_vbd.py:2100``/``:2702``) and ``state_out.particle_q``/
+``particle_qd`` receive the result (``:2704``, ``:3158-3169``).
+
+Every step runs in ``libvbd_b200.so`` (``vbd_step``): one forward kernel, ``iterations x colors``
+sweep kernels and one finalize kernel, replayed from a cached CUDA graph.  There is no CPU or
+eager fallback: without the library or a CUDA device the constructor raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import warnings
+
+import numpy as np
+import torch
+
+from .. import _lib
+from ..model import Contacts, Control, Model, State
+from .solver import SolverBase
+
+
+class SolverVBD(SolverBase):
+    def __init__(
+        self,
+        model: Model,
+        *,
+        iterations: int = 10,
+        friction_epsilon: float = 1e-2,
+        integrate_with_external_rigid_solver: bool = False,
+        particle_enable_self_contact: bool = False,
+        particle_self_contact_radius: float = 0.2,
+        particle_self_contact_margin: float = 0.2,
+        particle_enable_tile_solve: bool = True,
+        lanes_per_vertex: int = 0,
+        block_size: int = 0,
+        contacts_per_vertex: int = 4,
+        use_cuda_graph: bool = True,
+    ):
+        super().__init__(model)
+        self.iterations = int(iterations)
+        self.friction_epsilon = float(friction_epsilon)
+        self.integrate_with_external_rigid_solver = integrate_with_external_rigid_solver
+        self.particle_enable_self_contact = particle_enable_self_contact
+        self.particle_self_contact_radius = particle_self_contact_radius
+        self.particle_self_contact_margin = particle_self_contact_margin
+        self.particle_enable_tile_solve = particle_enable_tile_solve
+        self._handle = None
+        if model.particle_count == 0:
+            return
+        if particle_enable_self_contact:
+            if particle_self_contact_margin < particle_self_contact_radius:
+                raise ValueError(
+                    "particle_self_contact_margin is smaller than particle_self_contact_radius, this will result in "
+                    "missing contacts and cause instability.\nIt is advisable to make particle_self_contact_margin "
+                    "1.5-2 times larger than particle_self_contact_radius."
+                )
+            raise NotImplementedError("particle self-contact is not available in this build of the B200 VBD solver")
+        if len(model.particle_color_groups) == 0:
+            raise ValueError(
+                "model.particle_color_groups is empty! When using the SolverVBD you must call ModelBuilder.color() "
+                "or ModelBuilder.set_coloring() before calling ModelBuilder.finalize()."
+            )
+        if model.soft_mesh_adjacency is None:
+            raise ValueError("model.soft_mesh_adjacency is missing; finalize the model with ModelBuilder.")
+        self._lib = _lib.load()
+        dm = model.device_model()
+        opts = _lib.VbdSolverOptions()
+        opts.iterations = self.iterations
+        opts.friction_epsilon = self.friction_epsilon
+        opts.lanes_per_vertex = int(lanes_per_vertex)
+        opts.block_size = int(block_size)
+        opts.contacts_per_vertex = int(contacts_per_vertex)
+        opts.use_graph = 1 if use_cuda_graph else 0
+        h = ctypes.c_void_p()
+        with torch.cuda.device(model.device):
+            _lib.check(self._lib.vbd_solver_create(dm.handle, ctypes.byref(opts), ctypes.byref(h)))
+        self._handle = h
+        self._dm = dm  # keeps the device model alive as long as the solver
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                self._lib.vbd_solver_destroy(h)
+            except Exception:
+                pass
+            self._handle = None
+
+    # -----------------------------------------------------------------------------------
+    def _stream(self) -> ctypes.c_void_p:
+        return ctypes.c_void_p(torch.cuda.current_stream(self.model.device).cuda_stream)
+
+    @staticmethod
+    def _check_state(state: State, name: str, V: int, device) -> None:
+        for attr in ("particle_q", "particle_qd"):
+            t = getattr(state, attr)
+            if t is None:
+                raise ValueError(f"{name}.{attr} is None")
+            if t.dtype != torch.float32 or t.device != device or not t.is_contiguous() or t.numel() != 3 * V:
+                raise ValueError(f"{name}.{attr} must be a contiguous float32 [{V},3] tensor on {device}")
+
+    def _contacts(self, contacts: Contacts | None):
+        if contacts is None or self.model.shape_count == 0:
+            return None
+        return ctypes.byref(contacts.c_struct())
+
+    def step(self, state_in: State, state_out: State, control: Control | None, contacts: Contacts | None,
+             dt: float) -> None:
+        if self.model.particle_count == 0:
+            return
+        V = self.model.particle_count
+        dev = self.model.device
+        self._check_state(state_in, "state_in", V, dev)
+        self._check_state(state_out, "state_out", V, dev)
+        f = state_in.particle_f
+        _lib.check(
+            self._lib.vbd_step(
+                self._handle,
+                _lib.ptr(state_in.particle_q),
+                _lib.ptr(state_in.particle_qd),
+                _lib.ptr(f),
+                _lib.ptr(state_out.particle_q),
+                _lib.ptr(state_out.particle_qd),
+                self._contacts(contacts),
+                ctypes.c_float(dt),
+                self.iterations,
+                self._stream(),
+            )
+        )
+
+    # ---- staged pieces (parity tests, residual-gated loops) ------------------------------
+    def forward(self, state_in: State, contacts: Contacts | None, dt: float) -> None:
+        _lib.check(
+            self._lib.vbd_forward(
+                self._handle,
+                _lib.ptr(state_in.particle_q),
+                _lib.ptr(state_in.particle_qd),
+                _lib.ptr(state_in.particle_f),
+                self._contacts(contacts),
+                ctypes.c_float(dt),
+                self._stream(),
+            )
+        )
+
+    def sweep_color(self, color: int, contacts: Contacts | None, dt: float) -> None:
+        _lib.check(self._lib.vbd_sweep_color(self._handle, int(color), self._contacts(contacts), ctypes.c_float(dt),
+                                             self._stream()))
+
+    def iterate(self, contacts: Contacts | None, dt: float, iterations: int = 1) -> None:
+        for _ in range(iterations):
+            for c in range(len(self.model.particle_color_groups)):
+                self.sweep_color(c, contacts, dt)
+
+    def finalize(self, state_in: State, state_out: State, dt: float) -> None:
+        _lib.check(
+            self._lib.vbd_finalize(
+                self._handle,
+                _lib.ptr(state_in.particle_q),
+                _lib.ptr(state_out.particle_q),
+                _lib.ptr(state_out.particle_qd),
+                ctypes.c_float(dt),
+                self._stream(),
+            )
+        )
+
+    def positions(self) -> torch.Tensor:
+        out = torch.empty((self.model.particle_count, 3), dtype=torch.float32, device=self.model.device)
+        _lib.check(self._lib.vbd_get_positions(self._handle, _lib.ptr(out), self._stream()))
+        return out
+
+    def residual(self, contacts: Contacts | None, dt: float, per_vertex: bool = False):
+        """Max (and optionally per-vertex) force residual / (m |g|) at the current iterate."""
+        mx = torch.zeros(1, dtype=torch.float32, device=self.model.device)
+        pv = torch.zeros(self.model.particle_count, dtype=torch.float32, device=self.model.device) if per_vertex else None
+        _lib.check(self._lib.vbd_residual(self._handle, self._contacts(contacts), ctypes.c_float(dt), _lib.ptr(pv),
+                                          _lib.ptr(mx), self._stream()))
+        return (mx, pv) if per_vertex else mx
+
+    def status(self, reset: bool = False) -> dict:
+        st = _lib.VbdStatus()
+        _lib.check(self._lib.vbd_status(self._handle, ctypes.byref(st), 1 if reset else 0))
+        return {
+            "steps": st.steps,
+            "nonfinite_updates": st.nonfinite_updates,
+            "singular_blocks": st.singular_blocks,
+            "contact_overflow": st.contact_overflow,
+            "timeouts": st.timeouts,
+        }
+
+    def set_launch(self, lanes_per_vertex: int, block_size: int) -> None:
+        _lib.check(self._lib.vbd_set_launch(self._handle, int(lanes_per_vertex), int(block_size)))
+
+    def launch_info(self) -> dict:
+        c, l, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        _lib.check(self._lib.vbd_solver_info(self._handle, ctypes.byref(c), ctypes.byref(l), ctypes.byref(b)))
+        return {"colors": c.value, "lanes_per_vertex": l.value, "block_size": b.value}
+
+    def reset(self, state: State, world_mask=None, flags=None) -> None:
+        warnings.warn(
+            "SolverVBD.reset() does not support particle resets; particle solver history is unchanged.", stacklevel=2
+        )
+
+    def notify_model_changed(self, flags: int) -> None:
+        raise NotImplementedError("rebuild the solver after changing particle/cloth model data")

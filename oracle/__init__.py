@@ -1,0 +1,322 @@
+"""CPU oracle of Newton's particle VBD cloth step -- TEST INFRASTRUCTURE ONLY.
+
+A C++ restatement (``vbd_oracle.cpp``) of the reference's serial CPU path, FP32 and FP64, with a
+ctypes wrapper.  Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg
+use it, as the checker of the CUDA library; the product path never calls it.
+
+Parity pinning: the reference (Python + Warp) cannot run in this environment (``warp-lang`` is
+not installed), so the oracle is pinned against the known-answer tests of the reference's own
+test suite (``newton/tests/test_solver_vbd.py``), restated in ``tests/test_oracle_kat.py``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from .build_oracle import OUT, build
+
+_lib = None
+
+c_int32_p = ctypes.POINTER(ctypes.c_int32)
+c_float_p = ctypes.POINTER(ctypes.c_float)
+c_double_p = ctypes.POINTER(ctypes.c_double)
+
+
+class OracleShape(ctypes.Structure):
+    _fields_ = [
+        ("geo_type", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
+        ("world", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("xform", ctypes.c_float * 7),
+        ("scale", ctypes.c_float * 3),
+        ("margin", ctypes.c_float),
+        ("material_ke", ctypes.c_float),
+        ("material_kd", ctypes.c_float),
+        ("material_mu", ctypes.c_float),
+    ]
+
+
+class OracleModelDesc(ctypes.Structure):
+    _fields_ = [
+        ("particle_count", ctypes.c_int32),
+        ("tri_count", ctypes.c_int32),
+        ("edge_count", ctypes.c_int32),
+        ("shape_count", ctypes.c_int32),
+        ("color_count", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("particle_mass", c_float_p),
+        ("particle_inv_mass", c_float_p),
+        ("particle_radius", c_float_p),
+        ("particle_flags", c_int32_p),
+        ("particle_world", c_int32_p),
+        ("tri_indices", c_int32_p),
+        ("tri_poses", c_float_p),
+        ("tri_materials", c_float_p),
+        ("tri_areas", c_float_p),
+        ("edge_indices", c_int32_p),
+        ("edge_rest_angle", c_float_p),
+        ("edge_rest_length", c_float_p),
+        ("edge_bending_properties", c_float_p),
+        ("v_adj_tris_offsets", c_int32_p),
+        ("v_adj_tris", c_int32_p),
+        ("v_adj_edges_offsets", c_int32_p),
+        ("v_adj_edges", c_int32_p),
+        ("color_group_offsets", c_int32_p),
+        ("color_group_particles", c_int32_p),
+        ("gravity", ctypes.c_float * 3),
+        ("soft_contact_ke", ctypes.c_float),
+        ("soft_contact_kd", ctypes.c_float),
+        ("soft_contact_mu", ctypes.c_float),
+        ("shapes", ctypes.POINTER(OracleShape)),
+    ]
+
+
+def load():
+    global _lib
+    if _lib is None:
+        build()
+        lib = ctypes.CDLL(str(OUT))
+        vp = ctypes.c_void_p
+        lib.oracle_create.restype = vp
+        lib.oracle_create.argtypes = [ctypes.POINTER(OracleModelDesc), ctypes.c_int, ctypes.c_float, ctypes.c_int]
+        lib.oracle_destroy.argtypes = [vp]
+        lib.oracle_set_threads.argtypes = [vp, ctypes.c_int]
+        lib.oracle_set_contacts.argtypes = [vp, ctypes.c_int, c_int32_p, c_int32_p, c_float_p, c_float_p, c_float_p]
+        lib.oracle_forward.argtypes = [vp, c_float_p, c_float_p, c_float_p, ctypes.c_float]
+        lib.oracle_begin_iteration.argtypes = [vp]
+        lib.oracle_sweep_color.argtypes = [vp, ctypes.c_int, ctypes.c_float]
+        lib.oracle_finalize.argtypes = [vp, c_float_p, c_float_p, c_float_p, ctypes.c_float]
+        lib.oracle_step.argtypes = [vp, c_float_p, c_float_p, c_float_p, c_float_p, c_float_p, ctypes.c_float, ctypes.c_int]
+        lib.oracle_get_positions.argtypes = [vp, c_double_p]
+        lib.oracle_residual.argtypes = [vp, ctypes.c_float, c_float_p]
+        lib.oracle_set_positions.argtypes = [vp, c_float_p]
+        d = ctypes.c_double
+        lib.oracle_membrane.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_double_p, c_double_p, c_int32_p,
+                                        c_double_p, d, d, d, d, d, ctypes.c_int, c_double_p, c_double_p]
+        lib.oracle_bending.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_double_p, c_double_p, c_int32_p, d, d,
+                                       d, d, d, ctypes.c_int, c_double_p, c_double_p]
+        lib.oracle_contact.argtypes = [ctypes.c_int, c_double_p, c_double_p, c_double_p, c_double_p, c_double_p, d, d, d,
+                                       d, d, d, d, c_double_p, c_double_p]
+        lib.oracle_collide.restype = ctypes.c_int
+        lib.oracle_collide.argtypes = [ctypes.c_int, c_float_p, c_float_p, c_int32_p, c_int32_p, ctypes.c_int,
+                                       ctypes.POINTER(OracleShape), ctypes.c_float, ctypes.c_int, c_int32_p, c_int32_p,
+                                       c_float_p, c_float_p, c_float_p]
+        _lib = lib
+    return _lib
+
+
+def _f32(a):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+    return a, a.ctypes.data_as(c_float_p)
+
+
+def _i32(a):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+    return a, a.ctypes.data_as(c_int32_p)
+
+
+def _f64(a):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    return a, a.ctypes.data_as(c_double_p)
+
+
+def _shapes(model):
+    S = model.shape_count
+    arr = (OracleShape * max(S, 1))()
+    for s in range(S):
+        sh = arr[s]
+        sh.geo_type = int(model.shape_type[s])
+        sh.flags = int(model.shape_flags[s])
+        sh.world = int(model.shape_world[s])
+        for k in range(7):
+            sh.xform[k] = float(model.shape_transform[s, k])
+        for k in range(3):
+            sh.scale[k] = float(model.shape_scale[s, k])
+        sh.margin = float(model.shape_margin[s])
+        sh.material_ke = float(model.shape_material_ke[s])
+        sh.material_kd = float(model.shape_material_kd[s])
+        sh.material_mu = float(model.shape_material_mu[s])
+    return arr
+
+
+class VBDOracle:
+    """Stateful CPU oracle of one SolverVBD (particle path) on a finalized ``newton_b200.Model``."""
+
+    def __init__(self, model, precision: str = "f32", friction_epsilon: float = 1e-2, threads: int = 1):
+        lib = load()
+        self.model = model
+        self.V = model.particle_count
+        keep = []
+
+        def f(a):
+            arr, p = _f32(a)
+            keep.append(arr)
+            return p if arr.size else None
+
+        def i(a):
+            arr, p = _i32(a)
+            keep.append(arr)
+            return p if arr.size else None
+
+        d = OracleModelDesc()
+        d.particle_count = model.particle_count
+        d.tri_count = model.tri_count
+        d.edge_count = model.edge_count
+        d.shape_count = model.shape_count
+        d.color_count = len(model.particle_color_groups)
+        d.particle_mass = f(model.particle_mass)
+        d.particle_inv_mass = f(model.particle_inv_mass)
+        d.particle_radius = f(model.particle_radius)
+        d.particle_flags = i(model.particle_flags)
+        d.particle_world = i(model.particle_world)
+        d.tri_indices = i(model.tri_indices)
+        d.tri_poses = f(model.tri_poses)
+        d.tri_materials = f(model.tri_materials)
+        d.tri_areas = f(model.tri_areas)
+        d.edge_indices = i(model.edge_indices)
+        d.edge_rest_angle = f(model.edge_rest_angle)
+        d.edge_rest_length = f(model.edge_rest_length)
+        d.edge_bending_properties = f(model.edge_bending_properties)
+        adj = model.soft_mesh_adjacency
+        d.v_adj_tris_offsets = i(adj.v_adj_tris_offsets)
+        d.v_adj_tris = i(adj.v_adj_tris)
+        d.v_adj_edges_offsets = i(adj.v_adj_edges_offsets)
+        d.v_adj_edges = i(adj.v_adj_edges)
+        offs, flat = model.color_group_csr()
+        d.color_group_offsets = i(offs)
+        d.color_group_particles = i(flat)
+        g = np.asarray(model.gravity, dtype=np.float32).reshape(-1, 3)[0]
+        for k in range(3):
+            d.gravity[k] = float(g[k])
+        d.soft_contact_ke = float(np.float32(model.soft_contact_ke))
+        d.soft_contact_kd = float(np.float32(model.soft_contact_kd))
+        d.soft_contact_mu = float(np.float32(model.soft_contact_mu))
+        self._shapes = _shapes(model)
+        d.shapes = ctypes.cast(self._shapes, ctypes.POINTER(OracleShape))
+        self.precision = precision
+        self._h = lib.oracle_create(ctypes.byref(d), 1 if precision == "f64" else 0, friction_epsilon, threads)
+        self._lib = lib
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.oracle_destroy(self._h)
+            self._h = None
+
+    def set_threads(self, n: int) -> None:
+        self._lib.oracle_set_threads(self._h, int(n))
+
+    def set_contacts(self, particle, shape, body_pos, body_vel, normal) -> None:
+        n = len(particle)
+        a, pa = _i32(particle)
+        b, pb = _i32(shape)
+        c, pc = _f32(np.asarray(body_pos).reshape(-1, 3))
+        e, pe = _f32(np.asarray(body_vel).reshape(-1, 3))
+        g, pg = _f32(np.asarray(normal).reshape(-1, 3))
+        self._lib.oracle_set_contacts(self._h, n, pa, pb, pc, pe, pg)
+
+    def clear_contacts(self) -> None:
+        z = np.zeros(0)
+        self.set_contacts(np.zeros(0, np.int32), np.zeros(0, np.int32), z, z, z)
+
+    def step(self, q_in: np.ndarray, qd_in: np.ndarray, f_ext: np.ndarray | None, dt: float, iterations: int):
+        """One SolverVBD.step; returns (q_in_after, q_out, qd_out) as float32 [V,3] arrays."""
+        q, pq = _f32(np.array(q_in, dtype=np.float32).reshape(-1, 3))
+        qd, pqd = _f32(qd_in)
+        fe, pfe = _f32(f_ext) if f_ext is not None else (None, None)
+        q_out = np.zeros((self.V, 3), np.float32)
+        qd_out = np.zeros((self.V, 3), np.float32)
+        self._lib.oracle_step(self._h, pq, pqd, pfe, q_out.ctypes.data_as(c_float_p), qd_out.ctypes.data_as(c_float_p),
+                              float(dt), int(iterations))
+        return q, q_out, qd_out
+
+    def forward(self, q_in, qd_in, f_ext, dt: float) -> None:
+        q, pq = _f32(q_in)
+        qd, pqd = _f32(qd_in)
+        fe, pfe = _f32(f_ext) if f_ext is not None else (None, None)
+        self._lib.oracle_forward(self._h, pq, pqd, pfe, float(dt))
+
+    def begin_iteration(self) -> None:
+        self._lib.oracle_begin_iteration(self._h)
+
+    def sweep_color(self, color: int, dt: float) -> None:
+        self._lib.oracle_sweep_color(self._h, int(color), float(dt))
+
+    def finalize(self, dt: float):
+        q_in = np.zeros((self.V, 3), np.float32)
+        q_out = np.zeros((self.V, 3), np.float32)
+        qd_out = np.zeros((self.V, 3), np.float32)
+        self._lib.oracle_finalize(self._h, q_in.ctypes.data_as(c_float_p), q_out.ctypes.data_as(c_float_p),
+                                  qd_out.ctypes.data_as(c_float_p), float(dt))
+        return q_in, q_out, qd_out
+
+    def positions(self) -> np.ndarray:
+        out = np.zeros((self.V, 3), np.float64)
+        self._lib.oracle_get_positions(self._h, out.ctypes.data_as(c_double_p))
+        return out
+
+    def set_positions(self, q) -> None:
+        a, p = _f32(np.asarray(q).reshape(-1, 3))
+        self._lib.oracle_set_positions(self._h, p)
+
+    def residual(self, dt: float) -> np.ndarray:
+        out = np.zeros(self.V, np.float32)
+        self._lib.oracle_residual(self._h, float(dt), out.ctypes.data_as(c_float_p))
+        return out
+
+
+def collide(model, q: np.ndarray, margin: float):
+    """create_soft_contacts over the model's static shapes; returns record arrays (shape order per particle)."""
+    lib = load()
+    V, S = model.particle_count, model.shape_count
+    mx = V * S
+    particle = np.zeros(max(mx, 1), np.int32)
+    shape = np.zeros(max(mx, 1), np.int32)
+    bpos = np.zeros((max(mx, 1), 3), np.float32)
+    bvel = np.zeros((max(mx, 1), 3), np.float32)
+    nrm = np.zeros((max(mx, 1), 3), np.float32)
+    qa, pq = _f32(np.asarray(q).reshape(-1, 3))
+    ra, pr = _f32(model.particle_radius)
+    fa, pf = _i32(model.particle_flags)
+    wa, pw = _i32(model.particle_world)
+    shapes = _shapes(model)
+    n = lib.oracle_collide(V, pq, pr, pf, pw, S, ctypes.cast(shapes, ctypes.POINTER(OracleShape)), float(margin), mx,
+                           particle.ctypes.data_as(c_int32_p), shape.ctypes.data_as(c_int32_p),
+                           bpos.ctypes.data_as(c_float_p), bvel.ctypes.data_as(c_float_p), nrm.ctypes.data_as(c_float_p))
+    n = min(n, mx)
+    return particle[:n], shape[:n], bpos[:n], bvel[:n], nrm[:n]
+
+
+def _elem(fn, is_double, *args):
+    f = np.zeros(3, np.float64)
+    h = np.zeros(9, np.float64)
+    fn(is_double, *args, f.ctypes.data_as(c_double_p), h.ctypes.data_as(c_double_p))
+    return f, h.reshape(3, 3)
+
+
+def membrane(face, v_order, pos, anchor, tri_indices, pose, area, mu, lmbd, damping, dt, precision="f32"):
+    lib = load()
+    p, pp = _f64(np.asarray(pos).reshape(-1, 3))
+    a, pa = _f64(np.asarray(anchor).reshape(-1, 3))
+    t, pt = _i32(np.asarray(tri_indices).reshape(-1, 3))
+    ps, pps = _f64(np.asarray(pose).reshape(4))
+    return _elem(lib.oracle_membrane, 1 if precision == "f64" else 0, int(face), int(v_order), pp, pa, pt, pps,
+                 float(area), float(mu), float(lmbd), float(damping), float(dt), p.shape[0])
+
+
+def bending(edge, v_order, pos, anchor, edge_indices, rest_angle, rest_length, ke, kd, dt, precision="f32"):
+    lib = load()
+    p, pp = _f64(np.asarray(pos).reshape(-1, 3))
+    a, pa = _f64(np.asarray(anchor).reshape(-1, 3))
+    e, pe = _i32(np.asarray(edge_indices).reshape(-1, 4))
+    return _elem(lib.oracle_bending, 1 if precision == "f64" else 0, int(edge), int(v_order), pp, pa, pe,
+                 float(rest_angle), float(rest_length), float(ke), float(kd), float(dt), p.shape[0])
+
+
+def contact(x, x_prev, body_pos, body_vel, normal, radius, margin, ke, kd, mu, friction_epsilon, dt, precision="f32"):
+    lib = load()
+    arrs = [_f64(np.asarray(v).reshape(3)) for v in (x, x_prev, body_pos, body_vel, normal)]
+    return _elem(lib.oracle_contact, 1 if precision == "f64" else 0, *[p for _, p in arrs], float(radius), float(margin),
+                 float(ke), float(kd), float(mu), float(friction_epsilon), float(dt))

@@ -1,0 +1,209 @@
+"""GPU parity of the VBD cloth step against the CPU oracle (FP32 and FP64).
+
+Parity criterion (per step, from identical states): max |x_gpu - x_oracle| <= 1e-5 m after one
+``SolverVBD.step`` with the same inputs; the FP64 re-evaluation of the same step is reported
+alongside.  All calls go through the C-ABI library (``libvbd_b200.so``).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from newton_b200 import CollisionPipeline, scenes
+from newton_b200.solvers import SolverVBD
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP = 1.0e-5  # m, per step from identical states
+DT = 1.0 / 600.0
+
+
+def _gpu_step(model, solver, q, qd, pipe, dt, iterations=None):
+    s0, s1 = model.state(), model.state()
+    s0.particle_q.copy_(torch.from_numpy(np.ascontiguousarray(q)).to(s0.particle_q.device))
+    s0.particle_qd.copy_(torch.from_numpy(np.ascontiguousarray(qd)).to(s0.particle_q.device))
+    contacts = None
+    if pipe is not None:
+        contacts = pipe.contacts()
+        pipe.collide(s0, contacts)
+    if iterations is not None:
+        solver.iterations = iterations
+    solver.step(s0, s1, None, contacts, dt)
+    torch.cuda.synchronize()
+    return s0.particle_q.cpu().numpy(), s1.particle_q.cpu().numpy(), s1.particle_qd.cpu().numpy(), contacts
+
+
+def _oracle_step(model, orc, q, qd, margin, dt, iterations):
+    if model.shape_count:
+        orc.set_contacts(*oracle.collide(model, q, margin))
+    return orc.step(q, qd, None, dt, iterations)
+
+
+def _trajectory_parity(model, q0, steps, iterations, margin=5e-3, check_every=1):
+    orc32 = oracle.VBDOracle(model, "f32", threads=8)
+    orc64 = oracle.VBDOracle(model, "f64", threads=8)
+    solver = SolverVBD(model, iterations=iterations)
+    pipe = CollisionPipeline(model, soft_contact_margin=margin) if model.shape_count else None
+    q, qd = q0.astype(np.float32), np.zeros_like(q0, dtype=np.float32)
+    worst, worst64 = 0.0, 0.0
+    for k in range(steps):
+        q_next, qd_next = None, None
+        qin_o, q_o, qd_o = _oracle_step(model, orc32, q, qd, margin, DT, iterations)
+        if k % check_every == 0:
+            qin_g, q_g, qd_g, _ = _gpu_step(model, solver, q, qd, pipe, DT)
+            _, q_64, _ = _oracle_step(model, orc64, q, qd, margin, DT, iterations)
+            err = float(np.abs(q_g - q_o).max())
+            err64 = float(np.abs(q_g - q_64).max())
+            # aliasing: state_in.particle_q holds the solved positions, like the reference
+            assert np.array_equal(qin_g, q_g)
+            assert np.abs(qd_g - qd_o).max() <= 2.0 * TOL_STEP / DT
+            worst, worst64 = max(worst, err), max(worst64, err64)
+            assert err <= TOL_STEP, f"step {k}: max |dx| = {err:.3e} m vs FP32 oracle"
+        q, qd = q_o, qd_o
+    return worst, worst64
+
+
+def test_hanging_cloth_single_step():
+    model, q0 = scenes.hanging_cloth(seed=0)
+    worst, worst64 = _trajectory_parity(model, q0, steps=1, iterations=10)
+    print(f"hanging 32x32: max |dx| vs FP32 oracle {worst:.3e} m, vs FP64 {worst64:.3e} m")
+
+
+def test_hanging_cloth_trajectory_per_step():
+    """30 substeps (3 frames): every step from the oracle's own state stays within 1e-5 m."""
+    model, q0 = scenes.hanging_cloth(seed=1)
+    worst, worst64 = _trajectory_parity(model, q0, steps=30, iterations=10, check_every=3)
+    print(f"hanging 32x32 x30: max |dx| {worst:.3e} m (FP64 {worst64:.3e} m)")
+
+
+def test_draped_cloth_contacts_per_step():
+    """Sphere + ground contacts: cloth released just above the sphere so contacts are active."""
+    model, q0 = scenes.single_cloth(n=48, side=1.0, seed=2, pin_top_corners=False, ground=0.0,
+                                    sphere=((0.0, 0.0, 0.5), 0.4), height=0.905)
+    worst, worst64 = _trajectory_parity(model, q0, steps=12, iterations=10, check_every=2)
+    print(f"draped 48x48: max |dx| {worst:.3e} m (FP64 {worst64:.3e} m)")
+
+
+def test_collide_matches_oracle():
+    model, q0 = scenes.single_cloth(n=40, side=1.0, seed=3, pin_top_corners=False, ground=0.0,
+                                    sphere=((0.0, 0.0, 0.5), 0.4), height=0.902)
+    pipe = CollisionPipeline(model, soft_contact_margin=5e-3)
+    c = pipe.contacts()
+    s = model.state()
+    s.particle_q.copy_(torch.from_numpy(q0).cuda())
+    pipe.collide(s, c)
+    n = c.count()
+    assert n > 0
+    part = c.soft_contact_particle[:n].cpu().numpy()
+    shp = c.soft_contact_shape[:n].cpu().numpy()
+    order = np.lexsort((shp, part))
+    op, osh, obp, obv, onr = oracle.collide(model, q0, 5e-3)
+    assert n == len(op)
+    np.testing.assert_array_equal(part[order], op)
+    np.testing.assert_array_equal(shp[order], osh)
+    np.testing.assert_allclose(c.soft_contact_body_pos[:n].cpu().numpy()[order], obp, atol=1e-6)
+    np.testing.assert_allclose(c.soft_contact_normal[:n].cpu().numpy()[order], onr, atol=1e-6)
+    # records of one particle are consecutive and in shape order
+    for p in np.unique(part):
+        idx = np.flatnonzero(part == p)
+        assert np.all(np.diff(idx) == 1) and np.all(np.diff(shp[idx]) > 0)
+
+
+def test_staged_api_matches_step_and_oracle_per_color():
+    model, q0 = scenes.hanging_cloth(seed=4)
+    V = model.particle_count
+    qd = np.zeros((V, 3), np.float32)
+    solver = SolverVBD(model, iterations=2)
+    orc = oracle.VBDOracle(model, "f32")
+    s0 = model.state()
+    s0.particle_q.copy_(torch.from_numpy(q0).cuda())
+    solver.forward(s0, None, DT)
+    orc.forward(q0, qd, None, DT)
+    np.testing.assert_allclose(solver.positions().cpu().numpy(), orc.positions(), atol=1e-7)
+    for it in range(2):
+        orc.begin_iteration()
+        for c in range(len(model.particle_color_groups)):
+            solver.sweep_color(c, None, DT)
+            orc.sweep_color(c, DT)
+            err = np.abs(solver.positions().cpu().numpy() - orc.positions()).max()
+            assert err <= TOL_STEP, f"iteration {it} color {c}: {err:.3e}"
+    s1 = model.state()
+    solver.finalize(s0, s1, DT)
+    staged = s1.particle_q.cpu().numpy()
+    _, full, _, _ = _gpu_step(model, solver, q0, qd, None, DT)
+    np.testing.assert_array_equal(staged, full)
+
+
+def test_graph_replay_and_plain_launches_are_bitwise_equal_and_deterministic():
+    model, q0 = scenes.single_cloth(n=48, side=1.0, seed=5, pin_top_corners=False, ground=0.0,
+                                    sphere=((0.0, 0.0, 0.5), 0.4), height=0.905)
+    pipe = CollisionPipeline(model, soft_contact_margin=5e-3)
+    outs = []
+    for use_graph in (True, True, False):
+        solver = SolverVBD(model, iterations=5, use_cuda_graph=use_graph)
+        s0, s1 = model.state(), model.state()
+        s0.particle_q.copy_(torch.from_numpy(q0).cuda())
+        c = pipe.contacts()
+        for _ in range(6):
+            pipe.collide(s0, c)
+            solver.step(s0, s1, None, c, DT)
+            s0, s1 = s1, s0
+        torch.cuda.synchronize()
+        outs.append(s0.particle_q.cpu().numpy())
+        st = solver.status()
+        assert st["nonfinite_updates"] == 0 and st["contact_overflow"] == 0
+    np.testing.assert_array_equal(outs[0], outs[1])
+    np.testing.assert_array_equal(outs[0], outs[2])
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 4, 8, 16])
+def test_launch_shapes_agree(lanes):
+    model, q0 = scenes.hanging_cloth(seed=6)
+    qd = np.zeros_like(q0)
+    ref = None
+    for block in (64, 128, 256):
+        solver = SolverVBD(model, iterations=4, lanes_per_vertex=lanes, block_size=block)
+        _, q, _, _ = _gpu_step(model, solver, q0, qd, None, DT)
+        if ref is None:
+            ref = q
+        np.testing.assert_array_equal(q, ref)  # block size never changes the arithmetic
+    orc = oracle.VBDOracle(model, "f32")
+    _, q_o, _ = orc.step(q0, qd, None, DT, 4)
+    assert np.abs(ref - q_o).max() <= TOL_STEP
+
+
+def test_residual_matches_oracle():
+    """Jacobi force residual at the GPU's own iterate, GPU (FP32) vs oracle (FP64)."""
+    model, q0 = scenes.hanging_cloth(seed=7)
+    V = model.particle_count
+    qd = np.zeros((V, 3), np.float32)
+    solver = SolverVBD(model, iterations=3)
+    orc = oracle.VBDOracle(model, "f64")
+    s0 = model.state()
+    s0.particle_q.copy_(torch.from_numpy(q0).cuda())
+    solver.forward(s0, None, DT)
+    solver.iterate(None, DT, 3)
+    orc.forward(q0, qd, None, DT)
+    orc.set_positions(solver.positions().cpu().numpy())
+    mx, pv = solver.residual(None, DT, per_vertex=True)
+    r_gpu = pv.cpu().numpy()
+    r_orc = orc.residual(DT)
+    assert abs(float(mx.item()) - r_gpu.max()) <= 1e-6 * max(1.0, r_gpu.max())
+    assert r_orc.max() > 0
+    np.testing.assert_allclose(r_gpu, r_orc, rtol=1e-3, atol=1e-3 * max(1.0, r_orc.max()))
+
+
+def test_batched_worlds_per_step():
+    model, q0 = scenes.batched_worlds(num_worlds=6, seed=8, n_range=(8, 20))
+    worst, _ = _trajectory_parity(model, q0, steps=4, iterations=10, check_every=1)
+    print(f"batched 6 worlds: max |dx| {worst:.3e} m")
+
+
+def test_invalid_state_is_rejected():
+    model, q0 = scenes.hanging_cloth(seed=9)
+    solver = SolverVBD(model, iterations=1)
+    s0, s1 = model.state(), model.state()
+    s0.particle_q = s0.particle_q.double()
+    with pytest.raises(ValueError):
+        solver.step(s0, s1, None, None, DT)

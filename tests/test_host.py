@@ -1,0 +1,199 @@
+"""CPU tests: C-ABI exports, host model building, adjacency order, coloring, oracle properties."""
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from newton_b200 import ModelBuilder, _lib, scenes
+from newton_b200.coloring import construct_trimesh_graph_edges, validate_coloring
+from newton_b200.mesh import MeshAdjacency, compute_edge_adjacency
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+# ---- C ABI ---------------------------------------------------------------------------------
+def _declared_symbols():
+    text = (ROOT / "include" / "vbd_b200.h").read_text()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\*?\s+\*?(vbd_\w+)\s*\(", text, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    names = _declared_symbols()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(names) == set(_lib.SIGNATURES), "ctypes signatures must cover exactly the header"
+    assert b"sm_100a" in lib.vbd_version()
+
+
+def test_c_abi_rejects_invalid_arguments_without_a_gpu():
+    lib = _lib.load()
+    out = ctypes.c_void_p()
+    assert lib.vbd_model_create(None, ctypes.byref(out)) == _lib.VBD_ERR_INVALID_ARGUMENT
+    assert b"NULL" in lib.vbd_last_error()
+    d = _lib.VbdModelDesc()
+    d.particle_count = 4
+    assert lib.vbd_model_create(ctypes.byref(d), ctypes.byref(out)) == _lib.VBD_ERR_INVALID_ARGUMENT
+    assert lib.vbd_step(None, None, None, None, None, None, None, ctypes.c_float(0.01), 10, None) != 0
+    assert lib.vbd_solver_create(None, None, ctypes.byref(out)) == _lib.VBD_ERR_INVALID_ARGUMENT
+    colors = np.zeros(3, np.int32)
+    nc = ctypes.c_int32()
+    bad = np.array([[0, 5]], np.int32)
+    assert lib.vbd_color_graph(3, 1, _lib.as_i32p(bad), 0, 1, ctypes.c_float(1.1), _lib.as_i32p(colors),
+                               ctypes.byref(nc)) == _lib.VBD_ERR_INVALID_ARGUMENT
+
+
+# ---- adjacency -----------------------------------------------------------------------------
+def _edge_adjacency_loop(tris):
+    """Loop restatement of MeshAdjacency._compute_edge_adjacency (utils/mesh.py:465-531)."""
+    edges = {}
+    order = []
+    rows = []
+    for t, (a, b, c) in enumerate(tris):
+        for v0, v1, o in ((a, b, c), (b, c, a), (c, a, b)):
+            key = (min(v0, v1), max(v0, v1))
+            if key not in edges:
+                edges[key] = len(order)
+                order.append(key)
+                rows.append([o, -1, v0, v1])
+            else:
+                rows[edges[key]][1] = o
+    return np.array(rows, dtype=np.int32)
+
+
+def _csr_loop(elems, V, slot_order):
+    """Loop restatement of the serial count/fill kernels (utils/mesh.py:675-772)."""
+    lists = [[] for _ in range(V)]
+    for e, row in enumerate(elems):
+        for slot in slot_order:
+            v = row[slot]
+            if v != -1:
+                lists[v] += [e, slot]
+    offs = np.zeros(V + 1, np.int32)
+    offs[1:] = np.cumsum([len(x) for x in lists])
+    return np.array([x for l in lists for x in l], np.int32), offs
+
+
+def test_edge_and_vertex_adjacency_follow_reference_order():
+    rng = np.random.default_rng(0)
+    verts, tris = ModelBuilder.grid_mesh(7, 5, 0.1, 0.1)
+    tris = tris.reshape(-1, 3)
+    tris = tris[rng.permutation(len(tris))]  # arbitrary triangle order
+    e, _, _ = compute_edge_adjacency(tris)
+    np.testing.assert_array_equal(e, _edge_adjacency_loop(tris.tolist()))
+    V = verts.shape[0]
+    adj = MeshAdjacency(tris, e).init_vertex_adjacency(V)
+    vt, ot = _csr_loop(tris.tolist(), V, [0, 1, 2])
+    np.testing.assert_array_equal(adj.v_adj_tris, vt)
+    np.testing.assert_array_equal(adj.v_adj_tris_offsets, ot)
+    ve, oe = _csr_loop(e.tolist(), V, [2, 3, 0, 1])
+    np.testing.assert_array_equal(adj.v_adj_edges, ve)
+    np.testing.assert_array_equal(adj.v_adj_edges_offsets, oe)
+
+
+# ---- builder -------------------------------------------------------------------------------
+def test_cloth_grid_counts_masses_and_rest_data():
+    model, q0 = scenes.hanging_cloth(seed=0, device="cpu")
+    assert (model.particle_count, model.tri_count, model.edge_count) == (1024, 1922, 2945)
+    area = (1.0 / 31) ** 2 / 2
+    np.testing.assert_allclose(model.tri_areas, area, rtol=1e-6)
+    # lumped mass: density * area / 3 per incident triangle, pinned corners zeroed
+    counts = np.bincount(model.tri_indices.reshape(-1), minlength=1024)
+    expect = 0.1 * area / 3.0 * counts
+    pinned = np.flatnonzero((model.particle_flags & 1) == 0)
+    assert len(pinned) == 2
+    expect[pinned] = 0.0
+    np.testing.assert_allclose(model.particle_mass, expect, rtol=1e-6)
+    assert np.all(model.particle_inv_mass[pinned] == 0)
+    np.testing.assert_allclose(model.edge_rest_angle, 0.0, atol=1e-7)  # flat rest shape
+    interior = (model.edge_indices[:, 0] >= 0) & (model.edge_indices[:, 1] >= 0)
+    assert interior.sum() == 2945 - 4 * 31
+    assert np.abs(q0[:, 2] - model.particle_q[:, 2]).max() <= 1e-3
+    # DmInv maps the rest edges to the 2D rest frame: D * DmInv = I
+    t = model.tri_indices[0]
+    x = model.particle_q[t].astype(np.float64)
+    e1 = (x[1] - x[0]) / np.linalg.norm(x[1] - x[0])
+    n = np.cross(x[1] - x[0], x[2] - x[0])
+    e2 = np.cross(n / np.linalg.norm(n), e1)
+    D = np.array([e1, e2]) @ np.array([x[1] - x[0], x[2] - x[0]]).T
+    np.testing.assert_allclose(D @ model.tri_poses[0], np.eye(2), atol=1e-5)
+
+
+def test_coloring_valid_and_balanced():
+    for include_bending in (False, True):
+        model, _ = scenes.single_cloth(n=40, include_bending=include_bending, device="cpu")
+        b = ModelBuilder()
+        edges = construct_trimesh_graph_edges(model.tri_indices, None,
+                                              model.edge_indices if include_bending else None, None)
+        assert validate_coloring(edges, model.particle_color_groups, model.particle_count)
+        sizes = [len(g) for g in model.particle_color_groups]
+        assert max(sizes) / min(sizes) <= 1.1 + 1e-9
+        del b
+
+
+def test_batched_worlds_merge_colorings():
+    model, _ = scenes.batched_worlds(num_worlds=12, seed=1, device="cpu")
+    edges = construct_trimesh_graph_edges(model.tri_indices, None, model.edge_indices, None)
+    assert validate_coloring(edges, model.particle_color_groups, model.particle_count)
+    worlds = model.particle_world
+    assert set(np.unique(worlds)) == set(range(12))
+    # each world's ground plane belongs to that world
+    assert list(model.shape_world) == list(range(12))
+
+
+# ---- oracle properties ---------------------------------------------------------------------
+def test_oracle_thread_count_does_not_change_results():
+    model, q0 = scenes.hanging_cloth(seed=2, device="cpu")
+    qd = np.zeros_like(q0)
+    a = oracle.VBDOracle(model, "f32", threads=1).step(q0, qd, None, 1 / 600, 5)[1]
+    b = oracle.VBDOracle(model, "f32", threads=4).step(q0, qd, None, 1 / 600, 5)[1]
+    np.testing.assert_array_equal(a, b)
+
+
+def test_oracle_fp32_tracks_fp64():
+    model, q0 = scenes.hanging_cloth(seed=3, device="cpu")
+    qd = np.zeros_like(q0)
+    o32 = oracle.VBDOracle(model, "f32", threads=4)
+    o64 = oracle.VBDOracle(model, "f64", threads=4)
+    q32, q64, v32, v64 = q0, q0, qd, qd
+    for _ in range(10):
+        _, q32, v32 = o32.step(q32, v32, None, 1 / 600, 10)
+        _, q64, v64 = o64.step(q64, v64, None, 1 / 600, 10)
+    assert np.abs(q32 - q64).max() <= 1e-5
+    # pinned corners do not move; free vertices fall
+    pinned = np.flatnonzero((model.particle_flags & 1) == 0)
+    np.testing.assert_array_equal(q32[pinned], q0[pinned])
+    assert q32[:, 2].mean() < q0[:, 2].mean()
+
+
+def test_free_fall_matches_ballistic_motion():
+    """test_cloth.py:1116-1137: an unconstrained cloth free-falls by g t^2 / 2 (implicit Euler)."""
+    model, q0 = scenes.single_cloth(n=8, pin_top_corners=False, ground=None, device="cpu")
+    qd = np.zeros_like(q0)
+    orc = oracle.VBDOracle(model, "f64")
+    q, v = q0, qd
+    dt, n = 1 / 600, 60
+    for _ in range(n):
+        _, q, v = orc.step(q, v, None, dt, 5)
+    drop = (q0[:, 2] - q[:, 2]).mean()
+    t = n * dt
+    # implicit Euler falls g dt^2 n(n+1)/2
+    np.testing.assert_allclose(drop, 9.81 * dt * dt * n * (n + 1) / 2, rtol=1e-3)
+    assert abs(drop - 0.5 * 9.81 * t * t) < 0.2
+
+
+def test_solver_requires_coloring():
+    from newton_b200.solvers import SolverVBD
+
+    b = ModelBuilder()
+    verts, tris = ModelBuilder.grid_mesh(3, 3, 0.1, 0.1)
+    b.add_cloth_mesh(pos=(0, 0, 0), rot=(0, 0, 0, 1), scale=1.0, vel=(0, 0, 0), vertices=verts, indices=tris,
+                     density=0.1)
+    m = b.finalize(device="cpu")
+    with pytest.raises(ValueError, match="particle_color_groups is empty"):
+        SolverVBD(m)
