@@ -186,6 +186,22 @@ int vbd_solver_destroy(VbdSolver* solver);
 int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, const float* f_ext, float* q_out,
              float* qd_out, const VbdContacts* contacts, float dt, int32_t iterations, void* stream);
 
+/* Allocation-free variant of vbd_step (no counterpart in the reference, whose solver always
+ * allocates its scratch).  For callers that cannot call cudaMalloc -- code running during CUDA
+ * stream capture, host callbacks or real-time loops where an allocation could block or
+ * synchronize the device, and embedders whose device memory belongs to a framework allocator --
+ * and therefore cannot create a VbdSolver.  The step's scratch lives in a static device array of
+ * the library sized for at most 16384 particles (about 1.3 MiB, held on every GPU that loads the
+ * library until the process exits); larger models are rejected with VBD_ERR_INVALID_ARGUMENT.
+ * Allocates nothing and takes no solver: same arrays, aliasing and results as vbd_step with
+ * lanes_per_vertex 4, block_size 128 and 4 contacts per vertex.  The first call on a device looks
+ * up the array's device address; make that first call before any stream capture.  Every call
+ * shares the one array (it clears the parts that must start at zero), so calls that overlap on
+ * the GPU -- concurrent streams or threads -- race; serialize them. */
+int vbd_step_static(const VbdModel* model, float* q_in, const float* qd_in, const float* f_ext, float* q_out,
+                    float* qd_out, const VbdContacts* contacts, float dt, int32_t iterations,
+                    float friction_epsilon, void* stream);
+
 /* Staged pieces of vbd_step, for parity tests against a staged oracle. */
 int vbd_forward(VbdSolver* solver, const float* q_in, const float* qd_in, const float* f_ext,
                 const VbdContacts* contacts, float dt, void* stream);

@@ -125,6 +125,10 @@ SIGNATURES = {
         ctypes.c_int,
         [_VP, _VP, _VP, _VP, _VP, _VP, ctypes.POINTER(VbdContacts), ctypes.c_float, ctypes.c_int32, _VP],
     ),
+    "vbd_step_static": (
+        ctypes.c_int,
+        [_VP, _VP, _VP, _VP, _VP, _VP, ctypes.POINTER(VbdContacts), ctypes.c_float, ctypes.c_int32, ctypes.c_float, _VP],
+    ),
     "vbd_forward": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.POINTER(VbdContacts), ctypes.c_float, _VP]),
     "vbd_sweep_color": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(VbdContacts), ctypes.c_float, _VP]),
     "vbd_finalize": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_float, _VP]),

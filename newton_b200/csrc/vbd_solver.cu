@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -766,3 +767,98 @@ extern "C" int vbd_set_launch(VbdSolver* solver, int32_t lanes_per_vertex, int32
 }
 
 extern "C" const char* vbd_version(void) { return "vbd_b200 0.1 (sm_100a)"; }
+
+// ---------------------------------------------------------------------------------------------
+// Allocation-free step: vbd_step_static.
+//
+// Some callers cannot call cudaMalloc: code that runs while a stream is being captured into a
+// CUDA graph (allocation is not a capturable operation), host callbacks and real-time loops
+// where an allocation could block or implicitly synchronize the device, and embedders whose
+// device memory is owned by a framework allocator that forbids raw cudaMalloc (an ML framework's
+// custom-call / FFI handler, for instance).  vbd_solver_create allocates the step's scratch, so
+// those callers cannot create a VbdSolver.  vbd_step_static runs the same step without a solver:
+// its scratch (Gauss-Seidel iterate, step-start positions, inertia targets, displacements and the
+// per-vertex contact table) lives in the file-scope device array below, sized for at most
+// kStaticMaxParticles particles (~1.3 MiB, held by every GPU that loads the library until the
+// process exits).
+// ---------------------------------------------------------------------------------------------
+namespace vbd {
+namespace {
+
+constexpr int kStaticMaxParticles = 16384;
+constexpr int kStaticContactsPerVertex = 4;
+constexpr size_t kStaticVec4Bytes = static_cast<size_t>(kStaticMaxParticles) * sizeof(float4);
+constexpr size_t kStaticCountBytes = static_cast<size_t>(kStaticMaxParticles) * sizeof(int);
+constexpr size_t kStaticSlotBytes = static_cast<size_t>(kStaticMaxParticles) * kStaticContactsPerVertex * sizeof(int);
+constexpr size_t kStaticStatusBytes = 256;
+constexpr size_t kStaticScratchBytes = 4 * kStaticVec4Bytes + kStaticCountBytes + kStaticSlotBytes + kStaticStatusBytes;
+
+static __device__ __align__(256) unsigned char g_step_scratch[kStaticScratchBytes];
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mutex;
+unsigned char* g_static_scratch_ptr[kStaticMaxDevices] = {};
+
+// Device address of g_step_scratch on the current device (host code cannot use the symbol's
+// name as an address).  Looked up once per device, on that device's first call.
+int static_scratch(unsigned char** out) {
+    int dev = 0;
+    VBD_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kStaticMaxDevices) return fail(VBD_ERR_UNSUPPORTED, "vbd_step_static: device ordinal too large");
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_scratch_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_step_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_step_scratch)");
+        g_static_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_static_scratch_ptr[dev];
+    return VBD_OK;
+}
+
+}  // namespace
+}  // namespace vbd
+
+extern "C" int vbd_step_static(const VbdModel* model, float* q_in, const float* qd_in, const float* f_ext,
+                               float* q_out, float* qd_out, const VbdContacts* contacts, float dt, int32_t iterations,
+                               float friction_epsilon, void* stream) {
+    using namespace vbd;
+    if (!model) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_step_static: model is NULL");
+    const VbdModelImpl& m = model->m;
+    if (m.V > kStaticMaxParticles)
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_step_static: the model has " + std::to_string(m.V) +
+                                                  " particles; the static scratch holds at most " +
+                                                  std::to_string(kStaticMaxParticles) + " (use vbd_solver_create + vbd_step)");
+    if (m.V == 0) return VBD_OK;
+    int rc = check_state_args("vbd_step_static", q_in, qd_in);
+    if (rc) return rc;
+    if (!q_out || !qd_out) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_step_static: state_out arrays are NULL");
+    if (!(dt > 0.0f)) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_step_static: dt must be > 0");
+    if (iterations < 0) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_step_static: iterations must be >= 0");
+    if (contacts && !contacts->soft_contact_count) contacts = nullptr;
+    unsigned char* base = nullptr;
+    rc = static_scratch(&base);
+    if (rc) return rc;
+    SolverImpl s;  // host-side view of the static scratch; owns nothing
+    s.m = &m;
+    s.iterations = iterations;
+    s.friction_epsilon = friction_epsilon;
+    s.lanes = 4;
+    s.block = 128;
+    s.K = kStaticContactsPerVertex;
+    s.use_graph = false;
+    s.pos = reinterpret_cast<float4*>(base);
+    s.prev = reinterpret_cast<float4*>(base + kStaticVec4Bytes);
+    s.y = reinterpret_cast<float4*>(base + 2 * kStaticVec4Bytes);
+    s.disp = reinterpret_cast<float4*>(base + 3 * kStaticVec4Bytes);
+    s.ccount = reinterpret_cast<int*>(base + 4 * kStaticVec4Bytes);
+    s.cslot = reinterpret_cast<int*>(base + 4 * kStaticVec4Bytes + kStaticCountBytes);
+    s.status = reinterpret_cast<unsigned*>(base + 4 * kStaticVec4Bytes + kStaticCountBytes + kStaticSlotBytes);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the array keeps the previous call's contents: the contact table and counters must start at zero
+    VBD_CUDA_TRY(cudaMemsetAsync(s.ccount, 0, sizeof(int) * static_cast<size_t>(m.V), st));
+    VBD_CUDA_TRY(cudaMemsetAsync(s.status, 0, kStaticStatusBytes, st));
+    enqueue_step(s, q_in, qd_in, f_ext, q_out, qd_out, contacts, dt, iterations, st);
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
