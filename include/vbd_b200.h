@@ -121,8 +121,10 @@ typedef struct VbdModelDesc {
 typedef struct VbdSolverOptions {
     int32_t iterations;           /* default VBD iterations per step (reference default 10) */
     float friction_epsilon;       /* reference default 1e-2 */
-    int32_t lanes_per_vertex;     /* 1,2,4,8,16 or 0 = pick from the mesh (autotuner may override) */
-    int32_t block_size;           /* threads per block of the sweep, 0 = default 128 */
+    int32_t lanes_per_vertex;     /* 1,2,4,8,16 = that many lanes cooperate on one vertex; 0 = default (4);
+                                     -1 = record-parallel sweep (one thread per element record) */
+    int32_t block_size;           /* threads per block of the sweep, 0 = default 128 (64/128/256 when
+                                     lanes_per_vertex is 0) */
     int32_t contacts_per_vertex;  /* capacity of the per-vertex contact table, 0 = default 4 */
     int32_t use_graph;            /* 1: replay vbd_step from a cached CUDA graph */
 } VbdSolverOptions;
@@ -225,7 +227,8 @@ int vbd_status(VbdSolver* solver, VbdStatus* out, int32_t reset);
 int vbd_solver_info(const VbdSolver* solver, int32_t* color_count, int32_t* lanes_per_vertex,
                     int32_t* block_size);
 
-/* Override the sweep launch shape (used by the autotuner).  lanes in {1,2,4,8,16}. */
+/* Override the sweep launch shape (used by the autotuner): lanes_per_vertex 0 with block_size
+ * 64/128/256 (record-parallel), or lanes_per_vertex in {1,2,4,8,16} with a block_size multiple of 32. */
 int vbd_set_launch(VbdSolver* solver, int32_t lanes_per_vertex, int32_t block_size);
 
 /* Graph coloring of an undirected graph (host arrays): ModelBuilder.color -> color_graph

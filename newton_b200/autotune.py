@@ -13,7 +13,7 @@ import itertools
 
 import torch
 
-LANES = (1, 2, 4, 8, 16)
+LANES = (0, 1, 2, 4, 8, 16)   # 0 = record-parallel sweep
 BLOCKS = (64, 128, 256)
 
 

@@ -152,9 +152,10 @@ __device__ __forceinline__ void bending_eval(int order, float3 x0, float3 x1, fl
     const float3 e = x3 - x2;
     const float3 n1 = cross(x02, x03);
     const float3 n2 = cross(x13, x12);
-    const float n1n = length(n1), n2n = length(n2), en = length(e);
-    if (n1n < eps || n2n < eps || en < eps) return;
-    const float i1 = 1.0f / n1n, i2 = 1.0f / n2n, ie = 1.0f / en;
+    // |n| < eps  <=>  |n|^2 < eps^2; the unit vectors use the hardware reciprocal square root
+    const float d1 = dot(n1, n1), d2 = dot(n2, n2), de = dot(e, e);
+    if (d1 < eps * eps || d2 < eps * eps || de < eps * eps) return;
+    const float i1 = rsqrtf(d1), i2 = rsqrtf(d2), ie = rsqrtf(de);
     const float3 n1h = n1 * i1;
     const float3 n2h = n2 * i2;
     const float3 eh = e * ie;
@@ -192,11 +193,11 @@ __device__ __forceinline__ void bending_eval(int order, float3 x0, float3 x1, fl
         const float3 pe = a3 - a2;
         const float3 q1 = cross(p02, p03);
         const float3 q2 = cross(p13, p12);
-        const float q1n = length(q1), q2n = length(q2), qen = length(pe);
-        if (q1n < eps || q2n < eps || qen < eps) return;
-        const float3 q1h = q1 * (1.0f / q1n);
-        const float3 q2h = q2 * (1.0f / q2n);
-        const float3 qeh = pe * (1.0f / qen);
+        const float s1 = dot(q1, q1), s2 = dot(q2, q2), se = dot(pe, pe);
+        if (s1 < eps * eps || s2 < eps * eps || se < eps * eps) return;
+        const float3 q1h = q1 * rsqrtf(s1);
+        const float3 q2h = q2 * rsqrtf(s2);
+        const float3 qeh = pe * rsqrtf(se);
         const float theta_prev = atan2f(dot(cross(q1h, q2h), qeh), dot(q1h, q2h));
         float dth = theta - theta_prev;
         if (dth > 3.141592653589793f) {

@@ -147,7 +147,10 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
         pinfo[i] = make_float4(d->particle_mass[o], d->particle_inv_mass[o], d->particle_radius[o], fl);
         int4 a;
         a.x = static_cast<int>(tri_idx.size());
-        if (T > 0) {
+        // pinned / massless vertices are never solved (solve_elasticity returns early for them),
+        // so they own no element records
+        const bool solvable = (flags & VBD_PARTICLE_ACTIVE) && d->particle_mass[o] != 0.0f;
+        if (T > 0 && solvable) {
             const int b = d->v_adj_tris_offsets[o], e = d->v_adj_tris_offsets[o + 1];
             for (int k = b; k < e; k += 2) {
                 const int t = d->v_adj_tris[k], slot = d->v_adj_tris[k + 1];
@@ -165,7 +168,7 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
         }
         a.y = static_cast<int>(tri_idx.size());
         a.z = static_cast<int>(edge_idx.size());
-        if (E > 0) {
+        if (E > 0 && solvable) {
             const int b = d->v_adj_edges_offsets[o], e = d->v_adj_edges_offsets[o + 1];
             for (int k = b; k < e; k += 2) {
                 const int ed = d->v_adj_edges[k], slot = d->v_adj_edges[k + 1];

@@ -46,7 +46,7 @@ struct SolverImpl {
     const VbdModelImpl* m = nullptr;
     int iterations = 10;
     float friction_epsilon = 1e-2f;
-    int lanes = 4;
+    int lanes = 4;  // 0: record-parallel tiles; 1..16: lanes cooperating on one vertex
     int block = 128;
     int K = 4;
     bool use_graph = true;
@@ -308,6 +308,173 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs a) {
     if (a.write_pos) a.pos[i] = make_float4(pv.x + d.x, pv.y + d.y, pv.z + d.z, 0.f);
 }
 
+// Record-parallel variant of the same color update (lanes_per_vertex == 0).  A block owns
+// VT = TB/16 consecutive vertices of the color and the contiguous runs of element records they
+// own.  Every thread evaluates one record at a time (all triangles of the tile, then all hinges),
+// writing its force/Hessian contribution to shared memory; then 9 reducer threads per vertex --
+// one per component -- add the vertex's contributions in record order, starting from the
+// inertia term.  That is the summation order of the reference's serial path
+// (solve_elasticity, particle_vbd_kernels.py:2568-2706): inertia, triangles in CSR order, hinges
+// in CSR order, then the accumulated contact force and Hessian.  The order never depends on
+// thread scheduling, so results are deterministic.
+template <int TB, bool kDamp, bool kResidual>
+__global__ void __launch_bounds__(TB) tile_kernel(SweepArgs a) {
+    constexpr int VT = TB / 16;
+    constexpr int MAXR = 2 * TB;
+    constexpr int STRIDE = MAXR + 1;  // odd row stride: the 9 reducers of a vertex hit 9 banks
+    static_assert(VT * 9 <= TB, "one reducer thread per vertex component");
+    __shared__ float s_c[9 * STRIDE];
+    __shared__ int4 s_adj[VT];
+    __shared__ float s_sum[VT][9];
+    const int vb = a.v_begin + blockIdx.x * VT;
+    const int nv = min(VT, a.v_end - vb);
+    const int t = threadIdx.x;
+    if (t < nv) s_adj[t] = __ldg(&a.vadj[vb + t]);
+    __syncthreads();
+    const int rv = t / 9;
+    const int rc = t - 9 * rv;
+    const bool reducer = rv < nv;
+    float acc = 0.0f;
+    if (reducer) {
+        // inertia: f = m (y - x) / dt^2, H = m / dt^2 I  (zero for vertices that own no records)
+        const int4 ad = s_adj[rv];
+        if (ad.y > ad.x || ad.w > ad.z) {
+            const float4 yv = __ldg(&a.y[vb + rv]);
+            const float4 xv = a.pos[vb + rv];
+            const float m = yv.w;
+            if (rc < 3) {
+                const float d = rc == 0 ? yv.x - xv.x : (rc == 1 ? yv.y - xv.y : yv.z - xv.z);
+                acc = (m * d) * a.dt_sqr_recip;
+            } else if (rc == 3 || rc == 6 || rc == 8) {
+                acc = m * a.dt_sqr_recip;
+            }
+        }
+    }
+    // One merged list per tile: the tile's triangle records, then its hinge records.  Component
+    // order in shared memory: f.x f.y f.z h.xx h.xy h.xz h.yy h.yz h.zz.
+    const int tb = s_adj[0].x, nt = s_adj[nv - 1].y - tb;
+    const int eb = s_adj[0].z, ne = s_adj[nv - 1].w - eb;
+    const int ntot = nt + ne;
+    for (int base = 0; base < ntot; base += MAXR) {
+        const int n = min(MAXR, ntot - base);
+        for (int r = t; r < n; r += TB) {
+            float3 f = f3(0.f, 0.f, 0.f);
+            Sym3 h = zero_sym();
+            const int k = base + r;
+            if (k < nt) {
+                const int rec = tb + k;
+                const int4 ti = __ldg(&a.tri_idx[rec]);
+                const float4 D = __ldg(&a.tri_D[rec]);
+                const float4 mt = __ldg(&a.tri_mat[rec]);
+                const float3 x0 = xyz(a.pos[ti.x]), x1 = xyz(a.pos[ti.y]), x2 = xyz(a.pos[ti.z]);
+                float3 p0 = x0, p1 = x1, p2 = x2;
+                if (kDamp && mt.w > 0.0f) {
+                    p0 = xyz(__ldg(&a.prev[ti.x]));
+                    p1 = xyz(__ldg(&a.prev[ti.y]));
+                    p2 = xyz(__ldg(&a.prev[ti.z]));
+                }
+                membrane_eval<kDamp>(ti.w, x0, x1, x2, p0, p1, p2, D, mt, a.inv_dt, f, h);
+            } else {
+                const int rec = eb + (k - nt);
+                const int4 ei = __ldg(&a.edge_idx[rec]);
+                const float4 em = __ldg(&a.edge_mat[rec]);
+                const int order = static_cast<int>(static_cast<unsigned>(ei.x) >> 30);
+                const int o0 = ei.x & 0x3fffffff;
+                const float3 x0 = xyz(a.pos[o0]), x1 = xyz(a.pos[ei.y]), x2 = xyz(a.pos[ei.z]),
+                             x3 = xyz(a.pos[ei.w]);
+                float3 p0 = x0, p1 = x1, p2 = x2, p3 = x3;
+                if (kDamp && em.w > 0.0f) {
+                    p0 = xyz(__ldg(&a.prev[o0]));
+                    p1 = xyz(__ldg(&a.prev[ei.y]));
+                    p2 = xyz(__ldg(&a.prev[ei.z]));
+                    p3 = xyz(__ldg(&a.prev[ei.w]));
+                }
+                bending_eval<kDamp>(order, x0, x1, x2, x3, p0, p1, p2, p3, em, a.inv_dt, f, h);
+            }
+            s_c[0 * STRIDE + r] = f.x;
+            s_c[1 * STRIDE + r] = f.y;
+            s_c[2 * STRIDE + r] = f.z;
+            s_c[3 * STRIDE + r] = h.xx;
+            s_c[4 * STRIDE + r] = h.xy;
+            s_c[5 * STRIDE + r] = h.xz;
+            s_c[6 * STRIDE + r] = h.yy;
+            s_c[7 * STRIDE + r] = h.yz;
+            s_c[8 * STRIDE + r] = h.zz;
+        }
+        __syncthreads();
+        if (reducer) {
+            // this vertex's triangles, then its hinges, in record order
+            const int4 ad = s_adj[rv];
+            const float* row = s_c + rc * STRIDE - base;
+            int lo = max(ad.x - tb, base), hi = min(ad.y - tb, base + n);
+            for (int r = lo; r < hi; ++r) acc += row[r];
+            lo = max(nt + ad.z - eb, base);
+            hi = min(nt + ad.w - eb, base + n);
+            for (int r = lo; r < hi; ++r) acc += row[r];
+        }
+        __syncthreads();
+    }
+    if (reducer) s_sum[rv][rc] = acc;
+    __syncthreads();
+    if (t >= nv) return;
+    const int i = vb + t;
+    const float4 pv = a.prev[i];
+    const int4 ad = s_adj[t];
+    const float4 pi = __ldg(&a.pinfo[i]);
+    const bool solve = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
+    if (!solve) {
+        if (kResidual) {
+            if (a.resid_out) a.resid_out[a.perm[i]] = 0.0f;
+        } else {
+            a.disp[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (a.write_pos) a.pos[i] = pv;
+        }
+        return;
+    }
+    float3 f;
+    Sym3 h;
+    if (ad.y > ad.x || ad.w > ad.z) {
+        f = f3(s_sum[t][0], s_sum[t][1], s_sum[t][2]);
+        h.xx = s_sum[t][3];
+        h.xy = s_sum[t][4];
+        h.xz = s_sum[t][5];
+        h.yy = s_sum[t][6];
+        h.yz = s_sum[t][7];
+        h.zz = s_sum[t][8];
+    } else {
+        // a solvable vertex without elements: inertia only
+        const float4 yv = __ldg(&a.y[i]);
+        const float4 xv = a.pos[i];
+        f = (yv.w * (xyz(yv) - xyz(xv))) * a.dt_sqr_recip;
+        h = zero_sym();
+        add_diag(h, yv.w * a.dt_sqr_recip);
+    }
+    float3 fc = f3(0.f, 0.f, 0.f);
+    Sym3 hc = zero_sym();
+    if (a.ccount) accumulate_contacts(a, i, xyz(a.pos[i]), xyz(pv), pi.z, fc, hc);
+    add(h, hc);
+    f = f + fc;
+    if (kResidual) {
+        const float r = length(f) / pi.x * a.inv_g;
+        if (a.resid_out) a.resid_out[a.perm[i]] = r;
+        if (a.resid_max) atomicMax(reinterpret_cast<int*>(a.resid_max), __float_as_int(r));
+        return;
+    }
+    float3 dx;
+    float4 d = a.disp[i];
+    if (solve3(h, f, dx)) {
+        if (isfinite(dx.x) && isfinite(dx.y) && isfinite(dx.z)) {
+            d = make_float4(d.x + dx.x, d.y + dx.y, d.z + dx.z, 0.f);
+            a.disp[i] = d;
+        } else {
+            atomicAdd(&a.status[kNonfinite], 1u);
+        }
+    } else {
+        atomicAdd(&a.status[kSingular], 1u);
+    }
+    if (a.write_pos) a.pos[i] = make_float4(pv.x + d.x, pv.y + d.y, pv.z + d.z, 0.f);
+}
+
 // Commit of a color when the coloring is not conflict-free for every element stencil: the
 // sweep then leaves positions untouched (Jacobi within the color, as the reference's separate
 // apply_truncation_ts launch does) and this pass writes q = prev + disp.
@@ -416,7 +583,27 @@ static void launch_sweep_L(const SweepArgs& a, bool damp, bool residual, int blo
     }
 }
 
+template <int TB>
+static void launch_tile_TB(const SweepArgs& a, bool damp, bool residual, cudaStream_t st) {
+    constexpr int VT = TB / 16;
+    const int grid = (a.v_end - a.v_begin + VT - 1) / VT;
+    if (grid <= 0) return;
+    if (residual) {
+        if (damp) tile_kernel<TB, true, true><<<grid, TB, 0, st>>>(a);
+        else tile_kernel<TB, false, true><<<grid, TB, 0, st>>>(a);
+    } else {
+        if (damp) tile_kernel<TB, true, false><<<grid, TB, 0, st>>>(a);
+        else tile_kernel<TB, false, false><<<grid, TB, 0, st>>>(a);
+    }
+}
+
 static void launch_sweep(const SweepArgs& a, int lanes, bool damp, bool residual, int block, cudaStream_t st) {
+    if (lanes == 0) {
+        if (block <= 64) launch_tile_TB<64>(a, damp, residual, st);
+        else if (block <= 128) launch_tile_TB<128>(a, damp, residual, st);
+        else launch_tile_TB<256>(a, damp, residual, st);
+        return;
+    }
     switch (lanes) {
         case 1: launch_sweep_L<1>(a, damp, residual, block, st); break;
         case 2: launch_sweep_L<2>(a, damp, residual, block, st); break;
@@ -511,6 +698,19 @@ static void free_solver(SolverImpl& s) {
     s.capture_stream = nullptr;
 }
 
+// nullptr when (lanes, block) is a supported sweep launch shape, else the reason
+static const char* launch_shape_error(int lanes, int block) {
+    if (lanes == 0) {
+        if (block != 64 && block != 128 && block != 256)
+            return "block_size must be 64, 128 or 256 for the record-parallel sweep (lanes_per_vertex 0)";
+        return nullptr;
+    }
+    if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8 && lanes != 16)
+        return "lanes_per_vertex must be 0 (record-parallel), 1, 2, 4, 8 or 16";
+    if (block < 32 || block > 256 || (block % 32) != 0) return "block_size must be a multiple of 32 in [32, 256]";
+    return nullptr;
+}
+
 static bool same_contacts(const VbdContacts& a, const VbdContacts& b) { return std::memcmp(&a, &b, sizeof(a)) == 0; }
 
 static int check_state_args(const char* fn, const float* a, const float* b) {
@@ -537,18 +737,15 @@ extern "C" int vbd_solver_create(const VbdModel* model, const VbdSolverOptions* 
         }
         s.iterations = options->iterations;
         s.friction_epsilon = options->friction_epsilon;
-        if (options->lanes_per_vertex) s.lanes = options->lanes_per_vertex;
+        if (options->lanes_per_vertex > 0) s.lanes = options->lanes_per_vertex;
+        if (options->lanes_per_vertex < 0) s.lanes = 0;
         if (options->block_size) s.block = options->block_size;
         if (options->contacts_per_vertex) s.K = options->contacts_per_vertex;
         s.use_graph = options->use_graph != 0;
     }
-    if (s.lanes != 1 && s.lanes != 2 && s.lanes != 4 && s.lanes != 8 && s.lanes != 16) {
+    if (const char* why = launch_shape_error(s.lanes, s.block)) {
         delete h;
-        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_solver_create: lanes_per_vertex must be 1, 2, 4, 8 or 16");
-    }
-    if (s.block < 32 || s.block > 256 || (s.block % 32) != 0) {
-        delete h;
-        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_solver_create: block_size must be a multiple of 32 in [32, 256]");
+        return fail(VBD_ERR_INVALID_ARGUMENT, std::string("vbd_solver_create: ") + why);
     }
     if (s.K < 1 || s.K > 8) {
         delete h;
@@ -756,12 +953,9 @@ extern "C" int vbd_solver_info(const VbdSolver* solver, int32_t* color_count, in
 
 extern "C" int vbd_set_launch(VbdSolver* solver, int32_t lanes_per_vertex, int32_t block_size) {
     if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_launch: solver is NULL");
-    const int L = lanes_per_vertex;
-    if (L != 1 && L != 2 && L != 4 && L != 8 && L != 16)
-        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_launch: lanes_per_vertex must be 1, 2, 4, 8 or 16");
-    if (block_size < 32 || block_size > 256 || (block_size % 32) != 0)
-        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_launch: block_size must be a multiple of 32 in [32, 256]");
-    solver->s.lanes = L;
+    if (const char* why = launch_shape_error(lanes_per_vertex, block_size))
+        return fail(VBD_ERR_INVALID_ARGUMENT, std::string("vbd_set_launch: ") + why);
+    solver->s.lanes = lanes_per_vertex;
     solver->s.block = block_size;
     return VBD_OK;
 }

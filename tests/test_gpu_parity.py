@@ -157,7 +157,7 @@ def test_graph_replay_and_plain_launches_are_bitwise_equal_and_deterministic():
     np.testing.assert_array_equal(outs[0], outs[2])
 
 
-@pytest.mark.parametrize("lanes", [1, 2, 4, 8, 16])
+@pytest.mark.parametrize("lanes", [0, 1, 2, 4, 8, 16])
 def test_launch_shapes_agree(lanes):
     model, q0 = scenes.hanging_cloth(seed=6)
     qd = np.zeros_like(q0)
