@@ -316,6 +316,7 @@ def main() -> None:
         "config": {"workload": WORKLOAD, "vertices": V, "triangles": model.tri_count, "hinges": model.edge_count,
                    "colors": colors, "iterations": ITERATIONS, "dt": DT, "l2": "flushed between timed steps",
                    "parallelism": f"replicas x{world}", "launch": solver.launch_info(),
+                   "step_kernel": solver.step_kernel_info(),
                    "residual_gate": "not applied: fixed 10 iterations (plain VBD)"},
         "vertex_iterations_per_s": value * V * ITERATIONS,
         "residual_after_step": resid,

@@ -115,6 +115,8 @@ typedef struct VbdModelDesc {
     float soft_contact_kd;                 /* Model.soft_contact_kd */
     float soft_contact_mu;                 /* Model.soft_contact_mu */
     const VbdShape* shapes;                /* [S] */
+    const float* particle_q;               /* [V,3] rest/initial positions or NULL; used only to cut the
+                                              model into compact patches for the resident step kernel */
 } VbdModelDesc;
 
 /* Solver options (SolverVBD keyword arguments that touch the particle path, plus launch shape). */
@@ -127,6 +129,9 @@ typedef struct VbdSolverOptions {
                                      lanes_per_vertex is 0) */
     int32_t contacts_per_vertex;  /* capacity of the per-vertex contact table, 0 = default 4 */
     int32_t use_graph;            /* 1: replay vbd_step from a cached CUDA graph */
+    int32_t step_kernel;          /* 0 = one launch per color (default); 1 = one persistent
+                                     shared-memory-resident kernel per step when the model fits the
+                                     GPU's shared memory (else one launch per color) */
 } VbdSolverOptions;
 
 /* Soft-contact records in the reference layout (newton.Contacts soft_contact_*; DEVICE pointers). */
@@ -226,6 +231,16 @@ int vbd_status(VbdSolver* solver, VbdStatus* out, int32_t reset);
 /* Number of colors and vertex count of each color as laid out on the device (host out arrays). */
 int vbd_solver_info(const VbdSolver* solver, int32_t* color_count, int32_t* lanes_per_vertex,
                     int32_t* block_size);
+
+/* How vbd_step runs the colors: resident = 1 when one persistent shared-memory-resident kernel
+ * (cooperative launch, one CTA per patch, neighbour-only synchronisation) runs all colors of all
+ * iterations; 0 when each color is its own launch.  patches / smem_bytes describe the resident
+ * kernel (0 otherwise). */
+int vbd_solver_step_kernel(const VbdSolver* solver, int32_t* resident, int32_t* patches, int32_t* smem_bytes);
+
+/* Bound (in polling iterations) of every wait of the resident kernel; a wait that runs out counts
+ * in VbdStatus.timeouts and the kernel returns early instead of hanging.  Default 4,194,304. */
+int vbd_set_spin_limit(VbdSolver* solver, uint32_t spins);
 
 /* Override the sweep launch shape (used by the autotuner): lanes_per_vertex 0 with block_size
  * 64/128/256 (record-parallel), or lanes_per_vertex in {1,2,4,8,16} with a block_size multiple of 32. */

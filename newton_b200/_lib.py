@@ -72,6 +72,7 @@ class VbdModelDesc(ctypes.Structure):
         ("soft_contact_kd", ctypes.c_float),
         ("soft_contact_mu", ctypes.c_float),
         ("shapes", ctypes.POINTER(VbdShape)),
+        ("particle_q", c_float_p),
     ]
 
 
@@ -83,6 +84,7 @@ class VbdSolverOptions(ctypes.Structure):
         ("block_size", ctypes.c_int32),
         ("contacts_per_vertex", ctypes.c_int32),
         ("use_graph", ctypes.c_int32),
+        ("step_kernel", ctypes.c_int32),
     ]
 
 
@@ -137,6 +139,8 @@ SIGNATURES = {
     "vbd_status": (ctypes.c_int, [_VP, ctypes.POINTER(VbdStatus), ctypes.c_int32]),
     "vbd_solver_info": (ctypes.c_int, [_VP, c_int32_p, c_int32_p, c_int32_p]),
     "vbd_set_launch": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),
+    "vbd_solver_step_kernel": (ctypes.c_int, [_VP, c_int32_p, c_int32_p, c_int32_p]),
+    "vbd_set_spin_limit": (ctypes.c_int, [_VP, ctypes.c_uint32]),
     "vbd_color_graph": (
         ctypes.c_int,
         [ctypes.c_int32, ctypes.c_int64, c_int32_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, c_int32_p, c_int32_p],

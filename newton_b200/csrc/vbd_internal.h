@@ -64,6 +64,12 @@ struct VbdModelImpl {
     int* particle_flags_orig = nullptr;   // [V] original order (collide)
     float* particle_radius_orig = nullptr;  // [V] original order (collide)
     std::vector<DevShape> shapes_host;
+    // host copies of the layout (used to build the shared-memory-resident patches)
+    std::vector<float4> pinfo_h;
+    std::vector<int4> vadj_h, tri_idx_h, edge_idx_h;
+    std::vector<float4> tri_D_h, tri_mat_h, edge_mat_h;
+    std::vector<int> tri_elem_h, edge_elem_h;   // element id of each record (dedupe per patch)
+    std::vector<float> rest_q_h;                // [3V] initial positions in internal order (may be empty)
 };
 
 }  // namespace vbd

@@ -65,45 +65,43 @@ __device__ __forceinline__ Sym3 zero_sym() { Sym3 h = {0.f, 0.f, 0.f, 0.f, 0.f, 
 
 // ---------------------------------------------------------------------------------------------
 // Stable Neo-Hookean membrane of one triangle, force and Hessian block of vertex `order`.
-// D = DmInv (row-major 00, 01, 10, 11); mat = (area, mu, lambda, kd).
-// Restates particle_vbd_kernels.py:502-632 term by term.
+// D = DmInv (row-major 00, 01, 10, 11).  mat = (area*mu, area*(lambda+mu), alpha, area*kd) with
+// alpha = 1 + mu / lambda_nh, precomputed per record at model build: every term of the
+// reference's force and Hessian is linear in (mu, lambda_nh, kd), so folding the final
+// `* area` (particle_vbd_kernels.py:629-630) into the moduli is the same expression.
+// Restates particle_vbd_kernels.py:502-632 otherwise term by term.
 // ---------------------------------------------------------------------------------------------
 template <bool kDamping>
 __device__ __forceinline__ void membrane_eval(int order, float3 x0, float3 x1, float3 x2, float3 a0,
                                               float3 a1, float3 a2, float4 D, float4 mat, float inv_dt,
                                               float3& f, Sym3& h) {
-    const float area = mat.x, mu = mat.y, lmbd = mat.z, kd = mat.w;
+    const float mu = mat.x, lnh = mat.y, alpha = mat.z, kd = mat.w;
     const float3 x01 = x1 - x0;
     const float3 x02 = x2 - x0;
     const float3 F0 = x01 * D.x + x02 * D.z;
     const float3 F1 = x01 * D.y + x02 * D.w;
     const float c00 = dot(F0, F0), c11 = dot(F1, F1), c01 = dot(F0, F1);
-    float js2 = c00 * c11 - c01 * c01;
-    js2 = fmaxf(js2, 1.0e-20f);
-    const float js = sqrtf(js2);
-    const float inv_js = 1.0f / js;
-    const float lnh = lmbd + mu;
-    const float lsafe = (lnh < 0.0f ? -1.0f : 1.0f) * fmaxf(fabsf(lnh), 1.0e-6f);
-    const float alpha = 1.0f + mu / lsafe;
+    const float js2 = fmaxf(c00 * c11 - c01 * c01, 1.0e-20f);
+    const float inv_js = rsqrtf(js2);
+    const float js = js2 * inv_js;
     const float3 g0 = inv_js * (c11 * F0 - c01 * F1);
     const float3 g1 = inv_js * (c00 * F1 - c01 * F0);
     const float s = lnh * (js - alpha);
     const float3 P0 = mu * F0 + s * g0;
     const float3 P1 = mu * F1 + s * g1;
-    const float m0 = order == 0 ? 1.f : 0.f, m1 = order == 1 ? 1.f : 0.f, m2 = order == 2 ? 1.f : 0.f;
-    const float d0 = D.x * (m1 - m0) + D.z * (m2 - m0);
-    const float d1 = D.y * (m1 - m0) + D.w * (m2 - m0);
-    float3 force = -(P0 * d0 + P1 * d1);
+    // dF/dx of the selected vertex: vertex 0 -> -(D row 0 + D row 1), vertex 1 -> D row 0, vertex 2 -> D row 1
+    const float d0 = order == 0 ? -(D.x + D.z) : (order == 1 ? D.x : D.z);
+    const float d1 = order == 0 ? -(D.y + D.w) : (order == 1 ? D.y : D.w);
+    f = f - (P0 * d0 + P1 * d1);
 
     const float r = fmaxf(0.0f, s) * inv_js;
     const float cJ = lnh - r;
     const float3 dJ = g0 * d0 + g1 * d1;
     const float3 w = F1 * d0 - F0 * d1;
     const float icoef = mu * (d0 * d0 + d1 * d1) + r * (d0 * d0 * c11 + d1 * d1 * c00 - 2.0f * d0 * d1 * c01);
-    Sym3 H = zero_sym();
-    add_diag(H, icoef);
-    add_outer(H, cJ, dJ);
-    add_outer(H, -r, w);
+    add_diag(h, icoef);
+    add_outer(h, cJ, dJ);
+    add_outer(h, -r, w);
 
     if (kDamping && kd > 0.0f) {
         const float3 p01 = a1 - a0;
@@ -117,15 +115,36 @@ __device__ __forceinline__ void membrane_eval(int order, float3 x0, float3 x1, f
         const float3 e01 = d0 * F1 + d1 * F0;
         const float3 e11 = (2.0f * d1) * F1;
         const float3 fd = r00 * e00 + (2.0f * r01) * e01 + r11 * e11;
-        force = force + (-kd) * fd;
+        f = f + (-kd) * fd;
         const float kdt = kd * inv_dt;
-        add_outer(H, kdt, e00);
-        add_outer(H, 2.0f * kdt, e01);
-        add_outer(H, kdt, e11);
+        add_outer(h, kdt, e00);
+        add_outer(h, 2.0f * kdt, e01);
+        add_outer(h, kdt, e11);
     }
-    f = f + force * area;
-    scale(H, area);
-    add(h, H);
+}
+
+// atan2 from the arctangent approximation of Abramowitz & Stegun, Handbook of Mathematical
+// Functions, eq. 4.4.49 (C. Hastings): atan(x) = x (1 + a2 x^2 + ... + a16 x^16), 0 <= x <= 1,
+// |error| <= 2e-8, extended to the full circle by the usual octant reduction.
+__device__ __forceinline__ float atan2_as(float y, float x) {
+    const float ax = fabsf(x), ay = fabsf(y);
+    const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
+    if (!(mx > 0.0f)) return 0.0f;
+    const float z = __fdividef(mn, mx);
+    const float z2 = z * z;
+    float p = 0.0028662257f;
+    p = fmaf(p, z2, -0.0161657367f);
+    p = fmaf(p, z2, 0.0429096138f);
+    p = fmaf(p, z2, -0.0752896400f);
+    p = fmaf(p, z2, 0.1065626393f);
+    p = fmaf(p, z2, -0.1420889944f);
+    p = fmaf(p, z2, 0.1999355085f);
+    p = fmaf(p, z2, -0.3333314528f);
+    p = fmaf(p, z2, 1.0f);
+    float a = z * p;
+    if (ay > ax) a = 1.57079632679489662f - a;
+    if (x < 0.0f) a = 3.14159265358979324f - a;
+    return y < 0.0f ? -a : a;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -161,7 +180,7 @@ __device__ __forceinline__ void bending_eval(int order, float3 x0, float3 x1, fl
     const float3 eh = e * ie;
     const float sin_t = dot(cross(n1h, n2h), eh);
     const float cos_t = dot(n1h, n2h);
-    const float theta = atan2f(sin_t, cos_t);
+    const float theta = atan2_as(sin_t, cos_t);
     const float k = em.z * em.y;
     const float dE = k * (theta - em.x);
 
@@ -198,7 +217,7 @@ __device__ __forceinline__ void bending_eval(int order, float3 x0, float3 x1, fl
         const float3 q1h = q1 * rsqrtf(s1);
         const float3 q2h = q2 * rsqrtf(s2);
         const float3 qeh = pe * rsqrtf(se);
-        const float theta_prev = atan2f(dot(cross(q1h, q2h), qeh), dot(q1h, q2h));
+        const float theta_prev = atan2_as(dot(cross(q1h, q2h), qeh), dot(q1h, q2h));
         float dth = theta - theta_prev;
         if (dth > 3.141592653589793f) {
             dth = dth - 6.283185307179586f;
@@ -245,6 +264,39 @@ __device__ __forceinline__ void contact_eval(float3 x, float3 x_prev, float3 bx,
     }
     f = f + force;
     add(h, H);
+}
+
+// Contacts of one vertex (internal index i), summed in record order: the per-vertex table holds
+// up to K record ids written in arbitrary order by the scatter, so the few ids are sorted first
+// (the reference's serial launch adds a particle's records in record order).
+// `shape_mat(s)` returns the shape's mixed (ke, kd, mu, margin).
+template <typename ShapeMat>
+__device__ __forceinline__ void vertex_contacts(const int* ccount, const int* cslot, int K, int i, const int* c_shape,
+                                                const float* c_body_pos, const float* c_body_vel, const float* c_normal,
+                                                ShapeMat shape_mat, float3 x, float3 xp, float radius, float dt,
+                                                float eps_u, float3& f, Sym3& h) {
+    const int n = min(ccount[i], K);
+    if (n <= 0) return;
+    int ids[8];
+    const int nn = min(n, 8);
+    for (int k = 0; k < nn; ++k) ids[k] = cslot[i * K + k];
+    for (int p = 1; p < nn; ++p) {
+        const int v = ids[p];
+        int q = p - 1;
+        while (q >= 0 && ids[q] > v) {
+            ids[q + 1] = ids[q];
+            --q;
+        }
+        ids[q + 1] = v;
+    }
+    for (int k = 0; k < nn; ++k) {
+        const int r = ids[k];
+        const float4 sm = shape_mat(c_shape[r]);
+        const float3 bx = f3(c_body_pos[3 * r], c_body_pos[3 * r + 1], c_body_pos[3 * r + 2]);
+        const float3 bv = f3(c_body_vel[3 * r], c_body_vel[3 * r + 1], c_body_vel[3 * r + 2]);
+        const float3 nrm = f3(c_normal[3 * r], c_normal[3 * r + 1], c_normal[3 * r + 2]);
+        contact_eval(x, xp, bx, bv, nrm, radius, sm, dt, eps_u, f, h);
+    }
 }
 
 // |det H| > 1e-8 -> dx = H^-1 f by adjugate / determinant; returns false when singular.

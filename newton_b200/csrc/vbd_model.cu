@@ -160,9 +160,15 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
                 if (!(mat[0] > 0.0f || mat[1] > 0.0f)) continue;  // the reference skips such triangles
                 const int* ti = d->tri_indices + 3 * t;
                 tri_idx.push_back(make_int4(inv[ti[0]], inv[ti[1]], inv[ti[2]], slot));
+                m.tri_elem_h.push_back(t);
                 const float* P = d->tri_poses + 4 * t;
                 tri_D.push_back(make_float4(P[0], P[1], P[2], P[3]));
-                tri_mat.push_back(make_float4(d->tri_areas[t], mat[0], mat[1], mat[2]));
+                // (area*mu, area*lambda_nh, alpha, area*kd) with lambda_nh = lambda + mu and
+                // alpha = 1 + mu / lambda_nh (particle_vbd_kernels.py:561-565), in float32
+                const float area = d->tri_areas[t], mu = mat[0], lnh = mat[1] + mat[0];
+                const float lsafe = (lnh < 0.0f ? -1.0f : 1.0f) * std::max(std::fabs(lnh), 1.0e-6f);
+                const float alpha = 1.0f + mu / lsafe;
+                tri_mat.push_back(make_float4(area * mu, area * lnh, alpha, area * mat[2]));
                 if (mat[2] > 0.0f) m.any_tri_damping = true;
             }
         }
@@ -179,6 +185,7 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
                 if (!(ke > 0.0f)) continue;                 // not evaluated by the reference
                 if (ei[0] == -1 || ei[1] == -1) continue;   // boundary hinge: exact zero in the reference
                 edge_idx.push_back(make_int4(inv[ei[0]] | (slot << 30), inv[ei[1]], inv[ei[2]], inv[ei[3]]));
+                m.edge_elem_h.push_back(ed);
                 edge_mat.push_back(make_float4(d->edge_rest_angle[ed], d->edge_rest_length[ed], ke, kd));
                 if (kd > 0.0f) m.any_edge_damping = true;
             }
@@ -217,6 +224,11 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
         pradius[v] = d->particle_radius[v];
     }
 
+    if (d->particle_q) {
+        m.rest_q_h.resize(3 * static_cast<size_t>(V));
+        for (int i = 0; i < V; ++i)
+            for (int k = 0; k < 3; ++k) m.rest_q_h[3 * i + k] = d->particle_q[3 * perm[i] + k];
+    }
     int rc;
     if ((rc = upload(&m.perm, perm))) return rc;
     if ((rc = upload(&m.inv_perm, inv))) return rc;
@@ -231,6 +243,13 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
     if ((rc = upload(&m.particle_world, pworld))) return rc;
     if ((rc = upload(&m.particle_flags_orig, pflags))) return rc;
     if ((rc = upload(&m.particle_radius_orig, pradius))) return rc;
+    m.pinfo_h = std::move(pinfo);
+    m.vadj_h = std::move(vadj);
+    m.tri_idx_h = std::move(tri_idx);
+    m.tri_D_h = std::move(tri_D);
+    m.tri_mat_h = std::move(tri_mat);
+    m.edge_idx_h = std::move(edge_idx);
+    m.edge_mat_h = std::move(edge_mat);
     return VBD_OK;
 }
 

@@ -23,6 +23,7 @@
 
 #include "vbd_internal.h"
 #include "vbd_math.cuh"
+#include "vbd_resident.h"
 
 namespace vbd {
 
@@ -62,6 +63,10 @@ struct SolverImpl {
     float* resid_max = nullptr;  // [1] scratch for vbd_residual
     cudaStream_t capture_stream = nullptr;
     std::vector<GraphEntry> graphs;
+    // persistent shared-memory-resident step (used by vbd_step when the model fits)
+    bool resident_on = false;        // run steps with the resident kernel (when the plan is ready)
+    ResidentPlan resident;
+    unsigned spin_limit = 1u << 22;  // bound of every wait in the resident kernel
 };
 
 }  // namespace vbd
@@ -203,30 +208,9 @@ __device__ __forceinline__ void accumulate_elements(const SweepArgs& a, int i, i
 
 __device__ __forceinline__ void accumulate_contacts(const SweepArgs& a, int i, float3 x, float3 xp, float radius,
                                                     float3& f, Sym3& h) {
-    const int n = min(a.ccount[i], a.K);
-    if (n <= 0) return;
-    int ids[8];
-    const int nn = min(n, 8);
-    for (int k = 0; k < nn; ++k) ids[k] = a.cslot[i * a.K + k];
-    // records of one particle are summed in record order (the order the reference's serial
-    // launch adds them); the scatter in forward_kernel is unordered, so sort the few ids here
-    for (int p = 1; p < nn; ++p) {
-        const int v = ids[p];
-        int q = p - 1;
-        while (q >= 0 && ids[q] > v) {
-            ids[q + 1] = ids[q];
-            --q;
-        }
-        ids[q + 1] = v;
-    }
-    for (int k = 0; k < nn; ++k) {
-        const int r = ids[k];
-        const DevShape& sh = a.shapes[a.c_shape[r]];
-        const float3 bx = f3(a.c_body_pos[3 * r], a.c_body_pos[3 * r + 1], a.c_body_pos[3 * r + 2]);
-        const float3 bv = f3(a.c_body_vel[3 * r], a.c_body_vel[3 * r + 1], a.c_body_vel[3 * r + 2]);
-        const float3 nrm = f3(a.c_normal[3 * r], a.c_normal[3 * r + 1], a.c_normal[3 * r + 2]);
-        contact_eval(x, xp, bx, bv, nrm, radius, sh.mat, a.dt, a.eps_u, f, h);
-    }
+    const DevShape* shapes = a.shapes;
+    vertex_contacts(a.ccount, a.cslot, a.K, i, a.c_shape, a.c_body_pos, a.c_body_vel, a.c_normal,
+                    [shapes](int s) { return shapes[s].mat; }, x, xp, radius, a.dt, a.eps_u, f, h);
 }
 
 __device__ __forceinline__ float warp_sum(float v, int L) {
@@ -678,6 +662,34 @@ static void enqueue_finalize(SolverImpl& s, float* q_in, float* q_out, float* qd
 static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const float* f_ext, float* q_out,
                         float* qd_out, const VbdContacts* c, float dt, int iterations, cudaStream_t st) {
     enqueue_forward(s, q_in, qd_in, f_ext, c, dt, st);
+    if (s.resident_on && s.resident.ready && iterations > 0) {
+        const VbdModelImpl& m = *s.m;
+        ResidentLaunch L;
+        std::memset(&L, 0, sizeof(L));
+        L.pos = s.pos;
+        L.prev = s.prev;
+        L.y = s.y;
+        L.disp = s.disp;
+        if (c && m.S > 0) {
+            L.ccount = s.ccount;
+            L.cslot = s.cslot;
+            L.c_shape = c->soft_contact_shape;
+            L.c_body_pos = c->soft_contact_body_pos;
+            L.c_body_vel = c->soft_contact_body_vel;
+            L.c_normal = c->soft_contact_normal;
+        }
+        L.K = s.K;
+        L.status = s.status;
+        L.q_in = q_in;
+        L.q_out = q_out;
+        L.qd_out = qd_out;
+        L.ccount_clear = s.ccount;
+        L.dt = dt;
+        L.friction_epsilon = s.friction_epsilon;
+        L.iterations = iterations;
+        L.spin_limit = s.spin_limit;
+        return resident_enqueue(m, s.resident, L, st);
+    }
     for (int it = 0; it < iterations; ++it)
         for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st);
     enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
@@ -685,6 +697,7 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
 }
 
 static void free_solver(SolverImpl& s) {
+    resident_free(s.resident);
     for (auto& g : s.graphs) cudaGraphExecDestroy(g.exec);
     s.graphs.clear();
     void* ptrs[] = {s.pos, s.prev, s.y, s.disp, s.ccount, s.cslot, s.status, s.resid_max};
@@ -742,6 +755,7 @@ extern "C" int vbd_solver_create(const VbdModel* model, const VbdSolverOptions* 
         if (options->block_size) s.block = options->block_size;
         if (options->contacts_per_vertex) s.K = options->contacts_per_vertex;
         s.use_graph = options->use_graph != 0;
+        s.resident_on = options->step_kernel == 1;
     }
     if (const char* why = launch_shape_error(s.lanes, s.block)) {
         delete h;
@@ -771,6 +785,7 @@ extern "C" int vbd_solver_create(const VbdModel* model, const VbdSolverOptions* 
         cudaError_t e = cudaStreamCreateWithFlags(&s.capture_stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamCreateWithFlags");
     }
+    if (!rc && s.resident_on) rc = resident_build(m, s.resident);
     if (rc) {
         free_solver(s);
         delete h;
@@ -804,7 +819,8 @@ extern "C" int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, cons
     VBD_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
     if (!s.use_graph || cs != cudaStreamCaptureStatusNone) {
         // plain launches (also the path taken inside a caller's own stream capture)
-        enqueue_step(s, q_in, qd_in, f_ext, q_out, qd_out, contacts, dt, iters, st);
+        rc = enqueue_step(s, q_in, qd_in, f_ext, q_out, qd_out, contacts, dt, iters, st);
+        if (rc) return rc;
         VBD_CUDA_TRY(cudaGetLastError());
         return VBD_OK;
     }
@@ -819,21 +835,27 @@ extern "C" int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, cons
             return VBD_OK;
         }
     }
-    // capture the step on the private stream, instantiate, replay on the caller's stream
-    VBD_CUDA_TRY(cudaStreamBeginCapture(s.capture_stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_step(s, q_in, qd_in, f_ext, q_out, qd_out, contacts, dt, iters, s.capture_stream);
-    cudaGraph_t graph = nullptr;
-    cudaError_t e1 = cudaGetLastError();
-    cudaError_t e2 = cudaStreamEndCapture(s.capture_stream, &graph);
-    if (e1 != cudaSuccess) {
-        if (graph) cudaGraphDestroy(graph);
-        return cuda_fail(e1, "vbd_step capture");
-    }
-    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+    // capture the step on the private stream, instantiate, replay on the caller's stream; if the
+    // resident kernel cannot be captured on this driver, fall back to per-color launches
     cudaGraphExec_t exec = nullptr;
-    cudaError_t e3 = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e3 != cudaSuccess) return cuda_fail(e3, "cudaGraphInstantiate");
+    for (int attempt = 0; attempt < 2 && !exec; ++attempt) {
+        VBD_CUDA_TRY(cudaStreamBeginCapture(s.capture_stream, cudaStreamCaptureModeThreadLocal));
+        const int erc = enqueue_step(s, q_in, qd_in, f_ext, q_out, qd_out, contacts, dt, iters, s.capture_stream);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e1 = cudaGetLastError();
+        cudaError_t e2 = cudaStreamEndCapture(s.capture_stream, &graph);
+        cudaError_t e3 = cudaErrorUnknown;
+        if (erc == VBD_OK && e1 == cudaSuccess && e2 == cudaSuccess && graph) e3 = cudaGraphInstantiate(&exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (e3 == cudaSuccess) break;
+        exec = nullptr;
+        cudaGetLastError();
+        if (!s.resident.ready || !s.resident_on) {
+            if (erc) return erc;
+            return cuda_fail(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3), "vbd_step graph capture");
+        }
+        s.resident_on = false;  // retry with one launch per color
+    }
     if (s.graphs.size() >= 8) {
         cudaGraphExecDestroy(s.graphs.front().exec);
         s.graphs.erase(s.graphs.begin());
@@ -960,7 +982,26 @@ extern "C" int vbd_set_launch(VbdSolver* solver, int32_t lanes_per_vertex, int32
     return VBD_OK;
 }
 
-extern "C" const char* vbd_version(void) { return "vbd_b200 0.1 (sm_100a)"; }
+extern "C" int vbd_solver_step_kernel(const VbdSolver* solver, int32_t* resident, int32_t* patches,
+                                      int32_t* smem_bytes) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_solver_step_kernel: solver is NULL");
+    const SolverImpl& s = solver->s;
+    const bool on = s.resident_on && s.resident.ready;
+    if (resident) *resident = on ? 1 : 0;
+    if (patches) *patches = on ? s.resident.patches : 0;
+    if (smem_bytes) *smem_bytes = on ? s.resident.smem_bytes : 0;
+    return VBD_OK;
+}
+
+extern "C" int vbd_set_spin_limit(VbdSolver* solver, uint32_t spins) {
+    if (!solver || spins == 0) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_spin_limit: NULL solver or zero limit");
+    solver->s.spin_limit = spins;
+    for (auto& g : solver->s.graphs) cudaGraphExecDestroy(g.exec);  // the limit is baked into captured steps
+    solver->s.graphs.clear();
+    return VBD_OK;
+}
+
+extern "C" const char* vbd_version(void) { return "vbd_b200 0.2 (sm_100a)"; }
 
 // ---------------------------------------------------------------------------------------------
 // Allocation-free step: vbd_step_static.

@@ -173,6 +173,7 @@ class DeviceModel:
             sh.material_mu = float(model.shape_material_mu[s])
         self._keep.append(shapes)
         d.shapes = ctypes.cast(shapes, ctypes.POINTER(_lib.VbdShape))
+        d.particle_q = f32(model.particle_q)
         handle = ctypes.c_void_p()
         with torch.cuda.device(model.device):
             _lib.check(lib.vbd_model_create(ctypes.byref(d), ctypes.byref(handle)))

@@ -41,6 +41,7 @@ class SolverVBD(SolverBase):
         block_size: int = 0,
         contacts_per_vertex: int = 4,
         use_cuda_graph: bool = True,
+        resident_step: bool = False,
     ):
         super().__init__(model)
         self.iterations = int(iterations)
@@ -77,6 +78,7 @@ class SolverVBD(SolverBase):
         opts.block_size = int(block_size)
         opts.contacts_per_vertex = int(contacts_per_vertex)
         opts.use_graph = 1 if use_cuda_graph else 0
+        opts.step_kernel = 1 if resident_step else 0
         h = ctypes.c_void_p()
         with torch.cuda.device(model.device):
             _lib.check(self._lib.vbd_solver_create(dm.handle, ctypes.byref(opts), ctypes.byref(h)))
@@ -200,6 +202,14 @@ class SolverVBD(SolverBase):
         c, l, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         _lib.check(self._lib.vbd_solver_info(self._handle, ctypes.byref(c), ctypes.byref(l), ctypes.byref(b)))
         return {"colors": c.value, "lanes_per_vertex": l.value, "block_size": b.value}
+
+    def step_kernel_info(self) -> dict:
+        r, p, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        _lib.check(self._lib.vbd_solver_step_kernel(self._handle, ctypes.byref(r), ctypes.byref(p), ctypes.byref(b)))
+        return {"resident": bool(r.value), "patches": p.value, "smem_bytes": b.value}
+
+    def set_spin_limit(self, spins: int) -> None:
+        _lib.check(self._lib.vbd_set_spin_limit(self._handle, int(spins)))
 
     def reset(self, state: State, world_mask=None, flags=None) -> None:
         warnings.warn(
