@@ -215,6 +215,56 @@ int vbd_forward(VbdSolver* solver, const float* q_in, const float* qd_in, const 
 int vbd_sweep_color(VbdSolver* solver, int32_t color, const VbdContacts* contacts, float dt, void* stream);
 int vbd_finalize(VbdSolver* solver, float* q_in, float* q_out, float* qd_out, float dt, void* stream);
 
+/* Warm start (no reference counterpart): after vbd_forward, move the initial Gauss-Seidel iterate
+ * from the inertia target y to y + delta for every vertex the sweep solves.  delta: DEVICE [V,3]
+ * in model particle order (e.g. the learned per-vertex correction). */
+int vbd_warm_start(VbdSolver* solver, const float* delta, void* stream);
+
+/* ---- learned warm start (no reference counterpart) -----------------------------------------
+ * A per-vertex MLP 64 -> 128 -> 128 -> 3 (SiLU) with BF16 weights and FP32 accumulation on the
+ * tensor cores predicts how the coming step's correction x_solved - y differs from the previous
+ * step's, in units of the vertex's characteristic element length; the warm start is
+ * y + previous correction + prediction * length.  Parameters: an FP32 blob of vbd_mlp_sizes()->params floats
+ * (W1 [64][128], b1, W2 [128][128], b2, W3 [128][8] with columns 3..7 zero, b3 [8]) and its BF16
+ * copy of the three weight matrices (vbd_mlp_sizes()->weights16 values, refreshed by
+ * vbd_mlp_adam or vbd_mlp_pack_weights).  All pointers are DEVICE pointers. */
+int vbd_mlp_sizes(int32_t* params, int32_t* weights16, int32_t* in_features, int32_t* hidden, int32_t* out_features);
+/* Per-vertex features [V][64] (model particle order) of the step prepared by vbd_forward: inertia
+ * offset, the previous step's correction corr_prev [V][3] (may be NULL), 8 one-ring edge vectors
+ * and their corrections, log-stiffnesses, mass, contact and pin flags.  mean / inv_std [64]
+ * standardise them (both NULL = raw). */
+int vbd_mlp_features(VbdSolver* solver, const float* corr_prev, const float* mean, const float* inv_std, float* out,
+                     void* stream);
+/* Y [n][3] = MLP(X [n][64]). */
+int vbd_mlp_forward(const float* params, const uint16_t* w16, const float* X, int32_t n, float* Y, void* stream);
+/* Workspace bytes vbd_mlp_backward needs for n samples. */
+int vbd_mlp_workspace_bytes(int32_t n, int64_t* bytes);
+/* Gradients of L = grad_scale * sum |MLP(X) - T|^2 into grads (FP32 blob layout); loss (device
+ * scalar, may be NULL) accumulates the unscaled sum of squared errors. */
+int vbd_mlp_backward(const float* params, const uint16_t* w16, const float* X, const float* T, int32_t n,
+                     float grad_scale, float* grads, float* loss, void* workspace, int64_t workspace_bytes,
+                     void* stream);
+/* One Adam step (bias-corrected, step >= 1) on the FP32 parameters; refreshes the BF16 weights. */
+int vbd_mlp_adam(float* params, const float* grads, float* m1, float* m2, uint16_t* w16, int32_t step, float lr,
+                 float beta1, float beta2, float eps, void* stream);
+/* BF16 weights from the FP32 parameters. */
+int vbd_mlp_pack_weights(const float* params, uint16_t* w16, void* stream);
+/* After vbd_forward: features (corr_prev, the previous step's correction x_solved - y in model
+ * order, is an input feature; may be NULL) -> MLP -> start the iterations from y + prediction * L,
+ * L the vertex's mean rest edge length.  A network whose output is zero leaves the start at y
+ * exactly.  workspace holds V * 70 floats. */
+int vbd_mlp_warm_start(VbdSolver* solver, const float* params, const uint16_t* w16, const float* corr_prev,
+                       const float* mean, const float* inv_std, float* workspace, int64_t workspace_floats,
+                       void* stream);
+
+/* Learned warm start as a mode of vbd_step: every step becomes forward -> features -> MLP ->
+ * start from y + prediction -> `iterations` colour sweeps -> finalize, and the step's correction
+ * x_solved - y is kept (solver-owned) as the next step's feature.  params / w16 / mean / inv_std
+ * are caller-owned device buffers that must outlive the solver's use of them; params == NULL
+ * turns the mode off.  Allocates the solver's correction and workspace buffers on first use. */
+int vbd_set_warm_start(VbdSolver* solver, const float* params, const uint16_t* w16, const float* mean,
+                       const float* inv_std, int32_t iterations);
+
 /* Copy the solver's current Gauss-Seidel iterate (model particle order) into q_out [V,3] (DEVICE). */
 int vbd_get_positions(const VbdSolver* solver, float* q_out, void* stream);
 

@@ -135,6 +135,22 @@ SIGNATURES = {
     "vbd_sweep_color": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(VbdContacts), ctypes.c_float, _VP]),
     "vbd_finalize": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_float, _VP]),
     "vbd_get_positions": (ctypes.c_int, [_VP, _VP, _VP]),
+    "vbd_warm_start": (ctypes.c_int, [_VP, _VP, _VP]),
+    "vbd_mlp_sizes": (ctypes.c_int, [c_int32_p, c_int32_p, c_int32_p, c_int32_p, c_int32_p]),
+    "vbd_mlp_features": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
+    "vbd_mlp_forward": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int32, _VP, _VP]),
+    "vbd_mlp_workspace_bytes": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
+    "vbd_mlp_backward": (
+        ctypes.c_int,
+        [_VP, _VP, _VP, _VP, ctypes.c_int32, ctypes.c_float, _VP, _VP, _VP, ctypes.c_int64, _VP],
+    ),
+    "vbd_mlp_adam": (
+        ctypes.c_int,
+        [_VP, _VP, _VP, _VP, _VP, ctypes.c_int32, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _VP],
+    ),
+    "vbd_mlp_pack_weights": (ctypes.c_int, [_VP, _VP, _VP]),
+    "vbd_mlp_warm_start": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_int64, _VP]),
+    "vbd_set_warm_start": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, ctypes.c_int32]),
     "vbd_residual": (ctypes.c_int, [_VP, ctypes.POINTER(VbdContacts), ctypes.c_float, _VP, _VP, _VP]),
     "vbd_status": (ctypes.c_int, [_VP, ctypes.POINTER(VbdStatus), ctypes.c_int32]),
     "vbd_solver_info": (ctypes.c_int, [_VP, c_int32_p, c_int32_p, c_int32_p]),

@@ -60,6 +60,9 @@ struct VbdModelImpl {
     int4* edge_idx = nullptr;         // [n_edge_rec] o0, o1, v0, v1 (internal ids); order in bits 30-31 of .x
     float4* edge_mat = nullptr;       // [n_edge_rec] rest angle, rest length, ke, kd
     DevShape* shapes = nullptr;       // [S]
+    int* nbr8 = nullptr;              // [V*8] first 8 distinct one-ring neighbours (internal ids, -1 padded)
+    float4* vfeat = nullptr;          // [V] per-vertex material features: mean log10 tri ke, tri ka,
+                                      //     edge ke over incident elements, characteristic length
     int* particle_world = nullptr;    // [V] original order (collide)
     int* particle_flags_orig = nullptr;   // [V] original order (collide)
     float* particle_radius_orig = nullptr;  // [V] original order (collide)
@@ -71,6 +74,12 @@ struct VbdModelImpl {
     std::vector<int> tri_elem_h, edge_elem_h;   // element id of each record (dedupe per patch)
     std::vector<float> rest_q_h;                // [3V] initial positions in internal order (may be empty)
 };
+
+// learned warm start (vbd_mlp.cu): per-vertex features after the forward pass, and the warm-start
+// displacement = network output (in characteristic lengths) * length
+int mlp_features_launch(const VbdModelImpl& m, const float4* prev, const float4* y, const int* ccount,
+                        const float* corr_prev, const float* mean, const float* inv_std, float* out, cudaStream_t st);
+int mlp_scale_launch(const VbdModelImpl& m, const float* pred, float* delta, cudaStream_t st);
 
 }  // namespace vbd
 

@@ -36,8 +36,10 @@ static int upload(T** dst, const std::vector<T>& src) {
 }
 
 static void free_model(VbdModelImpl& m) {
-    void* ptrs[] = {m.perm, m.inv_perm, m.pinfo, m.vadj, m.tri_idx, m.tri_D, m.tri_mat, m.edge_idx,
-                    m.edge_mat, m.shapes, m.particle_world, m.particle_flags_orig, m.particle_radius_orig};
+    void* ptrs[] = {m.perm,       m.inv_perm, m.pinfo,          m.vadj,
+                    m.tri_idx,    m.tri_D,    m.tri_mat,        m.edge_idx,
+                    m.edge_mat,   m.shapes,   m.particle_world, m.particle_flags_orig,
+                    m.particle_radius_orig, m.nbr8, m.vfeat};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     m.perm = m.inv_perm = nullptr;
@@ -50,6 +52,8 @@ static void free_model(VbdModelImpl& m) {
     m.shapes = nullptr;
     m.particle_world = m.particle_flags_orig = nullptr;
     m.particle_radius_orig = nullptr;
+    m.nbr8 = nullptr;
+    m.vfeat = nullptr;
 }
 
 static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
@@ -216,6 +220,43 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
         m.shapes_host[s] = ds;
     }
 
+    // learned-warm-start inputs: one-ring neighbours and material features per vertex
+    std::vector<int> nbr8(static_cast<size_t>(V) * 8, -1);
+    std::vector<float4> vfeat(V);
+    for (int i = 0; i < V; ++i) {
+        const int o = perm[i];
+        int nn = 0;
+        double lke = 0, lka = 0, larea = 0, lek = 0;
+        int nt = 0, ne = 0;
+        if (T > 0) {
+            for (int k = d->v_adj_tris_offsets[o]; k < d->v_adj_tris_offsets[o + 1]; k += 2) {
+                const int t = d->v_adj_tris[k];
+                const int* ti = d->tri_indices + 3 * t;
+                const float* mat = d->tri_materials + 5 * t;
+                lke += std::log10(std::max(mat[0], 1e-12f));
+                lka += std::log10(std::max(mat[1], 1e-12f));
+                larea += std::sqrt(2.0 * std::max(d->tri_areas[t], 0.0f));
+                ++nt;
+                for (int c = 0; c < 3; ++c) {
+                    const int nb = inv[ti[c]];
+                    if (ti[c] == o || nn >= 8) continue;
+                    bool seen = false;
+                    for (int q = 0; q < nn; ++q) seen |= nbr8[8 * i + q] == nb;
+                    if (!seen) nbr8[8 * i + nn++] = nb;
+                }
+            }
+        }
+        if (E > 0) {
+            for (int k = d->v_adj_edges_offsets[o]; k < d->v_adj_edges_offsets[o + 1]; k += 2) {
+                const int e = d->v_adj_edges[k];
+                lek += std::log10(std::max(d->edge_bending_properties[2 * e], 1e-12f));
+                ++ne;
+            }
+        }
+        vfeat[i] = make_float4(nt ? float(lke / nt) : 0.f, nt ? float(lka / nt) : 0.f, ne ? float(lek / ne) : 0.f,
+                               nt ? float(larea / nt) : 1.f);
+    }
+
     std::vector<int> pworld(V, -1), pflags(V);
     std::vector<float> pradius(V);
     for (int v = 0; v < V; ++v) {
@@ -243,6 +284,8 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
     if ((rc = upload(&m.particle_world, pworld))) return rc;
     if ((rc = upload(&m.particle_flags_orig, pflags))) return rc;
     if ((rc = upload(&m.particle_radius_orig, pradius))) return rc;
+    if ((rc = upload(&m.nbr8, nbr8))) return rc;
+    if ((rc = upload(&m.vfeat, vfeat))) return rc;
     m.pinfo_h = std::move(pinfo);
     m.vadj_h = std::move(vadj);
     m.tri_idx_h = std::move(tri_idx);

@@ -67,6 +67,14 @@ struct SolverImpl {
     bool resident_on = false;        // run steps with the resident kernel (when the plan is ready)
     ResidentPlan resident;
     unsigned spin_limit = 1u << 22;  // bound of every wait in the resident kernel
+    // learned warm start (vbd_set_warm_start): caller-owned network, solver-owned buffers
+    const float* ws_params = nullptr;
+    const uint16_t* ws_w16 = nullptr;
+    const float* ws_mean = nullptr;
+    const float* ws_inv_std = nullptr;
+    int ws_iterations = 0;
+    float* ws_corr = nullptr;        // [V][3] previous step's correction x_solved - y (model order)
+    float* ws_work = nullptr;        // [V][70] features, prediction, displacement
 };
 
 }  // namespace vbd
@@ -119,12 +127,14 @@ __global__ void forward_kernel(ForwardArgs a) {
             if (a.f_ext) fe = f3(a.f_ext[3 * o], a.f_ext[3 * o + 1], a.f_ext[3 * o + 2]);
             const float3 vn = v + (a.g + fe * pi.y) * a.dt;
             yv = q + vn * a.dt;
-            dv = vn * a.dt;
+            dv = f3(__fmul_rn(vn.x, a.dt), __fmul_rn(vn.y, a.dt), __fmul_rn(vn.z, a.dt));
         }
         a.prev[i] = make_float4(q.x, q.y, q.z, 0.f);
         a.y[i] = make_float4(yv.x, yv.y, yv.z, pi.x);
         a.disp[i] = make_float4(dv.x, dv.y, dv.z, 0.f);
-        const float3 p = q + dv;
+        // the first iterate is x_prev + disp, rounded as two separate operations (no FMA), so that
+        // a warm start with a zero offset reproduces it bit for bit
+        const float3 p = f3(__fadd_rn(q.x, dv.x), __fadd_rn(q.y, dv.y), __fadd_rn(q.z, dv.z));
         a.pos[i] = make_float4(p.x, p.y, p.z, 0.f);
     }
     if (a.c_count) {
@@ -504,6 +514,36 @@ __global__ void finalize_kernel(FinalizeArgs a) {
     if (a.ccount) a.ccount[i] = 0;
 }
 
+// Warm start: the initial Gauss-Seidel iterate becomes inertia target + delta for every vertex the
+// sweep solves (pinned / massless vertices keep their position).
+__global__ void warm_start_kernel(const int* perm, const float4* pinfo, const float4* prev, float4* disp, float4* pos,
+                                  const float* delta, int V) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V) return;
+    const float4 pi = pinfo[i];
+    if (!((__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f)) return;
+    const int o = perm[i];
+    float4 d = disp[i];
+    d = make_float4(d.x + delta[3 * o], d.y + delta[3 * o + 1], d.z + delta[3 * o + 2], 0.f);
+    disp[i] = d;
+    const float4 p = prev[i];
+    pos[i] = make_float4(__fadd_rn(p.x, d.x), __fadd_rn(p.y, d.y), __fadd_rn(p.z, d.z), 0.f);
+}
+
+// correction of the finished step, x_solved - y (model order), the next step's warm-start feature
+__global__ void correction_kernel(const int* perm, const float4* pinfo, const float4* pos, const float4* y,
+                                  float* corr, int V) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V) return;
+    const int o = perm[i];
+    const float4 pi = pinfo[i];
+    const bool solvable = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
+    const float4 p = pos[i], yy = y[i];
+    corr[3 * o] = solvable ? p.x - yy.x : 0.f;
+    corr[3 * o + 1] = solvable ? p.y - yy.y : 0.f;
+    corr[3 * o + 2] = solvable ? p.z - yy.z : 0.f;
+}
+
 __global__ void gather_positions_kernel(const int* perm, const float4* pos, float* q, int V) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= V) return;
@@ -662,6 +702,24 @@ static void enqueue_finalize(SolverImpl& s, float* q_in, float* q_out, float* qd
 static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const float* f_ext, float* q_out,
                         float* qd_out, const VbdContacts* c, float dt, int iterations, cudaStream_t st) {
     enqueue_forward(s, q_in, qd_in, f_ext, c, dt, st);
+    if (s.ws_params) {
+        // learned warm start: features -> MLP -> iterate from y + prediction
+        const int V = s.m->V;
+        float* feats = s.ws_work;
+        float* pred = feats + static_cast<size_t>(V) * 64;
+        float* delta = pred + static_cast<size_t>(V) * 3;
+        int rc = mlp_features_launch(*s.m, s.prev, s.y, c ? s.ccount : nullptr, s.ws_corr, s.ws_mean, s.ws_inv_std,
+                                     feats, st);
+        if (!rc) rc = vbd_mlp_forward(s.ws_params, s.ws_w16, feats, V, pred, st);
+        if (!rc) rc = mlp_scale_launch(*s.m, pred, delta, st);
+        if (rc) return rc;
+        warm_start_kernel<<<(V + 255) / 256, 256, 0, st>>>(s.m->perm, s.m->pinfo, s.prev, s.disp, s.pos, delta, V);
+        for (int it = 0; it < s.ws_iterations; ++it)
+            for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st);
+        correction_kernel<<<(V + 255) / 256, 256, 0, st>>>(s.m->perm, s.m->pinfo, s.pos, s.y, s.ws_corr, V);
+        enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
+        return VBD_OK;
+    }
     if (s.resident_on && s.resident.ready && iterations > 0) {
         const VbdModelImpl& m = *s.m;
         ResidentLaunch L;
@@ -698,6 +756,9 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
 
 static void free_solver(SolverImpl& s) {
     resident_free(s.resident);
+    if (s.ws_corr) cudaFree(s.ws_corr);
+    if (s.ws_work) cudaFree(s.ws_work);
+    s.ws_corr = s.ws_work = nullptr;
     for (auto& g : s.graphs) cudaGraphExecDestroy(g.exec);
     s.graphs.clear();
     void* ptrs[] = {s.pos, s.prev, s.y, s.disp, s.ccount, s.cslot, s.status, s.resid_max};
@@ -913,6 +974,78 @@ extern "C" int vbd_finalize(VbdSolver* solver, float* q_in, float* q_out, float*
     enqueue_finalize(solver->s, q_in, q_out, qd_out, dt, static_cast<cudaStream_t>(stream));
     VBD_CUDA_TRY(cudaGetLastError());
     return VBD_OK;
+}
+
+extern "C" int vbd_warm_start(VbdSolver* solver, const float* delta, void* stream) {
+    if (!solver || !delta) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_warm_start: NULL argument");
+    SolverImpl& s = solver->s;
+    if (s.m->V == 0) return VBD_OK;
+    warm_start_kernel<<<(s.m->V + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        s.m->perm, s.m->pinfo, s.prev, s.disp, s.pos, delta, s.m->V);
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+extern "C" int vbd_mlp_features(VbdSolver* solver, const float* corr_prev, const float* mean, const float* inv_std,
+                                float* out, void* stream) {
+    if (!solver || !out || ((mean == nullptr) != (inv_std == nullptr)))
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_features: bad arguments");
+    SolverImpl& s = solver->s;
+    return mlp_features_launch(*s.m, s.prev, s.y, s.ccount, corr_prev, mean, inv_std, out,
+                               static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int vbd_set_warm_start(VbdSolver* solver, const float* params, const uint16_t* w16, const float* mean,
+                                  const float* inv_std, int32_t iterations) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_warm_start: solver is NULL");
+    SolverImpl& s = solver->s;
+    for (auto& g : s.graphs) cudaGraphExecDestroy(g.exec);  // captured steps change
+    s.graphs.clear();
+    if (!params) {
+        s.ws_params = nullptr;
+        s.ws_w16 = nullptr;
+        return VBD_OK;
+    }
+    if (!w16 || iterations < 0 || ((mean == nullptr) != (inv_std == nullptr)))
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_warm_start: bad arguments");
+    const size_t V = static_cast<size_t>(s.m->V);
+    if (!s.ws_corr) {
+        VBD_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&s.ws_corr), std::max<size_t>(V, 1) * 3 * sizeof(float)));
+        VBD_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&s.ws_work), std::max<size_t>(V, 1) * 70 * sizeof(float)));
+    }
+    VBD_CUDA_TRY(cudaMemset(s.ws_corr, 0, std::max<size_t>(V, 1) * 3 * sizeof(float)));
+    // make the MLP kernel's shared-memory opt-in outside any later stream capture
+    int rc = vbd_mlp_forward(params, w16, nullptr, 0, nullptr, nullptr);
+    if (rc) return rc;
+    s.ws_params = params;
+    s.ws_w16 = w16;
+    s.ws_mean = mean;
+    s.ws_inv_std = inv_std;
+    s.ws_iterations = iterations;
+    return VBD_OK;
+}
+
+extern "C" int vbd_mlp_warm_start(VbdSolver* solver, const float* params, const uint16_t* w16, const float* corr_prev,
+                                  const float* mean, const float* inv_std, float* workspace, int64_t workspace_floats,
+                                  void* stream) {
+    if (!solver || !params || !w16 || !workspace || ((mean == nullptr) != (inv_std == nullptr)))
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_warm_start: bad arguments");
+    SolverImpl& s = solver->s;
+    const int V = s.m->V;
+    if (workspace_floats < static_cast<int64_t>(V) * (64 + 3 + 3))
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_warm_start: workspace must hold V*70 floats");
+    if (V == 0) return VBD_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    float* feats = workspace;
+    float* pred = feats + static_cast<size_t>(V) * 64;
+    float* delta = pred + static_cast<size_t>(V) * 3;
+    int rc = mlp_features_launch(*s.m, s.prev, s.y, s.ccount, corr_prev, mean, inv_std, feats, st);
+    if (rc) return rc;
+    rc = vbd_mlp_forward(params, w16, feats, V, pred, stream);
+    if (rc) return rc;
+    rc = mlp_scale_launch(*s.m, pred, delta, st);
+    if (rc) return rc;
+    return vbd_warm_start(solver, delta, stream);
 }
 
 extern "C" int vbd_get_positions(const VbdSolver* solver, float* q_out, void* stream) {

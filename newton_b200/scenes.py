@@ -6,8 +6,8 @@
                      tri_ke = tri_ka = 1e4, tri_kd = 1e-3, edge_ke = 1e-2, edge_kd = 0,
                      density 0.1 kg/m^2, gravity -9.81 m/s^2.
 * ``hanging_cloth``  32 x 32 vertices, 1 m side, two top corners pinned, ground at z = -1.
-* ``draped_cloth``   256 x 256 vertices, 2 m side, falling onto a static sphere (r = 0.4 m) and
-                     the ground; contact ke = 1e4 (particle and shape side), margin 5 mm.
+* ``draped_cloth``   256 x 256 vertices, 2 m side, flat, falling onto a static sphere (r = 0.4 m)
+                     and the ground; contact ke = 1e4 (particle and shape side), margin 5 mm.
 * ``batched_worlds`` independent cloth worlds of uneven size (N ~ U{16..96}, side ~ U[0.5, 2] m,
                      tri_ke ~ logU[1e3, 1e5] with ka = ke, edge_ke ~ logU[1e-3, 1e-1], 0-4 random
                      boundary pins, a ground plane per world), merged into one model whose color
@@ -44,8 +44,8 @@ def _pin(builder: ModelBuilder, indices) -> None:
 def single_cloth(n: int = 32, side: float = 1.0, seed: int = 0, pin_top_corners: bool = True, ground: float | None = -1.0,
                  sphere: tuple | None = None, height: float = 0.0, particle_radius: float = 5.0e-3,
                  density: float = 0.1, material: dict | None = None, contact_ke: float = 1.0e4,
-                 include_bending: bool = True, device="cuda:0"):
-    """Returns (model, initial particle_q float32 [V,3] with z-noise)."""
+                 include_bending: bool = True, z_noise: float = 1.0e-3, device="cuda:0"):
+    """Returns (model, initial particle_q float32 [V,3] with U(-z_noise, z_noise) z-noise)."""
     material = dict(CLOTH_MATERIAL if material is None else material)
     b = ModelBuilder()
     start = _cloth(b, n, side, height, density, particle_radius, material)
@@ -62,7 +62,8 @@ def single_cloth(n: int = 32, side: float = 1.0, seed: int = 0, pin_top_corners:
     m.soft_contact_ke = contact_ke
     rng = np.random.default_rng(seed)
     q0 = m.particle_q.copy()
-    q0[:, 2] += rng.uniform(-1.0e-3, 1.0e-3, size=m.particle_count).astype(np.float32)
+    if z_noise > 0:
+        q0[:, 2] += rng.uniform(-z_noise, z_noise, size=m.particle_count).astype(np.float32)
     return m, q0
 
 
@@ -71,10 +72,11 @@ def hanging_cloth(seed: int = 0, device="cuda:0"):
     return single_cloth(n=32, side=1.0, seed=seed, pin_top_corners=True, ground=-1.0, device=device)
 
 
-def draped_cloth(n: int = 256, seed: int = 0, device="cuda:0"):
-    """256 x 256 vertices (130,050 triangles), 2 m side, 0.2 m above a static sphere of radius 0.4 m."""
+def draped_cloth(n: int = 256, seed: int = 0, device="cuda:0", offset: tuple = (0.0, 0.0), height: float = 1.1):
+    """256 x 256 vertices (130,050 triangles), 2 m side, flat and at rest 0.2 m above a static
+    sphere of radius 0.4 m (centre offset by ``offset`` in x, y), and the ground plane."""
     return single_cloth(n=n, side=2.0, seed=seed, pin_top_corners=False, ground=0.0,
-                        sphere=((0.0, 0.0, 0.5), 0.4), height=1.1, device=device)
+                        sphere=((offset[0], offset[1], 0.5), 0.4), height=height, z_noise=0.0, device=device)
 
 
 def batched_worlds(num_worlds: int = 512, seed: int = 0, n_range=(16, 96), device="cuda:0", include_bending=True):

@@ -171,6 +171,12 @@ class SolverVBD(SolverBase):
             )
         )
 
+    def warm_start(self, delta: torch.Tensor) -> None:
+        """After ``forward``: start the iterations from inertia target + ``delta`` ([V,3], model order)."""
+        if delta.dtype != torch.float32 or not delta.is_contiguous() or delta.numel() != 3 * self.model.particle_count:
+            raise ValueError("delta must be a contiguous float32 [V,3] tensor")
+        _lib.check(self._lib.vbd_warm_start(self._handle, _lib.ptr(delta), self._stream()))
+
     def positions(self) -> torch.Tensor:
         out = torch.empty((self.model.particle_count, 3), dtype=torch.float32, device=self.model.device)
         _lib.check(self._lib.vbd_get_positions(self._handle, _lib.ptr(out), self._stream()))
@@ -207,6 +213,16 @@ class SolverVBD(SolverBase):
         r, p, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         _lib.check(self._lib.vbd_solver_step_kernel(self._handle, ctypes.byref(r), ctypes.byref(p), ctypes.byref(b)))
         return {"resident": bool(r.value), "patches": p.value, "smem_bytes": b.value}
+
+    def set_warm_start(self, mlp, iterations: int) -> None:
+        """Learned warm start as the step mode: every ``step`` runs forward, the MLP's prediction,
+        ``iterations`` colour sweeps and finalize (``mlp=None`` turns it off)."""
+        self._warm = mlp  # keeps the network's buffers alive while the solver points at them
+        if mlp is None:
+            _lib.check(self._lib.vbd_set_warm_start(self._handle, None, None, None, None, 0))
+            return
+        _lib.check(self._lib.vbd_set_warm_start(self._handle, _lib.ptr(mlp.params), _lib.ptr(mlp.w16),
+                                                _lib.ptr(mlp.mean), _lib.ptr(mlp.inv_std), int(iterations)))
 
     def set_spin_limit(self, spins: int) -> None:
         _lib.check(self._lib.vbd_set_spin_limit(self._handle, int(spins)))
