@@ -165,6 +165,114 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def learned_ab(dev, n: int, plain_steps_per_s: float) -> dict:
+    """Learned warm start against plain VBD on the draped-cloth distribution (bounded: ~30 s).
+
+    Trains the warm-start network on two plain-VBD drapes (sphere offsets (0.2, -0.1) and
+    (-0.15, 0.25); targets: 20-iteration corrections; 2048 sampled vertices per step), then on a
+    held-out drape (offset (0.05, 0.1)) finds per checked step the fewest warm-started iterations
+    whose mean residual matches plain VBD's 10-iteration one on the same state, and times
+    ``SolverVBD.step`` in the learned mode at that count along its own trajectory."""
+    import torch
+
+    from newton_b200 import CollisionPipeline, _lib, scenes
+    from newton_b200 import learned as L
+    from newton_b200.solvers import SolverVBD
+
+    t0 = time.time()
+    Xs, Ts = [], []
+    for seed, off in ((1, (0.2, -0.1)), (4, (-0.15, 0.25))):
+        model, q0 = scenes.draped_cloth(n=n, seed=seed, device=dev, offset=off)
+        solver = SolverVBD(model, iterations=ITERATIONS)
+        pipe = CollisionPipeline(model, soft_contact_margin=MARGIN)
+        X, T = L.generate_dataset(model, q0, solver, pipe, steps=300, dt=DT, target_iterations=20,
+                                  samples_per_step=2048, seed=seed, trajectory_iterations=ITERATIONS)
+        Xs.append(X)
+        Ts.append(T)
+    X, T = torch.cat(Xs), torch.cat(Ts)
+    t_data = time.time() - t0
+    mlp = L.WarmStartMLP(dev, seed=0)
+    mlp.set_standardization(X)
+    t1 = time.time()
+    hist = mlp.train(mlp.standardize(X), T, epochs=20, batch=32768, lr=2e-3)
+    torch.cuda.synchronize()
+    t_train = time.time() - t1
+    target_var = float(T.var(0).mean())
+
+    model, q0 = scenes.draped_cloth(n=n, seed=2, device=dev, offset=(0.05, 0.1))
+    solver = SolverVBD(model, iterations=ITERATIONS)
+    pipe = CollisionPipeline(model, soft_contact_margin=MARGIN)
+    k, records = L.calibrate_iterations(model, q0, solver, pipe, mlp, steps=300, dt=DT, check_every=30)
+
+    # inference cost: features + MLP + start offset, after a forward pass
+    c = pipe.contacts()
+    s0 = model.state()
+    s0.particle_q.copy_(torch.from_numpy(q0).to(dev))
+    pipe.collide(s0, c)
+    solver.forward(s0, c, DT)
+    V = model.particle_count
+    work = torch.empty(V * 70, dtype=torch.float32, device=dev)
+    corr = torch.zeros((V, 3), dtype=torch.float32, device=dev)
+    lib = _lib.load()
+    stream = torch.cuda.current_stream(dev)
+
+    def infer():
+        _lib.check(lib.vbd_mlp_warm_start(solver._handle, _lib.ptr(mlp.params), _lib.ptr(mlp.w16), _lib.ptr(corr),
+                                          _lib.ptr(mlp.mean), _lib.ptr(mlp.inv_std), _lib.ptr(work), work.numel(),
+                                          solver._stream()))
+
+    for _ in range(3):
+        infer()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(20):
+        infer()
+    e1.record(stream)
+    e1.synchronize()
+    infer_ms = e0.elapsed_time(e1) / 20
+
+    # the learned step mode at the calibrated iteration count, along its own trajectory
+    k_run = min(k, 10)
+    solver = SolverVBD(model, iterations=ITERATIONS)
+    solver.set_warm_start(mlp, k_run)
+    s0, s1 = model.state(), model.state()
+    s0.particle_q.copy_(torch.from_numpy(q0).to(dev))
+
+    def substep():
+        nonlocal s0, s1
+        pipe.collide(s0, c)
+        solver.step(s0, s1, None, c, DT)
+        s0, s1 = s1, s0
+
+    for _ in range(200):
+        substep()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(300):
+        substep()
+    e1.record(stream)
+    e1.synchronize()
+    learned_sps = 300 * 1e3 / e0.elapsed_time(e1)
+    st = solver.status()
+    flops = 2 * (64 * 128 + 128 * 128 + 128 * 3) * V
+    return {
+        "iterations_to_equal_residual": k,
+        "not_reached_marker": 11,
+        "plain_iterations": ITERATIONS,
+        "plain_steps_per_s": plain_steps_per_s,
+        "learned_steps_per_s_at_that_count": learned_sps,
+        "speedup_at_equal_residual": (learned_sps / plain_steps_per_s) if k <= ITERATIONS else None,
+        "learned_trajectory_status": st,
+        "per_check": [{"step": r["step"], "plain_residual": r["plain"], "k_learned": r["k"],
+                       "k_previous_correction": r["k_previous_correction"]} for r in records],
+        "train": {"samples": int(X.shape[0]), "data_s": t_data, "train_s": t_train, "epochs": 20,
+                  "mse_first_epoch": hist[0], "mse_last_epoch": hist[-1], "target_variance": target_var},
+        "inference_ms": infer_ms,
+        "inference_tflops": flops / (infer_ms * 1e-3) / 1e12,
+        "residual": "mean over solvable vertices of |f_i| / (m_i |g|) after the iterations",
+    }
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -173,6 +281,7 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start A/B")
     ap.add_argument("--n", type=int, default=256, help="grid vertices per side")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -328,6 +437,8 @@ def main() -> None:
         "autotune": tune,
         "status": st,
     }
+    if rank == 0 and world == 1 and not args.no_learned:
+        line["learned"] = learned_ab(dev, args.n, value)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(model, q0)
     if rank == 0:
