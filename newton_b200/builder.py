@@ -78,8 +78,36 @@ def quat_between_vectors(a, b) -> tuple[float, float, float, float]:
     return tuple(float(v) for v in q)
 
 
+class _Chunked:
+    """A builder array kept as a list of appended chunks and concatenated on first read, so that
+    appending many worlds stays linear in the total size."""
+
+    def __set_name__(self, owner, name):
+        self.key = "_chunks_" + name
+
+    def __get__(self, obj, objtype=None):
+        if obj is None:
+            return self
+        chunks = obj.__dict__[self.key]
+        if len(chunks) > 1:
+            chunks[:] = [np.concatenate(chunks)]
+        return chunks[0]
+
+    def __set__(self, obj, value):
+        obj.__dict__[self.key] = [value]
+
+
 class ModelBuilder:
     """Host-side construction of a cloth Model."""
+
+    tri_indices = _Chunked()
+    tri_poses = _Chunked()
+    tri_materials = _Chunked()
+    tri_areas = _Chunked()
+    edge_indices = _Chunked()
+    edge_rest_angle = _Chunked()
+    edge_rest_length = _Chunked()
+    edge_bending_properties = _Chunked()
 
     @dataclass
     class ShapeConfig:
@@ -138,7 +166,27 @@ class ModelBuilder:
         self.shape_flags: list[int] = []
         self.shape_world: list[int] = []
         self.shape_body: list[int] = []
-        self.particle_color_groups: list[np.ndarray] = []
+        # color groups as a merge plan: [(size, [(group, index offset), ...]), ...]
+        self._color_plan: list = []
+
+    def _append(self, name: str, arr: np.ndarray) -> None:
+        self.__dict__["_chunks_" + name].append(arr)
+
+    def _count(self, name: str) -> int:
+        return int(sum(c.shape[0] for c in self.__dict__["_chunks_" + name]))
+
+    @property
+    def particle_color_groups(self) -> list[np.ndarray]:
+        groups = [
+            np.concatenate([np.asarray(g, dtype=np.int64) + off for g, off in chunks]).astype(np.int32)
+            for _, chunks in self._color_plan
+        ]
+        self._color_plan = [(len(g), [(g, 0)]) for g in groups]
+        return groups
+
+    @particle_color_groups.setter
+    def particle_color_groups(self, groups) -> None:
+        self._color_plan = [(len(g), [(np.asarray(g, dtype=np.int32), 0)]) for g in groups]
 
     # ---------------------------------------------------------------- particles
     def _flush_particles(self):
@@ -196,11 +244,11 @@ class ModelBuilder:
 
     @property
     def tri_count(self) -> int:
-        return int(self.tri_indices.shape[0])
+        return self._count("tri_indices")
 
     @property
     def edge_count(self) -> int:
-        return int(self.edge_indices.shape[0])
+        return self._count("edge_indices")
 
     @property
     def shape_count(self) -> int:
@@ -276,10 +324,10 @@ class ModelBuilder:
             axis=1,
         )
         inds = np.stack([i[valid], j[valid], k[valid]], axis=1).astype(np.int32)
-        self.tri_indices = np.concatenate([self.tri_indices, inds])
-        self.tri_poses = np.concatenate([self.tri_poses, inv_D[valid]])
-        self.tri_materials = np.concatenate([self.tri_materials, mats[valid]])
-        self.tri_areas = np.concatenate([self.tri_areas, areas[valid]])
+        self._append("tri_indices", inds)
+        self._append("tri_poses", inv_D[valid])
+        self._append("tri_materials", mats[valid])
+        self._append("tri_areas", areas[valid])
         return areas
 
     def add_edges(self, i, j, k, l, rest=None, edge_ke=None, edge_kd=None) -> None:
@@ -306,11 +354,11 @@ class ModelBuilder:
             v = d if v is None else v
             return np.broadcast_to(np.asarray(v, dtype=np.float64).reshape(-1), (ne,))
 
-        self.edge_indices = np.concatenate([self.edge_indices, np.stack([i_, j_, k_, l_], axis=1).astype(np.int32)])
-        self.edge_rest_angle = np.concatenate([self.edge_rest_angle, np.asarray(rest, dtype=np.float64)])
-        self.edge_rest_length = np.concatenate([self.edge_rest_length, np.linalg.norm(x4 - x3, axis=1)])
+        self._append("edge_indices", np.stack([i_, j_, k_, l_], axis=1).astype(np.int32))
+        self._append("edge_rest_angle", np.asarray(rest, dtype=np.float64))
+        self._append("edge_rest_length", np.linalg.norm(x4 - x3, axis=1))
         props = np.stack([col(edge_ke, self.default_edge_ke), col(edge_kd, self.default_edge_kd)], axis=1)
-        self.edge_bending_properties = np.concatenate([self.edge_bending_properties, props])
+        self._append("edge_bending_properties", props)
 
     def add_cloth_mesh(self, *, pos, rot, scale, vel, vertices, indices, density, tri_ke=None, tri_ka=None,
                        tri_kd=None, tri_drag=None, tri_lift=None, edge_ke=None, edge_kd=None, particle_radius=None,
@@ -475,16 +523,16 @@ class ModelBuilder:
             self._pflags.append(src["flags"].copy())
             self._pworld.append(np.full(len(src["mass"]), world, dtype=np.int32))
             self._pcache = None
-        self.tri_indices = np.concatenate([self.tri_indices, builder.tri_indices + start])
-        self.tri_poses = np.concatenate([self.tri_poses, builder.tri_poses])
-        self.tri_materials = np.concatenate([self.tri_materials, builder.tri_materials])
-        self.tri_areas = np.concatenate([self.tri_areas, builder.tri_areas])
+        self._append("tri_indices", builder.tri_indices + start)
+        self._append("tri_poses", builder.tri_poses)
+        self._append("tri_materials", builder.tri_materials)
+        self._append("tri_areas", builder.tri_areas)
         e = builder.edge_indices.copy()
         e[e >= 0] += start
-        self.edge_indices = np.concatenate([self.edge_indices, e])
-        self.edge_rest_angle = np.concatenate([self.edge_rest_angle, builder.edge_rest_angle])
-        self.edge_rest_length = np.concatenate([self.edge_rest_length, builder.edge_rest_length])
-        self.edge_bending_properties = np.concatenate([self.edge_bending_properties, builder.edge_bending_properties])
+        self._append("edge_indices", e)
+        self._append("edge_rest_angle", builder.edge_rest_angle)
+        self._append("edge_rest_length", builder.edge_rest_length)
+        self._append("edge_bending_properties", builder.edge_bending_properties)
         for s in range(builder.shape_count):
             self.shape_type.append(builder.shape_type[s])
             self.shape_transform.append(builder.shape_transform[s])
@@ -496,13 +544,9 @@ class ModelBuilder:
             self.shape_flags.append(builder.shape_flags[s])
             self.shape_world.append(world if builder.shape_world[s] == -1 else builder.shape_world[s])
             self.shape_body.append(builder.shape_body[s])
-        if builder.particle_color_groups:
-            plan = [(len(g), [(g, 0)]) for g in self.particle_color_groups]
-            plan = combine_independent_coloring_plan(plan, [(len(g), [(g, start)]) for g in builder.particle_color_groups])
-            self.particle_color_groups = [
-                np.concatenate([np.asarray(g, dtype=np.int64) + off for g, off in chunks]).astype(np.int32)
-                for _, chunks in plan
-            ]
+        if builder._color_plan:
+            other = [(size, [(g, off + start) for g, off in chunks]) for size, chunks in builder._color_plan]
+            self._color_plan = combine_independent_coloring_plan(self._color_plan, other)
 
     # ---------------------------------------------------------------- finalize
     def finalize(self, device="cuda:0", requires_grad: bool = False) -> Model:
