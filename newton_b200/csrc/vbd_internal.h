@@ -60,6 +60,9 @@ struct VbdModelImpl {
     int4* edge_idx = nullptr;         // [n_edge_rec] o0, o1, v0, v1 (internal ids); order in bits 30-31 of .x
     float4* edge_mat = nullptr;       // [n_edge_rec] rest angle, rest length, ke, kd
     DevShape* shapes = nullptr;       // [S]
+    int n_worlds = 0;                 // W: 1 + the largest particle or shape world id
+    int* world_shape_offsets = nullptr;   // [W+2] CSR rows: world w -> its shapes and the global ones
+    int* world_shapes = nullptr;      //     (ascending shape id); row W: every shape (global particles)
     int* nbr8 = nullptr;              // [V*8] first 8 distinct one-ring neighbours (internal ids, -1 padded)
     float4* vfeat = nullptr;          // [V] per-vertex material features: mean log10 tri ke, tri ka,
                                       //     edge ke over incident elements, characteristic length

@@ -39,7 +39,7 @@ static void free_model(VbdModelImpl& m) {
     void* ptrs[] = {m.perm,       m.inv_perm, m.pinfo,          m.vadj,
                     m.tri_idx,    m.tri_D,    m.tri_mat,        m.edge_idx,
                     m.edge_mat,   m.shapes,   m.particle_world, m.particle_flags_orig,
-                    m.particle_radius_orig, m.nbr8, m.vfeat};
+                    m.particle_radius_orig, m.nbr8, m.vfeat, m.world_shape_offsets, m.world_shapes};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     m.perm = m.inv_perm = nullptr;
@@ -54,6 +54,7 @@ static void free_model(VbdModelImpl& m) {
     m.particle_radius_orig = nullptr;
     m.nbr8 = nullptr;
     m.vfeat = nullptr;
+    m.world_shape_offsets = m.world_shapes = nullptr;
 }
 
 static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
@@ -259,11 +260,24 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
 
     std::vector<int> pworld(V, -1), pflags(V);
     std::vector<float> pradius(V);
+    int W = 0;
     for (int v = 0; v < V; ++v) {
         pworld[v] = d->particle_world ? d->particle_world[v] : -1;
         pflags[v] = d->particle_flags[v];
         pradius[v] = d->particle_radius[v];
+        W = std::max(W, pworld[v] + 1);
     }
+    for (int s = 0; s < S; ++s) W = std::max(W, d->shapes[s].world + 1);
+    // candidate shapes per particle world, in ascending shape id (the record order per particle)
+    std::vector<int> wso(static_cast<size_t>(W) + 2, 0), wsl;
+    for (int w = 0; w <= W; ++w) {
+        for (int s = 0; s < S; ++s) {
+            const int sw = d->shapes[s].world;
+            if (w == W || sw == -1 || sw == w) wsl.push_back(s);
+        }
+        wso[w + 1] = static_cast<int>(wsl.size());
+    }
+    m.n_worlds = W;
 
     if (d->particle_q) {
         m.rest_q_h.resize(3 * static_cast<size_t>(V));
@@ -284,6 +298,8 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
     if ((rc = upload(&m.particle_world, pworld))) return rc;
     if ((rc = upload(&m.particle_flags_orig, pflags))) return rc;
     if ((rc = upload(&m.particle_radius_orig, pradius))) return rc;
+    if ((rc = upload(&m.world_shape_offsets, wso))) return rc;
+    if ((rc = upload(&m.world_shapes, wsl))) return rc;
     if ((rc = upload(&m.nbr8, nbr8))) return rc;
     if ((rc = upload(&m.vfeat, vfeat))) return rc;
     m.pinfo_h = std::move(pinfo);
@@ -352,7 +368,9 @@ __device__ __forceinline__ bool shape_sdf(const DevShape& sh, float3 x, float& d
 
 struct CollideArgs {
     const DevShape* shapes;
-    int S, V;
+    const int* world_shape_offsets;
+    const int* world_shapes;
+    int S, V, W;
     const float* q;
     const float* radius;
     const int* flags;
@@ -394,9 +412,10 @@ __global__ void collide_kernel(CollideArgs a) {
             px = f3(a.q[3 * p], a.q[3 * p + 1], a.q[3 * p + 2]);
             radius = a.radius[p];
             pw = a.world ? a.world[p] : -1;
-            for (int s = 0; s < a.S; ++s) {
+            const int row = (pw >= 0 && pw < a.W) ? pw : a.W;
+            for (int k = a.world_shape_offsets[row]; k < a.world_shape_offsets[row + 1]; ++k) {
                 float3 bp, wn;
-                if (shape_test(a, s, pw, px, radius, bp, wn)) ++n;
+                if (shape_test(a, a.world_shapes[k], pw, px, radius, bp, wn)) ++n;
             }
         }
     }
@@ -413,7 +432,9 @@ __global__ void collide_kernel(CollideArgs a) {
     base = __shfl_sync(0xffffffffu, base, 31) + incl - n;
     if (n == 0) return;
     int k = 0;
-    for (int s = 0; s < a.S; ++s) {
+    const int row = (pw >= 0 && pw < a.W) ? pw : a.W;
+    for (int j = a.world_shape_offsets[row]; j < a.world_shape_offsets[row + 1]; ++j) {
+        const int s = a.world_shapes[j];
         float3 bp, wn;
         if (!shape_test(a, s, pw, px, radius, bp, wn)) continue;
         const int idx = base + k++;
@@ -482,6 +503,9 @@ extern "C" int vbd_collide(const VbdModel* model, const float* particle_q, float
         return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_collide: contact record arrays missing");
     CollideArgs a;
     a.shapes = m.shapes;
+    a.world_shape_offsets = m.world_shape_offsets;
+    a.world_shapes = m.world_shapes;
+    a.W = m.n_worlds;
     a.S = m.S;
     a.V = m.V;
     a.q = particle_q;

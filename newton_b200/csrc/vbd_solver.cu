@@ -138,12 +138,14 @@ __global__ void forward_kernel(ForwardArgs a) {
         a.pos[i] = make_float4(p.x, p.y, p.z, 0.f);
     }
     if (a.c_count) {
+        // the record count lives on the device: grid-stride over it (the grid is sized for the
+        // vertices, not for the record capacity V x shapes)
         const int n = min(*a.c_count, a.c_max);
-        if (tid < n) {
-            const int ip = a.inv_perm[a.c_particle[tid]];
+        for (int r = tid; r < n; r += gridDim.x * blockDim.x) {
+            const int ip = a.inv_perm[a.c_particle[r]];
             const int k = atomicAdd(&a.ccount[ip], 1);
             if (k < a.K) {
-                a.cslot[ip * a.K + k] = tid;
+                a.cslot[ip * a.K + k] = r;
             } else {
                 atomicAdd(&a.status[kOverflow], 1u);
             }
@@ -664,7 +666,7 @@ static int enqueue_forward(SolverImpl& s, const float* q_in, const float* qd_in,
         a.c_count = c->soft_contact_count;
         a.c_particle = c->soft_contact_particle;
         a.c_max = c->soft_contact_max;
-        n = std::max(n, c->soft_contact_max);
+        n = std::max(n, std::min(c->soft_contact_max, 148 * 2048));
     }
     const int block = 256;
     if (n > 0) forward_kernel<<<(n + block - 1) / block, block, 0, st>>>(a);
