@@ -115,8 +115,10 @@ typedef struct VbdModelDesc {
     float soft_contact_kd;                 /* Model.soft_contact_kd */
     float soft_contact_mu;                 /* Model.soft_contact_mu */
     const VbdShape* shapes;                /* [S] */
-    const float* particle_q;               /* [V,3] rest/initial positions or NULL; used only to cut the
-                                              model into compact patches for the resident step kernel */
+    const float* particle_q;               /* [V,3] rest/initial positions or NULL; used to cut the model
+                                              into compact patches for the resident step kernel and, with
+                                              self-contact, as the rest shape (grid cell size, rest
+                                              exclusion radius); required for self-contact */
 } VbdModelDesc;
 
 /* Solver options (SolverVBD keyword arguments that touch the particle path, plus launch shape). */
@@ -132,6 +134,17 @@ typedef struct VbdSolverOptions {
     int32_t step_kernel;          /* 0 = one launch per color (default); 1 = one persistent
                                      shared-memory-resident kernel per step when the model fits the
                                      GPU's shared memory (else one launch per color) */
+    /* particle self-contact (SolverVBD particle_* keywords, solver_vbd.py:231-241) */
+    int32_t self_contact;                  /* particle_enable_self_contact (0/1) */
+    float self_contact_radius;             /* particle_self_contact_radius (reference default 0.2) */
+    float self_contact_margin;             /* particle_self_contact_margin (0.2), must be >= radius */
+    float conservative_bound_relaxation;   /* particle_conservative_bound_relaxation (0.85) */
+    int32_t vertex_contact_buffer_size;    /* particle_vertex_contact_buffer_size (32) */
+    int32_t edge_contact_buffer_size;      /* particle_edge_contact_buffer_size (64) */
+    int32_t collision_detection_interval;  /* particle_collision_detection_interval (0) */
+    float edge_parallel_epsilon;           /* particle_edge_parallel_epsilon (1e-5) */
+    int32_t topological_filter_threshold;  /* particle_topological_contact_filter_threshold (2) */
+    float rest_exclusion_radius;           /* particle_rest_shape_contact_exclusion_radius (0) */
 } VbdSolverOptions;
 
 /* Soft-contact records in the reference layout (newton.Contacts soft_contact_*; DEVICE pointers). */
@@ -155,6 +168,9 @@ typedef struct VbdStatus {
     int32_t singular_blocks;      /* |det H| <= 1e-8: update skipped, as in the reference */
     int32_t contact_overflow;     /* contacts dropped because a vertex had more than the table holds */
     int32_t timeouts;             /* bounded grid-barrier waits that gave up */
+    int32_t self_contact_overflow;  /* self-contact candidates dropped because a fixed-size list was
+                                       full (the reference sets a resize flag in the same case) */
+    int32_t reserved;
 } VbdStatus;
 
 typedef struct VbdModel VbdModel;
@@ -213,6 +229,20 @@ int vbd_step_static(const VbdModel* model, float* q_in, const float* qd_in, cons
 int vbd_forward(VbdSolver* solver, const float* q_in, const float* qd_in, const float* f_ext,
                 const VbdContacts* contacts, float dt, void* stream);
 int vbd_sweep_color(VbdSolver* solver, int32_t color, const VbdContacts* contacts, float dt, void* stream);
+/* Start of iteration `iteration` of a staged step: with self-contact, the detection that
+ * particle_collision_detection_interval schedules there (solver_vbd.py:2540-2545); otherwise a
+ * no-op. */
+int vbd_begin_iteration(VbdSolver* solver, int32_t iteration, void* stream);
+
+/* Self-contact detection alone at particle_q (DEVICE [V,3], model order): the vertex-triangle
+ * and edge-edge queries of TriMeshCollisionDetector (solvers/vbd/tri_mesh_collision.py:645-730)
+ * with the solver's margin and filters.  vbd_self_contact_lists copies the result to HOST
+ * arrays (any may be NULL): per vertex the colliding triangle ids and per edge the colliding
+ * edge ids, ascending, -1 padded to the buffer sizes (vertex_contact_buffer_size,
+ * edge_contact_buffer_size); synchronizes the device. */
+int vbd_self_contact_detect(VbdSolver* solver, const float* particle_q, void* stream);
+int vbd_self_contact_lists(VbdSolver* solver, int32_t* vt_counts, int32_t* vt_lists, int32_t* ee_counts,
+                           int32_t* ee_lists);
 int vbd_finalize(VbdSolver* solver, float* q_in, float* q_out, float* qd_out, float dt, void* stream);
 
 /* Warm start (no reference counterpart): after vbd_forward, move the initial Gauss-Seidel iterate

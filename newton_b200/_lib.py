@@ -85,6 +85,16 @@ class VbdSolverOptions(ctypes.Structure):
         ("contacts_per_vertex", ctypes.c_int32),
         ("use_graph", ctypes.c_int32),
         ("step_kernel", ctypes.c_int32),
+        ("self_contact", ctypes.c_int32),
+        ("self_contact_radius", ctypes.c_float),
+        ("self_contact_margin", ctypes.c_float),
+        ("conservative_bound_relaxation", ctypes.c_float),
+        ("vertex_contact_buffer_size", ctypes.c_int32),
+        ("edge_contact_buffer_size", ctypes.c_int32),
+        ("collision_detection_interval", ctypes.c_int32),
+        ("edge_parallel_epsilon", ctypes.c_float),
+        ("topological_filter_threshold", ctypes.c_int32),
+        ("rest_exclusion_radius", ctypes.c_float),
     ]
 
 
@@ -110,6 +120,8 @@ class VbdStatus(ctypes.Structure):
         ("singular_blocks", ctypes.c_int32),
         ("contact_overflow", ctypes.c_int32),
         ("timeouts", ctypes.c_int32),
+        ("self_contact_overflow", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
@@ -133,6 +145,9 @@ SIGNATURES = {
     ),
     "vbd_forward": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.POINTER(VbdContacts), ctypes.c_float, _VP]),
     "vbd_sweep_color": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(VbdContacts), ctypes.c_float, _VP]),
+    "vbd_begin_iteration": (ctypes.c_int, [_VP, ctypes.c_int32, _VP]),
+    "vbd_self_contact_detect": (ctypes.c_int, [_VP, _VP, _VP]),
+    "vbd_self_contact_lists": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
     "vbd_finalize": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_float, _VP]),
     "vbd_get_positions": (ctypes.c_int, [_VP, _VP, _VP]),
     "vbd_warm_start": (ctypes.c_int, [_VP, _VP, _VP]),

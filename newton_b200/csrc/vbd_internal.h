@@ -76,6 +76,9 @@ struct VbdModelImpl {
     std::vector<float4> tri_D_h, tri_mat_h, edge_mat_h;
     std::vector<int> tri_elem_h, edge_elem_h;   // element id of each record (dedupe per patch)
     std::vector<float> rest_q_h;                // [3V] initial positions in internal order (may be empty)
+    // raw topology in model order (self-contact layer) and the model-level contact material
+    std::vector<int> tri_raw_h, edge_raw_h, adj_t_off_h, adj_t_h, adj_e_off_h, adj_e_h, pworld_h;
+    float soft_ke = 0.f, soft_kd = 0.f, soft_mu = 0.f;
 };
 
 // learned warm start (vbd_mlp.cu): per-vertex features after the forward pass, and the warm-start

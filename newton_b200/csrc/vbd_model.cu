@@ -302,6 +302,24 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
     if ((rc = upload(&m.world_shapes, wsl))) return rc;
     if ((rc = upload(&m.nbr8, nbr8))) return rc;
     if ((rc = upload(&m.vfeat, vfeat))) return rc;
+    m.tri_raw_h.assign(d->tri_indices, d->tri_indices + 3 * static_cast<size_t>(T));
+    m.edge_raw_h.assign(d->edge_indices, d->edge_indices + 4 * static_cast<size_t>(E));
+    if (T > 0) {
+        m.adj_t_off_h.assign(d->v_adj_tris_offsets, d->v_adj_tris_offsets + V + 1);
+        m.adj_t_h.assign(d->v_adj_tris, d->v_adj_tris + m.adj_t_off_h[V]);
+    } else {
+        m.adj_t_off_h.assign(V + 1, 0);
+    }
+    if (E > 0) {
+        m.adj_e_off_h.assign(d->v_adj_edges_offsets, d->v_adj_edges_offsets + V + 1);
+        m.adj_e_h.assign(d->v_adj_edges, d->v_adj_edges + m.adj_e_off_h[V]);
+    } else {
+        m.adj_e_off_h.assign(V + 1, 0);
+    }
+    m.pworld_h = pworld;
+    m.soft_ke = d->soft_contact_ke;
+    m.soft_kd = d->soft_contact_kd;
+    m.soft_mu = d->soft_contact_mu;
     m.pinfo_h = std::move(pinfo);
     m.vadj_h = std::move(vadj);
     m.tri_idx_h = std::move(tri_idx);

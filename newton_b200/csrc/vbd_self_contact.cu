@@ -1,0 +1,827 @@
+// vbd_self_contact.cu -- cloth self-contact for the VBD step on sm_100a.
+//
+// Restates the reference's particle self-contact path (SolverVBD with
+// particle_enable_self_contact=True):
+//   detection         TriMeshCollisionDetector.vertex_triangle_collision_detection /
+//                     edge_edge_collision_detection (solvers/vbd/tri_mesh_collision.py:645-730;
+//                     kernels geometry/kernels.py:1328-1497, :1499-1640), n-ring topological filter
+//                     (tri_mesh_collision.py:123-233), rest-shape exclusion radius
+//   forces            accumulate_self_contact_force_and_hessian (particle_vbd_kernels.py:1498-1639)
+//   truncation        apply_planar_truncation_parallel_by_collision (:2133-2263) + apply_truncation_ts
+//                     (:2266-2286) with max displacement margin * relaxation * 0.5
+//                     (solver_vbd.py:2026-2063)
+//   orchestration     solver_vbd.py:2065-2100 (detection before the forward step), :2540-2545
+//                     (detection interval), :3221-3237 (positions become the displacement base)
+//
+// B200 design.  The reference refits two BVHs and runs 4 threads per primitive with atomics into
+// the per-vertex force.  Here:
+//   * a hashed uniform grid (cell >= 2 * margin and >= the longest rest edge) is rebuilt every
+//     detection in four device passes -- count per bucket, exclusive scan (CUB), fill, query --
+//     so no host synchronisation is needed and a step stays graph-capturable;
+//   * each candidate pair is reported once, in the cell that is the minimum corner of the
+//     intersection of the two cell ranges, and kept in a sorted per-vertex / per-edge list;
+//   * forces are gathered per vertex of the current color in a fixed order (own vertex-triangle
+//     pairs, then the pairs of each incident triangle, then the edge-edge pairs of each incident
+//     edge), so results are deterministic;
+//   * truncation ratios are reduced with an integer atomicMin on the (non-negative) float bits,
+//     which is exact and order-independent.
+// Buffers are fixed-size (reference defaults: 32 triangles per vertex, 64 edges per edge; plus
+// 32 vertices per triangle for the gather); candidates beyond a buffer are dropped and counted.
+#include "vbd_self_contact.h"
+
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "vbd_self_contact_math.cuh"
+
+namespace vbd {
+
+namespace {
+
+constexpr int kMaxCells = 64;  // cells one element or query box may touch (else: counted, skipped)
+
+struct CellRange {
+    int3 lo, hi;
+};
+
+__device__ __forceinline__ int cell_coord(float x, float inv) { return static_cast<int>(floorf(x * inv)); }
+
+__device__ __forceinline__ CellRange cell_range(float3 lo, float3 hi, float inv) {
+    CellRange r;
+    r.lo = make_int3(cell_coord(lo.x, inv), cell_coord(lo.y, inv), cell_coord(lo.z, inv));
+    r.hi = make_int3(cell_coord(hi.x, inv), cell_coord(hi.y, inv), cell_coord(hi.z, inv));
+    return r;
+}
+
+__device__ __forceinline__ long long cell_count(const CellRange& r) {
+    return (static_cast<long long>(r.hi.x) - r.lo.x + 1) * (static_cast<long long>(r.hi.y) - r.lo.y + 1) *
+           (static_cast<long long>(r.hi.z) - r.lo.z + 1);
+}
+
+__device__ __forceinline__ unsigned cell_hash(int x, int y, int z, unsigned mask) {
+    return ((static_cast<unsigned>(x) * 73856093u) ^ (static_cast<unsigned>(y) * 19349663u) ^
+            (static_cast<unsigned>(z) * 83492791u)) &
+           mask;
+}
+
+__device__ __forceinline__ float3 fmin3(float3 a, float3 b) { return f3(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)); }
+__device__ __forceinline__ float3 fmax3(float3 a, float3 b) { return f3(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)); }
+
+struct GridArgs {
+    const float4* x;      // positions (internal order)
+    const int4* elem;     // triangles or edges
+    int n;
+    bool tri;
+    float inv_cell;
+    unsigned mask;
+    int* cnt;
+    const int* off;
+    int* cur;
+    int* items;
+    int cap;
+    unsigned* counters;
+};
+
+__device__ __forceinline__ void elem_box(const GridArgs& a, int e, float3& lo, float3& hi) {
+    const int4 el = a.elem[e];
+    const float3 p0 = xyz(a.x[el.x]), p1 = xyz(a.x[el.y]);
+    lo = fmin3(p0, p1);
+    hi = fmax3(p0, p1);
+    if (a.tri) {
+        const float3 p2 = xyz(a.x[el.z]);
+        lo = fmin3(lo, p2);
+        hi = fmax3(hi, p2);
+    }
+}
+
+__global__ void grid_count_kernel(GridArgs a) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.n) return;
+    float3 lo, hi;
+    elem_box(a, e, lo, hi);
+    const CellRange r = cell_range(lo, hi, a.inv_cell);
+    if (cell_count(r) > kMaxCells) {
+        atomicAdd(&a.counters[kScGridOverflow], 1u);
+        return;
+    }
+    for (int z = r.lo.z; z <= r.hi.z; ++z)
+        for (int y = r.lo.y; y <= r.hi.y; ++y)
+            for (int x = r.lo.x; x <= r.hi.x; ++x) atomicAdd(&a.cnt[cell_hash(x, y, z, a.mask)], 1);
+}
+
+__global__ void grid_fill_kernel(GridArgs a) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.n) return;
+    float3 lo, hi;
+    elem_box(a, e, lo, hi);
+    const CellRange r = cell_range(lo, hi, a.inv_cell);
+    if (cell_count(r) > kMaxCells) return;
+    for (int z = r.lo.z; z <= r.hi.z; ++z)
+        for (int y = r.lo.y; y <= r.hi.y; ++y)
+            for (int x = r.lo.x; x <= r.hi.x; ++x) {
+                const unsigned h = cell_hash(x, y, z, a.mask);
+                const int k = a.off[h] + atomicAdd(&a.cur[h], 1);
+                if (k < a.cap) a.items[k] = e;
+                else atomicAdd(&a.counters[kScGridOverflow], 1u);
+            }
+}
+
+// sorted insert without duplicates into row[0..n) of capacity cap; false when full
+__device__ __forceinline__ bool sorted_insert(int* row, int& n, int cap, int x) {
+    int k = 0;
+    while (k < n && row[k] < x) ++k;
+    if (k < n && row[k] == x) return true;
+    if (n >= cap) return false;
+    for (int j = n; j > k; --j) row[j] = row[j - 1];
+    row[k] = x;
+    ++n;
+    return true;
+}
+
+__device__ __forceinline__ bool list_contains(const int* b, const int* e, int x) {
+    for (const int* p = b; p < e; ++p)
+        if (*p == x) return true;
+    return false;
+}
+
+struct QueryArgs {
+    const float4* x;
+    const int* vworld;
+    const float4* rest;
+    const int4* tri;
+    const int4* edge;
+    const int* near_off;
+    const int* near;
+    int V, T, E;
+    float margin, inv_cell, par_eps, rest_excl;
+    unsigned tri_mask, edge_mask;
+    const int *tri_cnt, *tri_off, *tri_items;
+    const int *edge_cnt, *edge_off, *edge_items;
+    int tri_cap, edge_cap;
+    int vbuf, ebuf;
+    int* vt_count;
+    int* vt_list;
+    int* ee_count;
+    int* ee_list;
+    unsigned* counters;
+};
+
+__global__ void vt_query_kernel(QueryArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.V) return;
+    const float3 p = xyz(a.x[i]);
+    const float m = a.margin;
+    const CellRange q = cell_range(p - f3(m, m, m), p + f3(m, m, m), a.inv_cell);
+    int n = 0;
+    int* row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
+    if (cell_count(q) > kMaxCells) {
+        atomicAdd(&a.counters[kScGridOverflow], 1u);
+        a.vt_count[i] = 0;
+        return;
+    }
+    const int wv = a.vworld[i];
+    const int* nb = a.near + a.near_off[i];
+    const int* ne = a.near + a.near_off[i + 1];
+    bool full = false;
+    for (int z = q.lo.z; z <= q.hi.z; ++z)
+        for (int y = q.lo.y; y <= q.hi.y; ++y)
+            for (int x = q.lo.x; x <= q.hi.x; ++x) {
+                const unsigned h = cell_hash(x, y, z, a.tri_mask);
+                const int b = a.tri_off[h];
+                const int e = min(b + a.tri_cnt[h], a.tri_cap);
+                for (int k = b; k < e; ++k) {
+                    const int t = a.tri_items[k];
+                    const int4 tr = a.tri[t];
+                    if (tr.x == i || tr.y == i || tr.z == i) continue;
+                    if (wv >= 0 && tr.w >= 0 && wv != tr.w) continue;
+                    const float3 t0 = xyz(a.x[tr.x]), t1 = xyz(a.x[tr.y]), t2 = xyz(a.x[tr.z]);
+                    // report the pair only in the minimum corner cell of the two ranges
+                    const CellRange er = cell_range(fmin3(fmin3(t0, t1), t2), fmax3(fmax3(t0, t1), t2), a.inv_cell);
+                    const int cx = max(q.lo.x, er.lo.x), cy = max(q.lo.y, er.lo.y), cz = max(q.lo.z, er.lo.z);
+                    if (cx != x || cy != y || cz != z) continue;
+                    if (x > er.hi.x || y > er.hi.y || z > er.hi.z) continue;
+                    if (list_contains(nb, ne, tr.x) || list_contains(nb, ne, tr.y) || list_contains(nb, ne, tr.z))
+                        continue;
+                    float3 bary;
+                    const float dist = length(triangle_closest_point(t0, t1, t2, p, bary) - p);
+                    if (!(dist < m)) continue;
+                    if (a.rest_excl > 0.f) {
+                        const float3 rp = xyz(a.rest[i]);
+                        const float dr = length(triangle_closest_point(xyz(a.rest[tr.x]), xyz(a.rest[tr.y]),
+                                                                       xyz(a.rest[tr.z]), rp, bary) -
+                                                rp);
+                        if (dr < a.rest_excl) continue;
+                    }
+                    if (!sorted_insert(row, n, a.vbuf, t)) full = true;
+                }
+            }
+    a.vt_count[i] = n;
+    if (full) atomicAdd(&a.counters[kScVtOverflow], 1u);
+}
+
+__global__ void ee_query_kernel(QueryArgs a) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= a.E) return;
+    const int4 ed = a.edge[e];
+    const float3 a0 = xyz(a.x[ed.x]), a1 = xyz(a.x[ed.y]);
+    const float m = a.margin;
+    const CellRange q = cell_range(fmin3(a0, a1) - f3(m, m, m), fmax3(a0, a1) + f3(m, m, m), a.inv_cell);
+    int n = 0;
+    int* row = a.ee_list + static_cast<size_t>(e) * a.ebuf;
+    if (cell_count(q) > kMaxCells) {
+        atomicAdd(&a.counters[kScGridOverflow], 1u);
+        a.ee_count[e] = 0;
+        return;
+    }
+    const int* n0b = a.near + a.near_off[ed.x];
+    const int* n0e = a.near + a.near_off[ed.x + 1];
+    const int* n1b = a.near + a.near_off[ed.y];
+    const int* n1e = a.near + a.near_off[ed.y + 1];
+    bool full = false;
+    for (int z = q.lo.z; z <= q.hi.z; ++z)
+        for (int y = q.lo.y; y <= q.hi.y; ++y)
+            for (int x = q.lo.x; x <= q.hi.x; ++x) {
+                const unsigned h = cell_hash(x, y, z, a.edge_mask);
+                const int b = a.edge_off[h];
+                const int en = min(b + a.edge_cnt[h], a.edge_cap);
+                for (int k = b; k < en; ++k) {
+                    const int g = a.edge_items[k];
+                    const int4 gd = a.edge[g];
+                    if (gd.x == ed.x || gd.x == ed.y || gd.y == ed.x || gd.y == ed.y) continue;
+                    if (ed.z >= 0 && gd.z >= 0 && ed.z != gd.z) continue;
+                    const float3 b0 = xyz(a.x[gd.x]), b1 = xyz(a.x[gd.y]);
+                    const CellRange er = cell_range(fmin3(b0, b1), fmax3(b0, b1), a.inv_cell);
+                    const int cx = max(q.lo.x, er.lo.x), cy = max(q.lo.y, er.lo.y), cz = max(q.lo.z, er.lo.z);
+                    if (cx != x || cy != y || cz != z) continue;
+                    if (x > er.hi.x || y > er.hi.y || z > er.hi.z) continue;
+                    if (list_contains(n0b, n0e, gd.x) || list_contains(n0b, n0e, gd.y) ||
+                        list_contains(n1b, n1e, gd.x) || list_contains(n1b, n1e, gd.y))
+                        continue;
+                    float s, t, dist;
+                    closest_edge_edge(a0, a1, b0, b1, a.par_eps, s, t, dist);
+                    if (!(dist < m)) continue;
+                    if (a.rest_excl > 0.f) {
+                        float sr, tr, dr;
+                        closest_edge_edge(xyz(a.rest[ed.x]), xyz(a.rest[ed.y]), xyz(a.rest[gd.x]), xyz(a.rest[gd.y]),
+                                          a.par_eps, sr, tr, dr);
+                        if (dr < a.rest_excl) continue;
+                    }
+                    if (!sorted_insert(row, n, a.ebuf, g)) full = true;
+                }
+            }
+    a.ee_count[e] = n;
+    if (full) atomicAdd(&a.counters[kScEeOverflow], 1u);
+}
+
+__global__ void tri_reverse_kernel(int V, const int* vt_count, const int* vt_list, int vbuf, int* tv_count,
+                                   int* tv_list, int tcap, unsigned* counters) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V) return;
+    const int* row = vt_list + static_cast<size_t>(i) * vbuf;
+    for (int k = 0; k < vt_count[i]; ++k) {
+        const int t = row[k];
+        const int j = atomicAdd(&tv_count[t], 1);
+        if (j < tcap) tv_list[static_cast<size_t>(t) * tcap + j] = i;
+        else atomicAdd(&counters[kScTvOverflow], 1u);
+    }
+}
+
+__global__ void tri_sort_kernel(int T, int* tv_count, int* tv_list, int tcap) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const int n = min(tv_count[t], tcap);
+    tv_count[t] = n;
+    int* row = tv_list + static_cast<size_t>(t) * tcap;
+    for (int a = 1; a < n; ++a) {
+        const int x = row[a];
+        int b = a - 1;
+        while (b >= 0 && row[b] > x) {
+            row[b + 1] = row[b];
+            --b;
+        }
+        row[b + 1] = x;
+    }
+}
+
+__global__ void copy_positions_kernel(int V, const float4* src, float4* cd, float4* disp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V) return;
+    if (src != cd) cd[i] = src[i];
+    if (disp) disp[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+__global__ void load_positions_kernel(int V, const int* perm, const float* q, float4* cd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V) return;
+    const int o = perm[i];
+    cd[i] = make_float4(q[3 * o], q[3 * o + 1], q[3 * o + 2], 0.f);
+}
+
+struct AccumArgs {
+    const float4* x;
+    const float4* x0;   // anchor: the step's start positions
+    const int4* tri;
+    const int4* edge;
+    const int *inc_t_off, *inc_e_off;
+    const int2 *inc_t, *inc_e;
+    const int *vt_count, *vt_list, *ee_count, *ee_list, *tv_count, *tv_list;
+    int vbuf, ebuf, tcap;
+    int v_begin, v_end;
+    float r, ke, kd, mu, eps_u, dt, par_eps;
+    float4 *f, *h0, *h1;
+};
+
+__global__ void accumulate_kernel(AccumArgs a) {
+    const int i = a.v_begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.v_end) return;
+    float3 f = f3(0.f, 0.f, 0.f);
+    Sym3 H = zero_sym();
+    const float3 p = xyz(a.x[i]), p0 = xyz(a.x0[i]);
+    const int* row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
+    for (int k = 0; k < a.vt_count[i]; ++k) {
+        const int4 tr = a.tri[row[k]];
+        vt_contact_slot(xyz(a.x[tr.x]), xyz(a.x[tr.y]), xyz(a.x[tr.z]), p, xyz(a.x0[tr.x]), xyz(a.x0[tr.y]),
+                        xyz(a.x0[tr.z]), p0, 3, a.r, a.ke, a.kd, a.mu, a.eps_u, a.dt, f, H);
+    }
+    for (int k = a.inc_t_off[i]; k < a.inc_t_off[i + 1]; ++k) {
+        const int2 ts = a.inc_t[k];
+        const int4 tr = a.tri[ts.x];
+        const float3 t0 = xyz(a.x[tr.x]), t1 = xyz(a.x[tr.y]), t2 = xyz(a.x[tr.z]);
+        const float3 s0 = xyz(a.x0[tr.x]), s1 = xyz(a.x0[tr.y]), s2 = xyz(a.x0[tr.z]);
+        const int* vl = a.tv_list + static_cast<size_t>(ts.x) * a.tcap;
+        for (int j = 0; j < a.tv_count[ts.x]; ++j) {
+            const int q = vl[j];
+            vt_contact_slot(t0, t1, t2, xyz(a.x[q]), s0, s1, s2, xyz(a.x0[q]), ts.y, a.r, a.ke, a.kd, a.mu, a.eps_u,
+                            a.dt, f, H);
+        }
+    }
+    for (int k = a.inc_e_off[i]; k < a.inc_e_off[i + 1]; ++k) {
+        const int2 es = a.inc_e[k];
+        const int4 ed = a.edge[es.x];
+        const float3 e0 = xyz(a.x[ed.x]), e1 = xyz(a.x[ed.y]);
+        const float3 e0a = xyz(a.x0[ed.x]), e1a = xyz(a.x0[ed.y]);
+        const int* gl = a.ee_list + static_cast<size_t>(es.x) * a.ebuf;
+        for (int j = 0; j < a.ee_count[es.x]; ++j) {
+            const int4 gd = a.edge[gl[j]];
+            ee_contact_slot(e0, e1, xyz(a.x[gd.x]), xyz(a.x[gd.y]), e0a, e1a, xyz(a.x0[gd.x]), xyz(a.x0[gd.y]), es.y,
+                            a.r, a.ke, a.kd, a.mu, a.eps_u, a.dt, a.par_eps, f, H);
+        }
+    }
+    a.f[i] = make_float4(f.x, f.y, f.z, 0.f);
+    a.h0[i] = make_float4(H.xx, H.xy, H.xz, H.yy);
+    a.h1[i] = make_float4(H.yz, H.zz, 0.f, 0.f);
+}
+
+struct TruncArgs {
+    const float4* cd;
+    const float4* disp;
+    const int4* tri;
+    const int4* edge;
+    const int *vt_count, *vt_list, *ee_count, *ee_list;
+    int V, E, vbuf, ebuf;
+    float eps, gamma;
+    unsigned* ts;
+};
+
+__device__ __forceinline__ void ts_min(unsigned* ts, int i, float3 x, float3 dx, float3 n, float3 d, float eps,
+                                       float gamma) {
+    const float t = planar_truncation_t(x, dx, n, d, eps, gamma);
+    atomicMin(&ts[i], __float_as_uint(t));
+}
+
+__global__ void planar_kernel(TruncArgs a) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < a.V) {
+        const int i = idx;
+        const float3 v = xyz(a.cd[i]), dv = xyz(a.disp[i]);
+        const int* row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
+        for (int k = 0; k < a.vt_count[i]; ++k) {
+            const int4 tr = a.tri[row[k]];
+            const float3 t1 = xyz(a.cd[tr.x]), t2 = xyz(a.cd[tr.y]), t3 = xyz(a.cd[tr.z]);
+            const float3 d1 = xyz(a.disp[tr.x]), d2 = xyz(a.disp[tr.y]), d3 = xyz(a.disp[tr.z]);
+            float3 n, d;
+            const int dummy = vt_plane(v, dv, t1, d1, t2, d2, t3, d3, n, d);
+            if (!(dummy & 1)) ts_min(a.ts, i, v, dv, n, d, a.eps, a.gamma);
+            if (!(dummy & 2)) ts_min(a.ts, tr.x, t1, d1, n, d, a.eps, a.gamma);
+            if (!(dummy & 4)) ts_min(a.ts, tr.y, t2, d2, n, d, a.eps, a.gamma);
+            if (!(dummy & 8)) ts_min(a.ts, tr.z, t3, d3, n, d, a.eps, a.gamma);
+        }
+    }
+    if (idx < a.E) {
+        const int e = idx;
+        const int4 ed = a.edge[e];
+        const float3 a0 = xyz(a.cd[ed.x]), a1 = xyz(a.cd[ed.y]);
+        const float3 da0 = xyz(a.disp[ed.x]), da1 = xyz(a.disp[ed.y]);
+        const int* row = a.ee_list + static_cast<size_t>(e) * a.ebuf;
+        for (int k = 0; k < a.ee_count[e]; ++k) {
+            const int4 gd = a.edge[row[k]];
+            const float3 b0 = xyz(a.cd[gd.x]), b1 = xyz(a.cd[gd.y]);
+            const float3 db0 = xyz(a.disp[gd.x]), db1 = xyz(a.disp[gd.y]);
+            float3 n, d;
+            const int dummy = ee_plane(a0, da0, a1, da1, b0, db0, b1, db1, n, d);
+            if (!(dummy & 1)) ts_min(a.ts, ed.x, a0, da0, n, d, a.eps, a.gamma);
+            if (!(dummy & 2)) ts_min(a.ts, ed.y, a1, da1, n, d, a.eps, a.gamma);
+            if (!(dummy & 4)) ts_min(a.ts, gd.x, b0, db0, n, d, a.eps, a.gamma);
+            if (!(dummy & 8)) ts_min(a.ts, gd.y, b1, db1, n, d, a.eps, a.gamma);
+        }
+    }
+}
+
+// apply_truncation_ts: disp *= t, clamp |disp| to max_disp, pos = cd + disp; t is reset to 1
+__global__ void apply_truncation_kernel(int V, const float4* cd, float4* disp, float4* pos, unsigned* ts,
+                                        float max_disp) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V) return;
+    const float t = __uint_as_float(ts[i]);
+    ts[i] = __float_as_uint(1.0f);
+    const float4 d4 = disp[i];
+    float3 d = f3(d4.x * t, d4.y * t, d4.z * t);
+    const float l = length(d);
+    if (l > max_disp) d = f3(d.x * max_disp / l, d.y * max_disp / l, d.z * max_disp / l);
+    disp[i] = make_float4(d.x, d.y, d.z, 0.f);
+    const float4 c = cd[i];
+    pos[i] = make_float4(c.x + d.x, c.y + d.y, c.z + d.z, 0.f);
+}
+
+__global__ void fill_u32_kernel(unsigned* p, unsigned v, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+unsigned next_pow2(long long x) {
+    unsigned v = 1024;
+    while (static_cast<long long>(v) < x && v < (1u << 30)) v <<= 1;
+    return v;
+}
+
+template <typename T>
+int upload_vec(T** dst, const std::vector<T>& src) {
+    *dst = nullptr;
+    const size_t n = std::max<size_t>(src.size(), 1);
+    VBD_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(dst), n * sizeof(T)));
+    if (!src.empty()) VBD_CUDA_TRY(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return VBD_OK;
+}
+
+int alloc_zero(void** p, size_t bytes) {
+    bytes = std::max<size_t>(bytes, 16);
+    VBD_CUDA_TRY(cudaMalloc(p, bytes));
+    VBD_CUDA_TRY(cudaMemset(*p, 0, bytes));
+    return VBD_OK;
+}
+
+}  // namespace
+
+bool self_contact_detect_now(const SelfContact& sc, int it) {
+    if (!sc.on) return false;
+    if (sc.p.interval == 0) return it == 0;
+    if (sc.p.interval >= 1) return it % sc.p.interval == 0;
+    return false;
+}
+
+void self_contact_free(SelfContact& sc) {
+    void* ptrs[] = {sc.tri,      sc.edge,     sc.inc_t_off, sc.inc_t,    sc.inc_e_off,  sc.inc_e,     sc.near_off,
+                    sc.near,     sc.rest,     sc.tri_cnt,   sc.tri_off,  sc.tri_cur,    sc.tri_items, sc.edge_cnt,
+                    sc.edge_off, sc.edge_cur, sc.edge_items, sc.scan_tmp, sc.vt_count,  sc.vt_list,   sc.ee_count,
+                    sc.ee_list,  sc.tv_count, sc.tv_list,   sc.cd,       sc.sc_f,       sc.sc_h0,     sc.sc_h1,
+                    sc.ts,       sc.counters, sc.vworld};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    SelfContact empty;
+    sc = empty;
+}
+
+int self_contact_create(const VbdModelImpl& m, const SelfContactParams& p, SelfContact& sc) {
+    self_contact_free(sc);
+    if (!(p.margin >= p.radius))
+        return fail(VBD_ERR_INVALID_ARGUMENT,
+                    "particle_self_contact_margin is smaller than particle_self_contact_radius, this will result in "
+                    "missing contacts and cause instability.\nIt is advisable to make particle_self_contact_margin "
+                    "1.5-2 times larger than particle_self_contact_radius.");
+    if (!(p.radius > 0.f)) return fail(VBD_ERR_INVALID_ARGUMENT, "self contact: radius must be > 0");
+    if (p.vertex_buffer < 1 || p.vertex_buffer > 256 || p.edge_buffer < 1 || p.edge_buffer > 512)
+        return fail(VBD_ERR_INVALID_ARGUMENT, "self contact: buffer sizes must be in [1, 256] / [1, 512]");
+    if (p.filter_threshold > 4)
+        return fail(VBD_ERR_UNSUPPORTED, "self contact: topological filter threshold above 4 is not supported");
+    if (m.rest_q_h.size() != 3 * static_cast<size_t>(m.V))
+        return fail(VBD_ERR_INVALID_ARGUMENT, "self contact needs the model's rest positions (VbdModelDesc.particle_q)");
+    const int V = m.V, T = m.T, E = m.E;
+    sc.p = p;
+    sc.V = V;
+    sc.T = T;
+    sc.E = E;
+    sc.max_disp = static_cast<float>(static_cast<double>(p.margin) * static_cast<double>(p.relaxation) * 0.5);
+    std::vector<int> inv(V);
+    for (int i = 0; i < V; ++i) inv[m.perm_host[i]] = i;
+    // topology
+    std::vector<int4> tri(T), edge(E);
+    for (int t = 0; t < T; ++t) {
+        const int* ti = m.tri_raw_h.data() + 3 * t;
+        tri[t] = make_int4(inv[ti[0]], inv[ti[1]], inv[ti[2]], m.pworld_h[ti[0]]);
+    }
+    double max_edge = 0.0;
+    for (int e = 0; e < E; ++e) {
+        const int* ei = m.edge_raw_h.data() + 4 * e;
+        edge[e] = make_int4(inv[ei[2]], inv[ei[3]], m.pworld_h[ei[2]], 0);
+        const float* ra = m.rest_q_h.data() + 3 * static_cast<size_t>(inv[ei[2]]);
+        const float* rb = m.rest_q_h.data() + 3 * static_cast<size_t>(inv[ei[3]]);
+        const double dx = ra[0] - rb[0], dy = ra[1] - rb[1], dz = ra[2] - rb[2];
+        max_edge = std::max(max_edge, std::sqrt(dx * dx + dy * dy + dz * dz));
+    }
+    sc.cell = static_cast<float>(std::max(2.0 * p.margin, max_edge) * 1.0001);
+    // incidence (internal vertex -> triangles with slot, endpoint edges with endpoint)
+    std::vector<int> it_off(V + 1, 0), ie_off(V + 1, 0);
+    std::vector<int2> it_list, ie_list;
+    for (int i = 0; i < V; ++i) {
+        const int o = m.perm_host[i];
+        for (int k = m.adj_t_off_h[o]; k < m.adj_t_off_h[o + 1]; k += 2)
+            it_list.push_back(make_int2(m.adj_t_h[k], m.adj_t_h[k + 1]));
+        it_off[i + 1] = static_cast<int>(it_list.size());
+        for (int k = m.adj_e_off_h[o]; k < m.adj_e_off_h[o + 1]; k += 2)
+            if (m.adj_e_h[k + 1] >= 2) ie_list.push_back(make_int2(m.adj_e_h[k], m.adj_e_h[k + 1] - 2));
+        ie_off[i + 1] = static_cast<int>(ie_list.size());
+    }
+    // n-ring filter sets (internal ids): vertices within threshold - 1 edge rings
+    std::vector<int> near_off(V + 1, 0), near_list;
+    if (p.filter_threshold >= 2) {
+        std::vector<std::vector<int>> ring1(V);
+        for (int e = 0; e < E; ++e) {
+            ring1[edge[e].x].push_back(edge[e].y);
+            ring1[edge[e].y].push_back(edge[e].x);
+        }
+        for (auto& r : ring1) {
+            std::sort(r.begin(), r.end());
+            r.erase(std::unique(r.begin(), r.end()), r.end());
+        }
+        const int depth = p.filter_threshold - 1;
+        std::vector<int> seen, frontier, next;
+        for (int i = 0; i < V; ++i) {
+            seen.assign(1, i);
+            frontier.assign(1, i);
+            for (int k = 0; k < depth && !frontier.empty(); ++k) {
+                next.clear();
+                for (int u : frontier)
+                    for (int w : ring1[u])
+                        if (std::find(seen.begin(), seen.end(), w) == seen.end()) {
+                            seen.push_back(w);
+                            next.push_back(w);
+                        }
+                frontier.swap(next);
+            }
+            std::sort(seen.begin(), seen.end());
+            for (int w : seen)
+                if (w != i) near_list.push_back(w);
+            near_off[i + 1] = static_cast<int>(near_list.size());
+        }
+    }
+    std::vector<int> vworld(V);
+    for (int i = 0; i < V; ++i) vworld[i] = m.pworld_h[m.perm_host[i]];
+    std::vector<float4> rest(V);
+    for (int i = 0; i < V; ++i)
+        rest[i] = make_float4(m.rest_q_h[3 * i], m.rest_q_h[3 * i + 1], m.rest_q_h[3 * i + 2], 0.f);
+
+    int rc = VBD_OK;
+    if (!rc) rc = upload_vec(&sc.tri, tri);
+    if (!rc) rc = upload_vec(&sc.edge, edge);
+    if (!rc) rc = upload_vec(&sc.inc_t_off, it_off);
+    if (!rc) rc = upload_vec(&sc.inc_t, it_list);
+    if (!rc) rc = upload_vec(&sc.inc_e_off, ie_off);
+    if (!rc) rc = upload_vec(&sc.inc_e, ie_list);
+    if (!rc) rc = upload_vec(&sc.near_off, near_off);
+    if (!rc) rc = upload_vec(&sc.near, near_list);
+    if (!rc) rc = upload_vec(&sc.rest, rest);
+    if (!rc) rc = upload_vec(&sc.vworld, vworld);
+    const unsigned tn = next_pow2(2LL * std::max(T, 1)), en = next_pow2(2LL * std::max(E, 1));
+    sc.tri_mask = tn - 1;
+    sc.edge_mask = en - 1;
+    sc.tri_items_cap = 8 * std::max(T, 1) + 4096;
+    sc.edge_items_cap = 8 * std::max(E, 1) + 4096;
+    auto az = [&](void** ptr, size_t bytes) {
+        if (!rc) rc = alloc_zero(ptr, bytes);
+    };
+    az(reinterpret_cast<void**>(&sc.tri_cnt), tn * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.tri_off), tn * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.tri_cur), tn * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.tri_items), static_cast<size_t>(sc.tri_items_cap) * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.edge_cnt), en * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.edge_off), en * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.edge_cur), en * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.edge_items), static_cast<size_t>(sc.edge_items_cap) * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.vt_count), static_cast<size_t>(V) * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.vt_list), static_cast<size_t>(V) * p.vertex_buffer * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.ee_count), static_cast<size_t>(E) * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.ee_list), static_cast<size_t>(E) * p.edge_buffer * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.tv_count), static_cast<size_t>(T) * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.tv_list), static_cast<size_t>(T) * sc.tcap * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.cd), static_cast<size_t>(V) * sizeof(float4));
+    az(reinterpret_cast<void**>(&sc.sc_f), static_cast<size_t>(V) * sizeof(float4));
+    az(reinterpret_cast<void**>(&sc.sc_h0), static_cast<size_t>(V) * sizeof(float4));
+    az(reinterpret_cast<void**>(&sc.sc_h1), static_cast<size_t>(V) * sizeof(float4));
+    az(reinterpret_cast<void**>(&sc.ts), static_cast<size_t>(V) * sizeof(unsigned));
+    az(reinterpret_cast<void**>(&sc.counters), kScCounters * sizeof(unsigned));
+    if (!rc) {
+        size_t b1 = 0, b2 = 0;
+        cudaError_t e1 = cub::DeviceScan::ExclusiveSum(nullptr, b1, sc.tri_cnt, sc.tri_off, static_cast<int>(tn));
+        cudaError_t e2 = cub::DeviceScan::ExclusiveSum(nullptr, b2, sc.edge_cnt, sc.edge_off, static_cast<int>(en));
+        if (e1 != cudaSuccess) rc = cuda_fail(e1, "cub::DeviceScan::ExclusiveSum (size query)");
+        if (!rc && e2 != cudaSuccess) rc = cuda_fail(e2, "cub::DeviceScan::ExclusiveSum (size query)");
+        sc.scan_bytes = std::max(b1, b2);
+        az(&sc.scan_tmp, sc.scan_bytes);
+    }
+    if (!rc && V > 0) {
+        fill_u32_kernel<<<(V + 255) / 256, 256>>>(sc.ts, 0x3f800000u /* 1.0f */, V);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = cuda_fail(e, "fill_u32_kernel");
+        if (!rc) {
+            const cudaError_t s = cudaDeviceSynchronize();
+            if (s != cudaSuccess) rc = cuda_fail(s, "cudaDeviceSynchronize");
+        }
+    }
+    if (rc) {
+        self_contact_free(sc);
+        return rc;
+    }
+    sc.on = true;
+    return VBD_OK;
+}
+
+int self_contact_load_positions(const VbdModelImpl& m, SelfContact& sc, const float* q, cudaStream_t st) {
+    if (m.V == 0) return VBD_OK;
+    load_positions_kernel<<<(m.V + 255) / 256, 256, 0, st>>>(m.V, m.perm, q, sc.cd);
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* positions, float4* disp,
+                        bool reset_disp, cudaStream_t st) {
+    const int V = m.V, T = m.T, E = m.E;
+    if (V == 0) return VBD_OK;
+    copy_positions_kernel<<<(V + 255) / 256, 256, 0, st>>>(V, positions, sc.cd, reset_disp ? disp : nullptr);
+    VBD_CUDA_TRY(cudaGetLastError());
+    const unsigned tn = sc.tri_mask + 1, en = sc.edge_mask + 1;
+    VBD_CUDA_TRY(cudaMemsetAsync(sc.tri_cnt, 0, tn * sizeof(int), st));
+    VBD_CUDA_TRY(cudaMemsetAsync(sc.tri_cur, 0, tn * sizeof(int), st));
+    VBD_CUDA_TRY(cudaMemsetAsync(sc.edge_cnt, 0, en * sizeof(int), st));
+    VBD_CUDA_TRY(cudaMemsetAsync(sc.edge_cur, 0, en * sizeof(int), st));
+    if (T > 0) VBD_CUDA_TRY(cudaMemsetAsync(sc.tv_count, 0, static_cast<size_t>(T) * sizeof(int), st));
+    const float inv_cell = 1.0f / sc.cell;
+    GridArgs g;
+    g.x = sc.cd;
+    g.counters = sc.counters;
+    g.inv_cell = inv_cell;
+    // triangle grid
+    g.elem = sc.tri;
+    g.n = T;
+    g.tri = true;
+    g.mask = sc.tri_mask;
+    g.cnt = sc.tri_cnt;
+    g.off = sc.tri_off;
+    g.cur = sc.tri_cur;
+    g.items = sc.tri_items;
+    g.cap = sc.tri_items_cap;
+    if (T > 0) {
+        grid_count_kernel<<<(T + 255) / 256, 256, 0, st>>>(g);
+        VBD_CUDA_TRY(cudaGetLastError());
+        size_t bytes = sc.scan_bytes;
+        VBD_CUDA_TRY(cub::DeviceScan::ExclusiveSum(sc.scan_tmp, bytes, sc.tri_cnt, sc.tri_off, static_cast<int>(tn), st));
+        grid_fill_kernel<<<(T + 255) / 256, 256, 0, st>>>(g);
+        VBD_CUDA_TRY(cudaGetLastError());
+    }
+    // edge grid
+    g.elem = sc.edge;
+    g.n = E;
+    g.tri = false;
+    g.mask = sc.edge_mask;
+    g.cnt = sc.edge_cnt;
+    g.off = sc.edge_off;
+    g.cur = sc.edge_cur;
+    g.items = sc.edge_items;
+    g.cap = sc.edge_items_cap;
+    if (E > 0) {
+        grid_count_kernel<<<(E + 255) / 256, 256, 0, st>>>(g);
+        VBD_CUDA_TRY(cudaGetLastError());
+        size_t bytes = sc.scan_bytes;
+        VBD_CUDA_TRY(cub::DeviceScan::ExclusiveSum(sc.scan_tmp, bytes, sc.edge_cnt, sc.edge_off, static_cast<int>(en), st));
+        grid_fill_kernel<<<(E + 255) / 256, 256, 0, st>>>(g);
+        VBD_CUDA_TRY(cudaGetLastError());
+    }
+    QueryArgs q;
+    q.x = sc.cd;
+    q.vworld = sc.vworld;
+    q.rest = sc.rest;
+    q.tri = sc.tri;
+    q.edge = sc.edge;
+    q.near_off = sc.near_off;
+    q.near = sc.near;
+    q.V = V;
+    q.T = T;
+    q.E = E;
+    q.margin = sc.p.margin;
+    q.inv_cell = inv_cell;
+    q.par_eps = sc.p.edge_parallel_epsilon;
+    q.rest_excl = sc.p.rest_exclusion_radius;
+    q.tri_mask = sc.tri_mask;
+    q.edge_mask = sc.edge_mask;
+    q.tri_cnt = sc.tri_cnt;
+    q.tri_off = sc.tri_off;
+    q.tri_items = sc.tri_items;
+    q.edge_cnt = sc.edge_cnt;
+    q.edge_off = sc.edge_off;
+    q.edge_items = sc.edge_items;
+    q.tri_cap = sc.tri_items_cap;
+    q.edge_cap = sc.edge_items_cap;
+    q.vbuf = sc.p.vertex_buffer;
+    q.ebuf = sc.p.edge_buffer;
+    q.vt_count = sc.vt_count;
+    q.vt_list = sc.vt_list;
+    q.ee_count = sc.ee_count;
+    q.ee_list = sc.ee_list;
+    q.counters = sc.counters;
+    if (T > 0) {
+        vt_query_kernel<<<(V + 127) / 128, 128, 0, st>>>(q);
+        VBD_CUDA_TRY(cudaGetLastError());
+        tri_reverse_kernel<<<(V + 255) / 256, 256, 0, st>>>(V, sc.vt_count, sc.vt_list, sc.p.vertex_buffer,
+                                                            sc.tv_count, sc.tv_list, sc.tcap, sc.counters);
+        VBD_CUDA_TRY(cudaGetLastError());
+        tri_sort_kernel<<<(T + 255) / 256, 256, 0, st>>>(T, sc.tv_count, sc.tv_list, sc.tcap);
+        VBD_CUDA_TRY(cudaGetLastError());
+    } else {
+        VBD_CUDA_TRY(cudaMemsetAsync(sc.vt_count, 0, static_cast<size_t>(V) * sizeof(int), st));
+    }
+    if (E > 0) {
+        ee_query_kernel<<<(E + 127) / 128, 128, 0, st>>>(q);
+        VBD_CUDA_TRY(cudaGetLastError());
+    }
+    return VBD_OK;
+}
+
+int self_contact_accumulate(const VbdModelImpl& m, SelfContact& sc, const float4* pos, const float4* prev,
+                            int v_begin, int v_end, float dt, float friction_epsilon, cudaStream_t st) {
+    if (v_end <= v_begin) return VBD_OK;
+    AccumArgs a;
+    a.x = pos;
+    a.x0 = prev;
+    a.tri = sc.tri;
+    a.edge = sc.edge;
+    a.inc_t_off = sc.inc_t_off;
+    a.inc_e_off = sc.inc_e_off;
+    a.inc_t = sc.inc_t;
+    a.inc_e = sc.inc_e;
+    a.vt_count = sc.vt_count;
+    a.vt_list = sc.vt_list;
+    a.ee_count = sc.ee_count;
+    a.ee_list = sc.ee_list;
+    a.tv_count = sc.tv_count;
+    a.tv_list = sc.tv_list;
+    a.vbuf = sc.p.vertex_buffer;
+    a.ebuf = sc.p.edge_buffer;
+    a.tcap = sc.tcap;
+    a.v_begin = v_begin;
+    a.v_end = v_end;
+    a.r = sc.p.radius;
+    a.ke = m.soft_ke;
+    a.kd = m.soft_kd;
+    a.mu = m.soft_mu;
+    a.eps_u = friction_epsilon * dt;
+    a.dt = dt;
+    a.par_eps = sc.p.edge_parallel_epsilon;
+    a.f = sc.sc_f;
+    a.h0 = sc.sc_h0;
+    a.h1 = sc.sc_h1;
+    const int n = v_end - v_begin;
+    accumulate_kernel<<<(n + 127) / 128, 128, 0, st>>>(a);
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+int self_contact_truncate(const VbdModelImpl& m, SelfContact& sc, float4* pos, float4* disp, cudaStream_t st) {
+    const int V = m.V;
+    if (V == 0) return VBD_OK;
+    TruncArgs a;
+    a.cd = sc.cd;
+    a.disp = disp;
+    a.tri = sc.tri;
+    a.edge = sc.edge;
+    a.vt_count = sc.vt_count;
+    a.vt_list = sc.vt_list;
+    a.ee_count = sc.ee_count;
+    a.ee_list = sc.ee_list;
+    a.V = V;
+    a.E = m.E;
+    a.vbuf = sc.p.vertex_buffer;
+    a.ebuf = sc.p.edge_buffer;
+    a.eps = sc.p.edge_parallel_epsilon;
+    a.gamma = sc.p.relaxation;
+    a.ts = sc.ts;
+    const int n = std::max(V, m.E);
+    planar_kernel<<<(n + 127) / 128, 128, 0, st>>>(a);
+    VBD_CUDA_TRY(cudaGetLastError());
+    apply_truncation_kernel<<<(V + 255) / 256, 256, 0, st>>>(V, sc.cd, disp, pos, sc.ts, sc.max_disp);
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+}  // namespace vbd

@@ -24,6 +24,7 @@
 #include "vbd_internal.h"
 #include "vbd_math.cuh"
 #include "vbd_resident.h"
+#include "vbd_self_contact.h"
 
 namespace vbd {
 
@@ -75,6 +76,8 @@ struct SolverImpl {
     int ws_iterations = 0;
     float* ws_corr = nullptr;        // [V][3] previous step's correction x_solved - y (model order)
     float* ws_work = nullptr;        // [V][70] features, prediction, displacement
+    // particle self-contact (particle_enable_self_contact)
+    SelfContact sc;
 };
 
 }  // namespace vbd
@@ -174,6 +177,10 @@ struct SweepArgs {
     const float* c_body_vel;
     const float* c_normal;
     const DevShape* shapes;
+    // self-contact force / Hessian of the vertex (NULL without self-contact)
+    const float4* sc_f;
+    const float4* sc_h0;
+    const float4* sc_h1;
     // constants
     float dt, inv_dt, dt_sqr_recip, eps_u;
     unsigned* status;
@@ -223,6 +230,17 @@ __device__ __forceinline__ void accumulate_contacts(const SweepArgs& a, int i, f
     const DevShape* shapes = a.shapes;
     vertex_contacts(a.ccount, a.cslot, a.K, i, a.c_shape, a.c_body_pos, a.c_body_vel, a.c_normal,
                     [shapes](int s) { return shapes[s].mat; }, x, xp, radius, a.dt, a.eps_u, f, h);
+}
+
+__device__ __forceinline__ void add_self_contact(const SweepArgs& a, int i, float3& f, Sym3& h) {
+    const float4 sf = a.sc_f[i], h0 = a.sc_h0[i], h1 = a.sc_h1[i];
+    f = f + xyz(sf);
+    h.xx += h0.x;
+    h.xy += h0.y;
+    h.xz += h0.z;
+    h.yy += h0.w;
+    h.yz += h1.x;
+    h.zz += h1.y;
 }
 
 __device__ __forceinline__ float warp_sum(float v, int L) {
@@ -278,6 +296,7 @@ __global__ void __launch_bounds__(256) sweep_kernel(SweepArgs a) {
     float3 fc = f3(0.f, 0.f, 0.f);
     Sym3 hc = zero_sym();
     if (a.ccount) accumulate_contacts(a, i, x, xyz(pv), pi.z, fc, hc);
+    if (a.sc_f) add_self_contact(a, i, fc, hc);
     // h_total = h_elastic + m/dt^2 I + h_contact ; f_total = f_elastic + m (y - x)/dt^2 + f_contact
     add_diag(h, mass * a.dt_sqr_recip);
     add(h, hc);
@@ -448,6 +467,7 @@ __global__ void __launch_bounds__(TB) tile_kernel(SweepArgs a) {
     float3 fc = f3(0.f, 0.f, 0.f);
     Sym3 hc = zero_sym();
     if (a.ccount) accumulate_contacts(a, i, xyz(a.pos[i]), xyz(pv), pi.z, fc, hc);
+    if (a.sc_f) add_self_contact(a, i, fc, hc);
     add(h, hc);
     f = f + fc;
     if (kResidual) {
@@ -590,6 +610,13 @@ static SweepArgs make_sweep_args(const SolverImpl& s, const VbdContacts* c, floa
     a.eps_u = s.friction_epsilon * dt;
     a.status = s.status;
     a.write_pos = m.fused_commit ? 1 : 0;
+    if (s.sc.on) {
+        // positions are written by the truncation pass after the color (pos = cd + disp)
+        a.sc_f = s.sc.sc_f;
+        a.sc_h0 = s.sc.sc_h0;
+        a.sc_h1 = s.sc.sc_h1;
+        a.write_pos = 0;
+    }
     a.perm = m.perm;
     a.inv_g = m.gravity_norm > 0.f ? 1.0f / m.gravity_norm : 0.f;
     return a;
@@ -679,6 +706,12 @@ static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float 
     a.v_begin = m.color_start[color];
     a.v_end = m.color_start[color + 1];
     if (a.v_end <= a.v_begin) return;
+    if (s.sc.on) {
+        self_contact_accumulate(m, s.sc, s.pos, s.prev, a.v_begin, a.v_end, dt, s.friction_epsilon, st);
+        launch_sweep(a, s.lanes, m.any_tri_damping || m.any_edge_damping, false, s.block, st);
+        self_contact_truncate(m, s.sc, s.pos, s.disp, st);
+        return;
+    }
     launch_sweep(a, s.lanes, m.any_tri_damping || m.any_edge_damping, false, s.block, st);
     if (!m.fused_commit) {
         const int n = a.v_end - a.v_begin;
@@ -699,6 +732,15 @@ static void enqueue_finalize(SolverImpl& s, float* q_in, float* q_out, float* qd
     a.V = m.V;
     a.dt = dt;
     if (m.V > 0) finalize_kernel<<<(m.V + 255) / 256, 256, 0, st>>>(a);
+}
+
+// Self-contact at the step start, after the forward pass: detection at the step's input
+// positions (x_prev, which becomes pos_prev_collision_detection) and the first truncation of the
+// forward displacement (solver_vbd.py:2065-2100).
+static int self_contact_start(SolverImpl& s, cudaStream_t st) {
+    int rc = self_contact_detect(*s.m, s.sc, s.prev, s.disp, false, st);
+    if (!rc) rc = self_contact_truncate(*s.m, s.sc, s.pos, s.disp, st);
+    return rc;
 }
 
 static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const float* f_ext, float* q_out,
@@ -750,6 +792,16 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
         L.spin_limit = s.spin_limit;
         return resident_enqueue(m, s.resident, L, st);
     }
+    if (s.sc.on) {
+        int rc = self_contact_start(s, st);
+        for (int it = 0; it < iterations && !rc; ++it) {
+            if (self_contact_detect_now(s.sc, it)) rc = self_contact_detect(*s.m, s.sc, s.pos, s.disp, true, st);
+            for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st);
+        }
+        if (rc) return rc;
+        enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
+        return VBD_OK;
+    }
     for (int it = 0; it < iterations; ++it)
         for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st);
     enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
@@ -758,6 +810,7 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
 
 static void free_solver(SolverImpl& s) {
     resident_free(s.resident);
+    self_contact_free(s.sc);
     if (s.ws_corr) cudaFree(s.ws_corr);
     if (s.ws_work) cudaFree(s.ws_work);
     s.ws_corr = s.ws_work = nullptr;
@@ -819,6 +872,10 @@ extern "C" int vbd_solver_create(const VbdModel* model, const VbdSolverOptions* 
         if (options->contacts_per_vertex) s.K = options->contacts_per_vertex;
         s.use_graph = options->use_graph != 0;
         s.resident_on = options->step_kernel == 1;
+        if (options->self_contact && s.resident_on) {
+            delete h;
+            return fail(VBD_ERR_UNSUPPORTED, "vbd_solver_create: the resident step kernel has no self-contact");
+        }
     }
     if (const char* why = launch_shape_error(s.lanes, s.block)) {
         delete h;
@@ -849,6 +906,19 @@ extern "C" int vbd_solver_create(const VbdModel* model, const VbdSolverOptions* 
         if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamCreateWithFlags");
     }
     if (!rc && s.resident_on) rc = resident_build(m, s.resident);
+    if (!rc && options && options->self_contact && m.V > 0) {
+        SelfContactParams p;
+        p.radius = options->self_contact_radius;
+        p.margin = options->self_contact_margin;
+        p.relaxation = options->conservative_bound_relaxation;
+        p.edge_parallel_epsilon = options->edge_parallel_epsilon;
+        p.rest_exclusion_radius = options->rest_exclusion_radius;
+        p.vertex_buffer = options->vertex_contact_buffer_size;
+        p.edge_buffer = options->edge_contact_buffer_size;
+        p.interval = options->collision_detection_interval;
+        p.filter_threshold = options->topological_filter_threshold;
+        rc = self_contact_create(m, p, s.sc);
+    }
     if (rc) {
         free_solver(s);
         delete h;
@@ -955,6 +1025,52 @@ extern "C" int vbd_forward(VbdSolver* solver, const float* q_in, const float* qd
     VBD_CUDA_TRY(cudaMemsetAsync(s.ccount, 0, sizeof(int) * static_cast<size_t>(s.m->V), st));
     enqueue_forward(s, q_in, qd_in, f_ext, contacts, dt, st);
     VBD_CUDA_TRY(cudaGetLastError());
+    if (s.sc.on) return self_contact_start(s, st);
+    return VBD_OK;
+}
+
+extern "C" int vbd_begin_iteration(VbdSolver* solver, int32_t iteration, void* stream) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_begin_iteration: solver is NULL");
+    SolverImpl& s = solver->s;
+    if (iteration < 0) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_begin_iteration: iteration must be >= 0");
+    if (s.m->V == 0 || !self_contact_detect_now(s.sc, iteration)) return VBD_OK;
+    return self_contact_detect(*s.m, s.sc, s.pos, s.disp, true, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int vbd_self_contact_detect(VbdSolver* solver, const float* particle_q, void* stream) {
+    if (!solver || !particle_q) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_self_contact_detect: NULL argument");
+    SolverImpl& s = solver->s;
+    if (!s.sc.on) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_self_contact_detect: self-contact is not enabled");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = self_contact_load_positions(*s.m, s.sc, particle_q, st);
+    if (!rc) rc = self_contact_detect(*s.m, s.sc, s.sc.cd, nullptr, false, st);
+    return rc;
+}
+
+extern "C" int vbd_self_contact_lists(VbdSolver* solver, int32_t* vt_counts, int32_t* vt_lists, int32_t* ee_counts,
+                                      int32_t* ee_lists) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_self_contact_lists: solver is NULL");
+    SolverImpl& s = solver->s;
+    if (!s.sc.on) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_self_contact_lists: self-contact is not enabled");
+    const VbdModelImpl& m = *s.m;
+    const int V = m.V, E = m.E, vb = s.sc.p.vertex_buffer, eb = s.sc.p.edge_buffer;
+    VBD_CUDA_TRY(cudaDeviceSynchronize());
+    std::vector<int> vc(V), vl(static_cast<size_t>(V) * vb), ec(E), el(static_cast<size_t>(E) * eb);
+    if (V) VBD_CUDA_TRY(cudaMemcpy(vc.data(), s.sc.vt_count, vc.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    if (V) VBD_CUDA_TRY(cudaMemcpy(vl.data(), s.sc.vt_list, vl.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    if (E) VBD_CUDA_TRY(cudaMemcpy(ec.data(), s.sc.ee_count, ec.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    if (E) VBD_CUDA_TRY(cudaMemcpy(el.data(), s.sc.ee_list, el.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < V; ++i) {
+        const int o = m.perm_host[i];
+        if (vt_counts) vt_counts[o] = vc[i];
+        if (vt_lists)
+            for (int k = 0; k < vb; ++k) vt_lists[static_cast<size_t>(o) * vb + k] = k < vc[i] ? vl[static_cast<size_t>(i) * vb + k] : -1;
+    }
+    for (int e = 0; e < E; ++e) {
+        if (ee_counts) ee_counts[e] = ec[e];
+        if (ee_lists)
+            for (int k = 0; k < eb; ++k) ee_lists[static_cast<size_t>(e) * eb + k] = k < ec[e] ? el[static_cast<size_t>(e) * eb + k] : -1;
+    }
     return VBD_OK;
 }
 
@@ -1010,6 +1126,7 @@ extern "C" int vbd_set_warm_start(VbdSolver* solver, const float* params, const 
     }
     if (!w16 || iterations < 0 || ((mean == nullptr) != (inv_std == nullptr)))
         return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_warm_start: bad arguments");
+    if (s.sc.on) return fail(VBD_ERR_UNSUPPORTED, "vbd_set_warm_start: not available with self-contact");
     const size_t V = static_cast<size_t>(s.m->V);
     if (!s.ws_corr) {
         VBD_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&s.ws_corr), std::max<size_t>(V, 1) * 3 * sizeof(float)));
@@ -1071,6 +1188,10 @@ extern "C" int vbd_residual(VbdSolver* solver, const VbdContacts* contacts, floa
     float* mx = max_out ? max_out : s.resid_max;
     VBD_CUDA_TRY(cudaMemsetAsync(mx, 0, sizeof(float), st));
     if (per_vertex_out && m.V > m.swept) VBD_CUDA_TRY(cudaMemsetAsync(per_vertex_out, 0, sizeof(float) * m.V, st));
+    if (s.sc.on) {
+        const int rc = self_contact_accumulate(m, s.sc, s.pos, s.prev, 0, m.swept, dt, s.friction_epsilon, st);
+        if (rc) return rc;
+    }
     SweepArgs a = make_sweep_args(s, contacts, dt);
     a.v_begin = 0;
     a.v_end = m.swept;
@@ -1092,8 +1213,16 @@ extern "C" int vbd_status(VbdSolver* solver, VbdStatus* out, int32_t reset) {
     out->singular_blocks = static_cast<int32_t>(h[kSingular]);
     out->contact_overflow = static_cast<int32_t>(h[kOverflow]);
     out->timeouts = static_cast<int32_t>(h[kTimeout]);
+    out->self_contact_overflow = 0;
+    out->reserved = 0;
+    if (s.sc.on) {
+        unsigned c[kScCounters];
+        VBD_CUDA_TRY(cudaMemcpy(c, s.sc.counters, sizeof(c), cudaMemcpyDeviceToHost));
+        for (unsigned v : c) out->self_contact_overflow += static_cast<int32_t>(v);
+    }
     if (reset) {
         VBD_CUDA_TRY(cudaMemset(s.status, 0, sizeof(h)));
+        if (s.sc.on) VBD_CUDA_TRY(cudaMemset(s.sc.counters, 0, kScCounters * sizeof(unsigned)));
         s.steps = 0;
     }
     return VBD_OK;

@@ -36,7 +36,16 @@ class SolverVBD(SolverBase):
         particle_enable_self_contact: bool = False,
         particle_self_contact_radius: float = 0.2,
         particle_self_contact_margin: float = 0.2,
+        particle_conservative_bound_relaxation: float = 0.85,
+        particle_vertex_contact_buffer_size: int = 32,
+        particle_edge_contact_buffer_size: int = 64,
+        particle_collision_detection_interval: int = 0,
+        particle_edge_parallel_epsilon: float = 1e-5,
         particle_enable_tile_solve: bool = True,
+        particle_topological_contact_filter_threshold: int = 2,
+        particle_rest_shape_contact_exclusion_radius: float = 0.0,
+        particle_external_vertex_contact_filtering_map: dict | None = None,
+        particle_external_edge_contact_filtering_map: dict | None = None,
         lanes_per_vertex: int = 0,
         block_size: int = 0,
         contacts_per_vertex: int = 4,
@@ -51,6 +60,12 @@ class SolverVBD(SolverBase):
         self.particle_self_contact_radius = particle_self_contact_radius
         self.particle_self_contact_margin = particle_self_contact_margin
         self.particle_enable_tile_solve = particle_enable_tile_solve
+        self.particle_conservative_bound_relaxation = particle_conservative_bound_relaxation
+        self.particle_collision_detection_interval = particle_collision_detection_interval
+        self.particle_topological_contact_filter_threshold = particle_topological_contact_filter_threshold
+        self.particle_rest_shape_contact_exclusion_radius = particle_rest_shape_contact_exclusion_radius
+        self._sc_buffers = (int(particle_vertex_contact_buffer_size), int(particle_edge_contact_buffer_size))
+        self._iteration = 0
         self._handle = None
         if model.particle_count == 0:
             return
@@ -61,7 +76,8 @@ class SolverVBD(SolverBase):
                     "missing contacts and cause instability.\nIt is advisable to make particle_self_contact_margin "
                     "1.5-2 times larger than particle_self_contact_radius."
                 )
-            raise NotImplementedError("particle self-contact is not available in this build of the B200 VBD solver")
+            if particle_external_vertex_contact_filtering_map or particle_external_edge_contact_filtering_map:
+                raise NotImplementedError("external self-contact filtering maps are not supported by this solver")
         if len(model.particle_color_groups) == 0:
             raise ValueError(
                 "model.particle_color_groups is empty! When using the SolverVBD you must call ModelBuilder.color() "
@@ -79,6 +95,17 @@ class SolverVBD(SolverBase):
         opts.contacts_per_vertex = int(contacts_per_vertex)
         opts.use_graph = 1 if use_cuda_graph else 0
         opts.step_kernel = 1 if resident_step else 0
+        if particle_enable_self_contact:
+            opts.self_contact = 1
+            opts.self_contact_radius = float(particle_self_contact_radius)
+            opts.self_contact_margin = float(particle_self_contact_margin)
+            opts.conservative_bound_relaxation = float(particle_conservative_bound_relaxation)
+            opts.vertex_contact_buffer_size = int(particle_vertex_contact_buffer_size)
+            opts.edge_contact_buffer_size = int(particle_edge_contact_buffer_size)
+            opts.collision_detection_interval = int(particle_collision_detection_interval)
+            opts.edge_parallel_epsilon = float(particle_edge_parallel_epsilon)
+            opts.topological_filter_threshold = int(particle_topological_contact_filter_threshold)
+            opts.rest_exclusion_radius = float(particle_rest_shape_contact_exclusion_radius)
         h = ctypes.c_void_p()
         with torch.cuda.device(model.device):
             _lib.check(self._lib.vbd_solver_create(dm.handle, ctypes.byref(opts), ctypes.byref(h)))
@@ -138,6 +165,7 @@ class SolverVBD(SolverBase):
 
     # ---- staged pieces (parity tests, residual-gated loops) ------------------------------
     def forward(self, state_in: State, contacts: Contacts | None, dt: float) -> None:
+        self._iteration = 0
         _lib.check(
             self._lib.vbd_forward(
                 self._handle,
@@ -154,10 +182,30 @@ class SolverVBD(SolverBase):
         _lib.check(self._lib.vbd_sweep_color(self._handle, int(color), self._contacts(contacts), ctypes.c_float(dt),
                                              self._stream()))
 
+    def begin_iteration(self) -> None:
+        """Start the next iteration of a staged step (self-contact detection when it is scheduled)."""
+        _lib.check(self._lib.vbd_begin_iteration(self._handle, self._iteration, self._stream()))
+        self._iteration += 1
+
     def iterate(self, contacts: Contacts | None, dt: float, iterations: int = 1) -> None:
         for _ in range(iterations):
+            self.begin_iteration()
             for c in range(len(self.model.particle_color_groups)):
                 self.sweep_color(c, contacts, dt)
+
+    def self_contact_detect(self, particle_q: torch.Tensor):
+        """Self-contact candidates at ``particle_q``: (vt_counts [V], vt_lists [V, vertex buffer],
+        ee_counts [E], ee_lists [E, edge buffer]) as numpy arrays, ids ascending, -1 padded."""
+        V, E = self.model.particle_count, self.model.edge_count
+        vb, eb = self._sc_buffers
+        _lib.check(self._lib.vbd_self_contact_detect(self._handle, _lib.ptr(particle_q), self._stream()))
+        vc = np.zeros(V, np.int32)
+        vl = np.zeros((V, vb), np.int32)
+        ec = np.zeros(max(E, 1), np.int32)
+        el = np.zeros((max(E, 1), eb), np.int32)
+        _lib.check(self._lib.vbd_self_contact_lists(self._handle, vc.ctypes.data, vl.ctypes.data, ec.ctypes.data,
+                                                    el.ctypes.data))
+        return vc, vl, ec[:E], el[:E]
 
     def finalize(self, state_in: State, state_out: State, dt: float) -> None:
         _lib.check(
@@ -199,6 +247,7 @@ class SolverVBD(SolverBase):
             "singular_blocks": st.singular_blocks,
             "contact_overflow": st.contact_overflow,
             "timeouts": st.timeouts,
+            "self_contact_overflow": st.self_contact_overflow,
         }
 
     def set_launch(self, lanes_per_vertex: int, block_size: int) -> None:

@@ -74,6 +74,22 @@ class OracleModelDesc(ctypes.Structure):
     ]
 
 
+class OracleSelfContact(ctypes.Structure):
+    _fields_ = [
+        ("enabled", ctypes.c_int32),
+        ("radius", ctypes.c_float),
+        ("margin", ctypes.c_float),
+        ("relaxation", ctypes.c_float),
+        ("vertex_buffer", ctypes.c_int32),
+        ("edge_buffer", ctypes.c_int32),
+        ("interval", ctypes.c_int32),
+        ("edge_parallel_epsilon", ctypes.c_float),
+        ("filter_threshold", ctypes.c_int32),
+        ("rest_exclusion_radius", ctypes.c_float),
+        ("rest_q", ctypes.POINTER(ctypes.c_float)),
+    ]
+
+
 def load():
     global _lib
     if _lib is None:
@@ -104,6 +120,18 @@ def load():
         lib.oracle_collide.argtypes = [ctypes.c_int, c_float_p, c_float_p, c_int32_p, c_int32_p, ctypes.c_int,
                                        ctypes.POINTER(OracleShape), ctypes.c_float, ctypes.c_int, c_int32_p, c_int32_p,
                                        c_float_p, c_float_p, c_float_p]
+        lib.oracle_set_self_contact.argtypes = [vp, ctypes.POINTER(OracleSelfContact)]
+        lib.oracle_self_contact_detect.restype = ctypes.c_longlong
+        lib.oracle_self_contact_detect.argtypes = [vp, c_float_p, c_int32_p, c_int32_p, c_int32_p, c_int32_p]
+        lib.oracle_self_contact_norm.argtypes = [ctypes.c_int, d, d, d, c_double_p]
+        lib.oracle_vt_contact.restype = ctypes.c_int
+        lib.oracle_vt_contact.argtypes = [ctypes.c_int, c_double_p, c_double_p, d, d, d, d, d, d, c_double_p,
+                                          c_double_p]
+        lib.oracle_ee_contact.restype = ctypes.c_int
+        lib.oracle_ee_contact.argtypes = [ctypes.c_int, c_double_p, c_double_p, d, d, d, d, d, d, d, c_double_p,
+                                          c_double_p]
+        lib.oracle_closest_edge_edge.argtypes = [c_double_p, d, c_double_p]
+        lib.oracle_triangle_closest_point.argtypes = [c_double_p, c_double_p]
         _lib = lib
     return _lib
 
@@ -204,6 +232,38 @@ class VBDOracle:
         if getattr(self, "_h", None):
             self._lib.oracle_destroy(self._h)
             self._h = None
+
+    def set_self_contact(self, radius: float, margin: float, relaxation: float = 0.85, vertex_buffer: int = 32,
+                         edge_buffer: int = 64, interval: int = 0, edge_parallel_epsilon: float = 1e-5,
+                         filter_threshold: int = 2, rest_exclusion_radius: float = 0.0, rest_q=None,
+                         enabled: bool = True) -> None:
+        """SolverVBD's particle self-contact settings (solver_vbd.py:231-241)."""
+        p = OracleSelfContact()
+        p.enabled = 1 if enabled else 0
+        p.radius, p.margin, p.relaxation = radius, margin, relaxation
+        p.vertex_buffer, p.edge_buffer, p.interval = vertex_buffer, edge_buffer, interval
+        p.edge_parallel_epsilon = edge_parallel_epsilon
+        p.filter_threshold = filter_threshold
+        p.rest_exclusion_radius = rest_exclusion_radius
+        rq = None
+        if rest_q is not None:
+            rq, p.rest_q = _f32(np.asarray(rest_q).reshape(-1, 3))
+        self.sc_buffers = (vertex_buffer, edge_buffer)
+        self._lib.oracle_set_self_contact(self._h, ctypes.byref(p))
+
+    def self_contact_detect(self, q):
+        """Vertex-triangle and edge-edge candidates at q: (vt_counts, vt_lists, ee_counts, ee_lists, dropped)."""
+        vb, eb = self.sc_buffers
+        E = self.model.edge_count
+        vc = np.zeros(self.V, np.int32)
+        vl = np.zeros((self.V, vb), np.int32)
+        ec = np.zeros(E, np.int32)
+        el = np.zeros((max(E, 1), eb), np.int32)
+        qa, pq = _f32(np.asarray(q).reshape(-1, 3))
+        dropped = self._lib.oracle_self_contact_detect(self._h, pq, vc.ctypes.data_as(c_int32_p),
+                                                       vl.ctypes.data_as(c_int32_p), ec.ctypes.data_as(c_int32_p),
+                                                       el.ctypes.data_as(c_int32_p))
+        return vc, vl, ec, el[:E], int(dropped)
 
     def set_threads(self, n: int) -> None:
         self._lib.oracle_set_threads(self._h, int(n))
@@ -320,3 +380,48 @@ def contact(x, x_prev, body_pos, body_vel, normal, radius, margin, ke, kd, mu, f
     arrs = [_f64(np.asarray(v).reshape(3)) for v in (x, x_prev, body_pos, body_vel, normal)]
     return _elem(lib.oracle_contact, 1 if precision == "f64" else 0, *[p for _, p in arrs], float(radius), float(margin),
                  float(ke), float(kd), float(mu), float(friction_epsilon), float(dt))
+
+
+def self_contact_norm(dis, radius, k, precision="f32"):
+    out = np.zeros(2, np.float64)
+    load().oracle_self_contact_norm(1 if precision == "f64" else 0, float(dis), float(radius), float(k),
+                                    out.ctypes.data_as(c_double_p))
+    return out[0], out[1]
+
+
+def vt_contact(pos, anchor, radius, ke, kd, mu, friction_epsilon, dt, precision="f32"):
+    """Vertex-triangle self-contact; pos/anchor rows a, b, c, p.  Returns (has, F[4,3], H[4,3,3])."""
+    p, pp = _f64(np.asarray(pos).reshape(4, 3))
+    a, pa = _f64(np.asarray(anchor).reshape(4, 3))
+    f = np.zeros(12, np.float64)
+    h = np.zeros(36, np.float64)
+    has = load().oracle_vt_contact(1 if precision == "f64" else 0, pp, pa, float(radius), float(ke), float(kd),
+                                   float(mu), float(friction_epsilon), float(dt), f.ctypes.data_as(c_double_p),
+                                   h.ctypes.data_as(c_double_p))
+    return bool(has), f.reshape(4, 3), h.reshape(4, 3, 3)
+
+
+def ee_contact(pos, anchor, radius, ke, kd, mu, friction_epsilon, dt, parallel_epsilon=1e-5, precision="f32"):
+    """Edge-edge self-contact; pos/anchor rows e0, e1, f0, f1.  Returns (has, F[2,3], H[2,3,3]) for e0, e1."""
+    p, pp = _f64(np.asarray(pos).reshape(4, 3))
+    a, pa = _f64(np.asarray(anchor).reshape(4, 3))
+    f = np.zeros(6, np.float64)
+    h = np.zeros(18, np.float64)
+    has = load().oracle_ee_contact(1 if precision == "f64" else 0, pp, pa, float(radius), float(ke), float(kd),
+                                   float(mu), float(friction_epsilon), float(dt), float(parallel_epsilon),
+                                   f.ctypes.data_as(c_double_p), h.ctypes.data_as(c_double_p))
+    return bool(has), f.reshape(2, 3), h.reshape(2, 3, 3)
+
+
+def closest_edge_edge(p1, q1, p2, q2, eps=1e-5):
+    pts, pp = _f64(np.stack([p1, q1, p2, q2]).reshape(12))
+    out = np.zeros(3, np.float64)
+    load().oracle_closest_edge_edge(pp, float(eps), out.ctypes.data_as(c_double_p))
+    return out[0], out[1], out[2]
+
+
+def triangle_closest_point(a, b, c, p):
+    pts, pp = _f64(np.stack([a, b, c, p]).reshape(12))
+    out = np.zeros(6, np.float64)
+    load().oracle_triangle_closest_point(pp, out.ctypes.data_as(c_double_p))
+    return out[:3], out[3:]

@@ -18,11 +18,28 @@
 //   update_velocity             particle_vbd_kernels.py:1468-1471
 //   step orchestration          solver_vbd.py:1774-1825, :2065-2100, :2516-2704, :3158-3169
 //   soft-contact generation     create_soft_contacts geometry/kernels.py:1020-1184 (plane, sphere, box)
+//   self-contact (optional)     detection: vertex_triangle_collision_detection_kernel geometry/kernels.py:1328,
+//                               edge_colliding_edges_detection_kernel :1499, n-ring filters
+//                               solvers/vbd/tri_mesh_collision.py:123-233 (brute force here, all pairs);
+//                               forces: evaluate_self_contact_force_norm particle_vbd_kernels.py:819,
+//                               damp_collision :846, evaluate_edge_edge_contact_2_vertices :990,
+//                               evaluate_vertex_triangle_collision_force_hessian_4_vertices :1195,
+//                               compute_friction :1316; truncation: :1864-2286
+//                               (apply_planar_truncation_parallel_by_collision + apply_truncation_ts);
+//                               orchestration solver_vbd.py:2003-2063, :2540-2545, :3221-3237;
+//                               triangle_closest_point geometry/kernels.py:80-145;
+//                               orthonormal_basis math/__init__.py:236-275.  Warp's builtin
+//                               closest_point_edge_edge (not in the tree) is restated after Ericson,
+//                               Real-Time Collision Detection, 5.1.9.  Per vertex the self-contact
+//                               terms are summed in a fixed order (own vertex-triangle pairs, then
+//                               incident triangles' pairs, then incident edges' pairs); the reference
+//                               adds them with atomics in no fixed order.
 // The 3x3 inverse (Warp's wp.inverse, third-party) is restated as adjugate / determinant.
 //
 // Templated on the scalar: the float instantiation is the FP32 oracle, the double one is the
 // "FP64 re-evaluation" of the same step.  Compiled with -ffp-contract=off so the FP32 result
 // does not depend on whether the host compiler fuses multiply-adds.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -65,6 +82,16 @@ struct OracleModelDesc {
     float gravity[3];
     float soft_contact_ke, soft_contact_kd, soft_contact_mu;
     const OracleShape* shapes;
+};
+
+struct OracleSelfContact {
+    int32_t enabled;
+    float radius, margin, relaxation;
+    int32_t vertex_buffer, edge_buffer, interval;
+    float edge_parallel_epsilon;
+    int32_t filter_threshold;
+    float rest_exclusion_radius;
+    const float* rest_q;  // [3V] rest positions (the exclusion radius is measured there); may be NULL
 };
 
 }  // extern "C"
@@ -437,6 +464,7 @@ struct Oracle {
     std::vector<T> shape_ke, shape_kd, shape_mu;  // mixed per shape (init_body_particle_contacts)
     T g[3] = {0, 0, 0};
     T friction_eps = T(1e-2);
+    float soft_ke = 0.f, soft_kd = 0.f, soft_mu = 0.f;  // model.soft_contact_* (self-contact material)
     // scratch
     std::vector<T> q, q_prev, inertia, disp, pos_prev_cd, pf, ph;
     // contacts (reference record layout, per step)
@@ -444,6 +472,15 @@ struct Oracle {
     std::vector<int32_t> c_particle, c_shape;
     std::vector<T> c_body_pos, c_body_vel, c_normal;
     int threads = 1;
+    int iteration = 0;  // iterations begun since the last forward
+    // self-contact
+    OracleSelfContact sc{};
+    std::vector<T> rest_q;
+    std::vector<int32_t> near_off, near;        // vertices within (threshold-1) rings, sorted, self excluded
+    std::vector<int32_t> vt_count, vt_list;     // per vertex: colliding triangles (ascending), stride vertex_buffer
+    std::vector<int32_t> ee_count, ee_list;     // per edge: colliding edges (ascending), stride edge_buffer
+    std::vector<std::vector<int32_t>> tri_vs;   // per triangle: vertices that collide with it (ascending)
+    long long sc_overflow = 0;
 };
 
 template <typename T>
@@ -499,6 +536,9 @@ void init_oracle(Oracle<T>& o, const OracleModelDesc* d) {
         o.shape_mu[s] = T(mu);
     }
     for (int k = 0; k < 3; ++k) o.g[k] = T(d->gravity[k]);
+    o.soft_ke = d->soft_contact_ke;
+    o.soft_kd = d->soft_contact_kd;
+    o.soft_mu = d->soft_contact_mu;
     o.q.assign(3 * V, T(0));
     o.q_prev = o.q;
     o.inertia = o.q;
@@ -508,12 +548,614 @@ void init_oracle(Oracle<T>& o, const OracleModelDesc* d) {
     o.ph.assign(9 * V, T(0));
 }
 
+// ---- self-contact --------------------------------------------------------------------------
+template <typename T>
+T clamp01(T x) { return x < T(0) ? T(0) : (x > T(1) ? T(1) : x); }
+
+// triangle_closest_point (geometry/kernels.py:80-145): closest point of triangle abc to p and
+// its barycentric coordinates (Ericson's Voronoi-region walk).
+template <typename T>
+V3<T> triangle_closest_point(V3<T> a, V3<T> b, V3<T> c, V3<T> p, V3<T>& bary) {
+    const V3<T> ab = b - a, ac = c - a, ap = p - a;
+    const T d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= T(0) && d2 <= T(0)) {
+        bary = v3(T(1), T(0), T(0));
+        return a;
+    }
+    const V3<T> bp = p - b;
+    const T d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= T(0) && d4 <= d3) {
+        bary = v3(T(0), T(1), T(0));
+        return b;
+    }
+    const V3<T> cp = p - c;
+    const T d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= T(0) && d5 <= d6) {
+        bary = v3(T(0), T(0), T(1));
+        return c;
+    }
+    const T vc = d1 * d4 - d3 * d2;
+    if (vc <= T(0) && d1 >= T(0) && d3 <= T(0)) {
+        const T v = d1 / (d1 - d3);
+        bary = v3(T(1) - v, v, T(0));
+        return a + v * ab;
+    }
+    const T vb = d5 * d2 - d1 * d6;
+    if (vb <= T(0) && d2 >= T(0) && d6 <= T(0)) {
+        const T v = d2 / (d2 - d6);
+        bary = v3(T(1) - v, T(0), v);
+        return a + v * ac;
+    }
+    const T va = d3 * d6 - d5 * d4;
+    if (va <= T(0) && (d4 - d3) >= T(0) && (d5 - d6) >= T(0)) {
+        const T v = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        bary = v3(T(0), T(1) - v, v);
+        return b + v * (c - b);
+    }
+    const T denom = T(1) / (va + vb + vc);
+    const T v = vb * denom, w = vc * denom;
+    bary = v3(T(1) - v - w, v, w);
+    return a + v * ab + w * ac;
+}
+
+// Closest points of segments p1q1 and p2q2 (Ericson, Real-Time Collision Detection, 5.1.9):
+// s, t along the segments and the distance between the two points.  eps bounds degenerate
+// (point-like) segments; parallel segments (zero denominator) take s = 0.
+template <typename T>
+void closest_edge_edge(V3<T> p1, V3<T> q1, V3<T> p2, V3<T> q2, T eps, T& s, T& t, T& dist) {
+    const V3<T> d1 = q1 - p1, d2 = q2 - p2, r = p1 - p2;
+    const T a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+    if (a <= eps && e <= eps) {
+        s = t = T(0);
+    } else if (a <= eps) {
+        s = T(0);
+        t = clamp01(f / e);
+    } else {
+        const T c = dot(d1, r);
+        if (e <= eps) {
+            t = T(0);
+            s = clamp01(-c / a);
+        } else {
+            const T b = dot(d1, d2);
+            const T denom = a * e - b * b;
+            s = denom != T(0) ? clamp01((b * f - c * e) / denom) : T(0);
+            t = (b * s + f) / e;
+            if (t < T(0)) {
+                t = T(0);
+                s = clamp01(-c / a);
+            } else if (t > T(1)) {
+                t = T(1);
+                s = clamp01((b - c) / a);
+            }
+        }
+    }
+    dist = len((p1 + d1 * s) - (p2 + d2 * t));
+}
+
+// orthonormal_basis (math/__init__.py:236-275)
+template <typename T>
+void orthonormal_basis(V3<T> n, V3<T>& b1, V3<T>& b2) {
+    if (n.z < T(0)) {
+        const T a = T(1) / (T(1) - n.z);
+        const T b = n.x * n.y * a;
+        b1 = v3(T(1) - n.x * n.x * a, -b, n.x);
+        b2 = v3(b, n.y * n.y * a - T(1), -n.y);
+    } else {
+        const T a = T(1) / (T(1) + n.z);
+        const T b = -n.x * n.y * a;
+        b1 = v3(T(1) - n.x * n.x * a, b, -n.x);
+        b2 = v3(b, T(1) - n.y * n.y * a, -n.y);
+    }
+}
+
+// evaluate_self_contact_force_norm (particle_vbd_kernels.py:819-845): linear penalty for
+// d in [tau, r), log barrier in (1e-5, tau), its quadratic Taylor extension below 1e-5.
+template <typename T>
+void self_contact_norm(T dis, T r, T k, T& dEdD, T& d2E) {
+    const T pen = r - dis;
+    const T tau = r * T(0.5);
+    const T d_min = T(1.0e-5);
+    if (tau > dis && dis > d_min) {
+        const T k2 = tau * tau * k;
+        dEdD = -k2 / dis;
+        d2E = k2 / (dis * dis);
+    } else if (dis <= d_min) {
+        const T k2 = tau * tau * k;
+        const T d_min_sq = d_min * d_min;
+        dEdD = k2 * (dis - T(2) * d_min) / d_min_sq;
+        d2E = k2 / d_min_sq;
+    } else {
+        dEdD = -k * pen;
+        d2E = k;
+    }
+}
+
+// compute_friction (:1316-1345): IPC-smoothed friction in the tangent frame T = [b1 b2]
+template <typename T>
+void ipc_friction(T mu, T fn, V3<T> b1, V3<T> b2, T u0, T u1, T eps_u, V3<T>& f, M3<T>& H) {
+    const T un = std::sqrt(u0 * u0 + u1 * u1);
+    f = v3(T(0), T(0), T(0));
+    H = zero3<T>();
+    if (!(un > T(0))) return;
+    const T f1 = un > eps_u ? T(1) / un : (-un / eps_u + T(2)) / eps_u;
+    const T sf = -mu * fn;
+    const T w0 = f1 * u0, w1 = f1 * u1;
+    const T Tm[3][2] = {{b1.x, b2.x}, {b1.y, b2.y}, {b1.z, b2.z}};
+    T fv[3];
+    for (int i = 0; i < 3; ++i) fv[i] = (sf * Tm[i][0]) * w0 + (sf * Tm[i][1]) * w1;
+    f = v3(fv[0], fv[1], fv[2]);
+    const T sh = mu * fn;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) H.m[i][j] = ((sh * Tm[i][0]) * f1) * Tm[j][0] + ((sh * Tm[i][1]) * f1) * Tm[j][1];
+}
+
+// damp_collision (:846-858): damping on the contact's gap rate, only while the gap closes
+template <typename T>
+void damp_collision(T gap_rate, T b, V3<T> n, T kd, T dt, V3<T>& f, M3<T>& H) {
+    if (gap_rate < T(-1.0e-6)) {
+        f = ((-kd * gap_rate) * b) * n;
+        H = (((kd / dt) * b) * b) * outer(n, n);
+    } else {
+        f = v3(T(0), T(0), T(0));
+        H = zero3<T>();
+    }
+}
+
+// evaluate_vertex_triangle_collision_force_hessian_4_vertices (:1195-1313): vertex p against
+// triangle (a, b, c); outputs for a, b, c, p (indices 0..3).
+template <typename T>
+bool vt_contact(V3<T> a, V3<T> b, V3<T> c, V3<T> p, V3<T> a0, V3<T> b0, V3<T> c0, V3<T> p0, T r, T ke, T kd, T mu,
+                T feps, T dt, V3<T> F[4], M3<T> H[4]) {
+    V3<T> bary;
+    const V3<T> cp = triangle_closest_point(a, b, c, p, bary);
+    const V3<T> diff = p - cp;
+    const T dis = len(diff);
+    const V3<T> n = diff / dis;
+    if (!(T(0) < dis && dis < r)) return false;
+    const T bs[4] = {-bary.x, -bary.y, -bary.z, T(1)};
+    T dEdD, d2E;
+    self_contact_norm(dis, r, ke, dEdD, d2E);
+    const V3<T> cf = (-dEdD) * n;
+    const M3<T> ch = d2E * outer(n, n);
+    const V3<T> dxv = p - p0;
+    const V3<T> cprev = bary.x * a0 + bary.y * b0 + bary.z * c0;
+    const V3<T> dx = dxv - (cp - cprev);
+    V3<T> b1, b2;
+    orthonormal_basis(n, b1, b2);
+    V3<T> ff;
+    M3<T> fh;
+    ipc_friction(mu, -dEdD, b1, b2, dot(b1, dx), dot(b2, dx), feps * dt, ff, fh);
+    const T gap_rate = dot(n, dx) / dt;
+    for (int k = 0; k < 4; ++k) {
+        F[k] = cf * bs[k];
+        H[k] = bs[k] * (bs[k] * ch);
+        V3<T> df;
+        M3<T> dh;
+        damp_collision(gap_rate, bs[k], n, kd, dt, df, dh);
+        F[k] = F[k] + (df + bs[k] * ff);
+        H[k] = H[k] + (dh + (bs[k] * bs[k]) * fh);
+    }
+    return true;
+}
+
+// evaluate_edge_edge_contact_2_vertices (:990-1106): edge (e0, e1) against edge (f0, f1);
+// outputs for e0, e1.
+template <typename T>
+bool ee_contact(V3<T> e0, V3<T> e1, V3<T> f0, V3<T> f1, V3<T> e0a, V3<T> e1a, V3<T> f0a, V3<T> f1a, T r, T ke, T kd,
+                T mu, T feps, T dt, T par_eps, V3<T> F[2], M3<T> H[2]) {
+    T s, t, dis;
+    closest_edge_edge(e0, e1, f0, f1, par_eps, s, t, dis);
+    const V3<T> c1 = e0 + (e1 - e0) * s, c2 = f0 + (f1 - f0) * t;
+    const V3<T> n = (c1 - c2) / dis;
+    if (!(T(0) < dis && dis < r)) return false;
+    const T bs[2] = {T(1) - s, s};
+    T dEdD, d2E;
+    self_contact_norm(dis, r, ke, dEdD, d2E);
+    const V3<T> cf = (-dEdD) * n;
+    const M3<T> ch = d2E * outer(n, n);
+    const V3<T> c1p = e0a + (e1a - e0a) * s, c2p = f0a + (f1a - f0a) * t;
+    const V3<T> dx = (c1 - c1p) - (c2 - c2p);
+    V3<T> b1, b2;
+    orthonormal_basis(n, b1, b2);
+    V3<T> ff;
+    M3<T> fh;
+    ipc_friction(mu, -dEdD, b1, b2, dot(b1, dx), dot(b2, dx), feps * dt, ff, fh);
+    const T gap_rate = dot(n, dx) / dt;
+    for (int k = 0; k < 2; ++k) {
+        F[k] = cf * bs[k];
+        H[k] = bs[k] * (bs[k] * ch);
+        V3<T> df;
+        M3<T> dh;
+        damp_collision(gap_rate, bs[k], n, kd, dt, df, dh);
+        F[k] = F[k] + (df + bs[k] * ff);
+        H[k] = H[k] + (dh + (bs[k] * bs[k]) * fh);
+    }
+    return true;
+}
+
+// segment_plane_intersects (:1865-1887)
+template <typename T>
+bool segment_plane_intersects(V3<T> v, V3<T> dv, V3<T> n, V3<T> d, T eps_par, T eps_near, T eps_far) {
+    const T nv = dot(n, dv);
+    const T num = -dot(n, v - d);
+    if (std::fabs(nv) < eps_par) return false;
+    const T t = num / nv;
+    return t >= eps_near && t <= T(1) + eps_far;
+}
+
+template <typename T>
+V3<T> normalized(V3<T> a) {
+    return a / len(a);
+}
+
+// create_vertex_triangle_division_plane_closest_pt (:1890-1947): plane n.(x - d) = 0 between
+// vertex v and triangle t, n towards the vertex; dummy[k] marks a participant the plane does not
+// stop (order v, t1, t2, t3).  Returns false for a degenerate (touching) pair.
+template <typename T>
+void vt_plane(V3<T> v, V3<T> dv, V3<T> t1, V3<T> dt1, V3<T> t2, V3<T> dt2, V3<T> t3, V3<T> dt3, bool dummy[4],
+              V3<T>& n, V3<T>& d) {
+    V3<T> bary;
+    const V3<T> cp = triangle_closest_point(t1, t2, t3, v, bary);
+    const V3<T> nh = v - cp;
+    if (len(nh) < T(1e-12)) {
+        for (int k = 0; k < 4; ++k) dummy[k] = false;
+        n = v3(T(0), T(0), T(0));
+        d = v;
+        return;
+    }
+    n = normalized(nh);
+    const T dvn = std::max(-dot(n, dv), T(0));
+    const T dtn = std::max(std::max(dot(n, dt1), dot(n, dt2)), std::max(dot(n, dt3), T(0)));
+    if (dtn + dvn == T(0)) {
+        d = cp + T(0.5) * nh;
+    } else {
+        T l = dtn / (dtn + dvn);
+        l = l < T(0.05) ? T(0.05) : (l > T(0.95) ? T(0.95) : l);
+        d = cp + l * nh;
+    }
+    dummy[0] = dvn == T(0) ? true : !segment_plane_intersects(v, dv, n, d, T(1e-6), T(-1e-8), T(1e-8));
+    if (dtn == T(0)) {
+        dummy[1] = dummy[2] = dummy[3] = true;
+    } else {
+        dummy[1] = !segment_plane_intersects(t1, dt1, n, d, T(1e-6), T(-1e-8), T(1e-8));
+        dummy[2] = !segment_plane_intersects(t2, dt2, n, d, T(1e-6), T(-1e-8), T(1e-8));
+        dummy[3] = !segment_plane_intersects(t3, dt3, n, d, T(1e-6), T(-1e-8), T(1e-8));
+    }
+}
+
+// robust_edge_pair_normal (:1951-2016)
+template <typename T>
+V3<T> robust_edge_pair_normal(V3<T> a0, V3<T> a1, V3<T> b0, V3<T> b1) {
+    const T eps = T(1.0e-6);
+    V3<T> d0 = a1 - a0, d1 = b1 - b0;
+    const T l0 = len(d0), l1 = len(d1);
+    d0 = l0 > eps ? d0 / l0 : v3(T(0), T(0), T(0));
+    d1 = l1 > eps ? d1 / l1 : v3(T(0), T(0), T(0));
+    V3<T> n = cross(d0, d1);
+    T ln = len(n);
+    if (ln > eps) return n / ln;
+    V3<T> ref = d0;
+    if (len(ref) <= eps) ref = d1;
+    if (len(ref) <= eps) return v3(T(1), T(0), T(0));
+    const V3<T> bridge = T(0.5) * ((b0 + b1) - (a0 + a1));
+    const T bl = len(bridge);
+    if (bl > eps) {
+        n = cross(ref, bridge / bl);
+        ln = len(n);
+        if (ln > eps) return n / ln;
+    }
+    V3<T> axis = v3(T(1), T(0), T(0));
+    if (std::fabs(dot(ref, axis)) > T(0.9)) axis = v3(T(0), T(1), T(0));
+    n = cross(ref, axis);
+    ln = len(n);
+    if (ln > eps) return n / ln;
+    n = cross(ref, v3(T(0), T(0), T(1)));
+    ln = len(n);
+    if (ln > eps) return n / ln;
+    return v3(T(1), T(0), T(0));
+}
+
+// create_edge_edge_division_plane_closest_pt (:2020-2090); order e0v0, e0v1, e1v0, e1v1
+template <typename T>
+void ee_plane(V3<T> a0, V3<T> da0, V3<T> a1, V3<T> da1, V3<T> b0, V3<T> db0, V3<T> b1, V3<T> db1, bool dummy[4],
+              V3<T>& n, V3<T>& d) {
+    T s, t, dist;
+    closest_edge_edge(a0, a1, b0, b1, T(1e-6), s, t, dist);
+    const V3<T> c1 = a0 + (a1 - a0) * s, c2 = b0 + (b1 - b0) * t;
+    const V3<T> nh = c1 - c2;
+    if (len(nh) < T(1e-12)) {
+        for (int k = 0; k < 4; ++k) dummy[k] = false;
+        n = robust_edge_pair_normal(a0, a1, b0, b1);
+        d = c1 * T(0.5) + c2 * T(0.5);
+        return;
+    }
+    n = normalized(nh);
+    const T de0 = std::max(std::max(-dot(n, da0), -dot(n, da1)), T(0));
+    const T de1 = std::max(std::max(dot(n, db0), dot(n, db1)), T(0));
+    if (de0 + de1 == T(0)) {
+        d = c2 + T(0.5) * nh;
+    } else {
+        T l = de1 / (de1 + de0);
+        l = l < T(0.05) ? T(0.05) : (l > T(0.95) ? T(0.95) : l);
+        d = c2 + l * nh;
+    }
+    if (de0 == T(0)) {
+        dummy[0] = dummy[1] = true;
+    } else {
+        dummy[0] = !segment_plane_intersects(a0, da0, n, d, T(1e-6), T(-1e-8), T(1e-6));
+        dummy[1] = !segment_plane_intersects(a1, da1, n, d, T(1e-6), T(-1e-8), T(1e-6));
+    }
+    if (de1 == T(0)) {
+        dummy[2] = dummy[3] = true;
+    } else {
+        dummy[2] = !segment_plane_intersects(b0, db0, n, d, T(1e-6), T(-1e-8), T(1e-6));
+        dummy[3] = !segment_plane_intersects(b1, db1, n, d, T(1e-6), T(-1e-8), T(1e-6));
+    }
+}
+
+// planar_truncation_t (:2114-2130)
+template <typename T>
+T planar_truncation_t(V3<T> v, V3<T> dv, V3<T> n, V3<T> d, T eps, T gamma) {
+    const T denom = dot(n, dv);
+    if (std::fabs(denom) < eps) return T(1);
+    T t = dot(n, d - v) / denom;
+    if (t < T(0)) return T(1);
+    t = std::min(t * gamma, t - T(1e-3));
+    return clamp01(t);
+}
+
+template <typename T>
+bool sorted_contains(const int32_t* b, const int32_t* e, int32_t x) {
+    const int32_t* it = std::lower_bound(b, e, x);
+    return it != e && *it == x;
+}
+
+// vertices within (threshold - 1) edge rings of each vertex, itself excluded (the n-ring filter,
+// tri_mesh_collision.py:123-233): a triangle with a vertex in that set, or an edge with an
+// endpoint in the union of its endpoints' sets, is not a contact candidate.
+template <typename T>
+void build_near_sets(Oracle<T>& o) {
+    const int V = o.V;
+    std::vector<std::vector<int32_t>> ring1(V);
+    for (int e = 0; e < o.E; ++e) {
+        const int a = o.edges[4 * e + 2], b = o.edges[4 * e + 3];
+        ring1[a].push_back(b);
+        ring1[b].push_back(a);
+    }
+    for (auto& r : ring1) {
+        std::sort(r.begin(), r.end());
+        r.erase(std::unique(r.begin(), r.end()), r.end());
+    }
+    const int depth = o.sc.filter_threshold - 1;
+    o.near_off.assign(V + 1, 0);
+    o.near.clear();
+    for (int v = 0; v < V; ++v) {
+        std::vector<int32_t> seen{v}, frontier{v};
+        for (int k = 0; k < depth; ++k) {
+            std::vector<int32_t> next;
+            for (int u : frontier)
+                for (int w : ring1[u])
+                    if (std::find(seen.begin(), seen.end(), w) == seen.end()) {
+                        seen.push_back(w);
+                        next.push_back(w);
+                    }
+            frontier.swap(next);
+            if (frontier.empty()) break;
+        }
+        std::sort(seen.begin(), seen.end());
+        for (int w : seen)
+            if (w != v) o.near.push_back(w);
+        o.near_off[v + 1] = static_cast<int32_t>(o.near.size());
+    }
+}
+
+template <typename T>
+bool near_contains(const Oracle<T>& o, int v, int x) {
+    if (o.sc.filter_threshold < 2) return false;
+    return sorted_contains<T>(o.near.data() + o.near_off[v], o.near.data() + o.near_off[v + 1], x);
+}
+
+// vertex-triangle and edge-edge candidates within the margin at positions q (all pairs)
+template <typename T>
+void detect_self_contacts(Oracle<T>& o, const std::vector<T>& q) {
+    const int V = o.V, Tn = o.Tn, E = o.E;
+    const int vb = o.sc.vertex_buffer, eb = o.sc.edge_buffer;
+    const T margin = T(o.sc.margin);
+    const T excl = T(o.sc.rest_exclusion_radius);
+    const bool use_rest = excl > T(0) && !o.rest_q.empty();
+    o.vt_count.assign(V, 0);
+    o.vt_list.assign(static_cast<size_t>(V) * vb, -1);
+    o.ee_count.assign(E, 0);
+    o.ee_list.assign(static_cast<size_t>(E) * eb, -1);
+    o.tri_vs.assign(Tn, {});
+#pragma omp parallel for schedule(dynamic, 64) num_threads(o.threads) if (o.threads > 1)
+    for (int v = 0; v < V; ++v) {
+        const V3<T> p = load3(q.data(), v);
+        const int wv = o.world[v];
+        int n = 0;
+        long long over = 0;
+        for (int t = 0; t < Tn; ++t) {
+            const int a = o.tri[3 * t], b = o.tri[3 * t + 1], c = o.tri[3 * t + 2];
+            if (a == v || b == v || c == v) continue;
+            const int wt = o.world[a];
+            if (wv >= 0 && wt >= 0 && wv != wt) continue;
+            if (near_contains(o, v, a) || near_contains(o, v, b) || near_contains(o, v, c)) continue;
+            V3<T> bary;
+            const T dist = len(triangle_closest_point(load3(q.data(), a), load3(q.data(), b), load3(q.data(), c), p, bary) - p);
+            if (use_rest) {
+                const T dr = len(triangle_closest_point(load3(o.rest_q.data(), a), load3(o.rest_q.data(), b),
+                                                        load3(o.rest_q.data(), c), load3(o.rest_q.data(), v), bary) -
+                                 load3(o.rest_q.data(), v));
+                if (dr < excl) continue;
+            }
+            if (dist < margin) {
+                if (n < vb) o.vt_list[static_cast<size_t>(v) * vb + n] = t;
+                else ++over;
+                ++n;
+            }
+        }
+        o.vt_count[v] = std::min(n, vb);
+        if (over) {
+#pragma omp atomic
+            o.sc_overflow += over;
+        }
+    }
+#pragma omp parallel for schedule(dynamic, 64) num_threads(o.threads) if (o.threads > 1)
+    for (int e = 0; e < E; ++e) {
+        const int a0 = o.edges[4 * e + 2], a1 = o.edges[4 * e + 3];
+        const V3<T> pa0 = load3(q.data(), a0), pa1 = load3(q.data(), a1);
+        const int we = o.world[a0];
+        int n = 0;
+        long long over = 0;
+        for (int f = 0; f < E; ++f) {
+            const int b0 = o.edges[4 * f + 2], b1 = o.edges[4 * f + 3];
+            if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1) continue;
+            const int wf = o.world[b0];
+            if (we >= 0 && wf >= 0 && we != wf) continue;
+            if (near_contains(o, a0, b0) || near_contains(o, a0, b1) || near_contains(o, a1, b0) ||
+                near_contains(o, a1, b1))
+                continue;
+            T s, t, dist;
+            closest_edge_edge(pa0, pa1, load3(q.data(), b0), load3(q.data(), b1), T(o.sc.edge_parallel_epsilon), s, t,
+                              dist);
+            if (use_rest) {
+                T sr, tr, dr;
+                closest_edge_edge(load3(o.rest_q.data(), a0), load3(o.rest_q.data(), a1), load3(o.rest_q.data(), b0),
+                                  load3(o.rest_q.data(), b1), T(o.sc.edge_parallel_epsilon), sr, tr, dr);
+                if (dr < excl) continue;
+            }
+            if (dist < margin) {
+                if (n < eb) o.ee_list[static_cast<size_t>(e) * eb + n] = f;
+                else ++over;
+                ++n;
+            }
+        }
+        o.ee_count[e] = std::min(n, eb);
+        if (over) {
+#pragma omp atomic
+            o.sc_overflow += over;
+        }
+    }
+    for (int v = 0; v < V; ++v)
+        for (int k = 0; k < o.vt_count[v]; ++k) o.tri_vs[o.vt_list[static_cast<size_t>(v) * o.sc.vertex_buffer + k]].push_back(v);
+}
+
+// self-contact force and Hessian of vertex v (fixed order: own vertex-triangle pairs, then the
+// pairs of each incident triangle in CSR order, then each incident edge's edge-edge pairs)
+template <typename T>
+void self_contact_vertex(const Oracle<T>& o, int v, T ke, T kd, T mu, T dt, V3<T>& f, M3<T>& H) {
+    f = v3(T(0), T(0), T(0));
+    H = zero3<T>();
+    const T r = T(o.sc.radius);
+    const T* q = o.q.data();
+    const T* qa = o.q_prev.data();
+    V3<T> F[4];
+    M3<T> Hk[4];
+    auto vt = [&](int p, int t, int slot) {
+        const int a = o.tri[3 * t], b = o.tri[3 * t + 1], c = o.tri[3 * t + 2];
+        if (vt_contact(load3(q, a), load3(q, b), load3(q, c), load3(q, p), load3(qa, a), load3(qa, b), load3(qa, c),
+                       load3(qa, p), r, ke, kd, mu, o.friction_eps, dt, F, Hk)) {
+            f = f + F[slot];
+            H = H + Hk[slot];
+        }
+    };
+    const size_t vb = o.sc.vertex_buffer;
+    for (int k = 0; k < o.vt_count[v]; ++k) vt(v, o.vt_list[v * vb + k], 3);
+    if (o.Tn > 0)
+        for (int k = o.adj_t_off[v]; k < o.adj_t_off[v + 1]; k += 2) {
+            const int t = o.adj_t[k], slot = o.adj_t[k + 1];
+            for (int p : o.tri_vs[t]) vt(p, t, slot);
+        }
+    if (o.E > 0)
+        for (int k = o.adj_e_off[v]; k < o.adj_e_off[v + 1]; k += 2) {
+            const int e = o.adj_e[k], slot = o.adj_e[k + 1];
+            if (slot < 2) continue;
+            const int a0 = o.edges[4 * e + 2], a1 = o.edges[4 * e + 3];
+            const size_t eb = o.sc.edge_buffer;
+            for (int j = 0; j < o.ee_count[e]; ++j) {
+                const int g = o.ee_list[e * eb + j];
+                const int b0 = o.edges[4 * g + 2], b1 = o.edges[4 * g + 3];
+                if (ee_contact(load3(q, a0), load3(q, a1), load3(q, b0), load3(q, b1), load3(qa, a0), load3(qa, a1),
+                               load3(qa, b0), load3(qa, b1), r, ke, kd, mu, o.friction_eps, dt,
+                               T(o.sc.edge_parallel_epsilon), F, Hk)) {
+                    f = f + F[slot - 2];
+                    H = H + Hk[slot - 2];
+                }
+            }
+        }
+}
+
+// _penetration_free_truncation with self-contact (solver_vbd.py:2026-2063): per-vertex t from
+// every contact's division plane (minimum), then disp *= t, |disp| <= margin * relaxation / 2,
+// q = pos_prev_cd + disp for all particles.
+template <typename T>
+void planar_truncate(Oracle<T>& o) {
+    const int V = o.V;
+    std::vector<T> ts(V, T(1));
+    const T eps = T(o.sc.edge_parallel_epsilon), gamma = T(o.sc.relaxation);
+    const T* x = o.pos_prev_cd.data();
+    const T* dx = o.disp.data();
+    auto upd = [&](int i, V3<T> n, V3<T> d) {
+        const T t = planar_truncation_t(load3(x, i), load3(dx, i), n, d, eps, gamma);
+        if (t < ts[i]) ts[i] = t;
+    };
+    const size_t vb = o.sc.vertex_buffer, eb = o.sc.edge_buffer;
+    for (int v = 0; v < V; ++v)
+        for (int k = 0; k < o.vt_count[v]; ++k) {
+            const int t = o.vt_list[v * vb + k];
+            const int a = o.tri[3 * t], b = o.tri[3 * t + 1], c = o.tri[3 * t + 2];
+            bool dummy[4];
+            V3<T> n, d;
+            vt_plane(load3(x, v), load3(dx, v), load3(x, a), load3(dx, a), load3(x, b), load3(dx, b), load3(x, c),
+                     load3(dx, c), dummy, n, d);
+            if (!dummy[0]) upd(v, n, d);
+            if (!dummy[1]) upd(a, n, d);
+            if (!dummy[2]) upd(b, n, d);
+            if (!dummy[3]) upd(c, n, d);
+        }
+    for (int e = 0; e < o.E; ++e)
+        for (int j = 0; j < o.ee_count[e]; ++j) {
+            const int g = o.ee_list[e * eb + j];
+            const int a0 = o.edges[4 * e + 2], a1 = o.edges[4 * e + 3];
+            const int b0 = o.edges[4 * g + 2], b1 = o.edges[4 * g + 3];
+            bool dummy[4];
+            V3<T> n, d;
+            ee_plane(load3(x, a0), load3(dx, a0), load3(x, a1), load3(dx, a1), load3(x, b0), load3(dx, b0),
+                     load3(x, b1), load3(dx, b1), dummy, n, d);
+            if (!dummy[0]) upd(a0, n, d);
+            if (!dummy[1]) upd(a1, n, d);
+            if (!dummy[2]) upd(b0, n, d);
+            if (!dummy[3]) upd(b1, n, d);
+        }
+    const T maxd = T(static_cast<float>(double(o.sc.margin) * double(o.sc.relaxation) * 0.5));
+    for (int p = 0; p < V; ++p) {
+        V3<T> d = load3(o.disp.data(), p) * ts[p];
+        const T l = len(d);
+        if (l > maxd) d = d * maxd / l;
+        store3(o.disp.data(), p, d);
+        store3(o.q.data(), p, load3(o.pos_prev_cd.data(), p) + d);
+    }
+}
+
+// _collision_detection_penetration_free (solver_vbd.py:3221-3237)
+template <typename T>
+void collision_detection_penetration_free(Oracle<T>& o) {
+    o.pos_prev_cd = o.q;
+    std::fill(o.disp.begin(), o.disp.end(), T(0));
+    detect_self_contacts(o, o.q);
+}
+
 template <typename T>
 void forward(Oracle<T>& o, const float* q_in, const float* qd_in, const float* f_ext, T dt) {
     const int V = o.V;
     for (int i = 0; i < 3 * V; ++i) o.q[i] = T(q_in[i]);
-    o.pos_prev_cd = o.q;                       // pos_prev_collision_detection.assign(state_in.q)
-    std::fill(o.disp.begin(), o.disp.end(), T(0));
+    o.iteration = 0;
+    if (o.sc.enabled) {
+        collision_detection_penetration_free(o);
+    } else {
+        o.pos_prev_cd = o.q;                   // pos_prev_collision_detection.assign(state_in.q)
+        std::fill(o.disp.begin(), o.disp.end(), T(0));
+    }
     for (int p = 0; p < V; ++p) {              // forward_step
         const V3<T> x = load3(o.q.data(), p);
         store3(o.q_prev.data(), p, x);
@@ -528,6 +1170,10 @@ void forward(Oracle<T>& o, const float* q_in, const float* qd_in, const float* f
         const V3<T> vn = v + (v3(o.g[0], o.g[1], o.g[2]) + fe * o.inv_mass[p]) * dt;
         store3(o.inertia.data(), p, x + vn * dt);
         store3(o.disp.data(), p, vn * dt);
+    }
+    if (o.sc.enabled) {
+        planar_truncate(o);
+        return;
     }
     for (int p = 0; p < V; ++p)                // apply_truncation_ts (t = 1, max = inf)
         store3(o.q.data(), p, load3(o.pos_prev_cd.data(), p) + load3(o.disp.data(), p));
@@ -595,6 +1241,19 @@ template <typename T>
 void sweep_color(Oracle<T>& o, int color, T dt) {
     accumulate_contacts(o, color, dt);
     const int b = o.color_off[color], e = o.color_off[color + 1];
+    if (o.sc.enabled) {
+        const T ke = T(o.soft_ke), kd = T(o.soft_kd), mu = T(o.soft_mu);
+#pragma omp parallel for schedule(static) num_threads(o.threads) if (o.threads > 1)
+        for (int k = b; k < e; ++k) {
+            const int p = o.color_par[k];
+            V3<T> f;
+            M3<T> H;
+            self_contact_vertex(o, p, ke, kd, mu, dt, f, H);
+            store3(o.pf.data(), p, load3(o.pf.data(), p) + f);
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) o.ph[9 * p + 3 * i + j] += H.m[i][j];
+        }
+    }
 #pragma omp parallel for schedule(static) num_threads(o.threads) if (o.threads > 1)
     for (int k = b; k < e; ++k) {
         const int p = o.color_par[k];
@@ -610,6 +1269,10 @@ void sweep_color(Oracle<T>& o, int color, T dt) {
             store3(o.disp.data(), p, load3(o.disp.data(), p) + hi * f);
         }
     }
+    if (o.sc.enabled) {
+        planar_truncate(o);
+        return;
+    }
     // apply_truncation_ts over all particles
 #pragma omp parallel for schedule(static) num_threads(o.threads) if (o.threads > 1)
     for (int p = 0; p < o.V; ++p) store3(o.q.data(), p, load3(o.pos_prev_cd.data(), p) + load3(o.disp.data(), p));
@@ -617,6 +1280,10 @@ void sweep_color(Oracle<T>& o, int color, T dt) {
 
 template <typename T>
 void begin_iteration(Oracle<T>& o) {
+    // self-contact detection at iteration 0 (interval 0) or every `interval` iterations (:2540-2545)
+    const int it = o.iteration++;
+    if (o.sc.enabled && ((o.sc.interval == 0 && it == 0) || (o.sc.interval >= 1 && it % o.sc.interval == 0)))
+        collision_detection_penetration_free(o);
     std::fill(o.pf.begin(), o.pf.end(), T(0));
     std::fill(o.ph.begin(), o.ph.end(), T(0));
 }
@@ -658,6 +1325,16 @@ void residual(Oracle<T>& o, T dt, float* per_vertex) {
     std::fill(o.pf.begin(), o.pf.end(), T(0));
     std::fill(o.ph.begin(), o.ph.end(), T(0));
     for (int c = 0; c < o.C; ++c) accumulate_contacts(o, c, dt);
+    if (o.sc.enabled) {
+        for (int p = 0; p < o.V; ++p) {
+            V3<T> f;
+            M3<T> H;
+            self_contact_vertex(o, p, T(o.soft_ke), T(o.soft_kd), T(o.soft_mu), dt, f, H);
+            store3(o.pf.data(), p, load3(o.pf.data(), p) + f);
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) o.ph[9 * p + 3 * i + j] += H.m[i][j];
+        }
+    }
     const T gn = std::sqrt(o.g[0] * o.g[0] + o.g[1] * o.g[1] + o.g[2] * o.g[2]);
 #pragma omp parallel for schedule(static) num_threads(o.threads) if (o.threads > 1)
     for (int p = 0; p < o.V; ++p) {
@@ -769,6 +1446,129 @@ void oracle_set_positions(OracleHandle* h, const float* q) {
 }
 
 void oracle_residual(OracleHandle* h, float dt, float* per_vertex) { ORACLE_DISPATCH(h, residual(o, T(dt), per_vertex)); }
+
+// Self-contact (particle_enable_self_contact=True path): parameters, and detection alone.
+void oracle_set_self_contact(OracleHandle* h, const OracleSelfContact* p) {
+    ORACLE_DISPATCH(h, {
+        o.sc = *p;
+        o.sc.rest_q = nullptr;
+        o.rest_q.clear();
+        if (p->rest_q) o.rest_q.assign(p->rest_q, p->rest_q + 3 * o.V);
+        o.vt_count.assign(o.V, 0);
+        o.vt_list.assign(static_cast<size_t>(o.V) * std::max(1, p->vertex_buffer), -1);
+        o.ee_count.assign(o.E, 0);
+        o.ee_list.assign(static_cast<size_t>(o.E) * std::max(1, p->edge_buffer), -1);
+        o.tri_vs.assign(o.Tn, {});
+        if (p->enabled && p->filter_threshold >= 2) build_near_sets(o);
+    });
+}
+
+// Detection at positions q (model order): per-vertex colliding triangles and per-edge colliding
+// edges (ascending, -1 padded, strides vertex_buffer / edge_buffer).  Returns the number of
+// candidates dropped because a buffer was full.
+long long oracle_self_contact_detect(OracleHandle* h, const float* q, int32_t* vt_counts, int32_t* vt_lists,
+                                     int32_t* ee_counts, int32_t* ee_lists) {
+    long long over = 0;
+    ORACLE_DISPATCH(h, {
+        std::vector<T> qq(q, q + 3 * o.V);
+        o.sc_overflow = 0;
+        detect_self_contacts(o, qq);
+        over = o.sc_overflow;
+        std::copy(o.vt_count.begin(), o.vt_count.end(), vt_counts);
+        std::copy(o.vt_list.begin(), o.vt_list.end(), vt_lists);
+        std::copy(o.ee_count.begin(), o.ee_count.end(), ee_counts);
+        std::copy(o.ee_list.begin(), o.ee_list.end(), ee_lists);
+    });
+    return over;
+}
+
+// Element-level self-contact functions (known-answer tests).
+void oracle_self_contact_norm(int is_double, double dis, double r, double k, double* out) {
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        T a, b;
+        self_contact_norm<T>(T(dis), T(r), T(k), a, b);
+        out[0] = a;
+        out[1] = b;
+    };
+    if (is_double) run(double(0));
+    else run(float(0));
+}
+
+// pos / anchor: a, b, c, p (12 values each); outputs for a, b, c, p
+int oracle_vt_contact(int is_double, const double* pos, const double* anchor, double r, double ke, double kd,
+                      double mu, double feps, double dt, double* f_out, double* h_out) {
+    int has = 0;
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        V3<T> x[4], a[4], F[4];
+        M3<T> H[4];
+        for (int k = 0; k < 4; ++k) {
+            x[k] = v3(T(pos[3 * k]), T(pos[3 * k + 1]), T(pos[3 * k + 2]));
+            a[k] = v3(T(anchor[3 * k]), T(anchor[3 * k + 1]), T(anchor[3 * k + 2]));
+        }
+        has = vt_contact<T>(x[0], x[1], x[2], x[3], a[0], a[1], a[2], a[3], T(r), T(ke), T(kd), T(mu), T(feps), T(dt),
+                            F, H);
+        for (int k = 0; k < 4; ++k) {
+            f_out[3 * k] = has ? double(F[k].x) : 0.0;
+            f_out[3 * k + 1] = has ? double(F[k].y) : 0.0;
+            f_out[3 * k + 2] = has ? double(F[k].z) : 0.0;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) h_out[9 * k + 3 * i + j] = has ? double(H[k].m[i][j]) : 0.0;
+        }
+    };
+    if (is_double) run(double(0));
+    else run(float(0));
+    return has;
+}
+
+// pos / anchor: e0, e1, f0, f1 (12 values each); outputs for e0, e1
+int oracle_ee_contact(int is_double, const double* pos, const double* anchor, double r, double ke, double kd,
+                      double mu, double feps, double dt, double par_eps, double* f_out, double* h_out) {
+    int has = 0;
+    auto run = [&](auto tag) {
+        using T = decltype(tag);
+        V3<T> x[4], a[4], F[2];
+        M3<T> H[2];
+        for (int k = 0; k < 4; ++k) {
+            x[k] = v3(T(pos[3 * k]), T(pos[3 * k + 1]), T(pos[3 * k + 2]));
+            a[k] = v3(T(anchor[3 * k]), T(anchor[3 * k + 1]), T(anchor[3 * k + 2]));
+        }
+        has = ee_contact<T>(x[0], x[1], x[2], x[3], a[0], a[1], a[2], a[3], T(r), T(ke), T(kd), T(mu), T(feps), T(dt),
+                            T(par_eps), F, H);
+        for (int k = 0; k < 2; ++k) {
+            f_out[3 * k] = has ? double(F[k].x) : 0.0;
+            f_out[3 * k + 1] = has ? double(F[k].y) : 0.0;
+            f_out[3 * k + 2] = has ? double(F[k].z) : 0.0;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) h_out[9 * k + 3 * i + j] = has ? double(H[k].m[i][j]) : 0.0;
+        }
+    };
+    if (is_double) run(double(0));
+    else run(float(0));
+    return has;
+}
+
+// p1 q1 p2 q2 (12 values) -> s, t, distance
+void oracle_closest_edge_edge(const double* pts, double eps, double* out) {
+    V3<double> p[4];
+    for (int k = 0; k < 4; ++k) p[k] = v3(pts[3 * k], pts[3 * k + 1], pts[3 * k + 2]);
+    closest_edge_edge<double>(p[0], p[1], p[2], p[3], eps, out[0], out[1], out[2]);
+}
+
+// a b c p (12 values) -> closest point (3) and barycentric coordinates (3)
+void oracle_triangle_closest_point(const double* pts, double* out) {
+    V3<double> p[4];
+    for (int k = 0; k < 4; ++k) p[k] = v3(pts[3 * k], pts[3 * k + 1], pts[3 * k + 2]);
+    V3<double> bary;
+    const V3<double> c = triangle_closest_point<double>(p[0], p[1], p[2], p[3], bary);
+    out[0] = c.x;
+    out[1] = c.y;
+    out[2] = c.z;
+    out[3] = bary.x;
+    out[4] = bary.y;
+    out[5] = bary.z;
+}
 
 // Element-level entry points (used by the known-answer tests).
 void oracle_membrane(int is_double, int face, int v_order, const double* pos, const double* anchor,
