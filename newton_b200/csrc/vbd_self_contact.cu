@@ -15,14 +15,18 @@
 //
 // B200 design.  The reference refits two BVHs and runs 4 threads per primitive with atomics into
 // the per-vertex force.  Here:
-//   * a hashed uniform grid (cell >= 2 * margin and >= the longest rest edge) is rebuilt every
-//     detection in four device passes -- count per bucket, exclusive scan (CUB), fill, query --
-//     so no host synchronisation is needed and a step stays graph-capturable;
-//   * each candidate pair is reported once, in the cell that is the minimum corner of the
-//     intersection of the two cell ranges, and kept in a sorted per-vertex / per-edge list;
-//   * forces are gathered per vertex of the current color in a fixed order (own vertex-triangle
-//     pairs, then the pairs of each incident triangle, then the edge-edge pairs of each incident
-//     edge), so results are deterministic;
+//   * a hashed uniform grid (cell = margin + longest rest edge) is rebuilt every detection in
+//     four device passes -- count per bucket, exclusive scan (CUB), fill, query -- so no host
+//     synchronisation is needed and a step stays graph-capturable.  A triangle / edge of at most
+//     half a cell sits in the one bucket of its box centre's cell, a larger (stretched) one in
+//     every cell its box overlaps; the count pass keeps each element's box;
+//   * a query rejects candidates by box overlap before any filter or exact distance, skips
+//     entries of other cells that share its bucket, and keeps the survivors in a sorted
+//     per-vertex / per-edge list (so each pair is reported once);
+//   * forces are gathered per vertex of the current color, 8 lanes per vertex taking the pairs
+//     round-robin in a fixed order (own vertex-triangle pairs, then the pairs of each incident
+//     triangle, then the edge-edge pairs of each incident edge) and reduced with xor shuffles, so
+//     results are deterministic;
 //   * truncation ratios are reduced with an integer atomicMin on the (non-negative) float bits,
 //     which is exact and order-independent.
 // Buffers are fixed-size (reference defaults: 32 triangles per vertex, 64 edges per edge; plus
@@ -40,8 +44,6 @@
 namespace vbd {
 
 namespace {
-
-constexpr int kMaxCells = 64;  // cells one element or query box may touch (else: counted, skipped)
 
 struct CellRange {
     int3 lo, hi;
@@ -82,6 +84,7 @@ struct GridArgs {
     int* cur;
     int* items;
     int cap;
+    float4* box;          // [2n] element boxes (lo, hi; lo.w = 1 for a large element), count pass
     unsigned* counters;
 };
 
@@ -97,13 +100,34 @@ __device__ __forceinline__ void elem_box(const GridArgs& a, int e, float3& lo, f
     }
 }
 
+__device__ __forceinline__ int3 center_cell(float4 lo, float4 hi, float inv) {
+    return make_int3(cell_coord(0.5f * (lo.x + hi.x), inv), cell_coord(0.5f * (lo.y + hi.y), inv),
+                     cell_coord(0.5f * (lo.z + hi.z), inv));
+}
+
+// An element whose half-extent is at most half a cell goes into the one bucket of its box
+// centre's cell; a larger one (stretched) goes into every cell its box overlaps, up to
+// kMaxLargeCells, and is flagged (lo.w = 1).  Queries then only look margin + half a cell beyond
+// their own box, however far the cloth stretches elsewhere.
+constexpr int kMaxLargeCells = 4096;
+
 __global__ void grid_count_kernel(GridArgs a) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.n) return;
     float3 lo, hi;
     elem_box(a, e, lo, hi);
+    const float half = 0.5f * fmaxf(fmaxf(hi.x - lo.x, hi.y - lo.y), hi.z - lo.z);
+    const bool large = !(half <= 0.5f / a.inv_cell);
+    const float4 l4 = make_float4(lo.x, lo.y, lo.z, large ? 1.f : 0.f), h4 = make_float4(hi.x, hi.y, hi.z, 0.f);
+    a.box[2 * e] = l4;
+    a.box[2 * e + 1] = h4;
+    if (!large) {
+        const int3 c = center_cell(l4, h4, a.inv_cell);
+        atomicAdd(&a.cnt[cell_hash(c.x, c.y, c.z, a.mask)], 1);
+        return;
+    }
     const CellRange r = cell_range(lo, hi, a.inv_cell);
-    if (cell_count(r) > kMaxCells) {
+    if (!(cell_count(r) <= kMaxLargeCells)) {
         atomicAdd(&a.counters[kScGridOverflow], 1u);
         return;
     }
@@ -115,10 +139,17 @@ __global__ void grid_count_kernel(GridArgs a) {
 __global__ void grid_fill_kernel(GridArgs a) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.n) return;
-    float3 lo, hi;
-    elem_box(a, e, lo, hi);
-    const CellRange r = cell_range(lo, hi, a.inv_cell);
-    if (cell_count(r) > kMaxCells) return;
+    const float4 l4 = a.box[2 * e], h4 = a.box[2 * e + 1];
+    if (l4.w == 0.f) {
+        const int3 c = center_cell(l4, h4, a.inv_cell);
+        const unsigned h = cell_hash(c.x, c.y, c.z, a.mask);
+        const int k = a.off[h] + atomicAdd(&a.cur[h], 1);
+        if (k < a.cap) a.items[k] = e;
+        else atomicAdd(&a.counters[kScGridOverflow], 1u);
+        return;
+    }
+    const CellRange r = cell_range(xyz(l4), xyz(h4), a.inv_cell);
+    if (!(cell_count(r) <= kMaxLargeCells)) return;
     for (int z = r.lo.z; z <= r.hi.z; ++z)
         for (int y = r.lo.y; y <= r.hi.y; ++y)
             for (int x = r.lo.x; x <= r.hi.x; ++x) {
@@ -127,6 +158,21 @@ __global__ void grid_fill_kernel(GridArgs a) {
                 if (k < a.cap) a.items[k] = e;
                 else atomicAdd(&a.counters[kScGridOverflow], 1u);
             }
+}
+
+// whether bucket entry (box blo/bhi) belongs to cell (x, y, z): its centre cell, or for a large
+// element any cell its box overlaps
+__device__ __forceinline__ bool in_cell(float4 blo, float4 bhi, float inv, int x, int y, int z) {
+    if (blo.w == 0.f) {
+        const int3 c = center_cell(blo, bhi, inv);
+        return c.x == x && c.y == y && c.z == z;
+    }
+    const CellRange r = cell_range(xyz(blo), xyz(bhi), inv);
+    return x >= r.lo.x && x <= r.hi.x && y >= r.lo.y && y <= r.hi.y && z >= r.lo.z && z <= r.hi.z;
+}
+
+__device__ __forceinline__ bool boxes_overlap(float3 lo, float3 hi, float4 blo, float4 bhi) {
+    return !(blo.x > hi.x || bhi.x < lo.x || blo.y > hi.y || bhi.y < lo.y || blo.z > hi.z || bhi.z < lo.z);
 }
 
 // sorted insert without duplicates into row[0..n) of capacity cap; false when full
@@ -160,6 +206,7 @@ struct QueryArgs {
     unsigned tri_mask, edge_mask;
     const int *tri_cnt, *tri_off, *tri_items;
     const int *edge_cnt, *edge_off, *edge_items;
+    const float4 *tri_box, *edge_box;
     int tri_cap, edge_cap;
     int vbuf, ebuf;
     int* vt_count;
@@ -169,15 +216,21 @@ struct QueryArgs {
     unsigned* counters;
 };
 
+constexpr int kMaxQueryCells = 512;
+
 __global__ void vt_query_kernel(QueryArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.V) return;
     const float3 p = xyz(a.x[i]);
     const float m = a.margin;
-    const CellRange q = cell_range(p - f3(m, m, m), p + f3(m, m, m), a.inv_cell);
+    const float3 plo = p - f3(m, m, m), phi = p + f3(m, m, m);
+    // a small triangle within the margin has its box centre within margin + half a cell of p;
+    // a large one is in every cell its box overlaps
+    const float r = m + 0.5f / a.inv_cell;
+    const CellRange q = cell_range(p - f3(r, r, r), p + f3(r, r, r), a.inv_cell);
     int n = 0;
     int* row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
-    if (cell_count(q) > kMaxCells) {
+    if (!(cell_count(q) <= kMaxQueryCells)) {
         atomicAdd(&a.counters[kScGridOverflow], 1u);
         a.vt_count[i] = 0;
         return;
@@ -194,17 +247,15 @@ __global__ void vt_query_kernel(QueryArgs a) {
                 const int e = min(b + a.tri_cnt[h], a.tri_cap);
                 for (int k = b; k < e; ++k) {
                     const int t = a.tri_items[k];
+                    const float4 blo = a.tri_box[2 * t], bhi = a.tri_box[2 * t + 1];
+                    if (!boxes_overlap(plo, phi, blo, bhi)) continue;
+                    if (!in_cell(blo, bhi, a.inv_cell, x, y, z)) continue;  // another cell in this bucket
                     const int4 tr = a.tri[t];
                     if (tr.x == i || tr.y == i || tr.z == i) continue;
                     if (wv >= 0 && tr.w >= 0 && wv != tr.w) continue;
-                    const float3 t0 = xyz(a.x[tr.x]), t1 = xyz(a.x[tr.y]), t2 = xyz(a.x[tr.z]);
-                    // report the pair only in the minimum corner cell of the two ranges
-                    const CellRange er = cell_range(fmin3(fmin3(t0, t1), t2), fmax3(fmax3(t0, t1), t2), a.inv_cell);
-                    const int cx = max(q.lo.x, er.lo.x), cy = max(q.lo.y, er.lo.y), cz = max(q.lo.z, er.lo.z);
-                    if (cx != x || cy != y || cz != z) continue;
-                    if (x > er.hi.x || y > er.hi.y || z > er.hi.z) continue;
                     if (list_contains(nb, ne, tr.x) || list_contains(nb, ne, tr.y) || list_contains(nb, ne, tr.z))
                         continue;
+                    const float3 t0 = xyz(a.x[tr.x]), t1 = xyz(a.x[tr.y]), t2 = xyz(a.x[tr.z]);
                     float3 bary;
                     const float dist = length(triangle_closest_point(t0, t1, t2, p, bary) - p);
                     if (!(dist < m)) continue;
@@ -222,25 +273,27 @@ __global__ void vt_query_kernel(QueryArgs a) {
     if (full) atomicAdd(&a.counters[kScVtOverflow], 1u);
 }
 
+// Edge-edge pairs are symmetric: edge e only searches partners g > e and records the pair in both
+// lists through atomic slots; ee_sort_kernel then orders every list.  A small partner sits in one
+// bucket only; a large (multi-cell) partner is taken in the first cell of the query range it
+// occupies, so every pair is met exactly once.
 __global__ void ee_query_kernel(QueryArgs a) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= a.E) return;
     const int4 ed = a.edge[e];
     const float3 a0 = xyz(a.x[ed.x]), a1 = xyz(a.x[ed.y]);
     const float m = a.margin;
-    const CellRange q = cell_range(fmin3(a0, a1) - f3(m, m, m), fmax3(a0, a1) + f3(m, m, m), a.inv_cell);
-    int n = 0;
-    int* row = a.ee_list + static_cast<size_t>(e) * a.ebuf;
-    if (cell_count(q) > kMaxCells) {
+    const float3 qlo = fmin3(a0, a1) - f3(m, m, m), qhi = fmax3(a0, a1) + f3(m, m, m);
+    const float r = 0.5f / a.inv_cell;
+    const CellRange q = cell_range(qlo - f3(r, r, r), qhi + f3(r, r, r), a.inv_cell);
+    if (!(cell_count(q) <= kMaxQueryCells)) {
         atomicAdd(&a.counters[kScGridOverflow], 1u);
-        a.ee_count[e] = 0;
         return;
     }
     const int* n0b = a.near + a.near_off[ed.x];
     const int* n0e = a.near + a.near_off[ed.x + 1];
     const int* n1b = a.near + a.near_off[ed.y];
     const int* n1e = a.near + a.near_off[ed.y + 1];
-    bool full = false;
     for (int z = q.lo.z; z <= q.hi.z; ++z)
         for (int y = q.lo.y; y <= q.hi.y; ++y)
             for (int x = q.lo.x; x <= q.hi.x; ++x) {
@@ -249,17 +302,25 @@ __global__ void ee_query_kernel(QueryArgs a) {
                 const int en = min(b + a.edge_cnt[h], a.edge_cap);
                 for (int k = b; k < en; ++k) {
                     const int g = a.edge_items[k];
+                    if (g <= e) continue;
+                    const float4 blo = a.edge_box[2 * g], bhi = a.edge_box[2 * g + 1];
+                    if (!boxes_overlap(qlo, qhi, blo, bhi)) continue;
+                    if (blo.w == 0.f) {
+                        const int3 c = center_cell(blo, bhi, a.inv_cell);
+                        if (c.x != x || c.y != y || c.z != z) continue;
+                    } else {
+                        const CellRange gr = cell_range(xyz(blo), xyz(bhi), a.inv_cell);
+                        if (max(q.lo.x, gr.lo.x) != x || max(q.lo.y, gr.lo.y) != y || max(q.lo.z, gr.lo.z) != z)
+                            continue;
+                        if (x > gr.hi.x || y > gr.hi.y || z > gr.hi.z) continue;
+                    }
                     const int4 gd = a.edge[g];
                     if (gd.x == ed.x || gd.x == ed.y || gd.y == ed.x || gd.y == ed.y) continue;
                     if (ed.z >= 0 && gd.z >= 0 && ed.z != gd.z) continue;
-                    const float3 b0 = xyz(a.x[gd.x]), b1 = xyz(a.x[gd.y]);
-                    const CellRange er = cell_range(fmin3(b0, b1), fmax3(b0, b1), a.inv_cell);
-                    const int cx = max(q.lo.x, er.lo.x), cy = max(q.lo.y, er.lo.y), cz = max(q.lo.z, er.lo.z);
-                    if (cx != x || cy != y || cz != z) continue;
-                    if (x > er.hi.x || y > er.hi.y || z > er.hi.z) continue;
                     if (list_contains(n0b, n0e, gd.x) || list_contains(n0b, n0e, gd.y) ||
                         list_contains(n1b, n1e, gd.x) || list_contains(n1b, n1e, gd.y))
                         continue;
+                    const float3 b0 = xyz(a.x[gd.x]), b1 = xyz(a.x[gd.y]);
                     float s, t, dist;
                     closest_edge_edge(a0, a1, b0, b1, a.par_eps, s, t, dist);
                     if (!(dist < m)) continue;
@@ -269,11 +330,32 @@ __global__ void ee_query_kernel(QueryArgs a) {
                                           a.par_eps, sr, tr, dr);
                         if (dr < a.rest_excl) continue;
                     }
-                    if (!sorted_insert(row, n, a.ebuf, g)) full = true;
+                    // the distance of (e, g) and of (g, e) is the same test; record both sides
+                    const int ke = atomicAdd(&a.ee_count[e], 1);
+                    if (ke < a.ebuf) a.ee_list[static_cast<size_t>(e) * a.ebuf + ke] = g;
+                    else atomicAdd(&a.counters[kScEeOverflow], 1u);
+                    const int kg = atomicAdd(&a.ee_count[g], 1);
+                    if (kg < a.ebuf) a.ee_list[static_cast<size_t>(g) * a.ebuf + kg] = e;
+                    else atomicAdd(&a.counters[kScEeOverflow], 1u);
                 }
             }
-    a.ee_count[e] = n;
-    if (full) atomicAdd(&a.counters[kScEeOverflow], 1u);
+}
+
+__global__ void ee_sort_kernel(int E, int* ee_count, int* ee_list, int ebuf) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const int n = min(ee_count[e], ebuf);
+    ee_count[e] = n;
+    int* row = ee_list + static_cast<size_t>(e) * ebuf;
+    for (int a = 1; a < n; ++a) {
+        const int x = row[a];
+        int b = a - 1;
+        while (b >= 0 && row[b] > x) {
+            row[b + 1] = row[b];
+            --b;
+        }
+        row[b + 1] = x;
+    }
 }
 
 __global__ void tri_reverse_kernel(int V, const int* vt_count, const int* vt_list, int vbuf, int* tv_count,
@@ -306,6 +388,27 @@ __global__ void tri_sort_kernel(int T, int* tv_count, int* tv_list, int tcap) {
     }
 }
 
+// marks every vertex that takes part in a detected pair (the gather skips the others)
+__global__ void mark_contact_vertices_kernel(int V, int E, const int4* tri, const int4* edge, const int* vt_count,
+                                             const int* vt_list, int vbuf, const int* ee_count, unsigned char* flag) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < V && vt_count[idx] > 0) {
+        flag[idx] = 1;
+        const int* row = vt_list + static_cast<size_t>(idx) * vbuf;
+        for (int k = 0; k < vt_count[idx]; ++k) {
+            const int4 tr = tri[row[k]];
+            flag[tr.x] = 1;
+            flag[tr.y] = 1;
+            flag[tr.z] = 1;
+        }
+    }
+    if (idx < E && ee_count[idx] > 0) {
+        const int4 ed = edge[idx];
+        flag[ed.x] = 1;
+        flag[ed.y] = 1;
+    }
+}
+
 __global__ void copy_positions_kernel(int V, const float4* src, float4* cd, float4* disp) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= V) return;
@@ -331,45 +434,84 @@ struct AccumArgs {
     int vbuf, ebuf, tcap;
     int v_begin, v_end;
     float r, ke, kd, mu, eps_u, dt, par_eps;
+    const unsigned char* flag;
     float4 *f, *h0, *h1;
 };
 
+// L lanes per vertex: the vertex's pairs (own vertex-triangle list, then each incident triangle's
+// colliding vertices, then each incident edge's colliding edges) are dealt round-robin to the
+// lanes, and the partial sums are combined with xor shuffles -- a fixed order, so deterministic.
+constexpr int kAccumLanes = 8;
+
+__device__ __forceinline__ float lane_sum(float v) {
+    for (int off = kAccumLanes >> 1; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
 __global__ void accumulate_kernel(AccumArgs a) {
-    const int i = a.v_begin + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.v_end) return;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = a.v_begin + tid / kAccumLanes;
+    const int lane = tid & (kAccumLanes - 1);
     float3 f = f3(0.f, 0.f, 0.f);
     Sym3 H = zero_sym();
-    const float3 p = xyz(a.x[i]), p0 = xyz(a.x0[i]);
-    const int* row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
-    for (int k = 0; k < a.vt_count[i]; ++k) {
-        const int4 tr = a.tri[row[k]];
-        vt_contact_slot(xyz(a.x[tr.x]), xyz(a.x[tr.y]), xyz(a.x[tr.z]), p, xyz(a.x0[tr.x]), xyz(a.x0[tr.y]),
-                        xyz(a.x0[tr.z]), p0, 3, a.r, a.ke, a.kd, a.mu, a.eps_u, a.dt, f, H);
-    }
-    for (int k = a.inc_t_off[i]; k < a.inc_t_off[i + 1]; ++k) {
-        const int2 ts = a.inc_t[k];
-        const int4 tr = a.tri[ts.x];
-        const float3 t0 = xyz(a.x[tr.x]), t1 = xyz(a.x[tr.y]), t2 = xyz(a.x[tr.z]);
-        const float3 s0 = xyz(a.x0[tr.x]), s1 = xyz(a.x0[tr.y]), s2 = xyz(a.x0[tr.z]);
-        const int* vl = a.tv_list + static_cast<size_t>(ts.x) * a.tcap;
-        for (int j = 0; j < a.tv_count[ts.x]; ++j) {
-            const int q = vl[j];
-            vt_contact_slot(t0, t1, t2, xyz(a.x[q]), s0, s1, s2, xyz(a.x0[q]), ts.y, a.r, a.ke, a.kd, a.mu, a.eps_u,
-                            a.dt, f, H);
+    if (i < a.v_end && a.flag[i]) {
+        const float3 p = xyz(a.x[i]), p0 = xyz(a.x0[i]);
+        int idx = 0;  // running pair index of this vertex; lane takes idx % L == lane
+        const int* row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
+        const int nv = a.vt_count[i];
+        for (int k = lane; k < nv; k += kAccumLanes) {
+            const int4 tr = a.tri[row[k]];
+            vt_contact_slot(xyz(a.x[tr.x]), xyz(a.x[tr.y]), xyz(a.x[tr.z]), p, xyz(a.x0[tr.x]), xyz(a.x0[tr.y]),
+                            xyz(a.x0[tr.z]), p0, 3, a.r, a.ke, a.kd, a.mu, a.eps_u, a.dt, f, H);
+        }
+        idx += nv;
+        for (int k = a.inc_t_off[i]; k < a.inc_t_off[i + 1]; ++k) {
+            const int2 ts = a.inc_t[k];
+            const int n = a.tv_count[ts.x];
+            int j = (lane - idx) % kAccumLanes;
+            if (j < 0) j += kAccumLanes;
+            if (j < n) {
+                const int4 tr = a.tri[ts.x];
+                const float3 t0 = xyz(a.x[tr.x]), t1 = xyz(a.x[tr.y]), t2 = xyz(a.x[tr.z]);
+                const float3 s0 = xyz(a.x0[tr.x]), s1 = xyz(a.x0[tr.y]), s2 = xyz(a.x0[tr.z]);
+                const int* vl = a.tv_list + static_cast<size_t>(ts.x) * a.tcap;
+                for (; j < n; j += kAccumLanes) {
+                    const int q = vl[j];
+                    vt_contact_slot(t0, t1, t2, xyz(a.x[q]), s0, s1, s2, xyz(a.x0[q]), ts.y, a.r, a.ke, a.kd, a.mu,
+                                    a.eps_u, a.dt, f, H);
+                }
+            }
+            idx += n;
+        }
+        for (int k = a.inc_e_off[i]; k < a.inc_e_off[i + 1]; ++k) {
+            const int2 es = a.inc_e[k];
+            const int n = a.ee_count[es.x];
+            int j = (lane - idx) % kAccumLanes;
+            if (j < 0) j += kAccumLanes;
+            if (j < n) {
+                const int4 ed = a.edge[es.x];
+                const float3 e0 = xyz(a.x[ed.x]), e1 = xyz(a.x[ed.y]);
+                const float3 e0a = xyz(a.x0[ed.x]), e1a = xyz(a.x0[ed.y]);
+                const int* gl = a.ee_list + static_cast<size_t>(es.x) * a.ebuf;
+                for (; j < n; j += kAccumLanes) {
+                    const int4 gd = a.edge[gl[j]];
+                    ee_contact_slot(e0, e1, xyz(a.x[gd.x]), xyz(a.x[gd.y]), e0a, e1a, xyz(a.x0[gd.x]),
+                                    xyz(a.x0[gd.y]), es.y, a.r, a.ke, a.kd, a.mu, a.eps_u, a.dt, a.par_eps, f, H);
+                }
+            }
+            idx += n;
         }
     }
-    for (int k = a.inc_e_off[i]; k < a.inc_e_off[i + 1]; ++k) {
-        const int2 es = a.inc_e[k];
-        const int4 ed = a.edge[es.x];
-        const float3 e0 = xyz(a.x[ed.x]), e1 = xyz(a.x[ed.y]);
-        const float3 e0a = xyz(a.x0[ed.x]), e1a = xyz(a.x0[ed.y]);
-        const int* gl = a.ee_list + static_cast<size_t>(es.x) * a.ebuf;
-        for (int j = 0; j < a.ee_count[es.x]; ++j) {
-            const int4 gd = a.edge[gl[j]];
-            ee_contact_slot(e0, e1, xyz(a.x[gd.x]), xyz(a.x[gd.y]), e0a, e1a, xyz(a.x0[gd.x]), xyz(a.x0[gd.y]), es.y,
-                            a.r, a.ke, a.kd, a.mu, a.eps_u, a.dt, a.par_eps, f, H);
-        }
-    }
+    f.x = lane_sum(f.x);
+    f.y = lane_sum(f.y);
+    f.z = lane_sum(f.z);
+    H.xx = lane_sum(H.xx);
+    H.xy = lane_sum(H.xy);
+    H.xz = lane_sum(H.xz);
+    H.yy = lane_sum(H.yy);
+    H.yz = lane_sum(H.yz);
+    H.zz = lane_sum(H.zz);
+    if (i >= a.v_end || lane != 0) return;
     a.f[i] = make_float4(f.x, f.y, f.z, 0.f);
     a.h0[i] = make_float4(H.xx, H.xy, H.xz, H.yy);
     a.h1[i] = make_float4(H.yz, H.zz, 0.f, 0.f);
@@ -487,7 +629,7 @@ void self_contact_free(SelfContact& sc) {
                     sc.near,     sc.rest,     sc.tri_cnt,   sc.tri_off,  sc.tri_cur,    sc.tri_items, sc.edge_cnt,
                     sc.edge_off, sc.edge_cur, sc.edge_items, sc.scan_tmp, sc.vt_count,  sc.vt_list,   sc.ee_count,
                     sc.ee_list,  sc.tv_count, sc.tv_list,   sc.cd,       sc.sc_f,       sc.sc_h0,     sc.sc_h1,
-                    sc.ts,       sc.counters, sc.vworld};
+                    sc.ts,       sc.counters, sc.vworld,    sc.tri_box,  sc.edge_box,   sc.flag};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     SelfContact empty;
@@ -531,7 +673,9 @@ int self_contact_create(const VbdModelImpl& m, const SelfContactParams& p, SelfC
         const double dx = ra[0] - rb[0], dy = ra[1] - rb[1], dz = ra[2] - rb[2];
         max_edge = std::max(max_edge, std::sqrt(dx * dx + dy * dy + dz * dz));
     }
-    sc.cell = static_cast<float>(std::max(2.0 * p.margin, max_edge) * 1.0001);
+    // cell edge: margin + the longest rest edge (twice the largest rest half-extent), so a query
+    // spans about three cells per axis while elements keep their rest size
+    sc.cell = static_cast<float>(std::max(static_cast<double>(p.margin) + max_edge, 1e-6));
     // incidence (internal vertex -> triangles with slot, endpoint edges with endpoint)
     std::vector<int> it_off(V + 1, 0), ie_off(V + 1, 0);
     std::vector<int2> it_list, ie_list;
@@ -597,8 +741,8 @@ int self_contact_create(const VbdModelImpl& m, const SelfContactParams& p, SelfC
     const unsigned tn = next_pow2(2LL * std::max(T, 1)), en = next_pow2(2LL * std::max(E, 1));
     sc.tri_mask = tn - 1;
     sc.edge_mask = en - 1;
-    sc.tri_items_cap = 8 * std::max(T, 1) + 4096;
-    sc.edge_items_cap = 8 * std::max(E, 1) + 4096;
+    sc.tri_items_cap = 2 * std::max(T, 1) + 65536;  // large (stretched) elements take several cells
+    sc.edge_items_cap = 2 * std::max(E, 1) + 65536;
     auto az = [&](void** ptr, size_t bytes) {
         if (!rc) rc = alloc_zero(ptr, bytes);
     };
@@ -610,6 +754,9 @@ int self_contact_create(const VbdModelImpl& m, const SelfContactParams& p, SelfC
     az(reinterpret_cast<void**>(&sc.edge_off), en * sizeof(int));
     az(reinterpret_cast<void**>(&sc.edge_cur), en * sizeof(int));
     az(reinterpret_cast<void**>(&sc.edge_items), static_cast<size_t>(sc.edge_items_cap) * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.tri_box), 2 * static_cast<size_t>(std::max(T, 1)) * sizeof(float4));
+    az(reinterpret_cast<void**>(&sc.edge_box), 2 * static_cast<size_t>(std::max(E, 1)) * sizeof(float4));
+    az(reinterpret_cast<void**>(&sc.flag), static_cast<size_t>(V));
     az(reinterpret_cast<void**>(&sc.vt_count), static_cast<size_t>(V) * sizeof(int));
     az(reinterpret_cast<void**>(&sc.vt_list), static_cast<size_t>(V) * p.vertex_buffer * sizeof(int));
     az(reinterpret_cast<void**>(&sc.ee_count), static_cast<size_t>(E) * sizeof(int));
@@ -682,6 +829,8 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     g.cur = sc.tri_cur;
     g.items = sc.tri_items;
     g.cap = sc.tri_items_cap;
+    g.box = sc.tri_box;
+
     if (T > 0) {
         grid_count_kernel<<<(T + 255) / 256, 256, 0, st>>>(g);
         VBD_CUDA_TRY(cudaGetLastError());
@@ -700,6 +849,8 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     g.cur = sc.edge_cur;
     g.items = sc.edge_items;
     g.cap = sc.edge_items_cap;
+    g.box = sc.edge_box;
+
     if (E > 0) {
         grid_count_kernel<<<(E + 255) / 256, 256, 0, st>>>(g);
         VBD_CUDA_TRY(cudaGetLastError());
@@ -731,6 +882,8 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     q.edge_cnt = sc.edge_cnt;
     q.edge_off = sc.edge_off;
     q.edge_items = sc.edge_items;
+    q.tri_box = sc.tri_box;
+    q.edge_box = sc.edge_box;
     q.tri_cap = sc.tri_items_cap;
     q.edge_cap = sc.edge_items_cap;
     q.vbuf = sc.p.vertex_buffer;
@@ -752,9 +905,17 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
         VBD_CUDA_TRY(cudaMemsetAsync(sc.vt_count, 0, static_cast<size_t>(V) * sizeof(int), st));
     }
     if (E > 0) {
+        VBD_CUDA_TRY(cudaMemsetAsync(sc.ee_count, 0, static_cast<size_t>(E) * sizeof(int), st));
         ee_query_kernel<<<(E + 127) / 128, 128, 0, st>>>(q);
         VBD_CUDA_TRY(cudaGetLastError());
+        ee_sort_kernel<<<(E + 255) / 256, 256, 0, st>>>(E, sc.ee_count, sc.ee_list, sc.p.edge_buffer);
+        VBD_CUDA_TRY(cudaGetLastError());
     }
+    VBD_CUDA_TRY(cudaMemsetAsync(sc.flag, 0, static_cast<size_t>(V), st));
+    const int nm = std::max(V, E);
+    mark_contact_vertices_kernel<<<(nm + 255) / 256, 256, 0, st>>>(V, E, sc.tri, sc.edge, sc.vt_count, sc.vt_list,
+                                                                   sc.p.vertex_buffer, sc.ee_count, sc.flag);
+    VBD_CUDA_TRY(cudaGetLastError());
     return VBD_OK;
 }
 
@@ -788,11 +949,12 @@ int self_contact_accumulate(const VbdModelImpl& m, SelfContact& sc, const float4
     a.eps_u = friction_epsilon * dt;
     a.dt = dt;
     a.par_eps = sc.p.edge_parallel_epsilon;
+    a.flag = sc.flag;
     a.f = sc.sc_f;
     a.h0 = sc.sc_h0;
     a.h1 = sc.sc_h1;
-    const int n = v_end - v_begin;
-    accumulate_kernel<<<(n + 127) / 128, 128, 0, st>>>(a);
+    const long long threads = static_cast<long long>(v_end - v_begin) * kAccumLanes;
+    accumulate_kernel<<<static_cast<int>((threads + 127) / 128), 128, 0, st>>>(a);
     VBD_CUDA_TRY(cudaGetLastError());
     return VBD_OK;
 }

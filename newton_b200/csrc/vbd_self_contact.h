@@ -56,6 +56,7 @@ struct SelfContact {
     // grids
     int *tri_cnt = nullptr, *tri_off = nullptr, *tri_cur = nullptr, *tri_items = nullptr;
     int *edge_cnt = nullptr, *edge_off = nullptr, *edge_cur = nullptr, *edge_items = nullptr;
+    float4 *tri_box = nullptr, *edge_box = nullptr;   // [2T], [2E] element boxes of the last detection
     void* scan_tmp = nullptr;
     size_t scan_bytes = 0;
     // detection results
@@ -63,6 +64,7 @@ struct SelfContact {
     int *ee_count = nullptr, *ee_list = nullptr;   // [E], [E * edge_buffer] edge ids ascending
     int *tv_count = nullptr, *tv_list = nullptr;   // [T], [T * tcap] internal vertex ids ascending
     // per-iteration state
+    unsigned char* flag = nullptr;  // [V] 1: the vertex takes part in a detected pair
     float4* cd = nullptr;    // pos_prev_collision_detection (internal order)
     float4* sc_f = nullptr;  // [V] self-contact force
     float4* sc_h0 = nullptr; // [V] Hessian xx xy xz yy

@@ -8,6 +8,9 @@
 * ``hanging_cloth``  32 x 32 vertices, 1 m side, two top corners pinned, ground at z = -1.
 * ``draped_cloth``   256 x 256 vertices, 2 m side, flat, falling onto a static sphere (r = 0.4 m)
                      and the ground; contact ke = 1e4 (particle and shape side), margin 5 mm.
+* ``cloth_on_boxes`` 1024 x 1024 vertices, 4 m side, 0.8 m above 16 static boxes (seeded yaw and
+                     position in [-1.5, 1.5]^2, half-extents U[0.1, 0.4], resting on the ground);
+                     the self-contact workload (radius 2 mm, margin 3 mm in the solver).
 * ``batched_worlds`` independent cloth worlds of uneven size (N ~ U{16..96}, side ~ U[0.5, 2] m,
                      tri_ke ~ logU[1e3, 1e5] with ka = ke, edge_ke ~ logU[1e-3, 1e-1], 0-4 random
                      boundary pins, a ground plane per world), merged into one model whose color
@@ -77,6 +80,26 @@ def draped_cloth(n: int = 256, seed: int = 0, device="cuda:0", offset: tuple = (
     sphere of radius 0.4 m (centre offset by ``offset`` in x, y), and the ground plane."""
     return single_cloth(n=n, side=2.0, seed=seed, pin_top_corners=False, ground=0.0,
                         sphere=((offset[0], offset[1], 0.5), 0.4), height=height, z_noise=0.0, device=device)
+
+
+def cloth_on_boxes(n: int = 1024, side: float = 4.0, boxes: int = 16, seed: int = 0, height: float = 0.8,
+                   device="cuda:0"):
+    """Large cloth falling onto seeded static boxes on the ground (self-contact workload)."""
+    rng = np.random.default_rng(seed)
+    b = ModelBuilder()
+    _cloth(b, n, side, height, 0.1, 1.0e-3, dict(CLOTH_MATERIAL))
+    cfg = ModelBuilder.ShapeConfig(ke=1.0e4)
+    b.add_ground_plane(height=0.0, cfg=cfg)
+    for _ in range(boxes):
+        hx, hy, hz = (float(v) for v in rng.uniform(0.1, 0.4, size=3))
+        x, y = (float(v) for v in rng.uniform(-1.5, 1.5, size=2))
+        yaw = float(rng.uniform(0.0, 2.0 * np.pi))
+        rot = (0.0, 0.0, float(np.sin(0.5 * yaw)), float(np.cos(0.5 * yaw)))
+        b.add_shape_box(-1, xform=((x, y, hz), rot), hx=hx, hy=hy, hz=hz, cfg=cfg)
+    b.color(include_bending=True)
+    m = b.finalize(device=device)
+    m.soft_contact_ke = 1.0e4
+    return m, m.particle_q.copy()
 
 
 def batched_worlds(num_worlds: int = 512, seed: int = 0, n_range=(16, 96), device="cuda:0", include_bending=True):
