@@ -14,6 +14,14 @@ the cloth (a single cloth does not shard), so per-GPU work is fixed ("weak" scal
 ``--impl reference`` times the CPU oracle (the reference's VBD step restated in C++, OpenMP over
 the vertices of a color) on the host cores -- the reference itself needs Warp, which is not
 installed here.
+
+``--workload`` selects other cloth workloads (the default is the one above):
+  * ``batched-worlds``: 512 independent cloth worlds (1.89 M vertices), the worlds sharded over
+    the ranks by vertex count (no collective on the data path); ``value`` is whole-batch steps/s
+    ("strong" scaling: the batch is fixed as N grows);
+  * ``cloth-on-boxes``: 1024 x 1024 cloth (1.05 M vertices) on 16 static boxes with self-contact
+    (radius 2 mm, margin 3 mm); replicas per rank.
+The timed steps run inside an NVTX range named ``bench_timed`` (for ncu --nvtx-include).
 """
 
 from __future__ import annotations
@@ -35,6 +43,14 @@ ITERATIONS = 10
 MARGIN = 5.0e-3
 WORKLOAD = ("draped cloth 256x256 (65,536 vertices, 130,050 triangles, 195,585 hinges) on a static sphere + "
             "ground, plain VBD, 10 iterations, dt=1/600, fp32")
+WORKLOADS = {
+    "draped-cloth": WORKLOAD,
+    "batched-worlds": ("512 cloth worlds, N ~ U{16..96} per side (1.89 M vertices), side ~ U[0.5, 2] m, tri_ke ~ "
+                       "logU[1e3, 1e5], 0-4 pins, ground per world, plain VBD, 10 iterations, dt=1/600, fp32, worlds "
+                       "sharded over ranks"),
+    "cloth-on-boxes": ("cloth 1024x1024 (1,048,576 vertices, 2,093,058 triangles, 3,141,633 hinges), 4 m side, on "
+                       "16 static boxes + ground, self-contact radius 2 mm margin 3 mm, 10 iterations, dt=1/600, fp32"),
+}
 
 
 def algorithmic_bytes_per_iteration(model) -> int:
@@ -282,7 +298,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned warm-start A/B")
-    ap.add_argument("--n", type=int, default=256, help="grid vertices per side")
+    ap.add_argument("--n", type=int, default=0, help="grid vertices per side (default: the workload's)")
+    ap.add_argument("--workload", default="draped-cloth", choices=sorted(WORKLOADS))
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -306,8 +323,24 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
     W, K = max(args.warmup, 3), max(args.steps, 1)
-    model, q0 = scenes.draped_cloth(n=args.n, seed=rank, device=dev)
-    solver = SolverVBD(model, iterations=ITERATIONS)
+    solver_kw = {}
+    scaling, parallelism = "weak", f"replicas x{world}"
+    if args.workload == "draped-cloth":
+        model, q0 = scenes.draped_cloth(n=args.n or 256, seed=rank, device=dev)
+    elif args.workload == "cloth-on-boxes":
+        model, q0 = scenes.cloth_on_boxes(n=args.n or 1024, device=dev)
+        solver_kw = dict(particle_enable_self_contact=True, particle_self_contact_radius=0.002,
+                         particle_self_contact_margin=0.003)
+    else:
+        from newton_b200.sharding import extract_worlds, partition_worlds, world_vertex_counts
+
+        full, q_full = scenes.batched_worlds(512, seed=0, device="cpu")
+        ids = partition_worlds(world_vertex_counts(full), world)[rank]
+        model, pidx = extract_worlds(full, ids, device=dev)
+        q0 = q_full[pidx]
+        job_vertices = full.particle_count
+        scaling, parallelism = "strong", f"worlds sharded x{world}"
+    solver = SolverVBD(model, iterations=ITERATIONS, **solver_kw)
     pipe = CollisionPipeline(model, soft_contact_margin=MARGIN)
     contacts = pipe.contacts()
     s0, s1 = model.state(), model.state()
@@ -338,11 +371,13 @@ def main() -> None:
         dist.barrier()
     torch.cuda.synchronize()
     sampler.start()
+    torch.cuda.nvtx.range_push("bench_timed")
     for k in range(K):
         flush.zero_()
         evs[k][0].record(stream)
         substep()
         evs[k][1].record(stream)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -352,7 +387,7 @@ def main() -> None:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    value = world * 1e3 / ms
+    value = (1e3 if args.workload == "batched-worlds" else world * 1e3) / ms
 
     # ---- roofline of the dominant kernel: the per-color sweep --------------------------------
     # one graph of 4 full iterations (every color once per iteration) replayed between CUDA events
@@ -360,6 +395,7 @@ def main() -> None:
     pipe.collide(s0, contacts)
     flush.zero_()
     per_launch_ms = time_iterations(solver, s0, contacts, DT, iterations=4, repeats=10) / colors
+    # with self-contact an iteration also runs the contact gather and truncation passes
     b_iter = algorithmic_bytes_per_iteration(model)
     bytes_per_launch = b_iter / colors
     achieved = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
@@ -367,9 +403,11 @@ def main() -> None:
     tpv = sweep_traffic_per_vertex_iteration()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
-                "traffic": (tpv * model.particle_count / colors) if tpv else None,
+                "traffic": (tpv * model.particle_count / colors) if (tpv and args.workload == "draped-cloth") else None,
                 "kernel": "sweep_kernel (one color)", "algorithmic_bytes_per_launch": bytes_per_launch,
                 "ms_per_launch": per_launch_ms}
+    if solver_kw:
+        roofline["kernel"] = "one color: self-contact gather + sweep_kernel + truncation passes"
 
     # ---- residual reached by the plain 10-iteration step ------------------------------------
     pipe.collide(s0, contacts)
@@ -418,13 +456,14 @@ def main() -> None:
         "warmup": W,
         "ms_per_step": ms,
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": scaling,
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "vertices": V, "triangles": model.tri_count, "hinges": model.edge_count,
+        "config": {"workload": WORKLOADS[args.workload], "vertices": V, "triangles": model.tri_count,
+                   "hinges": model.edge_count,
                    "colors": colors, "iterations": ITERATIONS, "dt": DT, "l2": "flushed between timed steps",
-                   "parallelism": f"replicas x{world}", "launch": solver.launch_info(),
+                   "parallelism": parallelism, "launch": solver.launch_info(),
                    "step_kernel": solver.step_kernel_info(),
                    "residual_gate": "not applied: fixed 10 iterations (plain VBD)"},
         "vertex_iterations_per_s": value * V * ITERATIONS,
@@ -437,10 +476,20 @@ def main() -> None:
         "autotune": tune,
         "status": st,
     }
-    if rank == 0 and world == 1 and not args.no_learned:
-        line["learned"] = learned_ab(dev, args.n, value)
+    if args.workload == "batched-worlds":
+        line["config"]["worlds_on_rank0"] = int(len(np.unique(model.particle_world)))
+        line["config"]["batch_vertices"] = job_vertices
+        line["vertex_iterations_per_s"] = value * job_vertices * ITERATIONS
+        line["e2e"]["value"] = 1e3 / e2e_ms
+    if rank == 0 and world == 1 and not args.no_learned and args.workload == "draped-cloth":
+        line["learned"] = learned_ab(dev, args.n or 256, value)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(model, q0)
+        if args.workload == "cloth-on-boxes":
+            line["cpu_baseline"] = {"value": None, "unit": "steps/s", "cores": 0, "kind": "port",
+                                    "sample": "not measured: the oracle's all-pairs self-contact detection is "
+                                              "O(V*T) (2e12 pair tests per detection at this size)"}
+        else:
+            line["cpu_baseline"] = cpu_baseline(model, q0)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
