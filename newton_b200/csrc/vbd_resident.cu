@@ -215,7 +215,9 @@ __global__ void __launch_bounds__(kResidentThreads, 1) resident_kernel(ResidentK
                     membrane_eval<kDamp>(static_cast<int>(ref & 3u), x0, x1, x2, p0, p1, p2, s_tri_D[e], mt, inv_dt,
                                          f, h);
                 }
-                for (int r = vr.z + lane; r < vr.w; r += kLanes) {
+                // hinges continue the round-robin deal of the merged record list
+                const int lane_e = (lane - (vr.y - vr.x) % kLanes + kLanes) % kLanes;
+                for (int r = vr.z + lane_e; r < vr.w; r += kLanes) {
                     const unsigned ref = s_refs[r];
                     const int e = static_cast<int>(ref >> 2);
                     const ushort4 hi = s_hinge_idx[e];

@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -195,6 +196,10 @@ struct SweepArgs {
 template <bool kDamp>
 __device__ __forceinline__ void accumulate_elements(const SweepArgs& a, int i, int lane, int L, int4 adj, float3& f,
                                                     Sym3& h) {
+    // the vertex's records are dealt round-robin over one merged list (triangles, then hinges),
+    // so every lane gets the same number of records to within one
+    const int nt = adj.y - adj.x;
+    const int lane_e = (lane - nt % L + L) % L;  // first hinge slot of this lane
     for (int r = adj.x + lane; r < adj.y; r += L) {
         const int4 ti = __ldg(&a.tri_idx[r]);
         const float4 D = __ldg(&a.tri_D[r]);
@@ -208,7 +213,7 @@ __device__ __forceinline__ void accumulate_elements(const SweepArgs& a, int i, i
         }
         membrane_eval<kDamp>(ti.w, x0, x1, x2, p0, p1, p2, D, mt, a.inv_dt, f, h);
     }
-    for (int r = adj.z + lane; r < adj.w; r += L) {
+    for (int r = adj.z + lane_e; r < adj.w; r += L) {
         const int4 ei = __ldg(&a.edge_idx[r]);
         const float4 em = __ldg(&a.edge_mat[r]);
         const int order = static_cast<int>(static_cast<unsigned>(ei.x) >> 30);
@@ -252,8 +257,10 @@ __device__ __forceinline__ float warp_sum(float v, int L) {
 // (kResidual = true).  L lanes cooperate on one vertex: each lane takes every L-th element record
 // (triangles, then hinges, as the reference's 16-thread tile does), then the partial force and
 // Hessian are summed across the L lanes with xor shuffles.
-template <int L, bool kDamp, bool kResidual>
-__global__ void __launch_bounds__(256) sweep_kernel(SweepArgs a) {
+// kCap: the same kernel limited to 64 registers per thread (4 blocks of 256 per SM), used when the
+// uncapped kernel would need more than one wave of blocks (large colors, many lanes per vertex)
+template <int L, bool kDamp, bool kResidual, bool kCap>
+__global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = a.v_begin + tid / L;
     const int lane = tid & (L - 1);
@@ -622,17 +629,61 @@ static SweepArgs make_sweep_args(const SolverImpl& s, const VbdContacts* c, floa
     return a;
 }
 
+// blocks of `kernel` resident on the whole device at `block` threads (cached per kernel / block)
+static long long resident_blocks(const void* kernel, int block) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, long long> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_pair(kernel, block);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+    const long long n = static_cast<long long>(std::max(per_sm, 1)) * std::max(sms, 1);
+    cache[key] = n;
+    return n;
+}
+
+template <int L, bool kDamp, bool kResidual>
+static void launch_sweep_LDR(const SweepArgs& a, int grid, int block, cudaStream_t st) {
+    const void* uncapped = reinterpret_cast<const void*>(&sweep_kernel<L, kDamp, kResidual, false>);
+    if (grid > resident_blocks(uncapped, block)) sweep_kernel<L, kDamp, kResidual, true><<<grid, block, 0, st>>>(a);
+    else sweep_kernel<L, kDamp, kResidual, false><<<grid, block, 0, st>>>(a);
+}
+
+// occupancy queries happen here, outside any stream capture (solver creation, vbd_set_launch)
+template <int L>
+static void prime_occupancy_L(int block) {
+    resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, true, true, false>), block);
+    resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, false, true, false>), block);
+    resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, true, false, false>), block);
+    resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, false, false, false>), block);
+}
+
+static void prime_occupancy(int lanes, int block) {
+    switch (lanes) {
+        case 1: prime_occupancy_L<1>(block); break;
+        case 2: prime_occupancy_L<2>(block); break;
+        case 4: prime_occupancy_L<4>(block); break;
+        case 8: prime_occupancy_L<8>(block); break;
+        case 16: prime_occupancy_L<16>(block); break;
+        default: break;
+    }
+}
+
 template <int L>
 static void launch_sweep_L(const SweepArgs& a, bool damp, bool residual, int block, cudaStream_t st) {
     const long long threads = static_cast<long long>(a.v_end - a.v_begin) * L;
     const int grid = static_cast<int>((threads + block - 1) / block);
     if (grid <= 0) return;
     if (residual) {
-        if (damp) sweep_kernel<L, true, true><<<grid, block, 0, st>>>(a);
-        else sweep_kernel<L, false, true><<<grid, block, 0, st>>>(a);
+        if (damp) launch_sweep_LDR<L, true, true>(a, grid, block, st);
+        else launch_sweep_LDR<L, false, true>(a, grid, block, st);
     } else {
-        if (damp) sweep_kernel<L, true, false><<<grid, block, 0, st>>>(a);
-        else sweep_kernel<L, false, false><<<grid, block, 0, st>>>(a);
+        if (damp) launch_sweep_LDR<L, true, false>(a, grid, block, st);
+        else launch_sweep_LDR<L, false, false>(a, grid, block, st);
     }
 }
 
@@ -905,6 +956,7 @@ extern "C" int vbd_solver_create(const VbdModel* model, const VbdSolverOptions* 
         cudaError_t e = cudaStreamCreateWithFlags(&s.capture_stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamCreateWithFlags");
     }
+    if (!rc) prime_occupancy(s.lanes, s.block);
     if (!rc && s.resident_on) rc = resident_build(m, s.resident);
     if (!rc && options && options->self_contact && m.V > 0) {
         SelfContactParams p;
@@ -1243,6 +1295,7 @@ extern "C" int vbd_set_launch(VbdSolver* solver, int32_t lanes_per_vertex, int32
         return fail(VBD_ERR_INVALID_ARGUMENT, std::string("vbd_set_launch: ") + why);
     solver->s.lanes = lanes_per_vertex;
     solver->s.block = block_size;
+    prime_occupancy(lanes_per_vertex, block_size);
     return VBD_OK;
 }
 
@@ -1310,6 +1363,7 @@ int static_scratch(unsigned char** out) {
         cudaError_t e = cudaGetSymbolAddress(&p, g_step_scratch);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_step_scratch)");
         g_static_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+        prime_occupancy(4, 128);  // the launch shape of the static step, queried before any capture
     }
     *out = g_static_scratch_ptr[dev];
     return VBD_OK;
