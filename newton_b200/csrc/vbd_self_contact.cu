@@ -83,6 +83,7 @@ struct GridArgs {
     const int* off;
     int* cur;
     int* items;
+    float4* item_box;     // [2 cap] the box of every bucket entry, next to its id (fill pass)
     int cap;
     float4* box;          // [2n] element boxes (lo, hi; lo.w = 1 for a large element), count pass
     unsigned* counters;
@@ -144,8 +145,13 @@ __global__ void grid_fill_kernel(GridArgs a) {
         const int3 c = center_cell(l4, h4, a.inv_cell);
         const unsigned h = cell_hash(c.x, c.y, c.z, a.mask);
         const int k = a.off[h] + atomicAdd(&a.cur[h], 1);
-        if (k < a.cap) a.items[k] = e;
-        else atomicAdd(&a.counters[kScGridOverflow], 1u);
+        if (k < a.cap) {
+            a.items[k] = e;
+            a.item_box[2 * k] = l4;
+            a.item_box[2 * k + 1] = h4;
+        } else {
+            atomicAdd(&a.counters[kScGridOverflow], 1u);
+        }
         return;
     }
     const CellRange r = cell_range(xyz(l4), xyz(h4), a.inv_cell);
@@ -155,8 +161,13 @@ __global__ void grid_fill_kernel(GridArgs a) {
             for (int x = r.lo.x; x <= r.hi.x; ++x) {
                 const unsigned h = cell_hash(x, y, z, a.mask);
                 const int k = a.off[h] + atomicAdd(&a.cur[h], 1);
-                if (k < a.cap) a.items[k] = e;
-                else atomicAdd(&a.counters[kScGridOverflow], 1u);
+                if (k < a.cap) {
+                    a.items[k] = e;
+                    a.item_box[2 * k] = l4;
+                    a.item_box[2 * k + 1] = h4;
+                } else {
+                    atomicAdd(&a.counters[kScGridOverflow], 1u);
+                }
             }
 }
 
@@ -206,7 +217,7 @@ struct QueryArgs {
     unsigned tri_mask, edge_mask;
     const int *tri_cnt, *tri_off, *tri_items;
     const int *edge_cnt, *edge_off, *edge_items;
-    const float4 *tri_box, *edge_box;
+    const float4 *tri_item_box, *edge_item_box;
     int tri_cap, edge_cap;
     int vbuf, ebuf;
     int* vt_count;
@@ -246,9 +257,9 @@ __global__ void vt_query_kernel(QueryArgs a) {
                 const int b = a.tri_off[h];
                 const int e = min(b + a.tri_cnt[h], a.tri_cap);
                 for (int k = b; k < e; ++k) {
-                    const int t = a.tri_items[k];
-                    const float4 blo = a.tri_box[2 * t], bhi = a.tri_box[2 * t + 1];
+                    const float4 blo = a.tri_item_box[2 * k], bhi = a.tri_item_box[2 * k + 1];
                     if (!boxes_overlap(plo, phi, blo, bhi)) continue;
+                    const int t = a.tri_items[k];
                     if (!in_cell(blo, bhi, a.inv_cell, x, y, z)) continue;  // another cell in this bucket
                     const int4 tr = a.tri[t];
                     if (tr.x == i || tr.y == i || tr.z == i) continue;
@@ -303,7 +314,7 @@ __global__ void ee_query_kernel(QueryArgs a) {
                 for (int k = b; k < en; ++k) {
                     const int g = a.edge_items[k];
                     if (g <= e) continue;
-                    const float4 blo = a.edge_box[2 * g], bhi = a.edge_box[2 * g + 1];
+                    const float4 blo = a.edge_item_box[2 * k], bhi = a.edge_item_box[2 * k + 1];
                     if (!boxes_overlap(qlo, qhi, blo, bhi)) continue;
                     if (blo.w == 0.f) {
                         const int3 c = center_cell(blo, bhi, a.inv_cell);
@@ -629,7 +640,7 @@ void self_contact_free(SelfContact& sc) {
                     sc.near,     sc.rest,     sc.tri_cnt,   sc.tri_off,  sc.tri_cur,    sc.tri_items, sc.edge_cnt,
                     sc.edge_off, sc.edge_cur, sc.edge_items, sc.scan_tmp, sc.vt_count,  sc.vt_list,   sc.ee_count,
                     sc.ee_list,  sc.tv_count, sc.tv_list,   sc.cd,       sc.sc_f,       sc.sc_h0,     sc.sc_h1,
-                    sc.ts,       sc.counters, sc.vworld,    sc.tri_box,  sc.edge_box,   sc.flag};
+                    sc.ts,       sc.counters, sc.vworld,    sc.tri_box,  sc.edge_box,   sc.flag,      sc.tri_item_box, sc.edge_item_box};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     SelfContact empty;
@@ -756,6 +767,8 @@ int self_contact_create(const VbdModelImpl& m, const SelfContactParams& p, SelfC
     az(reinterpret_cast<void**>(&sc.edge_items), static_cast<size_t>(sc.edge_items_cap) * sizeof(int));
     az(reinterpret_cast<void**>(&sc.tri_box), 2 * static_cast<size_t>(std::max(T, 1)) * sizeof(float4));
     az(reinterpret_cast<void**>(&sc.edge_box), 2 * static_cast<size_t>(std::max(E, 1)) * sizeof(float4));
+    az(reinterpret_cast<void**>(&sc.tri_item_box), 2 * static_cast<size_t>(sc.tri_items_cap) * sizeof(float4));
+    az(reinterpret_cast<void**>(&sc.edge_item_box), 2 * static_cast<size_t>(sc.edge_items_cap) * sizeof(float4));
     az(reinterpret_cast<void**>(&sc.flag), static_cast<size_t>(V));
     az(reinterpret_cast<void**>(&sc.vt_count), static_cast<size_t>(V) * sizeof(int));
     az(reinterpret_cast<void**>(&sc.vt_list), static_cast<size_t>(V) * p.vertex_buffer * sizeof(int));
@@ -828,6 +841,7 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     g.off = sc.tri_off;
     g.cur = sc.tri_cur;
     g.items = sc.tri_items;
+    g.item_box = sc.tri_item_box;
     g.cap = sc.tri_items_cap;
     g.box = sc.tri_box;
 
@@ -848,6 +862,7 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     g.off = sc.edge_off;
     g.cur = sc.edge_cur;
     g.items = sc.edge_items;
+    g.item_box = sc.edge_item_box;
     g.cap = sc.edge_items_cap;
     g.box = sc.edge_box;
 
@@ -882,8 +897,8 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     q.edge_cnt = sc.edge_cnt;
     q.edge_off = sc.edge_off;
     q.edge_items = sc.edge_items;
-    q.tri_box = sc.tri_box;
-    q.edge_box = sc.edge_box;
+    q.tri_item_box = sc.tri_item_box;
+    q.edge_item_box = sc.edge_item_box;
     q.tri_cap = sc.tri_items_cap;
     q.edge_cap = sc.edge_items_cap;
     q.vbuf = sc.p.vertex_buffer;

@@ -57,6 +57,7 @@ struct SelfContact {
     int *tri_cnt = nullptr, *tri_off = nullptr, *tri_cur = nullptr, *tri_items = nullptr;
     int *edge_cnt = nullptr, *edge_off = nullptr, *edge_cur = nullptr, *edge_items = nullptr;
     float4 *tri_box = nullptr, *edge_box = nullptr;   // [2T], [2E] element boxes of the last detection
+    float4 *tri_item_box = nullptr, *edge_item_box = nullptr;  // [2 cap] boxes next to the bucket entries
     void* scan_tmp = nullptr;
     size_t scan_bytes = 0;
     // detection results

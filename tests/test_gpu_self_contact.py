@@ -12,7 +12,7 @@ import pytest
 import torch
 
 import oracle
-from newton_b200 import scenes
+from newton_b200 import CollisionPipeline, scenes
 from newton_b200.solvers import SolverVBD
 
 pytestmark = pytest.mark.gpu
@@ -22,8 +22,8 @@ RADIUS, MARGIN = 0.004, 0.006
 TOL = 1e-5
 
 
-def _folded(n=24, side=0.5, gap=0.003):
-    model, q0 = scenes.single_cloth(n=n, side=side, seed=0, pin_top_corners=False, ground=None, z_noise=0.0)
+def _folded(n=24, side=0.5, gap=0.003, ground=None):
+    model, q0 = scenes.single_cloth(n=n, side=side, seed=0, pin_top_corners=False, ground=ground, z_noise=0.0)
     q = q0.astype(np.float64).copy()
     right = q[:, 0] > 0.0
     q[right, 0] = -q[right, 0]
@@ -80,6 +80,34 @@ def test_step_matches_oracle(interval):
     st = solver.status()
     assert st["nonfinite_updates"] == 0 and st["self_contact_overflow"] == 0
     print(f"self-contact step parity (interval {interval}): max |dx| = {worst:.3e} m over 6 steps")
+    assert worst <= TOL, worst
+
+
+def test_step_with_body_contacts_matches_oracle():
+    """Self-contact and particle-shape contact in the same step: the lower layer lies in the
+    ground plane's contact band (plane 4 mm below, particle radius 5 mm, margin 5 mm)."""
+    model, q, _ = _folded(ground=-0.004)
+    solver = _solver(model)
+    orc = _oracle(model)
+    pipe = CollisionPipeline(model, soft_contact_margin=5e-3)
+    c = pipe.contacts()
+    a, b = model.state(), model.state()
+    a.particle_q.copy_(torch.from_numpy(q).cuda())
+    worst = 0.0
+    n_contacts = 0
+    for _ in range(4):
+        q_in = a.particle_q.cpu().numpy().copy()
+        qd_in = a.particle_qd.cpu().numpy().copy()
+        pipe.collide(a, c)
+        n_contacts = max(n_contacts, c.count())
+        solver.step(a, b, None, c, DT)
+        orc.set_contacts(*oracle.collide(model, q_in, 5e-3))
+        _, q_ref, _ = orc.step(q_in, qd_in, None, DT, 5)
+        worst = max(worst, float(np.abs(b.particle_q.cpu().numpy() - q_ref).max()))
+        a, b = b, a
+    print(f"self-contact + ground contact parity: max |dx| = {worst:.3e} m, {n_contacts} ground contacts")
+    assert n_contacts > 0
+    assert solver.status()["nonfinite_updates"] == 0
     assert worst <= TOL, worst
 
 
