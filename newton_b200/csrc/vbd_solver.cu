@@ -269,11 +269,17 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
     Sym3 h = zero_sym();
     bool solve = false;
     float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+    int4 adj = make_int4(0, 0, 0, 0);
     if (valid) {
+        // vertex info and record ranges never change during a step: read them before waiting on
+        // the previous kernel (programmatic dependent launch; a no-op in an ordinary launch)
         pi = __ldg(&a.pinfo[i]);
+        adj = __ldg(&a.vadj[i]);
         solve = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
-        if (solve) accumulate_elements<kDamp>(a, i, lane, L, __ldg(&a.vadj[i]), f, h);
     }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;");
+    if (valid && solve) accumulate_elements<kDamp>(a, i, lane, L, adj, f, h);
     if (L > 1) {
         f.x = warp_sum(f.x, L);
         f.y = warp_sum(f.y, L);
@@ -646,11 +652,29 @@ static long long resident_blocks(const void* kernel, int block) {
     return n;
 }
 
+// Sweeps are launched as programmatic dependents of the previous kernel on the stream: their
+// blocks may start while that kernel drains and wait (griddepcontrol.wait) before reading any
+// position, so consecutive colors overlap launch latency instead of serialising it.
+template <typename Kernel>
+static void launch_dependent(Kernel kernel, int grid, int block, cudaStream_t st, const SweepArgs& a) {
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = st;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
 template <int L, bool kDamp, bool kResidual>
 static void launch_sweep_LDR(const SweepArgs& a, int grid, int block, cudaStream_t st) {
     const void* uncapped = reinterpret_cast<const void*>(&sweep_kernel<L, kDamp, kResidual, false>);
-    if (grid > resident_blocks(uncapped, block)) sweep_kernel<L, kDamp, kResidual, true><<<grid, block, 0, st>>>(a);
-    else sweep_kernel<L, kDamp, kResidual, false><<<grid, block, 0, st>>>(a);
+    if (grid > resident_blocks(uncapped, block)) launch_dependent(sweep_kernel<L, kDamp, kResidual, true>, grid, block, st, a);
+    else launch_dependent(sweep_kernel<L, kDamp, kResidual, false>, grid, block, st, a);
 }
 
 // occupancy queries happen here, outside any stream capture (solver creation, vbd_set_launch)
