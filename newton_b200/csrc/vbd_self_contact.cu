@@ -36,6 +36,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <vector>
 
@@ -228,126 +229,275 @@ struct QueryArgs {
 };
 
 constexpr int kMaxQueryCells = 512;
+constexpr int kWarpUnionCells = 128;  // larger warp unions fall back to one walk per lane
+constexpr int kQueryBlock = 128;
+constexpr int kQueryWarps = kQueryBlock / 32;
 
-__global__ void vt_query_kernel(QueryArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.V) return;
-    const float3 p = xyz(a.x[i]);
-    const float m = a.margin;
-    const float3 plo = p - f3(m, m, m), phi = p + f3(m, m, m);
-    // a small triangle within the margin has its box centre within margin + half a cell of p;
-    // a large one is in every cell its box overlaps
-    const float r = m + 0.5f / a.inv_cell;
-    const CellRange q = cell_range(p - f3(r, r, r), p + f3(r, r, r), a.inv_cell);
-    int n = 0;
-    int* row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
-    if (!(cell_count(q) <= kMaxQueryCells)) {
-        atomicAdd(&a.counters[kScGridOverflow], 1u);
-        a.vt_count[i] = 0;
-        return;
+// ---- vertex-triangle candidates ------------------------------------------------------------
+struct VtQuery {
+    int i;
+    float3 p, plo, phi;
+    CellRange q;
+    int wv;
+    const int *nb, *ne;
+    int* row;
+    int n;
+    bool full;
+};
+
+// the tests after the box pre-filter; appends t to the vertex's sorted list
+__device__ __forceinline__ void vt_accept(const QueryArgs& a, VtQuery& v, int t) {
+    const int4 tr = a.tri[t];
+    const int i = v.i;
+    if (tr.x == i || tr.y == i || tr.z == i) return;
+    if (v.wv >= 0 && tr.w >= 0 && v.wv != tr.w) return;
+    if (list_contains(v.nb, v.ne, tr.x) || list_contains(v.nb, v.ne, tr.y) || list_contains(v.nb, v.ne, tr.z)) return;
+    float3 bary;
+    const float dist = length(triangle_closest_point(xyz(a.x[tr.x]), xyz(a.x[tr.y]), xyz(a.x[tr.z]), v.p, bary) - v.p);
+    if (!(dist < a.margin)) return;
+    if (a.rest_excl > 0.f) {
+        const float3 rp = xyz(a.rest[i]);
+        const float dr = length(
+            triangle_closest_point(xyz(a.rest[tr.x]), xyz(a.rest[tr.y]), xyz(a.rest[tr.z]), rp, bary) - rp);
+        if (dr < a.rest_excl) return;
     }
-    const int wv = a.vworld[i];
-    const int* nb = a.near + a.near_off[i];
-    const int* ne = a.near + a.near_off[i + 1];
-    bool full = false;
-    for (int z = q.lo.z; z <= q.hi.z; ++z)
-        for (int y = q.lo.y; y <= q.hi.y; ++y)
-            for (int x = q.lo.x; x <= q.hi.x; ++x) {
+    if (!sorted_insert(v.row, v.n, a.vbuf, t)) v.full = true;
+}
+
+__device__ __forceinline__ void vt_scan_lane(const QueryArgs& a, VtQuery& v) {
+    for (int z = v.q.lo.z; z <= v.q.hi.z; ++z)
+        for (int y = v.q.lo.y; y <= v.q.hi.y; ++y)
+            for (int x = v.q.lo.x; x <= v.q.hi.x; ++x) {
                 const unsigned h = cell_hash(x, y, z, a.tri_mask);
                 const int b = a.tri_off[h];
                 const int e = min(b + a.tri_cnt[h], a.tri_cap);
                 for (int k = b; k < e; ++k) {
                     const float4 blo = a.tri_item_box[2 * k], bhi = a.tri_item_box[2 * k + 1];
-                    if (!boxes_overlap(plo, phi, blo, bhi)) continue;
-                    const int t = a.tri_items[k];
+                    if (!boxes_overlap(v.plo, v.phi, blo, bhi)) continue;
                     if (!in_cell(blo, bhi, a.inv_cell, x, y, z)) continue;  // another cell in this bucket
-                    const int4 tr = a.tri[t];
-                    if (tr.x == i || tr.y == i || tr.z == i) continue;
-                    if (wv >= 0 && tr.w >= 0 && wv != tr.w) continue;
-                    if (list_contains(nb, ne, tr.x) || list_contains(nb, ne, tr.y) || list_contains(nb, ne, tr.z))
-                        continue;
-                    const float3 t0 = xyz(a.x[tr.x]), t1 = xyz(a.x[tr.y]), t2 = xyz(a.x[tr.z]);
-                    float3 bary;
-                    const float dist = length(triangle_closest_point(t0, t1, t2, p, bary) - p);
-                    if (!(dist < m)) continue;
-                    if (a.rest_excl > 0.f) {
-                        const float3 rp = xyz(a.rest[i]);
-                        const float dr = length(triangle_closest_point(xyz(a.rest[tr.x]), xyz(a.rest[tr.y]),
-                                                                       xyz(a.rest[tr.z]), rp, bary) -
-                                                rp);
-                        if (dr < a.rest_excl) continue;
-                    }
-                    if (!sorted_insert(row, n, a.vbuf, t)) full = true;
+                    vt_accept(a, v, a.tri_items[k]);
                 }
             }
-    a.vt_count[i] = n;
-    if (full) atomicAdd(&a.counters[kScVtOverflow], 1u);
 }
 
+__device__ __forceinline__ bool warp_union(bool ok, const CellRange& q, CellRange& u) {
+    const unsigned all = 0xffffffffu;
+    if (__ballot_sync(all, ok) == 0u) return false;
+    u.lo = make_int3(__reduce_min_sync(all, ok ? q.lo.x : INT_MAX), __reduce_min_sync(all, ok ? q.lo.y : INT_MAX),
+                     __reduce_min_sync(all, ok ? q.lo.z : INT_MAX));
+    u.hi = make_int3(__reduce_max_sync(all, ok ? q.hi.x : INT_MIN), __reduce_max_sync(all, ok ? q.hi.y : INT_MIN),
+                     __reduce_max_sync(all, ok ? q.hi.z : INT_MIN));
+    return true;
+}
+
+__device__ __forceinline__ bool in_range(const CellRange& q, int x, int y, int z) {
+    return x >= q.lo.x && x <= q.hi.x && y >= q.lo.y && y <= q.hi.y && z >= q.lo.z && z <= q.hi.z;
+}
+
+// A warp of 32 consecutive vertices walks the union of their query ranges once: every bucket
+// entry is staged in shared memory by one lane and tested by all lanes against their own query,
+// so the cheap rejections run with every lane active (a walk per lane diverges: its buckets
+// differ in length from its neighbours').
+__global__ void __launch_bounds__(kQueryBlock) vt_query_kernel(QueryArgs a) {
+    __shared__ int s_id[kQueryWarps][32];
+    __shared__ float4 s_box[kQueryWarps][64];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < a.V;
+    VtQuery v;
+    v.i = i;
+    v.n = 0;
+    v.full = false;
+    bool ok = false;
+    if (active) {
+        v.p = xyz(a.x[i]);
+        const float m = a.margin;
+        v.plo = v.p - f3(m, m, m);
+        v.phi = v.p + f3(m, m, m);
+        // a small triangle within the margin has its box centre within margin + half a cell of p;
+        // a large one is in every cell its box overlaps
+        const float r = m + 0.5f / a.inv_cell;
+        v.q = cell_range(v.p - f3(r, r, r), v.p + f3(r, r, r), a.inv_cell);
+        ok = cell_count(v.q) <= kMaxQueryCells;
+        if (!ok) {
+            atomicAdd(&a.counters[kScGridOverflow], 1u);
+            a.vt_count[i] = 0;
+        } else {
+            v.wv = a.vworld[i];
+            v.nb = a.near + a.near_off[i];
+            v.ne = a.near + a.near_off[i + 1];
+            v.row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
+        }
+    }
+    CellRange u;
+    if (!warp_union(ok, v.q, u)) return;
+    if (cell_count(u) > kWarpUnionCells) {
+        if (ok) vt_scan_lane(a, v);
+    } else {
+        for (int z = u.lo.z; z <= u.hi.z; ++z)
+            for (int y = u.lo.y; y <= u.hi.y; ++y)
+                for (int x = u.lo.x; x <= u.hi.x; ++x) {
+                    const bool mine = ok && in_range(v.q, x, y, z);
+                    if (!__any_sync(0xffffffffu, mine)) continue;
+                    const unsigned h = cell_hash(x, y, z, a.tri_mask);
+                    const int b = a.tri_off[h];
+                    const int cnt = min(b + a.tri_cnt[h], a.tri_cap) - b;
+                    for (int c = 0; c < cnt; c += 32) {
+                        if (c + lane < cnt) {
+                            const int k = b + c + lane;
+                            s_id[w][lane] = a.tri_items[k];
+                            s_box[w][2 * lane] = a.tri_item_box[2 * k];
+                            s_box[w][2 * lane + 1] = a.tri_item_box[2 * k + 1];
+                        }
+                        __syncwarp();
+                        const int mc = min(32, cnt - c);
+                        if (mine) {
+                            for (int t = 0; t < mc; ++t) {
+                                const float4 blo = s_box[w][2 * t], bhi = s_box[w][2 * t + 1];
+                                if (!boxes_overlap(v.plo, v.phi, blo, bhi)) continue;
+                                if (!in_cell(blo, bhi, a.inv_cell, x, y, z)) continue;
+                                vt_accept(a, v, s_id[w][t]);
+                            }
+                        }
+                        __syncwarp();
+                    }
+                }
+    }
+    if (ok) {
+        a.vt_count[i] = v.n;
+        if (v.full) atomicAdd(&a.counters[kScVtOverflow], 1u);
+    }
+}
+
+// ---- edge-edge candidates ------------------------------------------------------------------
 // Edge-edge pairs are symmetric: edge e only searches partners g > e and records the pair in both
 // lists through atomic slots; ee_sort_kernel then orders every list.  A small partner sits in one
 // bucket only; a large (multi-cell) partner is taken in the first cell of the query range it
 // occupies, so every pair is met exactly once.
-__global__ void ee_query_kernel(QueryArgs a) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= a.E) return;
-    const int4 ed = a.edge[e];
-    const float3 a0 = xyz(a.x[ed.x]), a1 = xyz(a.x[ed.y]);
-    const float m = a.margin;
-    const float3 qlo = fmin3(a0, a1) - f3(m, m, m), qhi = fmax3(a0, a1) + f3(m, m, m);
-    const float r = 0.5f / a.inv_cell;
-    const CellRange q = cell_range(qlo - f3(r, r, r), qhi + f3(r, r, r), a.inv_cell);
-    if (!(cell_count(q) <= kMaxQueryCells)) {
-        atomicAdd(&a.counters[kScGridOverflow], 1u);
-        return;
+struct EeQuery {
+    int e;
+    int4 ed;
+    float3 a0, a1, qlo, qhi;
+    CellRange q;
+    const int *n0b, *n0e, *n1b, *n1e;
+};
+
+__device__ __forceinline__ bool ee_owns(const EeQuery& v, float4 blo, float4 bhi, float inv, int x, int y, int z) {
+    if (blo.w == 0.f) {
+        const int3 c = center_cell(blo, bhi, inv);
+        return c.x == x && c.y == y && c.z == z;
     }
-    const int* n0b = a.near + a.near_off[ed.x];
-    const int* n0e = a.near + a.near_off[ed.x + 1];
-    const int* n1b = a.near + a.near_off[ed.y];
-    const int* n1e = a.near + a.near_off[ed.y + 1];
-    for (int z = q.lo.z; z <= q.hi.z; ++z)
-        for (int y = q.lo.y; y <= q.hi.y; ++y)
-            for (int x = q.lo.x; x <= q.hi.x; ++x) {
+    const CellRange gr = cell_range(xyz(blo), xyz(bhi), inv);
+    if (max(v.q.lo.x, gr.lo.x) != x || max(v.q.lo.y, gr.lo.y) != y || max(v.q.lo.z, gr.lo.z) != z) return false;
+    return x <= gr.hi.x && y <= gr.hi.y && z <= gr.hi.z;
+}
+
+__device__ __forceinline__ void ee_accept(const QueryArgs& a, const EeQuery& v, int g) {
+    const int4 gd = a.edge[g];
+    const int4 ed = v.ed;
+    if (gd.x == ed.x || gd.x == ed.y || gd.y == ed.x || gd.y == ed.y) return;
+    if (ed.z >= 0 && gd.z >= 0 && ed.z != gd.z) return;
+    if (list_contains(v.n0b, v.n0e, gd.x) || list_contains(v.n0b, v.n0e, gd.y) || list_contains(v.n1b, v.n1e, gd.x) ||
+        list_contains(v.n1b, v.n1e, gd.y))
+        return;
+    float s, t, dist;
+    closest_edge_edge(v.a0, v.a1, xyz(a.x[gd.x]), xyz(a.x[gd.y]), a.par_eps, s, t, dist);
+    if (!(dist < a.margin)) return;
+    if (a.rest_excl > 0.f) {
+        float sr, tr, dr;
+        closest_edge_edge(xyz(a.rest[ed.x]), xyz(a.rest[ed.y]), xyz(a.rest[gd.x]), xyz(a.rest[gd.y]), a.par_eps, sr,
+                          tr, dr);
+        if (dr < a.rest_excl) return;
+    }
+    // the distance of (e, g) and of (g, e) is the same test; record both sides
+    const int e = v.e;
+    const int ke = atomicAdd(&a.ee_count[e], 1);
+    if (ke < a.ebuf) a.ee_list[static_cast<size_t>(e) * a.ebuf + ke] = g;
+    else atomicAdd(&a.counters[kScEeOverflow], 1u);
+    const int kg = atomicAdd(&a.ee_count[g], 1);
+    if (kg < a.ebuf) a.ee_list[static_cast<size_t>(g) * a.ebuf + kg] = e;
+    else atomicAdd(&a.counters[kScEeOverflow], 1u);
+}
+
+__device__ __forceinline__ void ee_scan_lane(const QueryArgs& a, const EeQuery& v) {
+    for (int z = v.q.lo.z; z <= v.q.hi.z; ++z)
+        for (int y = v.q.lo.y; y <= v.q.hi.y; ++y)
+            for (int x = v.q.lo.x; x <= v.q.hi.x; ++x) {
                 const unsigned h = cell_hash(x, y, z, a.edge_mask);
                 const int b = a.edge_off[h];
                 const int en = min(b + a.edge_cnt[h], a.edge_cap);
                 for (int k = b; k < en; ++k) {
                     const int g = a.edge_items[k];
-                    if (g <= e) continue;
+                    if (g <= v.e) continue;
                     const float4 blo = a.edge_item_box[2 * k], bhi = a.edge_item_box[2 * k + 1];
-                    if (!boxes_overlap(qlo, qhi, blo, bhi)) continue;
-                    if (blo.w == 0.f) {
-                        const int3 c = center_cell(blo, bhi, a.inv_cell);
-                        if (c.x != x || c.y != y || c.z != z) continue;
-                    } else {
-                        const CellRange gr = cell_range(xyz(blo), xyz(bhi), a.inv_cell);
-                        if (max(q.lo.x, gr.lo.x) != x || max(q.lo.y, gr.lo.y) != y || max(q.lo.z, gr.lo.z) != z)
-                            continue;
-                        if (x > gr.hi.x || y > gr.hi.y || z > gr.hi.z) continue;
+                    if (!boxes_overlap(v.qlo, v.qhi, blo, bhi)) continue;
+                    if (!ee_owns(v, blo, bhi, a.inv_cell, x, y, z)) continue;
+                    ee_accept(a, v, g);
+                }
+            }
+}
+
+__global__ void __launch_bounds__(kQueryBlock) ee_query_kernel(QueryArgs a) {
+    __shared__ int s_id[kQueryWarps][32];
+    __shared__ float4 s_box[kQueryWarps][64];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    EeQuery v;
+    v.e = e;
+    bool ok = false;
+    if (e < a.E) {
+        v.ed = a.edge[e];
+        v.a0 = xyz(a.x[v.ed.x]);
+        v.a1 = xyz(a.x[v.ed.y]);
+        const float m = a.margin;
+        v.qlo = fmin3(v.a0, v.a1) - f3(m, m, m);
+        v.qhi = fmax3(v.a0, v.a1) + f3(m, m, m);
+        const float r = 0.5f / a.inv_cell;
+        v.q = cell_range(v.qlo - f3(r, r, r), v.qhi + f3(r, r, r), a.inv_cell);
+        ok = cell_count(v.q) <= kMaxQueryCells;
+        if (!ok) {
+            atomicAdd(&a.counters[kScGridOverflow], 1u);
+        } else {
+            v.n0b = a.near + a.near_off[v.ed.x];
+            v.n0e = a.near + a.near_off[v.ed.x + 1];
+            v.n1b = a.near + a.near_off[v.ed.y];
+            v.n1e = a.near + a.near_off[v.ed.y + 1];
+        }
+    }
+    CellRange u;
+    if (!warp_union(ok, v.q, u)) return;
+    if (cell_count(u) > kWarpUnionCells) {
+        if (ok) ee_scan_lane(a, v);
+        return;
+    }
+    for (int z = u.lo.z; z <= u.hi.z; ++z)
+        for (int y = u.lo.y; y <= u.hi.y; ++y)
+            for (int x = u.lo.x; x <= u.hi.x; ++x) {
+                const bool mine = ok && in_range(v.q, x, y, z);
+                if (!__any_sync(0xffffffffu, mine)) continue;
+                const unsigned h = cell_hash(x, y, z, a.edge_mask);
+                const int b = a.edge_off[h];
+                const int cnt = min(b + a.edge_cnt[h], a.edge_cap) - b;
+                for (int c = 0; c < cnt; c += 32) {
+                    if (c + lane < cnt) {
+                        const int k = b + c + lane;
+                        s_id[w][lane] = a.edge_items[k];
+                        s_box[w][2 * lane] = a.edge_item_box[2 * k];
+                        s_box[w][2 * lane + 1] = a.edge_item_box[2 * k + 1];
                     }
-                    const int4 gd = a.edge[g];
-                    if (gd.x == ed.x || gd.x == ed.y || gd.y == ed.x || gd.y == ed.y) continue;
-                    if (ed.z >= 0 && gd.z >= 0 && ed.z != gd.z) continue;
-                    if (list_contains(n0b, n0e, gd.x) || list_contains(n0b, n0e, gd.y) ||
-                        list_contains(n1b, n1e, gd.x) || list_contains(n1b, n1e, gd.y))
-                        continue;
-                    const float3 b0 = xyz(a.x[gd.x]), b1 = xyz(a.x[gd.y]);
-                    float s, t, dist;
-                    closest_edge_edge(a0, a1, b0, b1, a.par_eps, s, t, dist);
-                    if (!(dist < m)) continue;
-                    if (a.rest_excl > 0.f) {
-                        float sr, tr, dr;
-                        closest_edge_edge(xyz(a.rest[ed.x]), xyz(a.rest[ed.y]), xyz(a.rest[gd.x]), xyz(a.rest[gd.y]),
-                                          a.par_eps, sr, tr, dr);
-                        if (dr < a.rest_excl) continue;
+                    __syncwarp();
+                    const int mc = min(32, cnt - c);
+                    if (mine) {
+                        for (int t = 0; t < mc; ++t) {
+                            const int g = s_id[w][t];
+                            if (g <= e) continue;
+                            const float4 blo = s_box[w][2 * t], bhi = s_box[w][2 * t + 1];
+                            if (!boxes_overlap(v.qlo, v.qhi, blo, bhi)) continue;
+                            if (!ee_owns(v, blo, bhi, a.inv_cell, x, y, z)) continue;
+                            ee_accept(a, v, g);
+                        }
                     }
-                    // the distance of (e, g) and of (g, e) is the same test; record both sides
-                    const int ke = atomicAdd(&a.ee_count[e], 1);
-                    if (ke < a.ebuf) a.ee_list[static_cast<size_t>(e) * a.ebuf + ke] = g;
-                    else atomicAdd(&a.counters[kScEeOverflow], 1u);
-                    const int kg = atomicAdd(&a.ee_count[g], 1);
-                    if (kg < a.ebuf) a.ee_list[static_cast<size_t>(g) * a.ebuf + kg] = e;
-                    else atomicAdd(&a.counters[kScEeOverflow], 1u);
+                    __syncwarp();
                 }
             }
 }
@@ -909,7 +1059,7 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     q.ee_list = sc.ee_list;
     q.counters = sc.counters;
     if (T > 0) {
-        vt_query_kernel<<<(V + 127) / 128, 128, 0, st>>>(q);
+        vt_query_kernel<<<(V + kQueryBlock - 1) / kQueryBlock, kQueryBlock, 0, st>>>(q);
         VBD_CUDA_TRY(cudaGetLastError());
         tri_reverse_kernel<<<(V + 255) / 256, 256, 0, st>>>(V, sc.vt_count, sc.vt_list, sc.p.vertex_buffer,
                                                             sc.tv_count, sc.tv_list, sc.tcap, sc.counters);
@@ -921,7 +1071,7 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     }
     if (E > 0) {
         VBD_CUDA_TRY(cudaMemsetAsync(sc.ee_count, 0, static_cast<size_t>(E) * sizeof(int), st));
-        ee_query_kernel<<<(E + 127) / 128, 128, 0, st>>>(q);
+        ee_query_kernel<<<(E + kQueryBlock - 1) / kQueryBlock, kQueryBlock, 0, st>>>(q);
         VBD_CUDA_TRY(cudaGetLastError());
         ee_sort_kernel<<<(E + 255) / 256, 256, 0, st>>>(E, sc.ee_count, sc.ee_list, sc.p.edge_buffer);
         VBD_CUDA_TRY(cudaGetLastError());
