@@ -145,6 +145,14 @@ typedef struct VbdSolverOptions {
     float edge_parallel_epsilon;           /* particle_edge_parallel_epsilon (1e-5) */
     int32_t topological_filter_threshold;  /* particle_topological_contact_filter_threshold (2) */
     float rest_exclusion_radius;           /* particle_rest_shape_contact_exclusion_radius (0) */
+    /* particle_external_vertex_contact_filtering_map / ..._edge_... as HOST CSR arrays (may be NULL):
+       vertex v never collides with triangles vertex_filter_triangles[offsets[v] .. offsets[v+1]),
+       edge e never with edges edge_filter_edges[offsets[e] .. offsets[e+1]); each list ascending.
+       Copied at vbd_solver_create. */
+    const int32_t* vertex_filter_offsets;  /* [V+1] */
+    const int32_t* vertex_filter_triangles;
+    const int32_t* edge_filter_offsets;    /* [E+1] */
+    const int32_t* edge_filter_edges;
 } VbdSolverOptions;
 
 /* Soft-contact records in the reference layout (newton.Contacts soft_contact_*; DEVICE pointers). */

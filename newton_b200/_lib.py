@@ -95,6 +95,10 @@ class VbdSolverOptions(ctypes.Structure):
         ("edge_parallel_epsilon", ctypes.c_float),
         ("topological_filter_threshold", ctypes.c_int32),
         ("rest_exclusion_radius", ctypes.c_float),
+        ("vertex_filter_offsets", ctypes.c_void_p),
+        ("vertex_filter_triangles", ctypes.c_void_p),
+        ("edge_filter_offsets", ctypes.c_void_p),
+        ("edge_filter_edges", ctypes.c_void_p),
     ]
 
 

@@ -199,6 +199,18 @@ __device__ __forceinline__ bool sorted_insert(int* row, int& n, int cap, int x) 
     return true;
 }
 
+__device__ __forceinline__ bool filtered(const int* off, const int* list, int row, int x) {
+    if (!off) return false;
+    const int* b = list + off[row];
+    const int* e = list + off[row + 1];
+    while (b < e) {
+        const int* mid = b + (e - b) / 2;
+        if (*mid < x) b = mid + 1;
+        else e = mid;
+    }
+    return b < list + off[row + 1] && *b == x;
+}
+
 __device__ __forceinline__ bool list_contains(const int* b, const int* e, int x) {
     for (const int* p = b; p < e; ++p)
         if (*p == x) return true;
@@ -208,6 +220,7 @@ __device__ __forceinline__ bool list_contains(const int* b, const int* e, int x)
 struct QueryArgs {
     const float4* x;
     const int* vworld;
+    const int *vfilt_off, *vfilt, *efilt_off, *efilt;  // external filter lists (NULL: none)
     const float4* rest;
     const int4* tri;
     const int4* edge;
@@ -252,6 +265,7 @@ __device__ __forceinline__ void vt_accept(const QueryArgs& a, VtQuery& v, int t)
     if (tr.x == i || tr.y == i || tr.z == i) return;
     if (v.wv >= 0 && tr.w >= 0 && v.wv != tr.w) return;
     if (list_contains(v.nb, v.ne, tr.x) || list_contains(v.nb, v.ne, tr.y) || list_contains(v.nb, v.ne, tr.z)) return;
+    if (filtered(a.vfilt_off, a.vfilt, i, t)) return;
     float3 bary;
     const float dist = length(triangle_closest_point(xyz(a.x[tr.x]), xyz(a.x[tr.y]), xyz(a.x[tr.z]), v.p, bary) - v.p);
     if (!(dist < a.margin)) return;
@@ -409,14 +423,19 @@ __device__ __forceinline__ void ee_accept(const QueryArgs& a, const EeQuery& v, 
                           tr, dr);
         if (dr < a.rest_excl) return;
     }
-    // the distance of (e, g) and of (g, e) is the same test; record both sides
+    // the distance of (e, g) and of (g, e) is the same test; record both sides (each side's
+    // external filter applies to its own list)
     const int e = v.e;
-    const int ke = atomicAdd(&a.ee_count[e], 1);
-    if (ke < a.ebuf) a.ee_list[static_cast<size_t>(e) * a.ebuf + ke] = g;
-    else atomicAdd(&a.counters[kScEeOverflow], 1u);
-    const int kg = atomicAdd(&a.ee_count[g], 1);
-    if (kg < a.ebuf) a.ee_list[static_cast<size_t>(g) * a.ebuf + kg] = e;
-    else atomicAdd(&a.counters[kScEeOverflow], 1u);
+    if (!filtered(a.efilt_off, a.efilt, e, g)) {
+        const int ke = atomicAdd(&a.ee_count[e], 1);
+        if (ke < a.ebuf) a.ee_list[static_cast<size_t>(e) * a.ebuf + ke] = g;
+        else atomicAdd(&a.counters[kScEeOverflow], 1u);
+    }
+    if (!filtered(a.efilt_off, a.efilt, g, e)) {
+        const int kg = atomicAdd(&a.ee_count[g], 1);
+        if (kg < a.ebuf) a.ee_list[static_cast<size_t>(g) * a.ebuf + kg] = e;
+        else atomicAdd(&a.counters[kScEeOverflow], 1u);
+    }
 }
 
 __device__ __forceinline__ void ee_scan_lane(const QueryArgs& a, const EeQuery& v) {
@@ -790,7 +809,7 @@ void self_contact_free(SelfContact& sc) {
                     sc.near,     sc.rest,     sc.tri_cnt,   sc.tri_off,  sc.tri_cur,    sc.tri_items, sc.edge_cnt,
                     sc.edge_off, sc.edge_cur, sc.edge_items, sc.scan_tmp, sc.vt_count,  sc.vt_list,   sc.ee_count,
                     sc.ee_list,  sc.tv_count, sc.tv_list,   sc.cd,       sc.sc_f,       sc.sc_h0,     sc.sc_h1,
-                    sc.ts,       sc.counters, sc.vworld,    sc.tri_box,  sc.edge_box,   sc.flag,      sc.tri_item_box, sc.edge_item_box};
+                    sc.ts,       sc.counters, sc.vworld,    sc.tri_box,  sc.edge_box,   sc.flag,      sc.tri_item_box, sc.edge_item_box, sc.vfilt_off, sc.vfilt, sc.efilt_off, sc.efilt};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     SelfContact empty;
@@ -809,6 +828,20 @@ int self_contact_create(const VbdModelImpl& m, const SelfContactParams& p, SelfC
         return fail(VBD_ERR_INVALID_ARGUMENT, "self contact: buffer sizes must be in [1, 256] / [1, 512]");
     if (p.filter_threshold > 4)
         return fail(VBD_ERR_UNSUPPORTED, "self contact: topological filter threshold above 4 is not supported");
+    auto bad_csr = [](const std::vector<int>& off, const std::vector<int>& lst, int rows, int maxval) {
+        if (off.empty()) return false;
+        if (static_cast<int>(off.size()) != rows + 1 || off[0] != 0 || off[rows] != static_cast<int>(lst.size()))
+            return true;
+        for (int r = 0; r < rows; ++r) {
+            if (off[r + 1] < off[r]) return true;
+            for (int k = off[r]; k < off[r + 1]; ++k)
+                if (lst[k] < 0 || lst[k] >= maxval || (k > off[r] && lst[k] <= lst[k - 1])) return true;
+        }
+        return false;
+    };
+    if (bad_csr(p.vertex_filter_off, p.vertex_filter, m.V, m.T) || bad_csr(p.edge_filter_off, p.edge_filter, m.E, m.E))
+        return fail(VBD_ERR_INVALID_ARGUMENT,
+                    "self contact: external filter lists must be CSR rows of ascending element ids in range");
     if (m.rest_q_h.size() != 3 * static_cast<size_t>(m.V))
         return fail(VBD_ERR_INVALID_ARGUMENT, "self contact needs the model's rest positions (VbdModelDesc.particle_q)");
     const int V = m.V, T = m.T, E = m.E;
@@ -899,6 +932,21 @@ int self_contact_create(const VbdModelImpl& m, const SelfContactParams& p, SelfC
     if (!rc) rc = upload_vec(&sc.near, near_list);
     if (!rc) rc = upload_vec(&sc.rest, rest);
     if (!rc) rc = upload_vec(&sc.vworld, vworld);
+    if (!rc && !p.vertex_filter_off.empty()) {
+        std::vector<int> off(V + 1, 0), lst;
+        for (int i = 0; i < V; ++i) {
+            const int o = m.perm_host[i];
+            lst.insert(lst.end(), p.vertex_filter.begin() + p.vertex_filter_off[o],
+                       p.vertex_filter.begin() + p.vertex_filter_off[o + 1]);
+            off[i + 1] = static_cast<int>(lst.size());
+        }
+        rc = upload_vec(&sc.vfilt_off, off);
+        if (!rc) rc = upload_vec(&sc.vfilt, lst);
+    }
+    if (!rc && !p.edge_filter_off.empty()) {
+        rc = upload_vec(&sc.efilt_off, p.edge_filter_off);
+        if (!rc) rc = upload_vec(&sc.efilt, p.edge_filter);
+    }
     const unsigned tn = next_pow2(2LL * std::max(T, 1)), en = next_pow2(2LL * std::max(E, 1));
     sc.tri_mask = tn - 1;
     sc.edge_mask = en - 1;
@@ -1027,6 +1075,10 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     QueryArgs q;
     q.x = sc.cd;
     q.vworld = sc.vworld;
+    q.vfilt_off = sc.vfilt_off;
+    q.vfilt = sc.vfilt;
+    q.efilt_off = sc.efilt_off;
+    q.efilt = sc.efilt;
     q.rest = sc.rest;
     q.tri = sc.tri;
     q.edge = sc.edge;

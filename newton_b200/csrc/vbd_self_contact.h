@@ -15,6 +15,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "vbd_internal.h"
 
 namespace vbd {
@@ -29,6 +31,8 @@ struct SelfContactParams {
     int edge_buffer = 64;
     int interval = 0;
     int filter_threshold = 2;
+    // external filter lists (host CSR, ascending per row; may be empty)
+    std::vector<int> vertex_filter_off, vertex_filter, edge_filter_off, edge_filter;
 };
 
 enum SelfContactCounter { kScVtOverflow = 0, kScEeOverflow = 1, kScTvOverflow = 2, kScGridOverflow = 3, kScCounters = 4 };
@@ -53,6 +57,10 @@ struct SelfContact {
     int* near = nullptr;       // vertices within (threshold - 1) rings, self excluded
     float4* rest = nullptr;    // [V] rest positions (exclusion radius)
     int* vworld = nullptr;     // [V] particle world
+    int* vfilt_off = nullptr;  // [V+1] external vertex-triangle filter (internal vertex order), or NULL
+    int* vfilt = nullptr;
+    int* efilt_off = nullptr;  // [E+1] external edge-edge filter, or NULL
+    int* efilt = nullptr;
     // grids
     int *tri_cnt = nullptr, *tri_off = nullptr, *tri_cur = nullptr, *tri_items = nullptr;
     int *edge_cnt = nullptr, *edge_off = nullptr, *edge_cur = nullptr, *edge_items = nullptr;

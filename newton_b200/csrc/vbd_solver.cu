@@ -993,6 +993,17 @@ extern "C" int vbd_solver_create(const VbdModel* model, const VbdSolverOptions* 
         p.edge_buffer = options->edge_contact_buffer_size;
         p.interval = options->collision_detection_interval;
         p.filter_threshold = options->topological_filter_threshold;
+        if (options->vertex_filter_offsets) {
+            p.vertex_filter_off.assign(options->vertex_filter_offsets, options->vertex_filter_offsets + m.V + 1);
+            if (options->vertex_filter_triangles)
+                p.vertex_filter.assign(options->vertex_filter_triangles,
+                                       options->vertex_filter_triangles + p.vertex_filter_off[m.V]);
+        }
+        if (options->edge_filter_offsets) {
+            p.edge_filter_off.assign(options->edge_filter_offsets, options->edge_filter_offsets + m.E + 1);
+            if (options->edge_filter_edges)
+                p.edge_filter.assign(options->edge_filter_edges, options->edge_filter_edges + p.edge_filter_off[m.E]);
+        }
         rc = self_contact_create(m, p, s.sc);
     }
     if (rc) {

@@ -76,8 +76,7 @@ class SolverVBD(SolverBase):
                     "missing contacts and cause instability.\nIt is advisable to make particle_self_contact_margin "
                     "1.5-2 times larger than particle_self_contact_radius."
                 )
-            if particle_external_vertex_contact_filtering_map or particle_external_edge_contact_filtering_map:
-                raise NotImplementedError("external self-contact filtering maps are not supported by this solver")
+
         if len(model.particle_color_groups) == 0:
             raise ValueError(
                 "model.particle_color_groups is empty! When using the SolverVBD you must call ModelBuilder.color() "
@@ -106,6 +105,22 @@ class SolverVBD(SolverBase):
             opts.edge_parallel_epsilon = float(particle_edge_parallel_epsilon)
             opts.topological_filter_threshold = int(particle_topological_contact_filter_threshold)
             opts.rest_exclusion_radius = float(particle_rest_shape_contact_exclusion_radius)
+            self._filters = []  # keeps the CSR arrays alive while the library copies them
+            for mapping, rows, off_name, list_name in (
+                (particle_external_vertex_contact_filtering_map, model.particle_count, "vertex_filter_offsets",
+                 "vertex_filter_triangles"),
+                (particle_external_edge_contact_filtering_map, model.edge_count, "edge_filter_offsets",
+                 "edge_filter_edges"),
+            ):
+                if not mapping:
+                    continue
+                lists = [sorted({int(x) for x in mapping.get(r, ())}) for r in range(rows)]
+                off = np.zeros(rows + 1, np.int32)
+                off[1:] = np.cumsum([len(l) for l in lists])
+                flat = np.array([x for l in lists for x in l] or [0], dtype=np.int32)
+                self._filters += [off, flat]
+                setattr(opts, off_name, off.ctypes.data)
+                setattr(opts, list_name, flat.ctypes.data)
         h = ctypes.c_void_p()
         with torch.cuda.device(model.device):
             _lib.check(self._lib.vbd_solver_create(dm.handle, ctypes.byref(opts), ctypes.byref(h)))

@@ -87,7 +87,22 @@ class OracleSelfContact(ctypes.Structure):
         ("filter_threshold", ctypes.c_int32),
         ("rest_exclusion_radius", ctypes.c_float),
         ("rest_q", ctypes.POINTER(ctypes.c_float)),
+        ("vertex_filter_offsets", ctypes.POINTER(ctypes.c_int32)),
+        ("vertex_filter_triangles", ctypes.POINTER(ctypes.c_int32)),
+        ("edge_filter_offsets", ctypes.POINTER(ctypes.c_int32)),
+        ("edge_filter_edges", ctypes.POINTER(ctypes.c_int32)),
     ]
+
+
+def filter_map_csr(mapping, rows: int):
+    """{row: iterable of ids} -> (offsets [rows+1], ascending ids) int32 arrays, or (None, None)."""
+    if not mapping:
+        return None, None
+    lists = [sorted({int(x) for x in mapping.get(r, ())}) for r in range(rows)]
+    off = np.zeros(rows + 1, np.int32)
+    off[1:] = np.cumsum([len(l) for l in lists])
+    flat = np.array([x for l in lists for x in l], dtype=np.int32)
+    return off, flat
 
 
 def load():
@@ -236,7 +251,7 @@ class VBDOracle:
     def set_self_contact(self, radius: float, margin: float, relaxation: float = 0.85, vertex_buffer: int = 32,
                          edge_buffer: int = 64, interval: int = 0, edge_parallel_epsilon: float = 1e-5,
                          filter_threshold: int = 2, rest_exclusion_radius: float = 0.0, rest_q=None,
-                         enabled: bool = True) -> None:
+                         enabled: bool = True, vertex_filter_map=None, edge_filter_map=None) -> None:
         """SolverVBD's particle self-contact settings (solver_vbd.py:231-241)."""
         p = OracleSelfContact()
         p.enabled = 1 if enabled else 0
@@ -248,6 +263,17 @@ class VBDOracle:
         rq = None
         if rest_q is not None:
             rq, p.rest_q = _f32(np.asarray(rest_q).reshape(-1, 3))
+        keep = []
+        vo, vl = filter_map_csr(vertex_filter_map, self.V)
+        if vo is not None:
+            keep += [vo, vl]
+            p.vertex_filter_offsets = vo.ctypes.data_as(c_int32_p)
+            p.vertex_filter_triangles = vl.ctypes.data_as(c_int32_p)
+        eo, el = filter_map_csr(edge_filter_map, self.model.edge_count)
+        if eo is not None:
+            keep += [eo, el]
+            p.edge_filter_offsets = eo.ctypes.data_as(c_int32_p)
+            p.edge_filter_edges = el.ctypes.data_as(c_int32_p)
         self.sc_buffers = (vertex_buffer, edge_buffer)
         self._lib.oracle_set_self_contact(self._h, ctypes.byref(p))
 

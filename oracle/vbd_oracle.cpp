@@ -92,6 +92,11 @@ struct OracleSelfContact {
     int32_t filter_threshold;
     float rest_exclusion_radius;
     const float* rest_q;  // [3V] rest positions (the exclusion radius is measured there); may be NULL
+    // external filter maps as CSR (ascending rows; may be NULL): vertex -> triangles, edge -> edges
+    const int32_t* vertex_filter_offsets;
+    const int32_t* vertex_filter_triangles;
+    const int32_t* edge_filter_offsets;
+    const int32_t* edge_filter_edges;
 };
 
 }  // extern "C"
@@ -480,6 +485,7 @@ struct Oracle {
     std::vector<int32_t> vt_count, vt_list;     // per vertex: colliding triangles (ascending), stride vertex_buffer
     std::vector<int32_t> ee_count, ee_list;     // per edge: colliding edges (ascending), stride edge_buffer
     std::vector<std::vector<int32_t>> tri_vs;   // per triangle: vertices that collide with it (ascending)
+    std::vector<int32_t> vfilt_off, vfilt, efilt_off, efilt;  // external filter maps (CSR)
     long long sc_overflow = 0;
 };
 
@@ -980,6 +986,9 @@ void detect_self_contacts(Oracle<T>& o, const std::vector<T>& q) {
             const int wt = o.world[a];
             if (wv >= 0 && wt >= 0 && wv != wt) continue;
             if (near_contains(o, v, a) || near_contains(o, v, b) || near_contains(o, v, c)) continue;
+            if (!o.vfilt_off.empty() &&
+                sorted_contains<T>(o.vfilt.data() + o.vfilt_off[v], o.vfilt.data() + o.vfilt_off[v + 1], t))
+                continue;
             V3<T> bary;
             const T dist = len(triangle_closest_point(load3(q.data(), a), load3(q.data(), b), load3(q.data(), c), p, bary) - p);
             if (use_rest) {
@@ -1014,6 +1023,9 @@ void detect_self_contacts(Oracle<T>& o, const std::vector<T>& q) {
             if (we >= 0 && wf >= 0 && we != wf) continue;
             if (near_contains(o, a0, b0) || near_contains(o, a0, b1) || near_contains(o, a1, b0) ||
                 near_contains(o, a1, b1))
+                continue;
+            if (!o.efilt_off.empty() &&
+                sorted_contains<T>(o.efilt.data() + o.efilt_off[e], o.efilt.data() + o.efilt_off[e + 1], f))
                 continue;
             T s, t, dist;
             closest_edge_edge(pa0, pa1, load3(q.data(), b0), load3(q.data(), b1), T(o.sc.edge_parallel_epsilon), s, t,
@@ -1460,6 +1472,20 @@ void oracle_set_self_contact(OracleHandle* h, const OracleSelfContact* p) {
         o.ee_list.assign(static_cast<size_t>(o.E) * std::max(1, p->edge_buffer), -1);
         o.tri_vs.assign(o.Tn, {});
         if (p->enabled && p->filter_threshold >= 2) build_near_sets(o);
+        o.vfilt_off.clear();
+        o.vfilt.clear();
+        o.efilt_off.clear();
+        o.efilt.clear();
+        if (p->vertex_filter_offsets) {
+            o.vfilt_off.assign(p->vertex_filter_offsets, p->vertex_filter_offsets + o.V + 1);
+            o.vfilt.assign(p->vertex_filter_triangles, p->vertex_filter_triangles + o.vfilt_off[o.V]);
+        }
+        if (p->edge_filter_offsets) {
+            o.efilt_off.assign(p->edge_filter_offsets, p->edge_filter_offsets + o.E + 1);
+            o.efilt.assign(p->edge_filter_edges, p->edge_filter_edges + o.efilt_off[o.E]);
+        }
+        o.sc.vertex_filter_offsets = o.sc.vertex_filter_triangles = nullptr;
+        o.sc.edge_filter_offsets = o.sc.edge_filter_edges = nullptr;
     });
 }
 

@@ -83,6 +83,26 @@ def test_step_matches_oracle(interval):
     assert worst <= TOL, worst
 
 
+def test_detection_with_external_filter_maps_matches_oracle():
+    model, q, _ = _folded()
+    orc = _oracle(model, vb=64, eb=128)
+    ovc, ovl, oec, oel, _ = orc.self_contact_detect(q)
+    rng = np.random.default_rng(5)
+    vmap = {int(v): set(ovl[v, :ovc[v]][: 2].tolist()) for v in rng.choice(np.flatnonzero(ovc), 20, replace=False)}
+    emap = {int(e): set(oel[e, :oec[e]][::2].tolist()) for e in rng.choice(np.flatnonzero(oec), 40, replace=False)}
+    orc.set_self_contact(radius=RADIUS, margin=MARGIN, vertex_buffer=64, edge_buffer=128, rest_q=model.particle_q,
+                         vertex_filter_map=vmap, edge_filter_map=emap)
+    ovc, ovl, oec, oel, _ = orc.self_contact_detect(q)
+    solver = _solver(model, particle_vertex_contact_buffer_size=64, particle_edge_contact_buffer_size=128,
+                     particle_external_vertex_contact_filtering_map=vmap,
+                     particle_external_edge_contact_filtering_map=emap)
+    vc, vl, ec, el = solver.self_contact_detect(torch.from_numpy(q).cuda())
+    np.testing.assert_array_equal(vc, ovc)
+    np.testing.assert_array_equal(vl, ovl)
+    np.testing.assert_array_equal(ec, oec)
+    np.testing.assert_array_equal(el, oel)
+
+
 def test_step_with_body_contacts_matches_oracle():
     """Self-contact and particle-shape contact in the same step: the lower layer lies in the
     ground plane's contact band (plane 4 mm below, particle radius 5 mm, margin 5 mm)."""

@@ -139,3 +139,31 @@ def test_detection_matches_pairwise_filter_and_distance():
             assert not ({a0, a1} & {b0, b1}) and not ({b0, b1} & near)
             assert e in set(el[f, :ec[f]].tolist())  # symmetric
     assert vc.sum() > 0 and ec.sum() > 0
+
+
+def test_external_filter_maps_remove_exactly_their_pairs():
+    """particle_external_vertex/edge_contact_filtering_map: the listed candidates disappear from the
+    lists of the rows that name them, and nothing else changes (per side for edge-edge pairs)."""
+    model, q0 = scenes.single_cloth(n=10, side=0.5, seed=1, pin_top_corners=False, ground=None, device="cpu")
+    q = q0.copy().astype(np.float64)
+    right = q[:, 0] > 0.0
+    q[right, 0] = -q[right, 0]
+    q[right, 2] += 0.004
+    q = q.astype(np.float32)
+    orc = oracle.VBDOracle(model, "f32")
+    orc.set_self_contact(radius=0.004, margin=0.006, vertex_buffer=64, edge_buffer=128)
+    vc, vl, ec, el, _ = orc.self_contact_detect(q)
+    v = int(np.argmax(vc))
+    e = int(np.argmax(ec))
+    drop_t = set(vl[v, :2].tolist())
+    drop_g = set(el[e, :3].tolist())
+    orc.set_self_contact(radius=0.004, margin=0.006, vertex_buffer=64, edge_buffer=128,
+                         vertex_filter_map={v: drop_t}, edge_filter_map={e: drop_g})
+    vc2, vl2, ec2, el2, _ = orc.self_contact_detect(q)
+    assert set(vl2[v, :vc2[v]].tolist()) == set(vl[v, :vc[v]].tolist()) - drop_t
+    assert set(el2[e, :ec2[e]].tolist()) == set(el[e, :ec[e]].tolist()) - drop_g
+    other = np.ones(model.particle_count, bool)
+    other[v] = False
+    np.testing.assert_array_equal(vc2[other], vc[other])
+    for g in drop_g:  # the other side keeps the pair unless its own map names it
+        assert e in set(el2[g, :ec2[g]].tolist())
