@@ -9,7 +9,7 @@ from . import solvers
 from .builder import ModelBuilder
 from .collide import CollisionPipeline
 from .coloring import ColoringAlgorithm
-from .model import Contacts, Control, GeoType, Model, ParticleFlags, ShapeFlags, State
+from .model import Contacts, Control, GeoType, Model, ModelFlags, ParticleFlags, ShapeFlags, State
 
 __all__ = [
     "CollisionPipeline",
@@ -19,6 +19,7 @@ __all__ = [
     "GeoType",
     "Model",
     "ModelBuilder",
+    "ModelFlags",
     "ParticleFlags",
     "ShapeFlags",
     "State",

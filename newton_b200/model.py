@@ -10,10 +10,28 @@ from __future__ import annotations
 
 import ctypes
 
+from enum import IntEnum
+
 import numpy as np
 import torch
 
 from . import _lib
+
+
+class ModelFlags(IntEnum):
+    """Which parts of a Model changed (``newton.ModelFlags``, ``sim/enums.py:8-57``), for
+    ``SolverBase.notify_model_changed``."""
+
+    JOINT_PROPERTIES = 1 << 0
+    JOINT_DOF_PROPERTIES = 1 << 1
+    BODY_PROPERTIES = 1 << 2
+    BODY_INERTIAL_PROPERTIES = 1 << 3
+    SHAPE_PROPERTIES = 1 << 4
+    MODEL_PROPERTIES = 1 << 5
+    CONSTRAINT_PROPERTIES = 1 << 6
+    TENDON_PROPERTIES = 1 << 7
+    ACTUATOR_PROPERTIES = 1 << 8
+    ALL = (1 << 9) - 1
 
 
 class ParticleFlags:

@@ -21,7 +21,7 @@ import numpy as np
 import torch
 
 from .. import _lib
-from ..model import Contacts, Control, Model, State
+from ..model import Contacts, Control, Model, ModelFlags, State
 from .solver import SolverBase
 
 
@@ -85,7 +85,6 @@ class SolverVBD(SolverBase):
         if model.soft_mesh_adjacency is None:
             raise ValueError("model.soft_mesh_adjacency is missing; finalize the model with ModelBuilder.")
         self._lib = _lib.load()
-        dm = model.device_model()
         opts = _lib.VbdSolverOptions()
         opts.iterations = self.iterations
         opts.friction_epsilon = self.friction_epsilon
@@ -121,9 +120,15 @@ class SolverVBD(SolverBase):
                 self._filters += [off, flat]
                 setattr(opts, off_name, off.ctypes.data)
                 setattr(opts, list_name, flat.ctypes.data)
+        self._opts = opts
+        self._warm = None
+        self._create()
+
+    def _create(self) -> None:
+        dm = self.model.device_model()
         h = ctypes.c_void_p()
-        with torch.cuda.device(model.device):
-            _lib.check(self._lib.vbd_solver_create(dm.handle, ctypes.byref(opts), ctypes.byref(h)))
+        with torch.cuda.device(self.model.device):
+            _lib.check(self._lib.vbd_solver_create(dm.handle, ctypes.byref(self._opts), ctypes.byref(h)))
         self._handle = h
         self._dm = dm  # keeps the device model alive as long as the solver
 
@@ -282,6 +287,7 @@ class SolverVBD(SolverBase):
         """Learned warm start as the step mode: every ``step`` runs forward, the MLP's prediction,
         ``iterations`` colour sweeps and finalize (``mlp=None`` turns it off)."""
         self._warm = mlp  # keeps the network's buffers alive while the solver points at them
+        self._warm_iterations = int(iterations)
         if mlp is None:
             _lib.check(self._lib.vbd_set_warm_start(self._handle, None, None, None, None, 0))
             return
@@ -297,4 +303,24 @@ class SolverVBD(SolverBase):
         )
 
     def notify_model_changed(self, flags: int) -> None:
-        raise NotImplementedError("rebuild the solver after changing particle/cloth model data")
+        """``SolverBase.notify_model_changed`` (``solver.py:375``).  The reference's particle path
+        reads gravity, shapes and contact materials from the model at every step; here they live
+        in the device copy of the model, so MODEL_PROPERTIES or SHAPE_PROPERTIES rebuild that copy
+        and the native solver (same options, learned warm start kept).  Other flags concern rigid
+        bodies, joints and actuators and change nothing on the particle path."""
+        if self._handle is None:
+            return
+        if not int(flags) & (ModelFlags.MODEL_PROPERTIES | ModelFlags.SHAPE_PROPERTIES):
+            return
+        old = self._handle
+        self.model.notify_model_changed()
+        self._create()
+        self._lib.vbd_solver_destroy(old)
+        if self._warm is not None:
+            self.set_warm_start(self._warm, self._warm_iterations)
+
+    def rebuild_bvh(self, state: State) -> None:
+        """``SolverVBD.rebuild_bvh`` (``solver_vbd.py:3239``): the reference rebuilds its self-contact
+        BVHs from ``state``.  Self-contact detection here rebuilds its hash grid from the current
+        positions at every detection, so there is nothing to rebuild."""
+        return None
