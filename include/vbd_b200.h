@@ -341,6 +341,13 @@ int vbd_set_launch(VbdSolver* solver, int32_t lanes_per_vertex, int32_t block_si
 int vbd_color_graph(int32_t num_nodes, int64_t num_edges, const int32_t* edges, int32_t algorithm,
                     int32_t balance, float target_ratio, int32_t* colors_out, int32_t* num_colors_out);
 
+/* The conflict graph's edge list from raw vertex pairs (host arrays): the canonicalisation step of
+ * construct_trimesh_graph_edges (graph_coloring.py:99-197).  pairs: [num_pairs,2], any order,
+ * duplicates and self-pairs allowed.  edges_out ([num_pairs,2] capacity) receives the unique
+ * (min, max) pairs in lexicographic order; num_edges_out their count. */
+int vbd_coloring_graph_edges(int32_t num_nodes, int64_t num_pairs, const int32_t* pairs, int32_t* edges_out,
+                             int64_t* num_edges_out);
+
 #ifdef __cplusplus
 }
 #endif

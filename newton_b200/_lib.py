@@ -180,6 +180,10 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_int32, ctypes.c_int64, c_int32_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, c_int32_p, c_int32_p],
     ),
+    "vbd_coloring_graph_edges": (
+        ctypes.c_int,
+        [ctypes.c_int32, ctypes.c_int64, c_int32_p, c_int32_p, ctypes.POINTER(ctypes.c_int64)],
+    ),
 }
 
 _lib = None
@@ -259,3 +263,15 @@ def color_graph(num_nodes: int, edges: np.ndarray, algorithm: int = 0, balance: 
         )
     )
     return colors, int(nc.value)
+
+
+def canonical_edges(num_nodes: int, pairs: np.ndarray) -> np.ndarray:
+    """Unique (min, max) vertex pairs in lexicographic order (vbd_coloring_graph_edges)."""
+    lib = load()
+    pairs = np.ascontiguousarray(np.asarray(pairs, dtype=np.int32).reshape(-1, 2))
+    out = np.empty_like(pairs)
+    n = ctypes.c_int64(0)
+    if pairs.shape[0] == 0:
+        return out
+    check(lib.vbd_coloring_graph_edges(int(num_nodes), pairs.shape[0], as_i32p(pairs), as_i32p(out), ctypes.byref(n)))
+    return out[: n.value].copy()

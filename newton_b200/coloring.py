@@ -25,16 +25,10 @@ class ColoringAlgorithm(Enum):
 
 
 def _canonicalize_edges(edges: np.ndarray) -> np.ndarray:
+    """Unique (min, max) pairs without self-pairs, lexicographic (native counting sort)."""
     if edges.size == 0:
         return np.empty((0, 2), dtype=np.int32)
-    e = np.sort(edges.astype(np.int64), axis=1)
-    e = e[e[:, 0] != e[:, 1]]
-    if e.size == 0:
-        return np.empty((0, 2), dtype=np.int32)
-    # lexicographic unique of the (small, large) pairs through one int64 key per pair
-    base = int(e[:, 1].max()) + 1
-    keys = np.unique(e[:, 0] * base + e[:, 1])
-    return np.stack([keys // base, keys % base], axis=1).astype(np.int32)
+    return _lib.canonical_edges(int(edges.max()) + 1, edges)
 
 
 def construct_trimesh_graph_edges(tri_indices, tri_active_mask=None, bending_edge_indices=None,

@@ -161,3 +161,41 @@ extern "C" int vbd_color_graph(int32_t num_nodes, int64_t num_edges, const int32
     *num_colors_out = nc;
     return VBD_OK;
 }
+
+// Canonical edge list of the conflict graph: construct_trimesh_graph_edges / the sort-unique
+// step of graph_coloring.py:99-197.  Each pair becomes (min, max), self-pairs are dropped, and the
+// unique pairs come out in lexicographic order -- the order numpy.unique(axis=0) gives -- via a
+// counting sort by the smaller endpoint and a sort of each (short) row.
+extern "C" int vbd_coloring_graph_edges(int32_t num_nodes, int64_t num_pairs, const int32_t* pairs, int32_t* edges_out,
+                                        int64_t* num_edges_out) {
+    if (num_nodes < 0 || num_pairs < 0 || (num_pairs > 0 && (!pairs || !edges_out)) || !num_edges_out)
+        return vbd::fail(VBD_ERR_INVALID_ARGUMENT, "vbd_coloring_graph_edges: invalid arguments");
+    for (int64_t k = 0; k < 2 * num_pairs; ++k)
+        if (pairs[k] < 0 || pairs[k] >= num_nodes)
+            return vbd::fail(VBD_ERR_INVALID_ARGUMENT, "vbd_coloring_graph_edges: endpoint out of range");
+    std::vector<int64_t> off(static_cast<size_t>(num_nodes) + 1, 0);
+    for (int64_t k = 0; k < num_pairs; ++k) {
+        const int a = pairs[2 * k], b = pairs[2 * k + 1];
+        if (a != b) ++off[static_cast<size_t>(std::min(a, b)) + 1];
+    }
+    for (int v = 0; v < num_nodes; ++v) off[v + 1] += off[v];
+    std::vector<int32_t> nb(static_cast<size_t>(off[num_nodes]));
+    std::vector<int64_t> cur(off.begin(), off.end() - 1);
+    for (int64_t k = 0; k < num_pairs; ++k) {
+        const int a = pairs[2 * k], b = pairs[2 * k + 1];
+        if (a != b) nb[cur[std::min(a, b)]++] = std::max(a, b);
+    }
+    int64_t n = 0;
+    for (int v = 0; v < num_nodes; ++v) {
+        auto b = nb.begin() + off[v], e = nb.begin() + off[v + 1];
+        std::sort(b, e);
+        e = std::unique(b, e);
+        for (auto it = b; it != e; ++it) {
+            edges_out[2 * n] = v;
+            edges_out[2 * n + 1] = *it;
+            ++n;
+        }
+    }
+    *num_edges_out = n;
+    return VBD_OK;
+}
