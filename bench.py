@@ -219,6 +219,9 @@ def learned_ab(dev, n: int, plain_steps_per_s: float) -> dict:
     solver = SolverVBD(model, iterations=ITERATIONS)
     pipe = CollisionPipeline(model, soft_contact_margin=MARGIN)
     k, records = L.calibrate_iterations(model, q0, solver, pipe, mlp, steps=300, dt=DT, check_every=30)
+    solver_tf = SolverVBD(model, iterations=ITERATIONS)
+    k_tf, records_tf = L.calibrate_iterations(model, q0, solver_tf, pipe, mlp, steps=300, dt=DT, check_every=30,
+                                              advance="plain")
 
     # inference cost: features + MLP + start offset, after a forward pass
     c = pipe.contacts()
@@ -281,6 +284,16 @@ def learned_ab(dev, n: int, plain_steps_per_s: float) -> dict:
         "learned_trajectory_status": st,
         "per_check": [{"step": r["step"], "plain_residual": r["plain"], "k_learned": r["k"],
                        "k_previous_correction": r["k_previous_correction"]} for r in records],
+        "teacher_forced": {
+            "iterations_to_equal_residual": k_tf,
+            "note": "the state advances with plain VBD; at each checked step the learned start is scored on "
+                    "that state",
+            "per_check": [{"step": r["step"], "plain_residual": r["plain"], "k_learned": r["k"],
+                           "k_previous_correction": r["k_previous_correction"],
+                           "learned_residual_after_1_2_5_10": [r["warm"][i] for i in (0, 1, 4, 9)],
+                           "plain_residual_after_1_2_5_10": [r["plain_curve"][i] for i in (0, 1, 4, 9)]}
+                          for r in records_tf],
+        },
         "train": {"samples": int(X.shape[0]), "data_s": t_data, "train_s": t_train, "epochs": 20,
                   "mse_first_epoch": hist[0], "mse_last_epoch": hist[-1], "target_variance": target_var},
         "inference_ms": infer_ms,

@@ -218,10 +218,13 @@ def mean_residual(solver, contacts, dt: float) -> float:
 
 
 def calibrate_iterations(model, q0, solver, pipe, mlp: WarmStartMLP, steps: int, dt: float,
-                         plain_iterations: int = 10, max_iterations: int = 10, check_every: int = 10):
-    """Along a trajectory of the learned solver, find the fewest warm-started iterations whose
-    mean residual matches plain VBD's after ``plain_iterations`` on the same step (same state).
-    Returns (iterations, per-check records)."""
+                         plain_iterations: int = 10, max_iterations: int = 10, check_every: int = 10,
+                         advance: str = "learned"):
+    """At every ``check_every``-th step, find the fewest warm-started iterations whose mean
+    residual matches plain VBD's after ``plain_iterations`` on the same step (same state).  The
+    trajectory advances with the learned solver (``advance="learned"``) or with plain VBD
+    (``advance="plain"``: teacher forcing, which isolates the per-step effect of the start from
+    the stability of a trajectory driven by it).  Returns (iterations, per-check records)."""
     dev = model.device
     lib = _lib.load()
     s0, s1 = model.state(), model.state()
@@ -266,12 +269,14 @@ def calibrate_iterations(model, q0, solver, pipe, mlp: WarmStartMLP, steps: int,
             need.append(k_hit)
             records.append({"step": step, "plain": r_plain, "plain_curve": r_plain_k, "warm": r_k, "k": k_hit,
                             "k_previous_correction": k_prev})
-        # advance with the learned solver at the current working point
         solver.forward(s0, c, dt)
-        _lib.check(lib.vbd_mlp_warm_start(solver._handle, _lib.ptr(mlp.params), _lib.ptr(mlp.w16), _lib.ptr(corr),
-                                          _lib.ptr(mlp.mean), _lib.ptr(mlp.inv_std), _lib.ptr(work), work.numel(),
-                                          solver._stream()))
-        solver.iterate(c, dt, max(1, int(np.percentile(need, 90))) if need else plain_iterations)
+        if advance == "plain":
+            solver.iterate(c, dt, plain_iterations)
+        else:  # the learned solver at the current working point
+            _lib.check(lib.vbd_mlp_warm_start(solver._handle, _lib.ptr(mlp.params), _lib.ptr(mlp.w16), _lib.ptr(corr),
+                                              _lib.ptr(mlp.mean), _lib.ptr(mlp.inv_std), _lib.ptr(work), work.numel(),
+                                              solver._stream()))
+            solver.iterate(c, dt, max(1, int(np.percentile(need, 90))) if need else plain_iterations)
         solver.finalize(s0, s1, dt)
         corr = s1.particle_q - y
         s0, s1 = s1, s0
