@@ -589,6 +589,20 @@ __global__ void mark_contact_vertices_kernel(int V, int E, const int4* tri, cons
     }
 }
 
+// compact lists of the work the per-color passes do: contact-touching vertices by color, and
+// the non-empty vertex-triangle / edge-edge rows (the truncation planes)
+__global__ void compact_kernel(int V, int E, const unsigned char* flag, const int* vcolor, const int* color_start,
+                               const int* vt_count, const int* ee_count, int* act_v, int* act_vcnt, int* act_rows,
+                               int* act_cnt) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < V && flag[idx]) {
+        const int c = vcolor[idx];
+        if (c >= 0) act_v[color_start[c] + atomicAdd(&act_vcnt[c], 1)] = idx;
+    }
+    if (idx < V && vt_count[idx] > 0) act_rows[atomicAdd(&act_cnt[0], 1)] = idx;
+    if (idx < E && ee_count[idx] > 0) act_rows[V + atomicAdd(&act_cnt[1], 1)] = idx;
+}
+
 __global__ void copy_positions_kernel(int V, const float4* src, float4* cd, float4* disp) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= V) return;
@@ -612,9 +626,9 @@ struct AccumArgs {
     const int2 *inc_t, *inc_e;
     const int *vt_count, *vt_list, *ee_count, *ee_list, *tv_count, *tv_list;
     int vbuf, ebuf, tcap;
-    int v_begin, v_end;
+    const int* list;    // the color's contact-touching vertices
+    const int* count;   // how many (device)
     float r, ke, kd, mu, eps_u, dt, par_eps;
-    const unsigned char* flag;
     float4 *f, *h0, *h1;
 };
 
@@ -628,73 +642,87 @@ __device__ __forceinline__ float lane_sum(float v) {
     return v;
 }
 
+// this lane's share of vertex i's pairs (i < 0: an idle slot that only joins the shuffles)
+__device__ __forceinline__ void accumulate_lane(const AccumArgs& a, int i, int lane, float3& f, Sym3& H) {
+    if (i < 0) return;
+    const float3 p = xyz(a.x[i]), p0 = xyz(a.x0[i]);
+    int idx = 0;  // running pair index of this vertex; the lane takes idx % L == lane
+    const int* row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
+    const int nv = a.vt_count[i];
+    for (int k = lane; k < nv; k += kAccumLanes) {
+        const int4 tr = a.tri[row[k]];
+        vt_contact_slot(xyz(a.x[tr.x]), xyz(a.x[tr.y]), xyz(a.x[tr.z]), p, xyz(a.x0[tr.x]), xyz(a.x0[tr.y]),
+                        xyz(a.x0[tr.z]), p0, 3, a.r, a.ke, a.kd, a.mu, a.eps_u, a.dt, f, H);
+    }
+    idx += nv;
+    for (int k = a.inc_t_off[i]; k < a.inc_t_off[i + 1]; ++k) {
+        const int2 ts = a.inc_t[k];
+        const int n = a.tv_count[ts.x];
+        int j = (lane - idx) % kAccumLanes;
+        if (j < 0) j += kAccumLanes;
+        if (j < n) {
+            const int4 tr = a.tri[ts.x];
+            const float3 t0 = xyz(a.x[tr.x]), t1 = xyz(a.x[tr.y]), t2 = xyz(a.x[tr.z]);
+            const float3 s0 = xyz(a.x0[tr.x]), s1 = xyz(a.x0[tr.y]), s2 = xyz(a.x0[tr.z]);
+            const int* vl = a.tv_list + static_cast<size_t>(ts.x) * a.tcap;
+            for (; j < n; j += kAccumLanes) {
+                const int q = vl[j];
+                vt_contact_slot(t0, t1, t2, xyz(a.x[q]), s0, s1, s2, xyz(a.x0[q]), ts.y, a.r, a.ke, a.kd, a.mu,
+                                a.eps_u, a.dt, f, H);
+            }
+        }
+        idx += n;
+    }
+    for (int k = a.inc_e_off[i]; k < a.inc_e_off[i + 1]; ++k) {
+        const int2 es = a.inc_e[k];
+        const int n = a.ee_count[es.x];
+        int j = (lane - idx) % kAccumLanes;
+        if (j < 0) j += kAccumLanes;
+        if (j < n) {
+            const int4 ed = a.edge[es.x];
+            const float3 e0 = xyz(a.x[ed.x]), e1 = xyz(a.x[ed.y]);
+            const float3 e0a = xyz(a.x0[ed.x]), e1a = xyz(a.x0[ed.y]);
+            const int* gl = a.ee_list + static_cast<size_t>(es.x) * a.ebuf;
+            for (; j < n; j += kAccumLanes) {
+                const int4 gd = a.edge[gl[j]];
+                ee_contact_slot(e0, e1, xyz(a.x[gd.x]), xyz(a.x[gd.y]), e0a, e1a, xyz(a.x0[gd.x]), xyz(a.x0[gd.y]),
+                                es.y, a.r, a.ke, a.kd, a.mu, a.eps_u, a.dt, a.par_eps, f, H);
+            }
+        }
+        idx += n;
+    }
+}
+
+// Grid-stride over the color's contact-touching vertices (the others hold zero since the last
+// detection).  A warp serves 4 vertices per round and the round bound is the same for the whole
+// warp, so every lane joins every shuffle.
 __global__ void accumulate_kernel(AccumArgs a) {
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = a.v_begin + tid / kAccumLanes;
-    const int lane = tid & (kAccumLanes - 1);
-    float3 f = f3(0.f, 0.f, 0.f);
-    Sym3 H = zero_sym();
-    if (i < a.v_end && a.flag[i]) {
-        const float3 p = xyz(a.x[i]), p0 = xyz(a.x0[i]);
-        int idx = 0;  // running pair index of this vertex; lane takes idx % L == lane
-        const int* row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
-        const int nv = a.vt_count[i];
-        for (int k = lane; k < nv; k += kAccumLanes) {
-            const int4 tr = a.tri[row[k]];
-            vt_contact_slot(xyz(a.x[tr.x]), xyz(a.x[tr.y]), xyz(a.x[tr.z]), p, xyz(a.x0[tr.x]), xyz(a.x0[tr.y]),
-                            xyz(a.x0[tr.z]), p0, 3, a.r, a.ke, a.kd, a.mu, a.eps_u, a.dt, f, H);
-        }
-        idx += nv;
-        for (int k = a.inc_t_off[i]; k < a.inc_t_off[i + 1]; ++k) {
-            const int2 ts = a.inc_t[k];
-            const int n = a.tv_count[ts.x];
-            int j = (lane - idx) % kAccumLanes;
-            if (j < 0) j += kAccumLanes;
-            if (j < n) {
-                const int4 tr = a.tri[ts.x];
-                const float3 t0 = xyz(a.x[tr.x]), t1 = xyz(a.x[tr.y]), t2 = xyz(a.x[tr.z]);
-                const float3 s0 = xyz(a.x0[tr.x]), s1 = xyz(a.x0[tr.y]), s2 = xyz(a.x0[tr.z]);
-                const int* vl = a.tv_list + static_cast<size_t>(ts.x) * a.tcap;
-                for (; j < n; j += kAccumLanes) {
-                    const int q = vl[j];
-                    vt_contact_slot(t0, t1, t2, xyz(a.x[q]), s0, s1, s2, xyz(a.x0[q]), ts.y, a.r, a.ke, a.kd, a.mu,
-                                    a.eps_u, a.dt, f, H);
-                }
-            }
-            idx += n;
-        }
-        for (int k = a.inc_e_off[i]; k < a.inc_e_off[i + 1]; ++k) {
-            const int2 es = a.inc_e[k];
-            const int n = a.ee_count[es.x];
-            int j = (lane - idx) % kAccumLanes;
-            if (j < 0) j += kAccumLanes;
-            if (j < n) {
-                const int4 ed = a.edge[es.x];
-                const float3 e0 = xyz(a.x[ed.x]), e1 = xyz(a.x[ed.y]);
-                const float3 e0a = xyz(a.x0[ed.x]), e1a = xyz(a.x0[ed.y]);
-                const int* gl = a.ee_list + static_cast<size_t>(es.x) * a.ebuf;
-                for (; j < n; j += kAccumLanes) {
-                    const int4 gd = a.edge[gl[j]];
-                    ee_contact_slot(e0, e1, xyz(a.x[gd.x]), xyz(a.x[gd.y]), e0a, e1a, xyz(a.x0[gd.x]),
-                                    xyz(a.x0[gd.y]), es.y, a.r, a.ke, a.kd, a.mu, a.eps_u, a.dt, a.par_eps, f, H);
-                }
-            }
-            idx += n;
+    const int n = *a.count;
+    const int lane = threadIdx.x & (kAccumLanes - 1);
+    const int sub = (threadIdx.x & 31) / kAccumLanes;  // vertex slot of this lane in its warp
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    const int warp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    for (int base = 4 * warp; base < n; base += 4 * warps) {
+        const int slot = base + sub;
+        const int i = slot < n ? a.list[slot] : -1;
+        float3 f = f3(0.f, 0.f, 0.f);
+        Sym3 H = zero_sym();
+        accumulate_lane(a, i, lane, f, H);
+        f.x = lane_sum(f.x);
+        f.y = lane_sum(f.y);
+        f.z = lane_sum(f.z);
+        H.xx = lane_sum(H.xx);
+        H.xy = lane_sum(H.xy);
+        H.xz = lane_sum(H.xz);
+        H.yy = lane_sum(H.yy);
+        H.yz = lane_sum(H.yz);
+        H.zz = lane_sum(H.zz);
+        if (i >= 0 && lane == 0) {
+            a.f[i] = make_float4(f.x, f.y, f.z, 0.f);
+            a.h0[i] = make_float4(H.xx, H.xy, H.xz, H.yy);
+            a.h1[i] = make_float4(H.yz, H.zz, 0.f, 0.f);
         }
     }
-    f.x = lane_sum(f.x);
-    f.y = lane_sum(f.y);
-    f.z = lane_sum(f.z);
-    H.xx = lane_sum(H.xx);
-    H.xy = lane_sum(H.xy);
-    H.xz = lane_sum(H.xz);
-    H.yy = lane_sum(H.yy);
-    H.yz = lane_sum(H.yz);
-    H.zz = lane_sum(H.zz);
-    if (i >= a.v_end || lane != 0) return;
-    a.f[i] = make_float4(f.x, f.y, f.z, 0.f);
-    a.h0[i] = make_float4(H.xx, H.xy, H.xz, H.yy);
-    a.h1[i] = make_float4(H.yz, H.zz, 0.f, 0.f);
 }
 
 struct TruncArgs {
@@ -703,6 +731,8 @@ struct TruncArgs {
     const int4* tri;
     const int4* edge;
     const int *vt_count, *vt_list, *ee_count, *ee_list;
+    const int* rows;     // non-empty vertex-triangle rows [0, V), then edge-edge rows [V, V + E)
+    const int* counts;   // [2]
     int V, E, vbuf, ebuf;
     float eps, gamma;
     unsigned* ts;
@@ -714,40 +744,42 @@ __device__ __forceinline__ void ts_min(unsigned* ts, int i, float3 x, float3 dx,
     atomicMin(&ts[i], __float_as_uint(t));
 }
 
+// grid-stride over the non-empty rows: vertex-triangle rows first, then edge-edge rows
 __global__ void planar_kernel(TruncArgs a) {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx < a.V) {
-        const int i = idx;
-        const float3 v = xyz(a.cd[i]), dv = xyz(a.disp[i]);
-        const int* row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
-        for (int k = 0; k < a.vt_count[i]; ++k) {
-            const int4 tr = a.tri[row[k]];
-            const float3 t1 = xyz(a.cd[tr.x]), t2 = xyz(a.cd[tr.y]), t3 = xyz(a.cd[tr.z]);
-            const float3 d1 = xyz(a.disp[tr.x]), d2 = xyz(a.disp[tr.y]), d3 = xyz(a.disp[tr.z]);
-            float3 n, d;
-            const int dummy = vt_plane(v, dv, t1, d1, t2, d2, t3, d3, n, d);
-            if (!(dummy & 1)) ts_min(a.ts, i, v, dv, n, d, a.eps, a.gamma);
-            if (!(dummy & 2)) ts_min(a.ts, tr.x, t1, d1, n, d, a.eps, a.gamma);
-            if (!(dummy & 4)) ts_min(a.ts, tr.y, t2, d2, n, d, a.eps, a.gamma);
-            if (!(dummy & 8)) ts_min(a.ts, tr.z, t3, d3, n, d, a.eps, a.gamma);
-        }
-    }
-    if (idx < a.E) {
-        const int e = idx;
-        const int4 ed = a.edge[e];
-        const float3 a0 = xyz(a.cd[ed.x]), a1 = xyz(a.cd[ed.y]);
-        const float3 da0 = xyz(a.disp[ed.x]), da1 = xyz(a.disp[ed.y]);
-        const int* row = a.ee_list + static_cast<size_t>(e) * a.ebuf;
-        for (int k = 0; k < a.ee_count[e]; ++k) {
-            const int4 gd = a.edge[row[k]];
-            const float3 b0 = xyz(a.cd[gd.x]), b1 = xyz(a.cd[gd.y]);
-            const float3 db0 = xyz(a.disp[gd.x]), db1 = xyz(a.disp[gd.y]);
-            float3 n, d;
-            const int dummy = ee_plane(a0, da0, a1, da1, b0, db0, b1, db1, n, d);
-            if (!(dummy & 1)) ts_min(a.ts, ed.x, a0, da0, n, d, a.eps, a.gamma);
-            if (!(dummy & 2)) ts_min(a.ts, ed.y, a1, da1, n, d, a.eps, a.gamma);
-            if (!(dummy & 4)) ts_min(a.ts, gd.x, b0, db0, n, d, a.eps, a.gamma);
-            if (!(dummy & 8)) ts_min(a.ts, gd.y, b1, db1, n, d, a.eps, a.gamma);
+    const int nv = a.counts[0], ne = a.counts[1];
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nv + ne; w += gridDim.x * blockDim.x) {
+        if (w < nv) {
+            const int i = a.rows[w];
+            const float3 v = xyz(a.cd[i]), dv = xyz(a.disp[i]);
+            const int* row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
+            for (int k = 0; k < a.vt_count[i]; ++k) {
+                const int4 tr = a.tri[row[k]];
+                const float3 t1 = xyz(a.cd[tr.x]), t2 = xyz(a.cd[tr.y]), t3 = xyz(a.cd[tr.z]);
+                const float3 d1 = xyz(a.disp[tr.x]), d2 = xyz(a.disp[tr.y]), d3 = xyz(a.disp[tr.z]);
+                float3 n, d;
+                const int dummy = vt_plane(v, dv, t1, d1, t2, d2, t3, d3, n, d);
+                if (!(dummy & 1)) ts_min(a.ts, i, v, dv, n, d, a.eps, a.gamma);
+                if (!(dummy & 2)) ts_min(a.ts, tr.x, t1, d1, n, d, a.eps, a.gamma);
+                if (!(dummy & 4)) ts_min(a.ts, tr.y, t2, d2, n, d, a.eps, a.gamma);
+                if (!(dummy & 8)) ts_min(a.ts, tr.z, t3, d3, n, d, a.eps, a.gamma);
+            }
+        } else {
+            const int e = a.rows[a.V + (w - nv)];
+            const int4 ed = a.edge[e];
+            const float3 a0 = xyz(a.cd[ed.x]), a1 = xyz(a.cd[ed.y]);
+            const float3 da0 = xyz(a.disp[ed.x]), da1 = xyz(a.disp[ed.y]);
+            const int* row = a.ee_list + static_cast<size_t>(e) * a.ebuf;
+            for (int k = 0; k < a.ee_count[e]; ++k) {
+                const int4 gd = a.edge[row[k]];
+                const float3 b0 = xyz(a.cd[gd.x]), b1 = xyz(a.cd[gd.y]);
+                const float3 db0 = xyz(a.disp[gd.x]), db1 = xyz(a.disp[gd.y]);
+                float3 n, d;
+                const int dummy = ee_plane(a0, da0, a1, da1, b0, db0, b1, db1, n, d);
+                if (!(dummy & 1)) ts_min(a.ts, ed.x, a0, da0, n, d, a.eps, a.gamma);
+                if (!(dummy & 2)) ts_min(a.ts, ed.y, a1, da1, n, d, a.eps, a.gamma);
+                if (!(dummy & 4)) ts_min(a.ts, gd.x, b0, db0, n, d, a.eps, a.gamma);
+                if (!(dummy & 8)) ts_min(a.ts, gd.y, b1, db1, n, d, a.eps, a.gamma);
+            }
         }
     }
 }
@@ -809,7 +841,8 @@ void self_contact_free(SelfContact& sc) {
                     sc.near,     sc.rest,     sc.tri_cnt,   sc.tri_off,  sc.tri_cur,    sc.tri_items, sc.edge_cnt,
                     sc.edge_off, sc.edge_cur, sc.edge_items, sc.scan_tmp, sc.vt_count,  sc.vt_list,   sc.ee_count,
                     sc.ee_list,  sc.tv_count, sc.tv_list,   sc.cd,       sc.sc_f,       sc.sc_h0,     sc.sc_h1,
-                    sc.ts,       sc.counters, sc.vworld,    sc.tri_box,  sc.edge_box,   sc.flag,      sc.tri_item_box, sc.edge_item_box, sc.vfilt_off, sc.vfilt, sc.efilt_off, sc.efilt};
+                    sc.ts,       sc.counters, sc.vworld,    sc.tri_box,  sc.edge_box,   sc.flag,      sc.tri_item_box, sc.edge_item_box, sc.vfilt_off, sc.vfilt, sc.efilt_off, sc.efilt, sc.color_start, sc.vcolor,
+                    sc.act_v,    sc.act_vcnt, sc.act_rows, sc.act_cnt};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     SelfContact empty;
@@ -932,6 +965,12 @@ int self_contact_create(const VbdModelImpl& m, const SelfContactParams& p, SelfC
     if (!rc) rc = upload_vec(&sc.near, near_list);
     if (!rc) rc = upload_vec(&sc.rest, rest);
     if (!rc) rc = upload_vec(&sc.vworld, vworld);
+    sc.C = m.C;
+    std::vector<int> vcolor(V, -1);
+    for (int c = 0; c < m.C; ++c)
+        for (int i = m.color_start[c]; i < m.color_start[c + 1]; ++i) vcolor[i] = c;
+    if (!rc) rc = upload_vec(&sc.vcolor, vcolor);
+    if (!rc) rc = upload_vec(&sc.color_start, m.color_start);
     if (!rc && !p.vertex_filter_off.empty()) {
         std::vector<int> off(V + 1, 0), lst;
         for (int i = 0; i < V; ++i) {
@@ -968,6 +1007,10 @@ int self_contact_create(const VbdModelImpl& m, const SelfContactParams& p, SelfC
     az(reinterpret_cast<void**>(&sc.tri_item_box), 2 * static_cast<size_t>(sc.tri_items_cap) * sizeof(float4));
     az(reinterpret_cast<void**>(&sc.edge_item_box), 2 * static_cast<size_t>(sc.edge_items_cap) * sizeof(float4));
     az(reinterpret_cast<void**>(&sc.flag), static_cast<size_t>(V));
+    az(reinterpret_cast<void**>(&sc.act_v), static_cast<size_t>(V) * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.act_vcnt), static_cast<size_t>(std::max(m.C, 1)) * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.act_rows), static_cast<size_t>(V + E) * sizeof(int));
+    az(reinterpret_cast<void**>(&sc.act_cnt), 2 * sizeof(int));
     az(reinterpret_cast<void**>(&sc.vt_count), static_cast<size_t>(V) * sizeof(int));
     az(reinterpret_cast<void**>(&sc.vt_list), static_cast<size_t>(V) * p.vertex_buffer * sizeof(int));
     az(reinterpret_cast<void**>(&sc.ee_count), static_cast<size_t>(E) * sizeof(int));
@@ -1133,12 +1176,29 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     mark_contact_vertices_kernel<<<(nm + 255) / 256, 256, 0, st>>>(V, E, sc.tri, sc.edge, sc.vt_count, sc.vt_list,
                                                                    sc.p.vertex_buffer, sc.ee_count, sc.flag);
     VBD_CUDA_TRY(cudaGetLastError());
+    VBD_CUDA_TRY(cudaMemsetAsync(sc.act_vcnt, 0, static_cast<size_t>(std::max(sc.C, 1)) * sizeof(int), st));
+    VBD_CUDA_TRY(cudaMemsetAsync(sc.act_cnt, 0, 2 * sizeof(int), st));
+    compact_kernel<<<(nm + 255) / 256, 256, 0, st>>>(V, E, sc.flag, sc.vcolor, sc.color_start, sc.vt_count,
+                                                     sc.ee_count, sc.act_v, sc.act_vcnt, sc.act_rows, sc.act_cnt);
+    VBD_CUDA_TRY(cudaGetLastError());
+    // vertices that touch no pair keep a zero contact term until the next detection
+    VBD_CUDA_TRY(cudaMemsetAsync(sc.sc_f, 0, static_cast<size_t>(V) * sizeof(float4), st));
+    VBD_CUDA_TRY(cudaMemsetAsync(sc.sc_h0, 0, static_cast<size_t>(V) * sizeof(float4), st));
+    VBD_CUDA_TRY(cudaMemsetAsync(sc.sc_h1, 0, static_cast<size_t>(V) * sizeof(float4), st));
     return VBD_OK;
 }
 
 int self_contact_accumulate(const VbdModelImpl& m, SelfContact& sc, const float4* pos, const float4* prev,
-                            int v_begin, int v_end, float dt, float friction_epsilon, cudaStream_t st) {
-    if (v_end <= v_begin) return VBD_OK;
+                            int color, float dt, float friction_epsilon, cudaStream_t st) {
+    if (color < 0) {
+        for (int c = 0; c < m.C; ++c) {
+            const int rc = self_contact_accumulate(m, sc, pos, prev, c, dt, friction_epsilon, st);
+            if (rc) return rc;
+        }
+        return VBD_OK;
+    }
+    const int size = m.color_start[color + 1] - m.color_start[color];
+    if (size <= 0) return VBD_OK;
     AccumArgs a;
     a.x = pos;
     a.x0 = prev;
@@ -1157,8 +1217,8 @@ int self_contact_accumulate(const VbdModelImpl& m, SelfContact& sc, const float4
     a.vbuf = sc.p.vertex_buffer;
     a.ebuf = sc.p.edge_buffer;
     a.tcap = sc.tcap;
-    a.v_begin = v_begin;
-    a.v_end = v_end;
+    a.list = sc.act_v + m.color_start[color];
+    a.count = sc.act_vcnt + color;
     a.r = sc.p.radius;
     a.ke = m.soft_ke;
     a.kd = m.soft_kd;
@@ -1166,12 +1226,13 @@ int self_contact_accumulate(const VbdModelImpl& m, SelfContact& sc, const float4
     a.eps_u = friction_epsilon * dt;
     a.dt = dt;
     a.par_eps = sc.p.edge_parallel_epsilon;
-    a.flag = sc.flag;
     a.f = sc.sc_f;
     a.h0 = sc.sc_h0;
     a.h1 = sc.sc_h1;
-    const long long threads = static_cast<long long>(v_end - v_begin) * kAccumLanes;
-    accumulate_kernel<<<static_cast<int>((threads + 127) / 128), 128, 0, st>>>(a);
+    // enough warps for every vertex of the color in one round, capped: the kernel strides
+    const long long threads = static_cast<long long>(size) * kAccumLanes;
+    const int grid = static_cast<int>(std::min<long long>((threads + 127) / 128, 148 * 16));
+    accumulate_kernel<<<grid, 128, 0, st>>>(a);
     VBD_CUDA_TRY(cudaGetLastError());
     return VBD_OK;
 }
@@ -1195,8 +1256,10 @@ int self_contact_truncate(const VbdModelImpl& m, SelfContact& sc, float4* pos, f
     a.eps = sc.p.edge_parallel_epsilon;
     a.gamma = sc.p.relaxation;
     a.ts = sc.ts;
+    a.rows = sc.act_rows;
+    a.counts = sc.act_cnt;
     const int n = std::max(V, m.E);
-    planar_kernel<<<(n + 127) / 128, 128, 0, st>>>(a);
+    planar_kernel<<<std::min((n + 127) / 128, 148 * 16), 128, 0, st>>>(a);
     VBD_CUDA_TRY(cudaGetLastError());
     apply_truncation_kernel<<<(V + 255) / 256, 256, 0, st>>>(V, sc.cd, disp, pos, sc.ts, sc.max_disp);
     VBD_CUDA_TRY(cudaGetLastError());

@@ -74,6 +74,13 @@ struct SelfContact {
     int *tv_count = nullptr, *tv_list = nullptr;   // [T], [T * tcap] internal vertex ids ascending
     // per-iteration state
     unsigned char* flag = nullptr;  // [V] 1: the vertex takes part in a detected pair
+    int C = 0;
+    int* color_start = nullptr;  // [C+1] internal vertex ranges of the colors
+    int* vcolor = nullptr;       // [V] color of each internal vertex (-1: none)
+    int* act_v = nullptr;        // [V] contact-touching vertices, color c in [color_start[c], ...)
+    int* act_vcnt = nullptr;     // [C] how many per color
+    int* act_rows = nullptr;     // [V + E] non-empty vertex-triangle rows, then non-empty edge rows
+    int* act_cnt = nullptr;      // [2] their counts
     float4* cd = nullptr;    // pos_prev_collision_detection (internal order)
     float4* sc_f = nullptr;  // [V] self-contact force
     float4* sc_h0 = nullptr; // [V] Hessian xx xy xz yy
@@ -87,9 +94,10 @@ void self_contact_free(SelfContact& sc);
 // Detection at `positions` (internal order): cd := positions, and disp := 0 when reset_disp.
 int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* positions, float4* disp,
                         bool reset_disp, cudaStream_t st);
-// Force / Hessian of every pair of the vertices [v_begin, v_end) into sc_f / sc_h0 / sc_h1.
+// Force / Hessian of every pair of the contact-touching vertices of `color` (-1: all colors)
+// into sc_f / sc_h0 / sc_h1 (the other vertices hold zero since the last detection).
 int self_contact_accumulate(const VbdModelImpl& m, SelfContact& sc, const float4* pos, const float4* prev,
-                            int v_begin, int v_end, float dt, float friction_epsilon, cudaStream_t st);
+                            int color, float dt, float friction_epsilon, cudaStream_t st);
 // Planar truncation of all displacements, then pos := cd + disp for every vertex.
 int self_contact_truncate(const VbdModelImpl& m, SelfContact& sc, float4* pos, float4* disp, cudaStream_t st);
 // Whether iteration `it` begins with a detection (particle_collision_detection_interval).

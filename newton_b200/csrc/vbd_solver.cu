@@ -782,7 +782,7 @@ static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float 
     a.v_end = m.color_start[color + 1];
     if (a.v_end <= a.v_begin) return;
     if (s.sc.on) {
-        self_contact_accumulate(m, s.sc, s.pos, s.prev, a.v_begin, a.v_end, dt, s.friction_epsilon, st);
+        self_contact_accumulate(m, s.sc, s.pos, s.prev, color, dt, s.friction_epsilon, st);
         launch_sweep(a, s.lanes, m.any_tri_damping || m.any_edge_damping, false, s.block, st);
         self_contact_truncate(m, s.sc, s.pos, s.disp, st);
         return;
@@ -1276,7 +1276,7 @@ extern "C" int vbd_residual(VbdSolver* solver, const VbdContacts* contacts, floa
     VBD_CUDA_TRY(cudaMemsetAsync(mx, 0, sizeof(float), st));
     if (per_vertex_out && m.V > m.swept) VBD_CUDA_TRY(cudaMemsetAsync(per_vertex_out, 0, sizeof(float) * m.V, st));
     if (s.sc.on) {
-        const int rc = self_contact_accumulate(m, s.sc, s.pos, s.prev, 0, m.swept, dt, s.friction_epsilon, st);
+        const int rc = self_contact_accumulate(m, s.sc, s.pos, s.prev, -1, dt, s.friction_epsilon, st);
         if (rc) return rc;
     }
     SweepArgs a = make_sweep_args(s, contacts, dt);

@@ -91,8 +91,9 @@ def cloth_on_boxes(n: int = 1024, side: float = 4.0, boxes: int = 16, seed: int 
     cfg = ModelBuilder.ShapeConfig(ke=1.0e4)
     b.add_ground_plane(height=0.0, cfg=cfg)
     for _ in range(boxes):
-        hx, hy, hz = (float(v) for v in rng.uniform(0.1, 0.4, size=3))
-        x, y = (float(v) for v in rng.uniform(-1.5, 1.5, size=2))
+        # at the 4 m side: half-extents U[0.1, 0.4] m, centres in [-1.5, 1.5]^2 (scaled with the side)
+        hx, hy, hz = (float(v) for v in rng.uniform(0.025 * side, 0.1 * side, size=3))
+        x, y = (float(v) for v in rng.uniform(-0.375 * side, 0.375 * side, size=2))
         yaw = float(rng.uniform(0.0, 2.0 * np.pi))
         rot = (0.0, 0.0, float(np.sin(0.5 * yaw)), float(np.cos(0.5 * yaw)))
         b.add_shape_box(-1, xform=((x, y, hz), rot), hx=hx, hy=hy, hz=hz, cfg=cfg)
