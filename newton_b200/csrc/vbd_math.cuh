@@ -159,7 +159,11 @@ __device__ __forceinline__ float3 project_cross(float inv_len, float3 nh, float3
     return cross(p, u);
 }
 
-template <bool kDamping>
+// kSelect: form both projections for every order and select the result afterwards (straight-line
+// code, so that the caller can interleave the evaluation of independent hinges); otherwise branch
+// on the order (fewer live registers).  Both compute the same operations for a given order, so
+// they give the same bits.
+template <bool kDamping, bool kSelect = false>
 __device__ __forceinline__ void bending_eval(int order, float3 x0, float3 x1, float3 x2, float3 x3, float3 a0,
                                              float3 a1, float3 a2, float3 a3, float4 em, float inv_dt, float3& f,
                                              Sym3& h) {
@@ -186,7 +190,18 @@ __device__ __forceinline__ void bending_eval(int order, float3 x0, float3 x1, fl
 
     // Selected dtheta/dx (see header comment).
     float3 g;
-    if (order == 0) {
+    if (kSelect) {
+        //   order 0:  T1(y1) x e            order 2:  T2(y2) x x13 - T1(y1) x x03
+        //   order 1: -T2(y2) x e            order 3:  T1(y1) x x02 - T2(y2) x x12
+        const float3 y1 = -cos_t * cross(eh, n2h) - sin_t * n2h;
+        const float3 y2 = cos_t * cross(eh, n1h) - sin_t * n1h;
+        const float3 u1 = order == 0 ? e : (order == 2 ? x03 : x02);
+        const float3 u2 = order == 1 ? e : (order == 2 ? x13 : x12);
+        const float3 t1 = project_cross(i1, n1h, y1, u1);
+        const float3 t2 = project_cross(i2, n2h, y2, u2);
+        const float3 d12 = t1 - t2;
+        g = order == 0 ? t1 : (order == 1 ? -t2 : (order == 2 ? -d12 : d12));
+    } else if (order == 0) {
         const float3 y1 = -cos_t * cross(eh, n2h) - sin_t * n2h;
         g = project_cross(i1, n1h, y1, e);
     } else if (order == 1) {

@@ -61,6 +61,7 @@ struct SolverImpl {
     float4* disp = nullptr;   // particle_displacements
     int* ccount = nullptr;    // [V] contacts per vertex (internal order)
     int* cslot = nullptr;     // [V*K] record ids
+    float4* ctab = nullptr;   // [V*K][4] the step's contacts per vertex, packed and in record order
     unsigned* status = nullptr;  // [kStatusSlots]
     float* resid_max = nullptr;  // [1] scratch for vbd_residual
     cudaStream_t capture_stream = nullptr;
@@ -157,6 +158,58 @@ __global__ void forward_kernel(ForwardArgs a) {
     }
 }
 
+// Per-step packing of the contact table: the scatter above leaves each vertex's record ids in
+// arbitrary (atomic) order; this pass sorts them (the reference adds a particle's contacts in
+// record order) and gathers what the contact law reads into 4 float4 per contact:
+//   (body_pos, ke) (body_vel, kd) (normal, mu) (margin, 0, 0, 0)
+// so that every color sweep of the step reads one contiguous entry per contact instead of the
+// id -> record -> shape chain.
+struct PackArgs {
+    const int* ccount;
+    const int* cslot;
+    int K;
+    const int* c_shape;
+    const float* c_body_pos;
+    const float* c_body_vel;
+    const float* c_normal;
+    const DevShape* shapes;
+    float4* ctab;
+    int V;
+};
+
+__global__ void pack_contacts_kernel(PackArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.V) return;
+    const int n = min(a.ccount[i], a.K);
+    if (n <= 0) return;
+    // K <= 8: odd-even transposition sort of 8 slots (unused slots hold INT_MAX and sort last);
+    // the fixed indices keep the ids in registers
+    int ids[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) ids[k] = k < n ? a.cslot[i * a.K + k] : 0x7fffffff;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+#pragma unroll
+        for (int k = p & 1; k + 1 < 8; k += 2) {
+            const int lo = min(ids[k], ids[k + 1]), hi = max(ids[k], ids[k + 1]);
+            ids[k] = lo;
+            ids[k + 1] = hi;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        if (k < n) {
+            const int r = ids[k];
+            const float4 sm = a.shapes[a.c_shape[r]].mat;
+            float4* e = a.ctab + (static_cast<size_t>(i) * a.K + k) * 4;
+            e[0] = make_float4(a.c_body_pos[3 * r], a.c_body_pos[3 * r + 1], a.c_body_pos[3 * r + 2], sm.x);
+            e[1] = make_float4(a.c_body_vel[3 * r], a.c_body_vel[3 * r + 1], a.c_body_vel[3 * r + 2], sm.y);
+            e[2] = make_float4(a.c_normal[3 * r], a.c_normal[3 * r + 1], a.c_normal[3 * r + 2], sm.z);
+            e[3] = make_float4(sm.w, 0.f, 0.f, 0.f);
+        }
+    }
+}
+
 struct SweepArgs {
     float4* pos;
     const float4* prev;
@@ -178,6 +231,8 @@ struct SweepArgs {
     const float* c_body_vel;
     const float* c_normal;
     const DevShape* shapes;
+    // packed contact table (pack_contacts_kernel); NULL: read the records through cslot instead
+    const float4* ctab;
     // self-contact force / Hessian of the vertex (NULL without self-contact)
     const float4* sc_f;
     const float4* sc_h0;
@@ -230,6 +285,77 @@ __device__ __forceinline__ void accumulate_elements(const SweepArgs& a, int i, i
     }
 }
 
+// The same walk with two records in flight per lane: records r and r + L are loaded and evaluated
+// as two independent chains (zero-started partial sums, added in record order), so the latency of
+// one record's loads and math overlaps the other's.  Used where the launch leaves registers for
+// it (few lanes per vertex, uncapped build).  A lane with an odd count evaluates its last record
+// twice and keeps one result.
+template <bool kDamp>
+__device__ __forceinline__ void accumulate_elements_x2(const SweepArgs& a, int lane, int L, int4 adj, float3& f,
+                                                       Sym3& h) {
+    const int nt = adj.y - adj.x;
+    const int lane_e = (lane - nt % L + L) % L;
+    for (int r = adj.x + lane; r < adj.y; r += 2 * L) {
+        const bool two = r + L < adj.y;
+        const int rb = two ? r + L : r;
+        const int4 ta = __ldg(&a.tri_idx[r]), tb = __ldg(&a.tri_idx[rb]);
+        const float4 Da = __ldg(&a.tri_D[r]), Db = __ldg(&a.tri_D[rb]);
+        const float4 ma = __ldg(&a.tri_mat[r]), mb = __ldg(&a.tri_mat[rb]);
+        const float3 xa0 = xyz(a.pos[ta.x]), xa1 = xyz(a.pos[ta.y]), xa2 = xyz(a.pos[ta.z]);
+        const float3 xb0 = xyz(a.pos[tb.x]), xb1 = xyz(a.pos[tb.y]), xb2 = xyz(a.pos[tb.z]);
+        float3 pa0 = xa0, pa1 = xa1, pa2 = xa2, pb0 = xb0, pb1 = xb1, pb2 = xb2;
+        if (kDamp && (ma.w > 0.0f || mb.w > 0.0f)) {
+            pa0 = xyz(__ldg(&a.prev[ta.x]));
+            pa1 = xyz(__ldg(&a.prev[ta.y]));
+            pa2 = xyz(__ldg(&a.prev[ta.z]));
+            pb0 = xyz(__ldg(&a.prev[tb.x]));
+            pb1 = xyz(__ldg(&a.prev[tb.y]));
+            pb2 = xyz(__ldg(&a.prev[tb.z]));
+        }
+        float3 fa = f3(0.f, 0.f, 0.f), fb = fa;
+        Sym3 ha = zero_sym(), hb = zero_sym();
+        membrane_eval<kDamp>(ta.w, xa0, xa1, xa2, pa0, pa1, pa2, Da, ma, a.inv_dt, fa, ha);
+        membrane_eval<kDamp>(tb.w, xb0, xb1, xb2, pb0, pb1, pb2, Db, mb, a.inv_dt, fb, hb);
+        f = f + fa;
+        add(h, ha);
+        if (two) {
+            f = f + fb;
+            add(h, hb);
+        }
+    }
+    for (int r = adj.z + lane_e; r < adj.w; r += 2 * L) {
+        const bool two = r + L < adj.w;
+        const int rb = two ? r + L : r;
+        const int4 ea = __ldg(&a.edge_idx[r]), eb = __ldg(&a.edge_idx[rb]);
+        const float4 ma = __ldg(&a.edge_mat[r]), mb = __ldg(&a.edge_mat[rb]);
+        const int oa = static_cast<int>(static_cast<unsigned>(ea.x) >> 30), ob = static_cast<int>(static_cast<unsigned>(eb.x) >> 30);
+        const int a0 = ea.x & 0x3fffffff, b0 = eb.x & 0x3fffffff;
+        const float3 xa0 = xyz(a.pos[a0]), xa1 = xyz(a.pos[ea.y]), xa2 = xyz(a.pos[ea.z]), xa3 = xyz(a.pos[ea.w]);
+        const float3 xb0 = xyz(a.pos[b0]), xb1 = xyz(a.pos[eb.y]), xb2 = xyz(a.pos[eb.z]), xb3 = xyz(a.pos[eb.w]);
+        float3 pa0 = xa0, pa1 = xa1, pa2 = xa2, pa3 = xa3, pb0 = xb0, pb1 = xb1, pb2 = xb2, pb3 = xb3;
+        if (kDamp && (ma.w > 0.0f || mb.w > 0.0f)) {
+            pa0 = xyz(__ldg(&a.prev[a0]));
+            pa1 = xyz(__ldg(&a.prev[ea.y]));
+            pa2 = xyz(__ldg(&a.prev[ea.z]));
+            pa3 = xyz(__ldg(&a.prev[ea.w]));
+            pb0 = xyz(__ldg(&a.prev[b0]));
+            pb1 = xyz(__ldg(&a.prev[eb.y]));
+            pb2 = xyz(__ldg(&a.prev[eb.z]));
+            pb3 = xyz(__ldg(&a.prev[eb.w]));
+        }
+        float3 fa = f3(0.f, 0.f, 0.f), fb = fa;
+        Sym3 ha = zero_sym(), hb = zero_sym();
+        bending_eval<kDamp, true>(oa, xa0, xa1, xa2, xa3, pa0, pa1, pa2, pa3, ma, a.inv_dt, fa, ha);
+        bending_eval<kDamp, true>(ob, xb0, xb1, xb2, xb3, pb0, pb1, pb2, pb3, mb, a.inv_dt, fb, hb);
+        f = f + fa;
+        add(h, ha);
+        if (two) {
+            f = f + fb;
+            add(h, hb);
+        }
+    }
+}
+
 __device__ __forceinline__ void accumulate_contacts(const SweepArgs& a, int i, float3 x, float3 xp, float radius,
                                                     float3& f, Sym3& h) {
     const DevShape* shapes = a.shapes;
@@ -248,6 +374,10 @@ __device__ __forceinline__ void add_self_contact(const SweepArgs& a, int i, floa
     h.zz += h1.y;
 }
 
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
 __device__ __forceinline__ float warp_sum(float v, int L) {
     for (int off = L >> 1; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
     return v;
@@ -256,7 +386,7 @@ __device__ __forceinline__ float warp_sum(float v, int L) {
 // One Gauss-Seidel color (kResidual = false) or a Jacobi residual evaluation over a vertex range
 // (kResidual = true).  L lanes cooperate on one vertex: each lane takes every L-th element record
 // (triangles, then hinges, as the reference's 16-thread tile does), then the partial force and
-// Hessian are summed across the L lanes with xor shuffles.
+// Hessian are summed across the L lanes with xor shuffles and lane 0 adds the contacts and solves.
 // kCap: the same kernel limited to 64 registers per thread (4 blocks of 256 per SM), used when the
 // uncapped kernel would need more than one wave of blocks (large colors, many lanes per vertex)
 template <int L, bool kDamp, bool kResidual, bool kCap>
@@ -279,7 +409,29 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
     }
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;");
-    if (valid && solve) accumulate_elements<kDamp>(a, i, lane, L, adj, f, h);
+    if (valid && solve && lane == 0) {
+        // Warm L1 with everything lane 0 reads after the element walk (the vertex's own state,
+        // its contact count and first packed contact, its self-contact terms): a prefetch holds
+        // no register, so the walk keeps the register budget at which two color grids fit on an
+        // SM together and the next color's launch overlaps this one.
+        prefetch_l1(&a.prev[i]);
+        prefetch_l1(&a.pos[i]);
+        prefetch_l1(&a.y[i]);
+        prefetch_l1(&a.disp[i]);
+        if (a.ctab) {
+            prefetch_l1(&a.ccount[i]);
+            prefetch_l1(a.ctab + static_cast<size_t>(i) * a.K * 4);
+        }
+        if (a.sc_f) {
+            prefetch_l1(&a.sc_f[i]);
+            prefetch_l1(&a.sc_h0[i]);
+            prefetch_l1(&a.sc_h1[i]);
+        }
+    }
+    if (valid && solve) {
+        if (L <= 2 && !kCap) accumulate_elements_x2<kDamp>(a, lane, L, adj, f, h);
+        else accumulate_elements<kDamp>(a, i, lane, L, adj, f, h);
+    }
     if (L > 1) {
         f.x = warp_sum(f.x, L);
         f.y = warp_sum(f.y, L);
@@ -308,8 +460,28 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
     const float mass = yv.w;
     float3 fc = f3(0.f, 0.f, 0.f);
     Sym3 hc = zero_sym();
-    if (a.ccount) accumulate_contacts(a, i, x, xyz(pv), pi.z, fc, hc);
-    if (a.sc_f) add_self_contact(a, i, fc, hc);
+    if (a.ctab) {
+        // the step's packed contacts, already in record order
+        const int nc = min(a.ccount[i], a.K);
+        const float4* e = a.ctab + static_cast<size_t>(i) * a.K * 4;
+        for (int k = 0; k < nc; ++k, e += 4) {
+            const float4 e0 = e[0], e1 = e[1], e2 = e[2], e3 = e[3];
+            contact_eval(x, xyz(pv), xyz(e0), xyz(e1), xyz(e2), pi.z, make_float4(e0.w, e1.w, e2.w, e3.x), a.dt,
+                         a.eps_u, fc, hc);
+        }
+    } else if (a.ccount) {
+        accumulate_contacts(a, i, x, xyz(pv), pi.z, fc, hc);
+    }
+    if (a.sc_f) {
+        const float4 s0 = a.sc_f[i], s1 = a.sc_h0[i], s2 = a.sc_h1[i];
+        fc = fc + xyz(s0);
+        hc.xx += s1.x;
+        hc.xy += s1.y;
+        hc.xz += s1.z;
+        hc.yy += s1.w;
+        hc.yz += s2.x;
+        hc.zz += s2.y;
+    }
     // h_total = h_elastic + m/dt^2 I + h_contact ; f_total = f_elastic + m (y - x)/dt^2 + f_contact
     add_diag(h, mass * a.dt_sqr_recip);
     add(h, hc);
@@ -616,6 +788,7 @@ static SweepArgs make_sweep_args(const SolverImpl& s, const VbdContacts* c, floa
         a.c_body_vel = c->soft_contact_body_vel;
         a.c_normal = c->soft_contact_normal;
         a.shapes = m.shapes;
+        a.ctab = s.ctab;
     }
     a.dt = dt;
     a.inv_dt = 1.0f / dt;
@@ -772,6 +945,20 @@ static int enqueue_forward(SolverImpl& s, const float* q_in, const float* qd_in,
     }
     const int block = 256;
     if (n > 0) forward_kernel<<<(n + block - 1) / block, block, 0, st>>>(a);
+    if (a.c_count && s.ctab && m.V > 0) {
+        PackArgs p;
+        p.ccount = s.ccount;
+        p.cslot = s.cslot;
+        p.K = s.K;
+        p.c_shape = c->soft_contact_shape;
+        p.c_body_pos = c->soft_contact_body_pos;
+        p.c_body_vel = c->soft_contact_body_vel;
+        p.c_normal = c->soft_contact_normal;
+        p.shapes = m.shapes;
+        p.ctab = s.ctab;
+        p.V = m.V;
+        pack_contacts_kernel<<<(m.V + block - 1) / block, block, 0, st>>>(p);
+    }
     return VBD_OK;
 }
 
@@ -891,12 +1078,13 @@ static void free_solver(SolverImpl& s) {
     s.ws_corr = s.ws_work = nullptr;
     for (auto& g : s.graphs) cudaGraphExecDestroy(g.exec);
     s.graphs.clear();
-    void* ptrs[] = {s.pos, s.prev, s.y, s.disp, s.ccount, s.cslot, s.status, s.resid_max};
+    void* ptrs[] = {s.pos, s.prev, s.y, s.disp, s.ccount, s.cslot, s.ctab, s.status, s.resid_max};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s.capture_stream) cudaStreamDestroy(s.capture_stream);
     s.pos = s.prev = s.y = s.disp = nullptr;
     s.ccount = s.cslot = nullptr;
+    s.ctab = nullptr;
     s.status = nullptr;
     s.resid_max = nullptr;
     s.capture_stream = nullptr;
@@ -974,6 +1162,7 @@ extern "C" int vbd_solver_create(const VbdModel* model, const VbdSolverOptions* 
     if (!rc) rc = alloc(reinterpret_cast<void**>(&s.disp), V * sizeof(float4));
     if (!rc) rc = alloc(reinterpret_cast<void**>(&s.ccount), V * sizeof(int));
     if (!rc) rc = alloc(reinterpret_cast<void**>(&s.cslot), V * s.K * sizeof(int));
+    if (!rc && m.S > 0) rc = alloc(reinterpret_cast<void**>(&s.ctab), V * s.K * 4 * sizeof(float4));
     if (!rc) rc = alloc(reinterpret_cast<void**>(&s.status), kStatusSlots * sizeof(unsigned));
     if (!rc) rc = alloc(reinterpret_cast<void**>(&s.resid_max), sizeof(float));
     if (!rc) {
