@@ -458,7 +458,10 @@ def main() -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
 
-    launches_per_step = 3 + ITERATIONS * colors
+    # kernels of one timed step: the collide kernel + the kernel nodes of the solver's step graph
+    # (counted by the library when it captured the step)
+    step_kernels = solver.step_kernel_count()
+    launches_per_step = 1 + (step_kernels if step_kernels >= 0 else 3 + ITERATIONS * colors)
     st = solver.status()
     line = {
         "metric": METRIC,

@@ -326,6 +326,11 @@ int vbd_solver_info(const VbdSolver* solver, int32_t* color_count, int32_t* lane
  * kernel (0 otherwise). */
 int vbd_solver_step_kernel(const VbdSolver* solver, int32_t* resident, int32_t* patches, int32_t* smem_bytes);
 
+/* Kernel launches of the most recent vbd_step: the kernel nodes of the CUDA graph it replayed
+ * (memset nodes excluded), or -1 when that step ran as plain launches (use_cuda_graph = 0, or
+ * inside the caller's own stream capture).  Diagnostics; no reference counterpart. */
+int vbd_step_kernel_count(const VbdSolver* solver, int32_t* kernels);
+
 /* Bound (in polling iterations) of every wait of the resident kernel; a wait that runs out counts
  * in VbdStatus.timeouts and the kernel returns early instead of hanging.  Default 4,194,304. */
 int vbd_set_spin_limit(VbdSolver* solver, uint32_t spins);

@@ -175,6 +175,7 @@ SIGNATURES = {
     "vbd_solver_info": (ctypes.c_int, [_VP, c_int32_p, c_int32_p, c_int32_p]),
     "vbd_set_launch": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),
     "vbd_solver_step_kernel": (ctypes.c_int, [_VP, c_int32_p, c_int32_p, c_int32_p]),
+    "vbd_step_kernel_count": (ctypes.c_int, [_VP, c_int32_p]),
     "vbd_set_spin_limit": (ctypes.c_int, [_VP, ctypes.c_uint32]),
     "vbd_color_graph": (
         ctypes.c_int,

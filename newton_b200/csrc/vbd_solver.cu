@@ -42,6 +42,7 @@ struct GraphEntry {
     float dt;
     int iterations;
     int lanes, block;
+    int kernels;  // kernel nodes of the captured step
     cudaGraphExec_t exec;
 };
 
@@ -54,6 +55,7 @@ struct SolverImpl {
     int K = 4;
     bool use_graph = true;
     long long steps = 0;
+    int last_step_kernels = -1;  // kernel launches of the last vbd_step (graph kernel nodes; -1: not a graph)
     // scratch (allocated once at create)
     float4* pos = nullptr;    // Gauss-Seidel iterate (state_in.particle_q in the reference)
     float4* prev = nullptr;   // particle_q_prev == pos_prev_collision_detection (step start)
@@ -410,18 +412,16 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;");
     if (valid && solve && lane == 0) {
-        // Warm L1 with everything lane 0 reads after the element walk (the vertex's own state,
-        // its contact count and first packed contact, its self-contact terms): a prefetch holds
-        // no register, so the walk keeps the register budget at which two color grids fit on an
-        // SM together and the next color's launch overlaps this one.
+        // Warm L1 with what lane 0 reads after the element walk (the vertex's own state, its
+        // contact count, its self-contact terms): a prefetch holds no register, so the walk keeps
+        // the register budget at which two color grids fit on an SM together and the next color's
+        // launch overlaps this one.  (The packed contacts themselves are not prefetched: most
+        // vertices have none, and their unused entries would be fetched from DRAM.)
         prefetch_l1(&a.prev[i]);
         prefetch_l1(&a.pos[i]);
         prefetch_l1(&a.y[i]);
         prefetch_l1(&a.disp[i]);
-        if (a.ctab) {
-            prefetch_l1(&a.ccount[i]);
-            prefetch_l1(a.ctab + static_cast<size_t>(i) * a.K * 4);
-        }
+        if (a.ctab) prefetch_l1(&a.ccount[i]);
         if (a.sc_f) {
             prefetch_l1(&a.sc_f[i]);
             prefetch_l1(&a.sc_h0[i]);
@@ -1070,6 +1070,20 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
     return VBD_OK;
 }
 
+// kernel nodes of a captured graph (memset and other nodes excluded); -1 if it cannot be read
+static int kernel_nodes(cudaGraph_t graph) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(graph, nullptr, &n) != cudaSuccess) return -1;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n > 0 && cudaGraphGetNodes(graph, nodes.data(), &n) != cudaSuccess) return -1;
+    int k = 0;
+    for (size_t j = 0; j < n; ++j) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[j], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+    }
+    return k;
+}
+
 static void free_solver(SolverImpl& s) {
     resident_free(s.resident);
     self_contact_free(s.sc);
@@ -1228,6 +1242,7 @@ extern "C" int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, cons
     VBD_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
     if (!s.use_graph || cs != cudaStreamCaptureStatusNone) {
         // plain launches (also the path taken inside a caller's own stream capture)
+        s.last_step_kernels = -1;
         rc = enqueue_step(s, q_in, qd_in, f_ext, q_out, qd_out, contacts, dt, iters, st);
         if (rc) return rc;
         VBD_CUDA_TRY(cudaGetLastError());
@@ -1240,6 +1255,7 @@ extern "C" int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, cons
         if (g.q_in == q_in && g.qd_in == qd_in && g.f_ext == f_ext && g.q_out == q_out && g.qd_out == qd_out &&
             g.has_contacts == (contacts != nullptr) && same_contacts(g.contacts, ckey) && g.dt == dt &&
             g.iterations == iters && g.lanes == s.lanes && g.block == s.block) {
+            s.last_step_kernels = g.kernels;
             VBD_CUDA_TRY(cudaGraphLaunch(g.exec, st));
             return VBD_OK;
         }
@@ -1247,6 +1263,7 @@ extern "C" int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, cons
     // capture the step on the private stream, instantiate, replay on the caller's stream; if the
     // resident kernel cannot be captured on this driver, fall back to per-color launches
     cudaGraphExec_t exec = nullptr;
+    int kernels = -1;
     for (int attempt = 0; attempt < 2 && !exec; ++attempt) {
         VBD_CUDA_TRY(cudaStreamBeginCapture(s.capture_stream, cudaStreamCaptureModeThreadLocal));
         const int erc = enqueue_step(s, q_in, qd_in, f_ext, q_out, qd_out, contacts, dt, iters, s.capture_stream);
@@ -1255,6 +1272,7 @@ extern "C" int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, cons
         cudaError_t e2 = cudaStreamEndCapture(s.capture_stream, &graph);
         cudaError_t e3 = cudaErrorUnknown;
         if (erc == VBD_OK && e1 == cudaSuccess && e2 == cudaSuccess && graph) e3 = cudaGraphInstantiate(&exec, graph, 0);
+        if (e3 == cudaSuccess) kernels = kernel_nodes(graph);
         if (graph) cudaGraphDestroy(graph);
         if (e3 == cudaSuccess) break;
         exec = nullptr;
@@ -1281,8 +1299,10 @@ extern "C" int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, cons
     g.iterations = iters;
     g.lanes = s.lanes;
     g.block = s.block;
+    g.kernels = kernels;
     g.exec = exec;
     s.graphs.push_back(g);
+    s.last_step_kernels = kernels;
     VBD_CUDA_TRY(cudaGraphLaunch(exec, st));
     return VBD_OK;
 }
@@ -1531,6 +1551,12 @@ extern "C" int vbd_solver_step_kernel(const VbdSolver* solver, int32_t* resident
     if (resident) *resident = on ? 1 : 0;
     if (patches) *patches = on ? s.resident.patches : 0;
     if (smem_bytes) *smem_bytes = on ? s.resident.smem_bytes : 0;
+    return VBD_OK;
+}
+
+extern "C" int vbd_step_kernel_count(const VbdSolver* solver, int32_t* kernels) {
+    if (!solver || !kernels) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_step_kernel_count: NULL argument");
+    *kernels = solver->s.last_step_kernels;
     return VBD_OK;
 }
 

@@ -283,6 +283,13 @@ class SolverVBD(SolverBase):
         _lib.check(self._lib.vbd_solver_step_kernel(self._handle, ctypes.byref(r), ctypes.byref(p), ctypes.byref(b)))
         return {"resident": bool(r.value), "patches": p.value, "smem_bytes": b.value}
 
+    def step_kernel_count(self) -> int:
+        """Kernel launches of the most recent ``step`` (kernel nodes of the CUDA graph it replayed;
+        -1 when it ran as plain launches)."""
+        k = ctypes.c_int32()
+        _lib.check(self._lib.vbd_step_kernel_count(self._handle, ctypes.byref(k)))
+        return k.value
+
     def set_warm_start(self, mlp, iterations: int) -> None:
         """Learned warm start as the step mode: every ``step`` runs forward, the MLP's prediction,
         ``iterations`` colour sweeps and finalize (``mlp=None`` turns it off)."""

@@ -207,3 +207,26 @@ def test_invalid_state_is_rejected():
     s0.particle_q = s0.particle_q.double()
     with pytest.raises(ValueError):
         solver.step(s0, s1, None, None, DT)
+
+
+def test_step_kernel_count_matches_the_step_structure():
+    """The step graph holds forward (+ the contact pack when contacts are given), one sweep per
+    color and iteration, and finalize; a plain (non-graph) step reports -1."""
+    model, q0 = scenes.single_cloth(n=16, side=0.5, seed=3, pin_top_corners=False, ground=0.0,
+                                    sphere=((0.0, 0.0, -0.2), 0.2), height=0.002)
+    colors = len(model.particle_color_groups)
+    pipe = CollisionPipeline(model, soft_contact_margin=5e-3)
+    for contacts in (None, pipe.contacts()):
+        solver = SolverVBD(model, iterations=3)
+        s0, s1 = model.state(), model.state()
+        s0.particle_q.copy_(torch.from_numpy(q0).cuda())
+        if contacts is not None:
+            pipe.collide(s0, contacts)
+        solver.step(s0, s1, None, contacts, DT)
+        torch.cuda.synchronize()
+        expect = 1 + (1 if contacts is not None else 0) + 3 * colors + 1
+        assert solver.step_kernel_count() == expect
+    solver = SolverVBD(model, iterations=3, use_cuda_graph=False)
+    s0, s1 = model.state(), model.state()
+    solver.step(s0, s1, None, None, DT)
+    assert solver.step_kernel_count() == -1
