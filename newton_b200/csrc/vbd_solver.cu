@@ -380,6 +380,21 @@ __device__ __forceinline__ void prefetch_l1(const void* p) {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// L2 prefetch of the 128-byte lines holding records [b, e) of a 16-byte-per-record array, the
+// lines dealt round-robin over the vertex's L lanes
+__device__ __forceinline__ void prefetch_rows_l2(const void* base, int b, int e, int lane, int L) {
+    if (e <= b) return;
+    const char* p = static_cast<const char*>(base);
+    const uintptr_t first = reinterpret_cast<uintptr_t>(p + 16 * static_cast<size_t>(b)) & ~uintptr_t(127);
+    const uintptr_t last = reinterpret_cast<uintptr_t>(p + 16 * static_cast<size_t>(e) - 1) & ~uintptr_t(127);
+    for (uintptr_t line = first + 128 * static_cast<uintptr_t>(lane); line <= last; line += 128 * static_cast<uintptr_t>(L))
+        prefetch_l2(reinterpret_cast<const void*>(line));
+}
+
 __device__ __forceinline__ float warp_sum(float v, int L) {
     for (int off = L >> 1; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
     return v;
@@ -408,6 +423,16 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
         pi = __ldg(&a.pinfo[i]);
         adj = __ldg(&a.vadj[i]);
         solve = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
+        if (solve && !kResidual && !kCap) {
+            // the vertex's element records are static too: start bringing them into L2 while the
+            // previous color still runs (pays on the first iteration after the records left L2;
+            // the register-capped build, used for grids of several waves, runs slower with it)
+            prefetch_rows_l2(a.tri_idx, adj.x, adj.y, lane, L);
+            prefetch_rows_l2(a.tri_D, adj.x, adj.y, lane, L);
+            prefetch_rows_l2(a.tri_mat, adj.x, adj.y, lane, L);
+            prefetch_rows_l2(a.edge_idx, adj.z, adj.w, lane, L);
+            prefetch_rows_l2(a.edge_mat, adj.z, adj.w, lane, L);
+        }
     }
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;");
