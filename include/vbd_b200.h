@@ -217,6 +217,19 @@ int vbd_solver_destroy(VbdSolver* solver);
 int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, const float* f_ext, float* q_out,
              float* qd_out, const VbdContacts* contacts, float dt, int32_t iterations, void* stream);
 
+/* Batched step of `count` independent solvers (each with its own model and state) in one call:
+ * element b of every array is solver b's argument to vbd_step, and the steps are enqueued in
+ * order on `stream`, so the results are those of `count` vbd_step calls.  f_ext and contacts may
+ * be NULL as a whole (no external force / no contacts for every solver) or hold NULL entries;
+ * iterations may be NULL (every solver's default) or hold one count per solver (< 0: default).
+ * The reference batches by putting several worlds in one Model (ModelBuilder.add_world), which
+ * vbd_model_create supports directly and which is the faster layout for many small cloths (one
+ * launch per color for all worlds); this entry point is for models that cannot be merged.
+ * On an error no further solver is enqueued and the message names the failing index. */
+int vbd_batch_step(VbdSolver* const* solvers, int32_t count, float* const* q_in, const float* const* qd_in,
+                   const float* const* f_ext, float* const* q_out, float* const* qd_out,
+                   const VbdContacts* const* contacts, float dt, const int32_t* iterations, void* stream);
+
 /* Allocation-free variant of vbd_step (no counterpart in the reference, whose solver always
  * allocates its scratch).  For callers that cannot call cudaMalloc -- code running during CUDA
  * stream capture, host callbacks or real-time loops where an allocation could block or

@@ -143,6 +143,12 @@ SIGNATURES = {
         ctypes.c_int,
         [_VP, _VP, _VP, _VP, _VP, _VP, ctypes.POINTER(VbdContacts), ctypes.c_float, ctypes.c_int32, _VP],
     ),
+    "vbd_batch_step": (
+        ctypes.c_int,
+        [ctypes.POINTER(_VP), ctypes.c_int32, ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(_VP),
+         ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(ctypes.POINTER(VbdContacts)), ctypes.c_float,
+         ctypes.POINTER(ctypes.c_int32), _VP],
+    ),
     "vbd_step_static": (
         ctypes.c_int,
         [_VP, _VP, _VP, _VP, _VP, _VP, ctypes.POINTER(VbdContacts), ctypes.c_float, ctypes.c_int32, ctypes.c_float, _VP],

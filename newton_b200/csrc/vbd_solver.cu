@@ -1332,6 +1332,22 @@ extern "C" int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, cons
     return VBD_OK;
 }
 
+extern "C" int vbd_batch_step(VbdSolver* const* solvers, int32_t count, float* const* q_in, const float* const* qd_in,
+                              const float* const* f_ext, float* const* q_out, float* const* qd_out,
+                              const VbdContacts* const* contacts, float dt, const int32_t* iterations,
+                              void* stream) {
+    if (count < 0) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_batch_step: count must be >= 0");
+    if (count == 0) return VBD_OK;
+    if (!solvers || !q_in || !qd_in || !q_out || !qd_out)
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_batch_step: solvers and state array lists must not be NULL");
+    for (int b = 0; b < count; ++b) {
+        const int rc = vbd_step(solvers[b], q_in[b], qd_in[b], f_ext ? f_ext[b] : nullptr, q_out[b], qd_out[b],
+                                contacts ? contacts[b] : nullptr, dt, iterations ? iterations[b] : -1, stream);
+        if (rc) return fail(rc, "vbd_batch_step: solver " + std::to_string(b) + ": " + vbd_last_error());
+    }
+    return VBD_OK;
+}
+
 extern "C" int vbd_forward(VbdSolver* solver, const float* q_in, const float* qd_in, const float* f_ext,
                            const VbdContacts* contacts, float dt, void* stream) {
     if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_forward: solver is NULL");

@@ -183,6 +183,51 @@ class SolverVBD(SolverBase):
             )
         )
 
+    @staticmethod
+    def step_batch(solvers: list["SolverVBD"], states_in: list[State], states_out: list[State],
+                   contacts: list[Contacts | None] | None, dt: float) -> None:
+        """``step`` of several independent solvers in one library call (``vbd_batch_step``): the
+        same results as calling ``solvers[b].step(states_in[b], states_out[b], None, contacts[b],
+        dt)`` in order, enqueued on the current stream.  All solvers must live on one device; each
+        uses its own ``iterations``."""
+        n = len(solvers)
+        if not (len(states_in) == len(states_out) == n) or (contacts is not None and len(contacts) != n):
+            raise ValueError("step_batch: solvers, states_in, states_out and contacts must have the same length")
+        if contacts is None:
+            contacts = [None] * n
+        # models without particles have nothing to step (as in ``step``)
+        keep = [b for b in range(n) if solvers[b].model.particle_count > 0]
+        if not keep:
+            return
+        dev = solvers[keep[0]].model.device
+        for b in keep:
+            s = solvers[b]
+            if s.model.device != dev:
+                raise ValueError("step_batch: all solvers must be on one device")
+            V = s.model.particle_count
+            s._check_state(states_in[b], f"states_in[{b}]", V, dev)
+            s._check_state(states_out[b], f"states_out[{b}]", V, dev)
+
+        def addr(t):
+            p = _lib.ptr(t)
+            return None if p is None else p.value
+
+        m = len(keep)
+        arr = ctypes.c_void_p * m
+        handles = arr(*[solvers[b]._handle.value for b in keep])
+        q_in = arr(*[addr(states_in[b].particle_q) for b in keep])
+        qd_in = arr(*[addr(states_in[b].particle_qd) for b in keep])
+        f_ext = arr(*[addr(states_in[b].particle_f) for b in keep])
+        q_out = arr(*[addr(states_out[b].particle_q) for b in keep])
+        qd_out = arr(*[addr(states_out[b].particle_qd) for b in keep])
+        cp = ctypes.POINTER(_lib.VbdContacts)
+        cptrs = (cp * m)(*[cp(contacts[b].c_struct()) if (contacts[b] is not None and solvers[b].model.shape_count > 0)
+                           else cp() for b in keep])
+        iters = (ctypes.c_int32 * m)(*[solvers[b].iterations for b in keep])
+        s0 = solvers[keep[0]]
+        _lib.check(s0._lib.vbd_batch_step(handles, m, q_in, qd_in, f_ext, q_out, qd_out, cptrs, ctypes.c_float(dt),
+                                          iters, s0._stream()))
+
     # ---- staged pieces (parity tests, residual-gated loops) ------------------------------
     def forward(self, state_in: State, contacts: Contacts | None, dt: float) -> None:
         self._iteration = 0

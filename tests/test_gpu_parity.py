@@ -230,3 +230,48 @@ def test_step_kernel_count_matches_the_step_structure():
     s0, s1 = model.state(), model.state()
     solver.step(s0, s1, None, None, DT)
     assert solver.step_kernel_count() == -1
+
+
+def test_batch_step_equals_individual_steps():
+    """vbd_batch_step over independent solvers (different meshes, with and without contacts, their
+    own iteration counts) gives bit-identical results to one step call per solver."""
+    specs = [
+        scenes.single_cloth(n=12, side=0.5, seed=4, pin_top_corners=True, ground=0.0,
+                            sphere=((0.0, 0.0, -0.2), 0.2), height=0.002),
+        scenes.hanging_cloth(seed=8),
+        scenes.single_cloth(n=20, side=0.8, seed=9, pin_top_corners=False, ground=0.0,
+                            sphere=((0.0, 0.0, 0.3), 0.3), height=0.61),
+    ]
+    iters = [3, 5, 4]
+
+    def setup():
+        out = []
+        for (model, q0), it in zip(specs, iters):
+            solver = SolverVBD(model, iterations=it)
+            pipe = CollisionPipeline(model, soft_contact_margin=5e-3)
+            c = pipe.contacts() if model.shape_count > 0 else None
+            s0, s1 = model.state(), model.state()
+            s0.particle_q.copy_(torch.from_numpy(q0).cuda())
+            out.append((solver, pipe, c, s0, s1))
+        return out
+
+    single, batch = setup(), setup()
+    for _ in range(3):
+        for solver, pipe, c, s0, s1 in single:
+            if c is not None:
+                pipe.collide(s0, c)
+            solver.step(s0, s1, None, c, DT)
+            s0.assign(s1)
+        for solver, pipe, c, s0, s1 in batch:
+            if c is not None:
+                pipe.collide(s0, c)
+        SolverVBD.step_batch([b[0] for b in batch], [b[3] for b in batch], [b[4] for b in batch],
+                             [b[2] for b in batch], DT)
+        for b in batch:
+            b[3].assign(b[4])
+    torch.cuda.synchronize()
+    for a, b in zip(single, batch):
+        assert torch.equal(a[4].particle_q, b[4].particle_q)
+        assert torch.equal(a[4].particle_qd, b[4].particle_qd)
+    with pytest.raises(ValueError):
+        SolverVBD.step_batch([single[0][0]], [], [], None, DT)
