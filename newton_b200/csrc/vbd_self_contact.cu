@@ -78,6 +78,7 @@ struct GridArgs {
     const int4* elem;     // triangles or edges
     int n;
     bool tri;
+    bool all_cells;       // every element goes into every cell its box overlaps (edge grid)
     float inv_cell;
     unsigned mask;
     int* cnt;
@@ -107,10 +108,14 @@ __device__ __forceinline__ int3 center_cell(float4 lo, float4 hi, float inv) {
                      cell_coord(0.5f * (lo.z + hi.z), inv));
 }
 
-// An element whose half-extent is at most half a cell goes into the one bucket of its box
-// centre's cell; a larger one (stretched) goes into every cell its box overlaps, up to
-// kMaxLargeCells, and is flagged (lo.w = 1).  Queries then only look margin + half a cell beyond
-// their own box, however far the cloth stretches elsewhere.
+// Triangle grid (queried by points): a triangle whose half-extent is at most half a cell goes into
+// the one bucket of its box centre's cell; a larger one (stretched) goes into every cell its box
+// overlaps, up to kMaxLargeCells, and is flagged (lo.w = 1).  A vertex query then looks margin +
+// half a cell around its point, however far the cloth stretches elsewhere.
+// Edge grid (queried by edge boxes): every edge goes into every cell its box overlaps (flagged),
+// so an edge query only covers its box grown by the margin -- for edges shorter than a cell that
+// is fewer bucket entries than centre binning's extra half cell on every side -- and a pair is
+// taken only in the first cell the two ranges share.
 constexpr int kMaxLargeCells = 4096;
 
 __global__ void grid_count_kernel(GridArgs a) {
@@ -119,7 +124,7 @@ __global__ void grid_count_kernel(GridArgs a) {
     float3 lo, hi;
     elem_box(a, e, lo, hi);
     const float half = 0.5f * fmaxf(fmaxf(hi.x - lo.x, hi.y - lo.y), hi.z - lo.z);
-    const bool large = !(half <= 0.5f / a.inv_cell);
+    const bool large = a.all_cells || !(half <= 0.5f / a.inv_cell);
     const float4 l4 = make_float4(lo.x, lo.y, lo.z, large ? 1.f : 0.f), h4 = make_float4(hi.x, hi.y, hi.z, 0.f);
     a.box[2 * e] = l4;
     a.box[2 * e + 1] = h4;
@@ -385,9 +390,9 @@ __global__ void __launch_bounds__(kQueryBlock) vt_query_kernel(QueryArgs a) {
 
 // ---- edge-edge candidates ------------------------------------------------------------------
 // Edge-edge pairs are symmetric: edge e only searches partners g > e and records the pair in both
-// lists through atomic slots; ee_sort_kernel then orders every list.  A small partner sits in one
-// bucket only; a large (multi-cell) partner is taken in the first cell of the query range it
-// occupies, so every pair is met exactly once.
+// lists through atomic slots; ee_sort_kernel then orders every list.  A partner sits in every
+// cell its box overlaps and is taken only in the first cell of the query range it occupies, so
+// every pair is met exactly once.
 struct EeQuery {
     int e;
     int4 ed;
@@ -471,8 +476,8 @@ __global__ void __launch_bounds__(kQueryBlock) ee_query_kernel(QueryArgs a) {
         const float m = a.margin;
         v.qlo = fmin3(v.a0, v.a1) - f3(m, m, m);
         v.qhi = fmax3(v.a0, v.a1) + f3(m, m, m);
-        const float r = 0.5f / a.inv_cell;
-        v.q = cell_range(v.qlo - f3(r, r, r), v.qhi + f3(r, r, r), a.inv_cell);
+        // every partner sits in all the cells its box overlaps: the query's own cells suffice
+        v.q = cell_range(v.qlo, v.qhi, a.inv_cell);
         ok = cell_count(v.q) <= kMaxQueryCells;
         if (!ok) {
             atomicAdd(&a.counters[kScGridOverflow], 1u);
@@ -990,7 +995,7 @@ int self_contact_create(const VbdModelImpl& m, const SelfContactParams& p, SelfC
     sc.tri_mask = tn - 1;
     sc.edge_mask = en - 1;
     sc.tri_items_cap = 2 * std::max(T, 1) + 65536;  // large (stretched) elements take several cells
-    sc.edge_items_cap = 2 * std::max(E, 1) + 65536;
+    sc.edge_items_cap = 8 * std::max(E, 1) + 65536;  // an edge shorter than a cell overlaps at most 8 cells
     auto az = [&](void** ptr, size_t bytes) {
         if (!rc) rc = alloc_zero(ptr, bytes);
     };
@@ -1077,6 +1082,7 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     g.elem = sc.tri;
     g.n = T;
     g.tri = true;
+    g.all_cells = false;
     g.mask = sc.tri_mask;
     g.cnt = sc.tri_cnt;
     g.off = sc.tri_off;
@@ -1098,6 +1104,7 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     g.elem = sc.edge;
     g.n = E;
     g.tri = false;
+    g.all_cells = true;
     g.mask = sc.edge_mask;
     g.cnt = sc.edge_cnt;
     g.off = sc.edge_off;
