@@ -250,6 +250,7 @@ constexpr int kMaxQueryCells = 512;
 constexpr int kWarpUnionCells = 128;  // larger warp unions fall back to one walk per lane
 constexpr int kQueryBlock = 128;
 constexpr int kQueryWarps = kQueryBlock / 32;
+constexpr int kEeLanes = 4;  // lanes per edge-edge query (4 measured best of 2, 4, 8)
 
 // ---- vertex-triangle candidates ------------------------------------------------------------
 struct VtQuery {
@@ -461,11 +462,15 @@ __device__ __forceinline__ void ee_scan_lane(const QueryArgs& a, const EeQuery& 
             }
 }
 
+// kEeLanes lanes serve one edge query, so a warp holds 32 / kEeLanes consecutive (spatially
+// adjacent) edges: their union of cell ranges stays close to one query's range, and each lane
+// tests every kEeLanes-th staged entry.  Each (edge, partner) test runs on exactly one lane.
 __global__ void __launch_bounds__(kQueryBlock) ee_query_kernel(QueryArgs a) {
     __shared__ int s_id[kQueryWarps][32];
     __shared__ float4 s_box[kQueryWarps][64];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int e = (blockIdx.x * blockDim.x + threadIdx.x) / kEeLanes;
+    const int sub = lane % kEeLanes;
     EeQuery v;
     v.e = e;
     bool ok = false;
@@ -480,7 +485,7 @@ __global__ void __launch_bounds__(kQueryBlock) ee_query_kernel(QueryArgs a) {
         v.q = cell_range(v.qlo, v.qhi, a.inv_cell);
         ok = cell_count(v.q) <= kMaxQueryCells;
         if (!ok) {
-            atomicAdd(&a.counters[kScGridOverflow], 1u);
+            if (sub == 0) atomicAdd(&a.counters[kScGridOverflow], 1u);
         } else {
             v.n0b = a.near + a.near_off[v.ed.x];
             v.n0e = a.near + a.near_off[v.ed.x + 1];
@@ -491,7 +496,7 @@ __global__ void __launch_bounds__(kQueryBlock) ee_query_kernel(QueryArgs a) {
     CellRange u;
     if (!warp_union(ok, v.q, u)) return;
     if (cell_count(u) > kWarpUnionCells) {
-        if (ok) ee_scan_lane(a, v);
+        if (ok && sub == 0) ee_scan_lane(a, v);
         return;
     }
     for (int z = u.lo.z; z <= u.hi.z; ++z)
@@ -512,7 +517,7 @@ __global__ void __launch_bounds__(kQueryBlock) ee_query_kernel(QueryArgs a) {
                     __syncwarp();
                     const int mc = min(32, cnt - c);
                     if (mine) {
-                        for (int t = 0; t < mc; ++t) {
+                        for (int t = sub; t < mc; t += kEeLanes) {
                             const int g = s_id[w][t];
                             if (g <= e) continue;
                             const float4 blo = s_box[w][2 * t], bhi = s_box[w][2 * t + 1];
@@ -1173,7 +1178,8 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     }
     if (E > 0) {
         VBD_CUDA_TRY(cudaMemsetAsync(sc.ee_count, 0, static_cast<size_t>(E) * sizeof(int), st));
-        ee_query_kernel<<<(E + kQueryBlock - 1) / kQueryBlock, kQueryBlock, 0, st>>>(q);
+        const long long ee_threads = static_cast<long long>(E) * kEeLanes;
+        ee_query_kernel<<<static_cast<unsigned>((ee_threads + kQueryBlock - 1) / kQueryBlock), kQueryBlock, 0, st>>>(q);
         VBD_CUDA_TRY(cudaGetLastError());
         ee_sort_kernel<<<(E + 255) / 256, 256, 0, st>>>(E, sc.ee_count, sc.ee_list, sc.p.edge_buffer);
         VBD_CUDA_TRY(cudaGetLastError());
