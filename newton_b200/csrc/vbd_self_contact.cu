@@ -231,6 +231,7 @@ struct QueryArgs {
     const int4* edge;
     const int* near_off;
     const int* near;
+    const int* vt_order;  // query slot -> vertex
     int V, T, E;
     float margin, inv_cell, par_eps, rest_excl;
     unsigned tri_mask, edge_mask;
@@ -322,7 +323,11 @@ __global__ void __launch_bounds__(kQueryBlock) vt_query_kernel(QueryArgs a) {
     __shared__ int s_id[kQueryWarps][32];
     __shared__ float4 s_box[kQueryWarps][64];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    // consecutive query slots are spatially close vertices (Morton order of the rest shape; the
+    // internal vertex order is color-major, so neighbours in it are far apart), which keeps the
+    // warp's union of cell ranges small
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = slot < a.V ? a.vt_order[slot] : a.V;
     const bool active = i < a.V;
     VtQuery v;
     v.i = i;
@@ -830,6 +835,43 @@ int upload_vec(T** dst, const std::vector<T>& src) {
     return VBD_OK;
 }
 
+// spreads the low 10 bits of x to every third bit (Morton interleaving)
+uint32_t spread3(uint32_t x) {
+    x &= 0x3ffu;
+    x = (x | (x << 16)) & 0x030000ffu;
+    x = (x | (x << 8)) & 0x0300f00fu;
+    x = (x | (x << 4)) & 0x030c30c3u;
+    x = (x | (x << 2)) & 0x09249249u;
+    return x;
+}
+
+// indices of pts in Z-order of their position quantised to 1024 steps per axis of the bounding
+// box (ties by index), so that consecutive indices are spatially close
+std::vector<int> morton_order(const std::vector<float3>& pts) {
+    const size_t n = pts.size();
+    std::vector<int> order(n);
+    for (size_t k = 0; k < n; ++k) order[k] = static_cast<int>(k);
+    if (n == 0) return order;
+    float3 lo = pts[0], hi = pts[0];
+    for (const float3& p : pts) {
+        lo = make_float3(std::min(lo.x, p.x), std::min(lo.y, p.y), std::min(lo.z, p.z));
+        hi = make_float3(std::max(hi.x, p.x), std::max(hi.y, p.y), std::max(hi.z, p.z));
+    }
+    const float ext = std::max(std::max(hi.x - lo.x, hi.y - lo.y), std::max(hi.z - lo.z, 1e-12f));
+    const float s = 1023.0f / ext;
+    std::vector<uint32_t> code(n);
+    for (size_t k = 0; k < n; ++k) {
+        const float3 p = pts[k];
+        auto q = [&](float v, float l) {
+            const float t = (v - l) * s;
+            return static_cast<uint32_t>(std::isfinite(t) ? std::min(std::max(t, 0.0f), 1023.0f) : 0.0f);
+        };
+        code[k] = (spread3(q(p.x, lo.x)) << 2) | (spread3(q(p.y, lo.y)) << 1) | spread3(q(p.z, lo.z));
+    }
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return code[a] < code[b]; });
+    return order;
+}
+
 int alloc_zero(void** p, size_t bytes) {
     bytes = std::max<size_t>(bytes, 16);
     VBD_CUDA_TRY(cudaMalloc(p, bytes));
@@ -848,7 +890,7 @@ bool self_contact_detect_now(const SelfContact& sc, int it) {
 
 void self_contact_free(SelfContact& sc) {
     void* ptrs[] = {sc.tri,      sc.edge,     sc.inc_t_off, sc.inc_t,    sc.inc_e_off,  sc.inc_e,     sc.near_off,
-                    sc.near,     sc.rest,     sc.tri_cnt,   sc.tri_off,  sc.tri_cur,    sc.tri_items, sc.edge_cnt,
+                    sc.near,     sc.rest,     sc.vt_order,     sc.tri_cnt,   sc.tri_off,  sc.tri_cur,    sc.tri_items, sc.edge_cnt,
                     sc.edge_off, sc.edge_cur, sc.edge_items, sc.scan_tmp, sc.vt_count,  sc.vt_list,   sc.ee_count,
                     sc.ee_list,  sc.tv_count, sc.tv_list,   sc.cd,       sc.sc_f,       sc.sc_h0,     sc.sc_h1,
                     sc.ts,       sc.counters, sc.vworld,    sc.tri_box,  sc.edge_box,   sc.flag,      sc.tri_item_box, sc.edge_item_box, sc.vfilt_off, sc.vfilt, sc.efilt_off, sc.efilt, sc.color_start, sc.vcolor,
@@ -963,6 +1005,9 @@ int self_contact_create(const VbdModelImpl& m, const SelfContactParams& p, SelfC
     std::vector<float4> rest(V);
     for (int i = 0; i < V; ++i)
         rest[i] = make_float4(m.rest_q_h[3 * i], m.rest_q_h[3 * i + 1], m.rest_q_h[3 * i + 2], 0.f);
+    std::vector<float3> vp(V);
+    for (int i = 0; i < V; ++i) vp[i] = make_float3(rest[i].x, rest[i].y, rest[i].z);
+    const std::vector<int> vt_order = morton_order(vp);
 
     int rc = VBD_OK;
     if (!rc) rc = upload_vec(&sc.tri, tri);
@@ -973,6 +1018,7 @@ int self_contact_create(const VbdModelImpl& m, const SelfContactParams& p, SelfC
     if (!rc) rc = upload_vec(&sc.inc_e, ie_list);
     if (!rc) rc = upload_vec(&sc.near_off, near_off);
     if (!rc) rc = upload_vec(&sc.near, near_list);
+    if (!rc) rc = upload_vec(&sc.vt_order, vt_order);
     if (!rc) rc = upload_vec(&sc.rest, rest);
     if (!rc) rc = upload_vec(&sc.vworld, vworld);
     sc.C = m.C;
@@ -1138,6 +1184,7 @@ int self_contact_detect(const VbdModelImpl& m, SelfContact& sc, const float4* po
     q.tri = sc.tri;
     q.edge = sc.edge;
     q.near_off = sc.near_off;
+    q.vt_order = sc.vt_order;
     q.near = sc.near;
     q.V = V;
     q.T = T;

@@ -56,6 +56,7 @@ struct SelfContact {
     int* near_off = nullptr;   // [V+1]
     int* near = nullptr;       // vertices within (threshold - 1) rings, self excluded
     float4* rest = nullptr;    // [V] rest positions (exclusion radius)
+    int* vt_order = nullptr;   // [V] order in which vertex queries run (Morton order of rest positions)
     int* vworld = nullptr;     // [V] particle world
     int* vfilt_off = nullptr;  // [V+1] external vertex-triangle filter (internal vertex order), or NULL
     int* vfilt = nullptr;
