@@ -759,15 +759,21 @@ __device__ __forceinline__ void ts_min(unsigned* ts, int i, float3 x, float3 dx,
     atomicMin(&ts[i], __float_as_uint(t));
 }
 
-// grid-stride over the non-empty rows: vertex-triangle rows first, then edge-edge rows
+// grid-stride over the non-empty rows (vertex-triangle rows first, then edge-edge rows), kPlanarLanes
+// lanes per row taking its pairs round-robin: the truncation factors are reduced with atomicMin,
+// which does not depend on the order
+constexpr int kPlanarLanes = 4;
+
 __global__ void planar_kernel(TruncArgs a) {
     const int nv = a.counts[0], ne = a.counts[1];
-    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < nv + ne; w += gridDim.x * blockDim.x) {
+    const int sub = threadIdx.x % kPlanarLanes;
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) / kPlanarLanes; w < nv + ne;
+         w += gridDim.x * blockDim.x / kPlanarLanes) {
         if (w < nv) {
             const int i = a.rows[w];
             const float3 v = xyz(a.cd[i]), dv = xyz(a.disp[i]);
             const int* row = a.vt_list + static_cast<size_t>(i) * a.vbuf;
-            for (int k = 0; k < a.vt_count[i]; ++k) {
+            for (int k = sub; k < a.vt_count[i]; k += kPlanarLanes) {
                 const int4 tr = a.tri[row[k]];
                 const float3 t1 = xyz(a.cd[tr.x]), t2 = xyz(a.cd[tr.y]), t3 = xyz(a.cd[tr.z]);
                 const float3 d1 = xyz(a.disp[tr.x]), d2 = xyz(a.disp[tr.y]), d3 = xyz(a.disp[tr.z]);
@@ -784,7 +790,7 @@ __global__ void planar_kernel(TruncArgs a) {
             const float3 a0 = xyz(a.cd[ed.x]), a1 = xyz(a.cd[ed.y]);
             const float3 da0 = xyz(a.disp[ed.x]), da1 = xyz(a.disp[ed.y]);
             const int* row = a.ee_list + static_cast<size_t>(e) * a.ebuf;
-            for (int k = 0; k < a.ee_count[e]; ++k) {
+            for (int k = sub; k < a.ee_count[e]; k += kPlanarLanes) {
                 const int4 gd = a.edge[row[k]];
                 const float3 b0 = xyz(a.cd[gd.x]), b1 = xyz(a.cd[gd.y]);
                 const float3 db0 = xyz(a.disp[gd.x]), db1 = xyz(a.disp[gd.y]);
@@ -1318,8 +1324,8 @@ int self_contact_truncate(const VbdModelImpl& m, SelfContact& sc, float4* pos, f
     a.ts = sc.ts;
     a.rows = sc.act_rows;
     a.counts = sc.act_cnt;
-    const int n = std::max(V, m.E);
-    planar_kernel<<<std::min((n + 127) / 128, 148 * 16), 128, 0, st>>>(a);
+    const long long n = static_cast<long long>(std::max(V, m.E)) * kPlanarLanes;
+    planar_kernel<<<static_cast<int>(std::min<long long>((n + 127) / 128, 148 * 32)), 128, 0, st>>>(a);
     VBD_CUDA_TRY(cudaGetLastError());
     apply_truncation_kernel<<<(V + 255) / 256, 256, 0, st>>>(V, sc.cd, disp, pos, sc.ts, sc.max_disp);
     VBD_CUDA_TRY(cudaGetLastError());
