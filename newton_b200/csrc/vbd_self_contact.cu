@@ -23,7 +23,7 @@
 //   * a query rejects candidates by box overlap before any filter or exact distance, skips
 //     entries of other cells that share its bucket, and keeps the survivors in a sorted
 //     per-vertex / per-edge list (so each pair is reported once);
-//   * forces are gathered per vertex of the current color, 8 lanes per vertex taking the pairs
+//   * forces are gathered per vertex of the current color, 16 lanes per vertex taking the pairs
 //     round-robin in a fixed order (own vertex-triangle pairs, then the pairs of each incident
 //     triangle, then the edge-edge pairs of each incident edge) and reduced with xor shuffles, so
 //     results are deterministic;
@@ -650,7 +650,7 @@ struct AccumArgs {
 // L lanes per vertex: the vertex's pairs (own vertex-triangle list, then each incident triangle's
 // colliding vertices, then each incident edge's colliding edges) are dealt round-robin to the
 // lanes, and the partial sums are combined with xor shuffles -- a fixed order, so deterministic.
-constexpr int kAccumLanes = 8;
+constexpr int kAccumLanes = 16;
 
 __device__ __forceinline__ float lane_sum(float v) {
     for (int off = kAccumLanes >> 1; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
@@ -709,15 +709,16 @@ __device__ __forceinline__ void accumulate_lane(const AccumArgs& a, int i, int l
 }
 
 // Grid-stride over the color's contact-touching vertices (the others hold zero since the last
-// detection).  A warp serves 4 vertices per round and the round bound is the same for the whole
-// warp, so every lane joins every shuffle.
+// detection).  A warp serves 32 / kAccumLanes vertices per round and the round bound is the same
+// for the whole warp, so every lane joins every shuffle.
 __global__ void accumulate_kernel(AccumArgs a) {
     const int n = *a.count;
     const int lane = threadIdx.x & (kAccumLanes - 1);
     const int sub = (threadIdx.x & 31) / kAccumLanes;  // vertex slot of this lane in its warp
     const int warps = gridDim.x * (blockDim.x >> 5);
     const int warp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    for (int base = 4 * warp; base < n; base += 4 * warps) {
+    constexpr int kVerts = 32 / kAccumLanes;  // vertices per warp and round
+    for (int base = kVerts * warp; base < n; base += kVerts * warps) {
         const int slot = base + sub;
         const int i = slot < n ? a.list[slot] : -1;
         float3 f = f3(0.f, 0.f, 0.f);
@@ -762,7 +763,7 @@ __device__ __forceinline__ void ts_min(unsigned* ts, int i, float3 x, float3 dx,
 // grid-stride over the non-empty rows (vertex-triangle rows first, then edge-edge rows), kPlanarLanes
 // lanes per row taking its pairs round-robin: the truncation factors are reduced with atomicMin,
 // which does not depend on the order
-constexpr int kPlanarLanes = 4;
+constexpr int kPlanarLanes = 16;
 
 __global__ void planar_kernel(TruncArgs a) {
     const int nv = a.counts[0], ne = a.counts[1];
