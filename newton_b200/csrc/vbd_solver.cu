@@ -56,6 +56,7 @@ struct SolverImpl {
     bool use_graph = true;
     long long steps = 0;
     int last_step_kernels = -1;  // kernel launches of the last vbd_step (graph kernel nodes; -1: not a graph)
+    int staged_iteration = 0;    // iteration of the staged API (vbd_forward resets, vbd_begin_iteration sets)
     // scratch (allocated once at create)
     float4* pos = nullptr;    // Gauss-Seidel iterate (state_in.particle_q in the reference)
     float4* prev = nullptr;   // particle_q_prev == pos_prev_collision_detection (step start)
@@ -244,6 +245,7 @@ struct SweepArgs {
     unsigned* status;
     int v_begin, v_end;
     int write_pos;           // 1: commit q = prev + disp in place (conflict-free coloring)
+    int prefetch_records;    // 1: prefetch the vertices' element records into L2 (first iteration of a step)
     float* resid_out;        // residual mode: per-vertex residual (original order) or NULL
     float* resid_max;        // residual mode: max residual (float bits, atomicMax)
     const int* perm;
@@ -423,10 +425,11 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
         pi = __ldg(&a.pinfo[i]);
         adj = __ldg(&a.vadj[i]);
         solve = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
-        if (solve && !kResidual && !kCap) {
+        if (solve && !kResidual && !kCap && a.prefetch_records) {
             // the vertex's element records are static too: start bringing them into L2 while the
-            // previous color still runs (pays on the first iteration after the records left L2;
-            // the register-capped build, used for grids of several waves, runs slower with it)
+            // previous color still runs (asked for on the first iteration of a step, after the
+            // records may have left L2; the register-capped build, used for grids of several
+            // waves, runs slower with it)
             prefetch_rows_l2(a.tri_idx, adj.x, adj.y, lane, L);
             prefetch_rows_l2(a.tri_D, adj.x, adj.y, lane, L);
             prefetch_rows_l2(a.tri_mat, adj.x, adj.y, lane, L);
@@ -987,9 +990,11 @@ static int enqueue_forward(SolverImpl& s, const float* q_in, const float* qd_in,
     return VBD_OK;
 }
 
-static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float dt, cudaStream_t st) {
+static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float dt, cudaStream_t st,
+                          bool first_iteration = true) {
     const VbdModelImpl& m = *s.m;
     SweepArgs a = make_sweep_args(s, c, dt);
+    a.prefetch_records = first_iteration ? 1 : 0;
     a.v_begin = m.color_start[color];
     a.v_end = m.color_start[color + 1];
     if (a.v_end <= a.v_begin) return;
@@ -1046,7 +1051,7 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
         if (rc) return rc;
         warm_start_kernel<<<(V + 255) / 256, 256, 0, st>>>(s.m->perm, s.m->pinfo, s.prev, s.disp, s.pos, delta, V);
         for (int it = 0; it < s.ws_iterations; ++it)
-            for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st);
+            for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st, it == 0);
         correction_kernel<<<(V + 255) / 256, 256, 0, st>>>(s.m->perm, s.m->pinfo, s.pos, s.y, s.ws_corr, V);
         enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
         return VBD_OK;
@@ -1083,14 +1088,14 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
         int rc = self_contact_start(s, st);
         for (int it = 0; it < iterations && !rc; ++it) {
             if (self_contact_detect_now(s.sc, it)) rc = self_contact_detect(*s.m, s.sc, s.pos, s.disp, true, st);
-            for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st);
+            for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st, it == 0);
         }
         if (rc) return rc;
         enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
         return VBD_OK;
     }
     for (int it = 0; it < iterations; ++it)
-        for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st);
+        for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st, it == 0);
     enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
     return VBD_OK;
 }
@@ -1360,6 +1365,7 @@ extern "C" int vbd_forward(VbdSolver* solver, const float* q_in, const float* qd
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // a staged sequence starts from an empty contact table
     VBD_CUDA_TRY(cudaMemsetAsync(s.ccount, 0, sizeof(int) * static_cast<size_t>(s.m->V), st));
+    s.staged_iteration = 0;
     enqueue_forward(s, q_in, qd_in, f_ext, contacts, dt, st);
     VBD_CUDA_TRY(cudaGetLastError());
     if (s.sc.on) return self_contact_start(s, st);
@@ -1370,6 +1376,7 @@ extern "C" int vbd_begin_iteration(VbdSolver* solver, int32_t iteration, void* s
     if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_begin_iteration: solver is NULL");
     SolverImpl& s = solver->s;
     if (iteration < 0) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_begin_iteration: iteration must be >= 0");
+    s.staged_iteration = iteration;
     if (s.m->V == 0 || !self_contact_detect_now(s.sc, iteration)) return VBD_OK;
     return self_contact_detect(*s.m, s.sc, s.pos, s.disp, true, static_cast<cudaStream_t>(stream));
 }
@@ -1418,7 +1425,7 @@ extern "C" int vbd_sweep_color(VbdSolver* solver, int32_t color, const VbdContac
     if (color < 0 || color >= s.m->C) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_sweep_color: color out of range");
     if (!(dt > 0.0f)) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_sweep_color: dt must be > 0");
     if (contacts && !contacts->soft_contact_count) contacts = nullptr;
-    enqueue_color(s, color, contacts, dt, static_cast<cudaStream_t>(stream));
+    enqueue_color(s, color, contacts, dt, static_cast<cudaStream_t>(stream), s.staged_iteration == 0);
     VBD_CUDA_TRY(cudaGetLastError());
     return VBD_OK;
 }
