@@ -431,11 +431,26 @@ def main() -> None:
     # ---- end to end through the public API with host buffers --------------------------------
     # every step: H2D of the step's inputs (positions, velocities) from pinned host memory,
     # collide + step, D2H of the step's result (positions, velocities)
+    # positions and velocities live in one [2, V, 3] block on each side (the states' arrays are
+    # views of it), so each direction is one copy
     V = model.particle_count
-    h_q = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
-    h_qd = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
-    h_q.copy_(s0.particle_q)
-    h_qd.copy_(s0.particle_qd)
+    h_state = torch.empty((2, V, 3), dtype=torch.float32, pin_memory=True)
+    d_in = torch.empty((2, V, 3), dtype=torch.float32, device=dev)
+    d_out = torch.empty((2, V, 3), dtype=torch.float32, device=dev)
+    e_in, e_out = model.state(), model.state()
+    e_in.particle_q, e_in.particle_qd = d_in[0], d_in[1]
+    e_out.particle_q, e_out.particle_qd = d_out[0], d_out[1]
+    h_state[0].copy_(s0.particle_q)
+    h_state[1].copy_(s0.particle_qd)
+
+    def e2e_step():
+        d_in.copy_(h_state, non_blocking=True)
+        pipe.collide(e_in, contacts)
+        solver.step(e_in, e_out, None, contacts, DT)
+        h_state.copy_(d_out, non_blocking=True)
+
+    for _ in range(W):  # the solver captures its step graph for these buffers here, untimed
+        e2e_step()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     Ke = max(K // 4, 10)
@@ -443,12 +458,7 @@ def main() -> None:
     for k in range(Ke):
         flush.zero_()
         e0.record(stream)
-        s0.particle_q.copy_(h_q, non_blocking=True)
-        s0.particle_qd.copy_(h_qd, non_blocking=True)
-        pipe.collide(s0, contacts)
-        solver.step(s0, s1, None, contacts, DT)
-        h_q.copy_(s1.particle_q, non_blocking=True)
-        h_qd.copy_(s1.particle_qd, non_blocking=True)
+        e2e_step()
         e1.record(stream)
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)
