@@ -23,7 +23,7 @@
 //   * a query rejects candidates by box overlap before any filter or exact distance, skips
 //     entries of other cells that share its bucket, and keeps the survivors in a sorted
 //     per-vertex / per-edge list (so each pair is reported once);
-//   * forces are gathered per vertex of the current color, 16 lanes per vertex taking the pairs
+//   * forces are gathered per vertex of the current color, one warp per vertex taking the pairs
 //     round-robin in a fixed order (own vertex-triangle pairs, then the pairs of each incident
 //     triangle, then the edge-edge pairs of each incident edge) and reduced with xor shuffles, so
 //     results are deterministic;
@@ -650,7 +650,7 @@ struct AccumArgs {
 // L lanes per vertex: the vertex's pairs (own vertex-triangle list, then each incident triangle's
 // colliding vertices, then each incident edge's colliding edges) are dealt round-robin to the
 // lanes, and the partial sums are combined with xor shuffles -- a fixed order, so deterministic.
-constexpr int kAccumLanes = 16;
+constexpr int kAccumLanes = 32;
 
 __device__ __forceinline__ float lane_sum(float v) {
     for (int off = kAccumLanes >> 1; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
