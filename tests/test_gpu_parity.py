@@ -275,3 +275,63 @@ def test_batch_step_equals_individual_steps():
         assert torch.equal(a[4].particle_qd, b[4].particle_qd)
     with pytest.raises(ValueError):
         SolverVBD.step_batch([single[0][0]], [], [], None, DT)
+
+
+def test_full_size_draped_cloth_step_matches_oracle():
+    """The benchmark's draped cloth at its full size (256 x 256, 65,536 vertices, sphere + ground):
+    drape it on the GPU until it rests on the sphere, then one GPU step and one FP32 oracle step
+    from that same state agree to TOL_STEP, contacts included."""
+    import os
+
+    model, q0 = scenes.draped_cloth(n=256, seed=0)
+    solver = SolverVBD(model, iterations=10)
+    pipe = CollisionPipeline(model, soft_contact_margin=5e-3)
+    c = pipe.contacts()
+    s0, s1 = model.state(), model.state()
+    s0.particle_q.copy_(torch.from_numpy(q0).cuda())
+    for _ in range(300):  # 0.5 s: the cloth lands on the sphere after ~0.2 s
+        pipe.collide(s0, c)
+        solver.step(s0, s1, None, c, DT)
+        s0, s1 = s1, s0
+    torch.cuda.synchronize()
+    q = s0.particle_q.cpu().numpy()
+    qd = s0.particle_qd.cpu().numpy()
+    assert np.isfinite(q).all()
+    _, q_g, qd_g, contacts = _gpu_step(model, solver, q, qd, pipe, DT)
+    assert contacts.count() > 1000, "the cloth should rest on the sphere"
+    orc = oracle.VBDOracle(model, "f32", threads=os.cpu_count() or 1)
+    _, q_o, qd_o = _oracle_step(model, orc, q, qd, 5e-3, DT, 10)
+    err = float(np.abs(q_g - q_o).max())
+    print(f"full-size draped cloth, {contacts.count()} contacts: max |dx| GPU vs oracle {err:.3e} m")
+    assert err <= TOL_STEP
+    assert np.abs(qd_g - qd_o).max() <= 2.0 * TOL_STEP / DT
+
+
+def test_full_size_batched_worlds_step_matches_oracle():
+    """The 512-world batch at its full size (1.89 M vertices, one ground plane per world): after 260
+    GPU steps (the cloths, released 0.5 m up, are on the ground by then), one GPU step and one FP32
+    oracle step from that state agree to TOL_STEP, ground contacts included."""
+    import os
+
+    model, q0 = scenes.batched_worlds(512, seed=0)
+    solver = SolverVBD(model, iterations=10)
+    pipe = CollisionPipeline(model, soft_contact_margin=5e-3)
+    c = pipe.contacts()
+    s0, s1 = model.state(), model.state()
+    s0.particle_q.copy_(torch.from_numpy(q0).cuda())
+    for _ in range(260):
+        pipe.collide(s0, c)
+        solver.step(s0, s1, None, c, DT)
+        s0, s1 = s1, s0
+    torch.cuda.synchronize()
+    q = s0.particle_q.cpu().numpy()
+    qd = s0.particle_qd.cpu().numpy()
+    assert np.isfinite(q).all()
+    _, q_g, _, contacts = _gpu_step(model, solver, q, qd, pipe, DT)
+    assert contacts.count() > 10000, "the cloths should lie on their ground planes"
+    orc = oracle.VBDOracle(model, "f32", threads=os.cpu_count() or 1)
+    _, q_o, _ = _oracle_step(model, orc, q, qd, 5e-3, DT, 10)
+    err = float(np.abs(q_g - q_o).max())
+    print(f"full-size batched worlds ({model.particle_count} vertices, {contacts.count()} contacts): "
+          f"max |dx| GPU vs oracle {err:.3e} m")
+    assert err <= TOL_STEP
