@@ -1,0 +1,89 @@
+"""Host-side measurement helpers of bench.py (no GPU): the algorithmic byte count the roofline
+uses, the parsing of the nvidia-smi clock samples taken during the timed region, and the peak
+lookup with its fallback."""
+
+import json
+import os
+import tempfile
+
+import numpy as np
+
+import bench
+from newton_b200 import scenes
+
+
+def test_algorithmic_bytes_follow_the_per_element_formula():
+    model, _ = scenes.hanging_cloth(seed=0, device="cpu")
+    adj = model.soft_mesh_adjacency
+    n_csr = (len(adj.v_adj_tris) + len(adj.v_adj_edges)) // 2
+    V, T, E = model.particle_count, model.tri_count, model.edge_count
+    expect = 60 * V + 44 * T + 32 * E + 8 * n_csr + 8 * (V + 1)
+    assert bench.algorithmic_bytes_per_iteration(model) == expect
+    # a regular grid: every triangle appears in 3 vertex rows; ~394 B per vertex-iteration at scale
+    assert len(adj.v_adj_tris) // 2 == 3 * T
+    per_vertex = expect / V
+    assert 300.0 < per_vertex < 420.0
+
+
+class _FakeProc:
+    def terminate(self):
+        pass
+
+    def wait(self, timeout=None):
+        return 0
+
+
+def _sampler_with(lines):
+    s = bench.ClockSampler(0)
+    fd, path = tempfile.mkstemp(suffix=".csv")
+    with os.fdopen(fd, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    s.path = path
+    s.f = open(os.devnull, "w")
+    s.proc = _FakeProc()
+    return s
+
+
+def test_clock_samples_give_median_max_and_active_reasons():
+    rows = [
+        "0, 1965, 1965, 700.5, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active",
+        "0, 1950, 1965, 990.1, 0x0000000000000004, Not Active, Not Active, Not Active, Active",
+        "0, 1965, 1965, 701.0, 0x0000000000000000, Not Active, Not Active, Not Active, Not Active",
+        "garbage line",
+    ]
+    out = _sampler_with(rows).stop()
+    assert out == {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
+
+
+def test_clock_samples_flag_the_rejecting_reasons():
+    rows = ["0, 1200, 1965, 800.0, 0x0000000000000008, Active, Not Active, Active, Not Active"]
+    out = _sampler_with(rows).stop()
+    assert out["reasons"] == ["hw_slowdown", "sw_thermal_slowdown"]
+    assert out["sm_mhz"] == 1200.0
+
+
+def test_clock_sampler_without_samples_reports_none():
+    assert _sampler_with([]).stop() is None
+    s = bench.ClockSampler(0)
+    assert s.stop() is None  # never started
+
+
+def test_measured_peaks_read_the_file_or_fall_back(tmp_path, monkeypatch):
+    here = os.path.dirname(os.path.abspath(bench.__file__))
+    p = os.path.join(here, "MEASURED_PEAKS.json")
+    peaks = bench.measured_peaks()
+    if os.path.exists(p):
+        with open(p) as f:
+            assert peaks == {"hbm_gbs": float(json.load(f)["hbm_gbs"]), "source": "measured"}
+    else:
+        assert peaks == {"hbm_gbs": 6650.0, "source": "fallback"}
+    # the fallback when the file cannot be read
+    monkeypatch.setattr(bench.os.path, "abspath", lambda _p: str(tmp_path / "bench.py"))
+    assert bench.measured_peaks() == {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def test_sweep_traffic_summary_is_per_vertex_iteration():
+    t = bench.sweep_traffic_per_vertex_iteration()
+    assert t is not None and np.isfinite(t)
+    # 14.18 MB of cold-cache DRAM per color launch of 16,384 vertices (profiles/)
+    assert abs(t - 14.18e6 / 16384) < 5.0
