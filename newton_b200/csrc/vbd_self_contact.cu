@@ -504,6 +504,9 @@ __global__ void __launch_bounds__(kQueryBlock) ee_query_kernel(QueryArgs a) {
         if (ok && sub == 0) ee_scan_lane(a, v);
         return;
     }
+    // partners with id <= the warp's smallest query id are rejected by every lane (g > e): they
+    // are dropped while staging, so the lanes only walk the entries that can pass
+    const int e_min = __reduce_min_sync(0xffffffffu, ok ? e : INT_MAX);
     for (int z = u.lo.z; z <= u.hi.z; ++z)
         for (int y = u.lo.y; y <= u.hi.y; ++y)
             for (int x = u.lo.x; x <= u.hi.x; ++x) {
@@ -513,14 +516,19 @@ __global__ void __launch_bounds__(kQueryBlock) ee_query_kernel(QueryArgs a) {
                 const int b = a.edge_off[h];
                 const int cnt = min(b + a.edge_cnt[h], a.edge_cap) - b;
                 for (int c = 0; c < cnt; c += 32) {
-                    if (c + lane < cnt) {
+                    int gid = -1;
+                    if (c + lane < cnt) gid = a.edge_items[b + c + lane];
+                    const bool keep = gid > e_min;
+                    const unsigned kept = __ballot_sync(0xffffffffu, keep);
+                    if (keep) {
                         const int k = b + c + lane;
-                        s_id[w][lane] = a.edge_items[k];
-                        s_box[w][2 * lane] = a.edge_item_box[2 * k];
-                        s_box[w][2 * lane + 1] = a.edge_item_box[2 * k + 1];
+                        const int slot = __popc(kept & ((1u << lane) - 1u));
+                        s_id[w][slot] = gid;
+                        s_box[w][2 * slot] = a.edge_item_box[2 * k];
+                        s_box[w][2 * slot + 1] = a.edge_item_box[2 * k + 1];
                     }
                     __syncwarp();
-                    const int mc = min(32, cnt - c);
+                    const int mc = __popc(kept);
                     if (mine) {
                         for (int t = sub; t < mc; t += kEeLanes) {
                             const int g = s_id[w][t];
