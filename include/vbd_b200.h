@@ -366,6 +366,22 @@ int vbd_color_graph(int32_t num_nodes, int64_t num_edges, const int32_t* edges, 
 int vbd_coloring_graph_edges(int32_t num_nodes, int64_t num_pairs, const int32_t* pairs, int32_t* edges_out,
                              int64_t* num_edges_out);
 
+/* Bending-edge table of a triangle mesh (host arrays): MeshAdjacency._compute_edge_adjacency
+ * (utils/mesh.py:465-531).  tris [nt,3].  Undirected edges are numbered in first-occurrence order
+ * of the traversal (triangle t, local edge k = (tris[t][k], tris[t][k+1]), opposite tris[t][k+2]);
+ * edge_indices rows are [o0, o1, v0, v1] (o1 = -1 on a boundary), edge_tri the two triangles,
+ * tri_edge [nt,3] each triangle's edges.  Outputs sized for 3 nt edges; num_edges receives the
+ * count, nonmanifold (may be NULL) the number of triangle sides beyond the second on an edge. */
+int vbd_mesh_edge_adjacency(const int32_t* tris, int32_t nt, int32_t* edge_indices, int32_t* edge_tri,
+                            int32_t* tri_edge, int32_t* num_edges, int32_t* nonmanifold);
+
+/* Per-vertex CSR of (element id, local slot) records (host arrays): init_vertex_adjacency and its
+ * count / fill kernels (utils/mesh.py:595-655, :675-772).  entries [n_elements, per_element] are
+ * vertex ids (-1 skipped) and slot_of[per_element] the slot each position records; records are in
+ * element order.  values receives 2 ints per record; offsets [particle_count + 1] counts ints. */
+int vbd_mesh_vertex_csr(const int32_t* entries, int32_t n_elements, int32_t per_element, const int32_t* slot_of,
+                        int32_t particle_count, int32_t* values, int32_t* offsets);
+
 #ifdef __cplusplus
 }
 #endif

@@ -191,6 +191,14 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_int32, ctypes.c_int64, c_int32_p, c_int32_p, ctypes.POINTER(ctypes.c_int64)],
     ),
+    "vbd_mesh_edge_adjacency": (
+        ctypes.c_int,
+        [c_int32_p, ctypes.c_int32, c_int32_p, c_int32_p, c_int32_p, c_int32_p, c_int32_p],
+    ),
+    "vbd_mesh_vertex_csr": (
+        ctypes.c_int,
+        [c_int32_p, ctypes.c_int32, ctypes.c_int32, c_int32_p, ctypes.c_int32, c_int32_p, c_int32_p],
+    ),
 }
 
 _lib = None
@@ -270,6 +278,36 @@ def color_graph(num_nodes: int, edges: np.ndarray, algorithm: int = 0, balance: 
         )
     )
     return colors, int(nc.value)
+
+
+def mesh_edge_adjacency(tris: np.ndarray) -> tuple[np.ndarray, np.ndarray, np.ndarray, int]:
+    """(edge_indices [ne,4], edge_tri [ne,2], tri_edge [nt,3], non-manifold sides) of a triangle
+    mesh (vbd_mesh_edge_adjacency)."""
+    lib = load()
+    tris = np.ascontiguousarray(np.asarray(tris, dtype=np.int32).reshape(-1, 3))
+    nt = tris.shape[0]
+    edges = np.empty((3 * nt, 4), np.int32)
+    edge_tri = np.empty((3 * nt, 2), np.int32)
+    tri_edge = np.empty((nt, 3), np.int32)
+    ne, bad = ctypes.c_int32(0), ctypes.c_int32(0)
+    if nt:
+        check(lib.vbd_mesh_edge_adjacency(as_i32p(tris), nt, as_i32p(edges), as_i32p(edge_tri), as_i32p(tri_edge),
+                                          ctypes.byref(ne), ctypes.byref(bad)))
+    return edges[: ne.value].copy(), edge_tri[: ne.value].copy(), tri_edge, bad.value
+
+
+def mesh_vertex_csr(entries: np.ndarray, slot_of, particle_count: int) -> tuple[np.ndarray, np.ndarray]:
+    """(values, offsets) of the per-vertex (element, slot) CSR (vbd_mesh_vertex_csr)."""
+    lib = load()
+    entries = np.ascontiguousarray(np.asarray(entries, dtype=np.int32))
+    n_el, per = entries.shape
+    slots = np.ascontiguousarray(np.asarray(slot_of, dtype=np.int32).reshape(-1))
+    n_rec = int(np.count_nonzero(entries != -1))
+    values = np.empty(max(2 * n_rec, 2), np.int32)
+    offsets = np.zeros(particle_count + 1, np.int32)
+    check(lib.vbd_mesh_vertex_csr(as_i32p(entries), n_el, per, as_i32p(slots), int(particle_count), as_i32p(values),
+                                  as_i32p(offsets)))
+    return values[: 2 * n_rec].copy(), offsets
 
 
 def canonical_edges(num_nodes: int, pairs: np.ndarray) -> np.ndarray:

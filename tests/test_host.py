@@ -49,20 +49,35 @@ def test_c_abi_rejects_invalid_arguments_without_a_gpu():
 
 
 # ---- adjacency -----------------------------------------------------------------------------
-def _edge_adjacency_loop(tris):
+def _edge_adjacency_loop(tris, with_maps=False):
     """Loop restatement of MeshAdjacency._compute_edge_adjacency (utils/mesh.py:465-531)."""
     edges = {}
     order = []
     rows = []
+    edge_tri = []
+    tri_edge = []
+    seen = []
     for t, (a, b, c) in enumerate(tris):
+        te = []
         for v0, v1, o in ((a, b, c), (b, c, a), (c, a, b)):
             key = (min(v0, v1), max(v0, v1))
             if key not in edges:
                 edges[key] = len(order)
                 order.append(key)
                 rows.append([o, -1, v0, v1])
+                edge_tri.append([t, -1])
+                seen.append(1)
             else:
-                rows[edges[key]][1] = o
+                e = edges[key]
+                if seen[e] == 1:  # the second side fills o1; a third or later one is non-manifold
+                    rows[e][1] = o
+                    edge_tri[e][1] = t
+                seen[e] += 1
+            te.append(edges[key])
+        tri_edge.append(te)
+    if with_maps:
+        return (np.array(rows, dtype=np.int32).reshape(-1, 4), np.array(edge_tri, dtype=np.int32).reshape(-1, 2),
+                np.array(tri_edge, dtype=np.int32).reshape(-1, 3))
     return np.array(rows, dtype=np.int32)
 
 
@@ -94,6 +109,36 @@ def test_edge_and_vertex_adjacency_follow_reference_order():
     ve, oe = _csr_loop(e.tolist(), V, [2, 3, 0, 1])
     np.testing.assert_array_equal(adj.v_adj_edges, ve)
     np.testing.assert_array_equal(adj.v_adj_edges_offsets, oe)
+
+
+def test_edge_adjacency_of_non_manifold_soups_matches_the_reference_rules():
+    """Random triangle soups (edges shared by 3+ triangles, isolated vertices): the second side
+    fills o1 / tri1, later sides only warn, as in utils/mesh.py:510-525; the per-vertex CSRs keep
+    element order and skip -1 (boundary) opposites."""
+    import warnings
+
+    rng = np.random.default_rng(7)
+    for _ in range(20):
+        nv = int(rng.integers(3, 40))
+        nt = int(rng.integers(1, 200))
+        tris = np.stack([rng.choice(nv, 3, replace=False) for _ in range(nt)]).astype(np.int32)
+        with warnings.catch_warnings(record=True) as w:
+            warnings.simplefilter("always")
+            e, et, te = compute_edge_adjacency(tris)
+        re, ret, rte = _edge_adjacency_loop(tris.tolist(), with_maps=True)
+        np.testing.assert_array_equal(e, re)
+        np.testing.assert_array_equal(et, ret)
+        np.testing.assert_array_equal(te, rte)
+        counts = np.unique(np.sort(np.concatenate([tris[:, [0, 1]], tris[:, [1, 2]], tris[:, [2, 0]]]), axis=1),
+                           axis=0, return_counts=True)[1]
+        assert any("non-manifold" in str(x.message) for x in w) == bool((counts > 2).any())
+        adj = MeshAdjacency(tris, e).init_vertex_adjacency(nv + 3)  # trailing isolated vertices
+        vt, ot = _csr_loop(tris.tolist(), nv + 3, [0, 1, 2])
+        np.testing.assert_array_equal(adj.v_adj_tris, vt)
+        np.testing.assert_array_equal(adj.v_adj_tris_offsets, ot)
+        ve, oe = _csr_loop(e.tolist(), nv + 3, [2, 3, 0, 1])
+        np.testing.assert_array_equal(adj.v_adj_edges, ve)
+        np.testing.assert_array_equal(adj.v_adj_edges_offsets, oe)
 
 
 # ---- builder -------------------------------------------------------------------------------
