@@ -366,6 +366,14 @@ int vbd_color_graph(int32_t num_nodes, int64_t num_edges, const int32_t* edges, 
 int vbd_coloring_graph_edges(int32_t num_nodes, int64_t num_pairs, const int32_t* pairs, int32_t* edges_out,
                              int64_t* num_edges_out);
 
+/* The conflict graph of construct_trimesh_graph_edges (graph_coloring.py:99-197) straight from the
+ * element arrays (host, already filtered by the active masks): each triangle [nt,3] adds its 3
+ * vertex pairs, each bending hinge [nb,4] (may be NULL when nb = 0) all 6 pairs of its vertices,
+ * pairs with a negative id skipped; edges_out ([3 nt + 6 nb, 2] capacity) receives the unique
+ * (min, max) pairs in lexicographic order, num_edges_out their count. */
+int vbd_trimesh_graph_edges(int32_t num_nodes, const int32_t* tris, int64_t nt, const int32_t* bend, int64_t nb,
+                            int32_t* edges_out, int64_t* num_edges_out);
+
 /* Bending-edge table of a triangle mesh (host arrays): MeshAdjacency._compute_edge_adjacency
  * (utils/mesh.py:465-531).  tris [nt,3].  Undirected edges are numbered in first-occurrence order
  * of the traversal (triangle t, local edge k = (tris[t][k], tris[t][k+1]), opposite tris[t][k+2]);

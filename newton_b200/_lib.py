@@ -191,6 +191,11 @@ SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_int32, ctypes.c_int64, c_int32_p, c_int32_p, ctypes.POINTER(ctypes.c_int64)],
     ),
+    "vbd_trimesh_graph_edges": (
+        ctypes.c_int,
+        [ctypes.c_int32, c_int32_p, ctypes.c_int64, c_int32_p, ctypes.c_int64, c_int32_p,
+         ctypes.POINTER(ctypes.c_int64)],
+    ),
     "vbd_mesh_edge_adjacency": (
         ctypes.c_int,
         [c_int32_p, ctypes.c_int32, c_int32_p, c_int32_p, c_int32_p, c_int32_p, c_int32_p],
@@ -308,6 +313,21 @@ def mesh_vertex_csr(entries: np.ndarray, slot_of, particle_count: int) -> tuple[
     check(lib.vbd_mesh_vertex_csr(as_i32p(entries), n_el, per, as_i32p(slots), int(particle_count), as_i32p(values),
                                   as_i32p(offsets)))
     return values[: 2 * n_rec].copy(), offsets
+
+
+def trimesh_graph_edges(num_nodes: int, tris: np.ndarray, bend: np.ndarray | None) -> np.ndarray:
+    """Canonical conflict-graph edges of triangles + bending hinges (vbd_trimesh_graph_edges)."""
+    lib = load()
+    tris = np.ascontiguousarray(np.asarray(tris, dtype=np.int32).reshape(-1, 3))
+    bend = np.ascontiguousarray(np.asarray(bend if bend is not None else np.empty((0, 4)), dtype=np.int32)
+                                .reshape(-1, 4))
+    cap = 3 * tris.shape[0] + 6 * bend.shape[0]
+    out = np.empty((max(cap, 1), 2), np.int32)
+    n = ctypes.c_int64(0)
+    check(lib.vbd_trimesh_graph_edges(int(num_nodes), as_i32p(tris) if tris.size else None, tris.shape[0],
+                                      as_i32p(bend) if bend.size else None, bend.shape[0], as_i32p(out),
+                                      ctypes.byref(n)))
+    return out[: n.value].copy()
 
 
 def canonical_edges(num_nodes: int, pairs: np.ndarray) -> np.ndarray:

@@ -33,30 +33,23 @@ def _canonicalize_edges(edges: np.ndarray) -> np.ndarray:
 
 def construct_trimesh_graph_edges(tri_indices, tri_active_mask=None, bending_edge_indices=None,
                                   bending_edge_active_mask=None) -> np.ndarray:
-    parts = []
+    tris = np.empty((0, 3), np.int32)
+    bend = np.empty((0, 4), np.int32)
     if tri_indices is not None:
         tris = np.asarray(tri_indices, dtype=np.int32).reshape(-1, 3)
         if tri_active_mask is not None:
             m = np.asarray(tri_active_mask).astype(bool)
             tris = tris if m.ndim == 0 and m else (tris[:0] if m.ndim == 0 else tris[m])
-        if tris.size:
-            parts.append(np.concatenate([tris[:, [0, 1]], tris[:, [0, 2]], tris[:, [1, 2]]], axis=0))
     if bending_edge_indices is not None:
         bend = np.asarray(bending_edge_indices, dtype=np.int32).reshape(-1, 4)
         if bending_edge_active_mask is not None:
             m = np.asarray(bending_edge_active_mask).astype(bool)
             bend = bend if m.ndim == 0 and m else (bend[:0] if m.ndim == 0 else bend[m])
-        if bend.size:
-            pairs = np.concatenate(
-                [bend[:, [0, 1]], bend[:, [0, 2]], bend[:, [0, 3]], bend[:, [1, 2]], bend[:, [1, 3]], bend[:, [2, 3]]],
-                axis=0,
-            )
-            pairs = pairs[np.all(pairs >= 0, axis=1)]
-            if pairs.size:
-                parts.append(pairs)
-    if not parts:
+    if tris.size == 0 and bend.size == 0:
         return np.empty((0, 2), dtype=np.int32)
-    return _canonicalize_edges(np.concatenate(parts, axis=0))
+    num_nodes = int(max(tris.max() if tris.size else -1, bend.max() if bend.size else -1)) + 1
+    # the pairs are generated and canonicalised natively (no [3 nt + 6 nb, 2] intermediate)
+    return _lib.trimesh_graph_edges(num_nodes, tris, bend)
 
 
 def convert_to_color_groups(num_colors: int, particle_colors: np.ndarray) -> list[np.ndarray]:

@@ -162,29 +162,22 @@ extern "C" int vbd_color_graph(int32_t num_nodes, int64_t num_edges, const int32
     return VBD_OK;
 }
 
-// Canonical edge list of the conflict graph: construct_trimesh_graph_edges / the sort-unique
-// step of graph_coloring.py:99-197.  Each pair becomes (min, max), self-pairs are dropped, and the
-// unique pairs come out in lexicographic order -- the order numpy.unique(axis=0) gives -- via a
-// counting sort by the smaller endpoint and a sort of each (short) row.
-extern "C" int vbd_coloring_graph_edges(int32_t num_nodes, int64_t num_pairs, const int32_t* pairs, int32_t* edges_out,
-                                        int64_t* num_edges_out) {
-    if (num_nodes < 0 || num_pairs < 0 || (num_pairs > 0 && (!pairs || !edges_out)) || !num_edges_out)
-        return vbd::fail(VBD_ERR_INVALID_ARGUMENT, "vbd_coloring_graph_edges: invalid arguments");
-    for (int64_t k = 0; k < 2 * num_pairs; ++k)
-        if (pairs[k] < 0 || pairs[k] >= num_nodes)
-            return vbd::fail(VBD_ERR_INVALID_ARGUMENT, "vbd_coloring_graph_edges: endpoint out of range");
+// Canonical edge list of the conflict graph (the sort-unique step of graph_coloring.py:99-197):
+// the unique (min, max) pairs of the pairs `for_each(visit)` emits, self-pairs dropped, in
+// lexicographic order -- the order numpy.unique(axis=0) gives -- via a counting sort by the
+// smaller endpoint and a sort of each (short) row.
+template <typename ForEach>
+static int64_t canonical_pairs(int32_t num_nodes, ForEach&& for_each, int32_t* edges_out) {
     std::vector<int64_t> off(static_cast<size_t>(num_nodes) + 1, 0);
-    for (int64_t k = 0; k < num_pairs; ++k) {
-        const int a = pairs[2 * k], b = pairs[2 * k + 1];
+    for_each([&](int a, int b) {
         if (a != b) ++off[static_cast<size_t>(std::min(a, b)) + 1];
-    }
+    });
     for (int v = 0; v < num_nodes; ++v) off[v + 1] += off[v];
     std::vector<int32_t> nb(static_cast<size_t>(off[num_nodes]));
     std::vector<int64_t> cur(off.begin(), off.end() - 1);
-    for (int64_t k = 0; k < num_pairs; ++k) {
-        const int a = pairs[2 * k], b = pairs[2 * k + 1];
+    for_each([&](int a, int b) {
         if (a != b) nb[cur[std::min(a, b)]++] = std::max(a, b);
-    }
+    });
     int64_t n = 0;
     for (int v = 0; v < num_nodes; ++v) {
         auto b = nb.begin() + off[v], e = nb.begin() + off[v + 1];
@@ -196,6 +189,58 @@ extern "C" int vbd_coloring_graph_edges(int32_t num_nodes, int64_t num_pairs, co
             ++n;
         }
     }
-    *num_edges_out = n;
+    return n;
+}
+
+// ... of an explicit pair list
+extern "C" int vbd_coloring_graph_edges(int32_t num_nodes, int64_t num_pairs, const int32_t* pairs, int32_t* edges_out,
+                                        int64_t* num_edges_out) {
+    if (num_nodes < 0 || num_pairs < 0 || (num_pairs > 0 && (!pairs || !edges_out)) || !num_edges_out)
+        return vbd::fail(VBD_ERR_INVALID_ARGUMENT, "vbd_coloring_graph_edges: invalid arguments");
+    for (int64_t k = 0; k < 2 * num_pairs; ++k)
+        if (pairs[k] < 0 || pairs[k] >= num_nodes)
+            return vbd::fail(VBD_ERR_INVALID_ARGUMENT, "vbd_coloring_graph_edges: endpoint out of range");
+    *num_edges_out = canonical_pairs(
+        num_nodes,
+        [&](auto&& visit) {
+            for (int64_t k = 0; k < num_pairs; ++k) visit(pairs[2 * k], pairs[2 * k + 1]);
+        },
+        edges_out);
+    return VBD_OK;
+}
+
+// The whole conflict-graph construction of construct_trimesh_graph_edges
+// (graph_coloring.py:99-197) from the (already mask-filtered) element arrays: each triangle adds
+// (a,b) (a,c) (b,c), each bending hinge all 6 pairs of its 4 vertices, pairs with a negative id
+// skipped; the result is canonicalised as vbd_coloring_graph_edges does.  edges_out needs room for
+// 3 nt + 6 nb pairs.
+extern "C" int vbd_trimesh_graph_edges(int32_t num_nodes, const int32_t* tris, int64_t nt, const int32_t* bend,
+                                       int64_t nb, int32_t* edges_out, int64_t* num_edges_out) {
+    if (num_nodes < 0 || nt < 0 || nb < 0 || (nt > 0 && !tris) || (nb > 0 && !bend) ||
+        ((nt > 0 || nb > 0) && !edges_out) || !num_edges_out)
+        return vbd::fail(VBD_ERR_INVALID_ARGUMENT, "vbd_trimesh_graph_edges: invalid arguments");
+    for (int64_t k = 0; k < 3 * nt; ++k)
+        if (tris[k] < 0 || tris[k] >= num_nodes)
+            return vbd::fail(VBD_ERR_INVALID_ARGUMENT, "vbd_trimesh_graph_edges: triangle vertex out of range");
+    for (int64_t k = 0; k < 4 * nb; ++k)
+        if (bend[k] >= num_nodes)
+            return vbd::fail(VBD_ERR_INVALID_ARGUMENT, "vbd_trimesh_graph_edges: hinge vertex out of range");
+    *num_edges_out = canonical_pairs(
+        num_nodes,
+        [&](auto&& visit) {
+            for (int64_t t = 0; t < nt; ++t) {
+                const int32_t* r = tris + 3 * t;
+                visit(r[0], r[1]);
+                visit(r[0], r[2]);
+                visit(r[1], r[2]);
+            }
+            for (int64_t e = 0; e < nb; ++e) {
+                const int32_t* r = bend + 4 * e;
+                static const int kPairs[6][2] = {{0, 1}, {0, 2}, {0, 3}, {1, 2}, {1, 3}, {2, 3}};
+                for (const auto& p : kPairs)
+                    if (r[p[0]] >= 0 && r[p[1]] >= 0) visit(r[p[0]], r[p[1]]);
+            }
+        },
+        edges_out);
     return VBD_OK;
 }
