@@ -169,6 +169,38 @@ def test_cloth_grid_counts_masses_and_rest_data():
     np.testing.assert_allclose(D @ model.tri_poses[0], np.eye(2), atol=1e-5)
 
 
+def _graph_edges_loop(tris, bend):
+    """Set restatement of construct_trimesh_graph_edges (graph_coloring.py:99-197)."""
+    pairs = set()
+    for a, b, c in tris:
+        for u, v in ((a, b), (a, c), (b, c)):
+            if u != v:
+                pairs.add((min(u, v), max(u, v)))
+    for row in bend:
+        for i in range(4):
+            for j in range(i + 1, 4):
+                u, v = row[i], row[j]
+                if u >= 0 and v >= 0 and u != v:
+                    pairs.add((min(u, v), max(u, v)))
+    return np.array(sorted(pairs), dtype=np.int32).reshape(-1, 2)
+
+
+def test_conflict_graph_edges_match_a_set_restatement():
+    rng = np.random.default_rng(11)
+    for k in range(25):
+        nv = int(rng.integers(3, 40))
+        nt = int(rng.integers(1, 150))
+        tris = np.stack([rng.choice(nv, 3, replace=False) for _ in range(nt)]).astype(np.int32)
+        bend = compute_edge_adjacency(tris)[0]
+        tmask = rng.random(nt) > 0.25
+        bmask = rng.random(len(bend)) > 0.25
+        got = construct_trimesh_graph_edges(tris, tmask, bend, bmask)
+        np.testing.assert_array_equal(got, _graph_edges_loop(tris[tmask].tolist(), bend[bmask].tolist()))
+        got = construct_trimesh_graph_edges(tris, None, None, None)
+        np.testing.assert_array_equal(got, _graph_edges_loop(tris.tolist(), []))
+    assert construct_trimesh_graph_edges(None, None, None, None).shape == (0, 2)
+
+
 def test_coloring_valid_and_balanced():
     for include_bending in (False, True):
         model, _ = scenes.single_cloth(n=40, include_bending=include_bending, device="cpu")
