@@ -4,6 +4,8 @@ import ctypes
 import re
 from pathlib import Path
 
+import warnings
+
 import numpy as np
 import pytest
 
@@ -191,7 +193,9 @@ def test_conflict_graph_edges_match_a_set_restatement():
         nv = int(rng.integers(3, 40))
         nt = int(rng.integers(1, 150))
         tris = np.stack([rng.choice(nv, 3, replace=False) for _ in range(nt)]).astype(np.int32)
-        bend = compute_edge_adjacency(tris)[0]
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")  # random soups have non-manifold edges
+            bend = compute_edge_adjacency(tris)[0]
         tmask = rng.random(nt) > 0.25
         bmask = rng.random(len(bend)) > 0.25
         got = construct_trimesh_graph_edges(tris, tmask, bend, bmask)
