@@ -48,6 +48,23 @@ def test_c_abi_rejects_invalid_arguments_without_a_gpu():
     bad = np.array([[0, 5]], np.int32)
     assert lib.vbd_color_graph(3, 1, _lib.as_i32p(bad), 0, 1, ctypes.c_float(1.1), _lib.as_i32p(colors),
                                ctypes.byref(nc)) == _lib.VBD_ERR_INVALID_ARGUMENT
+    # host setup functions: NULL outputs and out-of-range vertex ids are errors, not crashes
+    tri = np.array([[0, 1, 2]], np.int32)
+    n32 = ctypes.c_int32()
+    assert lib.vbd_mesh_edge_adjacency(_lib.as_i32p(tri), 1, None, None, None, ctypes.byref(n32),
+                                       None) == _lib.VBD_ERR_INVALID_ARGUMENT
+    vals = np.zeros(8, np.int32)
+    offs = np.zeros(3, np.int32)
+    slots = np.array([0, 1, 2], np.int32)
+    assert lib.vbd_mesh_vertex_csr(_lib.as_i32p(tri), 1, 3, _lib.as_i32p(slots), 2, _lib.as_i32p(vals),
+                                   _lib.as_i32p(offs)) == _lib.VBD_ERR_INVALID_ARGUMENT
+    assert b"out of range" in lib.vbd_last_error()
+    out = np.zeros((3, 2), np.int32)
+    n64 = ctypes.c_int64()
+    assert lib.vbd_trimesh_graph_edges(2, _lib.as_i32p(tri), 1, None, 0, _lib.as_i32p(out),
+                                       ctypes.byref(n64)) == _lib.VBD_ERR_INVALID_ARGUMENT
+    assert lib.vbd_trimesh_graph_edges(3, _lib.as_i32p(tri), 1, None, 0, _lib.as_i32p(out), ctypes.byref(n64)) == 0
+    assert n64.value == 3 and out.tolist() == [[0, 1], [0, 2], [1, 2]]
 
 
 # ---- adjacency -----------------------------------------------------------------------------
