@@ -235,16 +235,23 @@ int vbd_batch_step(VbdSolver* const* solvers, int32_t count, float* const* q_in,
  * stream capture, host callbacks or real-time loops where an allocation could block or
  * synchronize the device, and embedders whose device memory belongs to a framework allocator --
  * and therefore cannot create a VbdSolver.  The step's scratch lives in a static device array of
- * the library sized for at most 16384 particles (about 1.3 MiB, held on every GPU that loads the
+ * the library sized for at most 16384 particles (about 5.3 MiB, held on every GPU that loads the
  * library until the process exits); larger models are rejected with VBD_ERR_INVALID_ARGUMENT.
- * Allocates nothing and takes no solver: same arrays, aliasing and results as vbd_step with
- * lanes_per_vertex 4, block_size 128 and 4 contacts per vertex.  The first call on a device looks
- * up the array's device address; make that first call before any stream capture.  Every call
- * shares the one array (it clears the parts that must start at zero), so calls that overlap on
- * the GPU -- concurrent streams or threads -- race; serialize them. */
+ * Allocates nothing and takes no solver: same arrays, aliasing and bit-identical results as
+ * vbd_step of a solver with the default options (lanes_per_vertex 4, block_size 128, 4 contacts
+ * per vertex, no self-contact, no warm start).  Call it with the model's device current (another
+ * current device is rejected).  The first call on a device looks up the array's device address;
+ * make that first call before any stream capture.  Every call shares the one array (it clears
+ * the parts that must start at zero), so calls that overlap on the GPU -- concurrent streams or
+ * threads -- race; serialize them. */
 int vbd_step_static(const VbdModel* model, float* q_in, const float* qd_in, const float* f_ext, float* q_out,
                     float* qd_out, const VbdContacts* contacts, float dt, int32_t iterations,
                     float friction_epsilon, void* stream);
+/* Diagnostics of the last vbd_step_static on the current device (the counters vbd_status reports
+ * for vbd_step: non-finite updates, singular blocks, contacts beyond 4 per vertex, timeouts;
+ * `steps` and `self_contact_overflow` are 0).  Copies from the static array without allocating;
+ * synchronize the stream of the step first.  The next vbd_step_static clears the counters. */
+int vbd_step_static_status(VbdStatus* out);
 
 /* Staged pieces of vbd_step, for parity tests against a staged oracle. */
 int vbd_forward(VbdSolver* solver, const float* q_in, const float* qd_in, const float* f_ext,

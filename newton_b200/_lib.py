@@ -153,6 +153,7 @@ SIGNATURES = {
         ctypes.c_int,
         [_VP, _VP, _VP, _VP, _VP, _VP, ctypes.POINTER(VbdContacts), ctypes.c_float, ctypes.c_int32, ctypes.c_float, _VP],
     ),
+    "vbd_step_static_status": (ctypes.c_int, [ctypes.POINTER(VbdStatus)]),
     "vbd_forward": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.POINTER(VbdContacts), ctypes.c_float, _VP]),
     "vbd_sweep_color": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(VbdContacts), ctypes.c_float, _VP]),
     "vbd_begin_iteration": (ctypes.c_int, [_VP, ctypes.c_int32, _VP]),

@@ -8,8 +8,8 @@
 // step: its owned vertices and their halo (every vertex any owned vertex's elements touch), the
 // triangles and hinges of its owned vertices (deduplicated, 16-bit local vertex ids), and each
 // owned vertex's list of (element, slot) references in the reference's CSR order.  The static
-// part is one contiguous image per patch, copied with a TMA bulk copy (cp.async.bulk, no
-// multicast) at kernel start.
+// part is one contiguous image per patch, brought into shared memory by one bulk asynchronous
+// copy per CTA (cp.async.bulk, global to shared, this CTA only) at kernel start.
 //
 // Ordering without a grid barrier.  Step t = iteration * C + color.  A patch starts step t only
 // after every neighbour patch (owner of one of its halo vertices; the relation is symmetric) has

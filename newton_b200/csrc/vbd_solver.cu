@@ -1627,10 +1627,10 @@ extern "C" const char* vbd_version(void) { return "vbd_b200 0.2 (sm_100a)"; }
 // device memory is owned by a framework allocator that forbids raw cudaMalloc (an ML framework's
 // custom-call / FFI handler, for instance).  vbd_solver_create allocates the step's scratch, so
 // those callers cannot create a VbdSolver.  vbd_step_static runs the same step without a solver:
-// its scratch (Gauss-Seidel iterate, step-start positions, inertia targets, displacements and the
-// per-vertex contact table) lives in the file-scope device array below, sized for at most
-// kStaticMaxParticles particles (~1.3 MiB, held by every GPU that loads the library until the
-// process exits).
+// its scratch (Gauss-Seidel iterate, step-start positions, inertia targets, displacements, the
+// per-vertex contact slots and the packed contact table) lives in the file-scope device array
+// below, sized for at most kStaticMaxParticles particles (~5.3 MiB, held by every GPU that loads
+// the library until the process exits).
 // ---------------------------------------------------------------------------------------------
 namespace vbd {
 namespace {
@@ -1640,8 +1640,13 @@ constexpr int kStaticContactsPerVertex = 4;
 constexpr size_t kStaticVec4Bytes = static_cast<size_t>(kStaticMaxParticles) * sizeof(float4);
 constexpr size_t kStaticCountBytes = static_cast<size_t>(kStaticMaxParticles) * sizeof(int);
 constexpr size_t kStaticSlotBytes = static_cast<size_t>(kStaticMaxParticles) * kStaticContactsPerVertex * sizeof(int);
+constexpr size_t kStaticTableBytes = static_cast<size_t>(kStaticMaxParticles) * kStaticContactsPerVertex * 4 * sizeof(float4);
 constexpr size_t kStaticStatusBytes = 256;
-constexpr size_t kStaticScratchBytes = 4 * kStaticVec4Bytes + kStaticCountBytes + kStaticSlotBytes + kStaticStatusBytes;
+constexpr size_t kStaticScratchBytes =
+    4 * kStaticVec4Bytes + kStaticCountBytes + kStaticSlotBytes + kStaticTableBytes + kStaticStatusBytes;
+constexpr size_t kStaticTableOffset = 4 * kStaticVec4Bytes + kStaticCountBytes + kStaticSlotBytes;
+constexpr size_t kStaticStatusOffset = kStaticTableOffset + kStaticTableBytes;
+static_assert(kStaticTableOffset % 16 == 0 && kStaticStatusOffset % 16 == 0, "16-byte aligned sections");
 
 static __device__ __align__(256) unsigned char g_step_scratch[kStaticScratchBytes];
 
@@ -1650,10 +1655,12 @@ std::mutex g_static_mutex;
 unsigned char* g_static_scratch_ptr[kStaticMaxDevices] = {};
 
 // Device address of g_step_scratch on the current device (host code cannot use the symbol's
-// name as an address).  Looked up once per device, on that device's first call.
-int static_scratch(unsigned char** out) {
+// name as an address).  Looked up once per device, on that device's first call.  `dev_out`
+// receives the current device ordinal.
+int static_scratch(unsigned char** out, int* dev_out) {
     int dev = 0;
     VBD_CUDA_TRY(cudaGetDevice(&dev));
+    *dev_out = dev;
     if (dev < 0 || dev >= kStaticMaxDevices) return fail(VBD_ERR_UNSUPPORTED, "vbd_step_static: device ordinal too large");
     std::lock_guard<std::mutex> lock(g_static_mutex);
     if (!g_static_scratch_ptr[dev]) {
@@ -1688,8 +1695,13 @@ extern "C" int vbd_step_static(const VbdModel* model, float* q_in, const float* 
     if (iterations < 0) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_step_static: iterations must be >= 0");
     if (contacts && !contacts->soft_contact_count) contacts = nullptr;
     unsigned char* base = nullptr;
-    rc = static_scratch(&base);
+    int dev = -1;
+    rc = static_scratch(&base, &dev);
     if (rc) return rc;
+    if (dev != m.device)
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_step_static: the current device is " + std::to_string(dev) +
+                                                  " but the model lives on device " + std::to_string(m.device) +
+                                                  "; make the model's device current");
     SolverImpl s;  // host-side view of the static scratch; owns nothing
     s.m = &m;
     s.iterations = iterations;
@@ -1704,12 +1716,29 @@ extern "C" int vbd_step_static(const VbdModel* model, float* q_in, const float* 
     s.disp = reinterpret_cast<float4*>(base + 3 * kStaticVec4Bytes);
     s.ccount = reinterpret_cast<int*>(base + 4 * kStaticVec4Bytes);
     s.cslot = reinterpret_cast<int*>(base + 4 * kStaticVec4Bytes + kStaticCountBytes);
-    s.status = reinterpret_cast<unsigned*>(base + 4 * kStaticVec4Bytes + kStaticCountBytes + kStaticSlotBytes);
+    if (m.S > 0) s.ctab = reinterpret_cast<float4*>(base + kStaticTableOffset);
+    s.status = reinterpret_cast<unsigned*>(base + kStaticStatusOffset);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    // the array keeps the previous call's contents: the contact table and counters must start at zero
+    // the array keeps the previous call's contents: the contact slot counts and the status
+    // counters must start at zero (the packed table is rewritten for every slot that is read)
     VBD_CUDA_TRY(cudaMemsetAsync(s.ccount, 0, sizeof(int) * static_cast<size_t>(m.V), st));
     VBD_CUDA_TRY(cudaMemsetAsync(s.status, 0, kStaticStatusBytes, st));
-    enqueue_step(s, q_in, qd_in, f_ext, q_out, qd_out, contacts, dt, iterations, st);
+    rc = enqueue_step(s, q_in, qd_in, f_ext, q_out, qd_out, contacts, dt, iterations, st);
+    if (rc) return rc;
     VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+extern "C" int vbd_step_static_status(VbdStatus* out) {
+    using namespace vbd;
+    if (!out) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_step_static_status: out is NULL");
+    unsigned h[kStatusSlots];
+    // a copy from the symbol: no address lookup and no allocation
+    VBD_CUDA_TRY(cudaMemcpyFromSymbol(h, g_step_scratch, sizeof(h), kStaticStatusOffset, cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof(*out));
+    out->nonfinite_updates = static_cast<int32_t>(h[kNonfinite]);
+    out->singular_blocks = static_cast<int32_t>(h[kSingular]);
+    out->contact_overflow = static_cast<int32_t>(h[kOverflow]);
+    out->timeouts = static_cast<int32_t>(h[kTimeout]);
     return VBD_OK;
 }

@@ -5,7 +5,10 @@
                      plane and sphere collider.  Materials default to the cloth workload:
                      tri_ke = tri_ka = 1e4, tri_kd = 1e-3, edge_ke = 1e-2, edge_kd = 0,
                      density 0.1 kg/m^2, gravity -9.81 m/s^2.
-* ``hanging_cloth``  32 x 32 vertices, 1 m side, two top corners pinned, ground at z = -1.
+* ``hanging_cloth``  32 x 32 vertices, 1 m side, hanging in the XZ plane (top edge at z = 0.05,
+                     bottom edge 5 cm above the ground at z = -1), two top corners pinned; the
+                     1 mm noise is applied normal to the cloth (along y): noise along z would lie
+                     in the plane of a cloth hanging in XZ.
 * ``draped_cloth``   256 x 256 vertices, 2 m side, flat, falling onto a static sphere (r = 0.4 m)
                      and the ground; contact ke = 1e4 (particle and shape side), margin 5 mm.
 * ``cloth_on_boxes`` 1024 x 1024 vertices, 4 m side, 0.8 m above 16 static boxes (seeded yaw and
@@ -28,12 +31,18 @@ CLOTH_MATERIAL = dict(tri_ke=1.0e4, tri_ka=1.0e4, tri_kd=1.0e-3, edge_ke=1.0e-2,
 
 
 def _cloth(builder: ModelBuilder, n: int, side: float, height: float, density: float, particle_radius: float,
-           material: dict, center=(0.0, 0.0)) -> int:
+           material: dict, center=(0.0, 0.0), vertical: bool = False) -> int:
     verts, tris = ModelBuilder.grid_mesh(n - 1, n - 1, side / (n - 1), side / (n - 1))
     start = builder.particle_count
-    builder.add_cloth_mesh(pos=(center[0] - 0.5 * side, center[1] - 0.5 * side, height), rot=(0.0, 0.0, 0.0, 1.0),
-                           scale=1.0, vel=(0.0, 0.0, 0.0), vertices=verts, indices=tris, density=density,
-                           particle_radius=particle_radius, **material)
+    if vertical:
+        # rotation by +90 degrees about x: grid (x, y, 0) -> (x, 0, y); the top edge (largest grid y)
+        # ends at z = height
+        s2 = float(np.sqrt(0.5))
+        pos, rot = (center[0] - 0.5 * side, center[1], height - side), (s2, 0.0, 0.0, s2)
+    else:
+        pos, rot = (center[0] - 0.5 * side, center[1] - 0.5 * side, height), (0.0, 0.0, 0.0, 1.0)
+    builder.add_cloth_mesh(pos=pos, rot=rot, scale=1.0, vel=(0.0, 0.0, 0.0), vertices=verts, indices=tris,
+                           density=density, particle_radius=particle_radius, **material)
     return start
 
 
@@ -47,11 +56,13 @@ def _pin(builder: ModelBuilder, indices) -> None:
 def single_cloth(n: int = 32, side: float = 1.0, seed: int = 0, pin_top_corners: bool = True, ground: float | None = -1.0,
                  sphere: tuple | None = None, height: float = 0.0, particle_radius: float = 5.0e-3,
                  density: float = 0.1, material: dict | None = None, contact_ke: float = 1.0e4,
-                 include_bending: bool = True, z_noise: float = 1.0e-3, device="cuda:0"):
-    """Returns (model, initial particle_q float32 [V,3] with U(-z_noise, z_noise) z-noise)."""
+                 include_bending: bool = True, z_noise: float = 1.0e-3, vertical: bool = False, device="cuda:0"):
+    """Returns (model, initial particle_q float32 [V,3] with U(-z_noise, z_noise) noise normal to the
+    cloth: along z for a horizontal cloth, along y for a ``vertical`` one (XZ plane, top edge at
+    z = ``height``))."""
     material = dict(CLOTH_MATERIAL if material is None else material)
     b = ModelBuilder()
-    start = _cloth(b, n, side, height, density, particle_radius, material)
+    start = _cloth(b, n, side, height, density, particle_radius, material, vertical=vertical)
     if pin_top_corners:
         _pin(b, [start + (n - 1) * n, start + n * n - 1])
     cfg = ModelBuilder.ShapeConfig(ke=contact_ke)
@@ -66,13 +77,15 @@ def single_cloth(n: int = 32, side: float = 1.0, seed: int = 0, pin_top_corners:
     rng = np.random.default_rng(seed)
     q0 = m.particle_q.copy()
     if z_noise > 0:
-        q0[:, 2] += rng.uniform(-z_noise, z_noise, size=m.particle_count).astype(np.float32)
+        q0[:, 1 if vertical else 2] += rng.uniform(-z_noise, z_noise, size=m.particle_count).astype(np.float32)
     return m, q0
 
 
 def hanging_cloth(seed: int = 0, device="cuda:0"):
-    """32 x 32 vertices (1,922 triangles), 1 m side, two top corners pinned, ground at z = -1."""
-    return single_cloth(n=32, side=1.0, seed=seed, pin_top_corners=True, ground=-1.0, device=device)
+    """32 x 32 vertices (1,922 triangles), 1 m side, hanging in the XZ plane from its two pinned top
+    corners (top edge at z = 0.05), ground at z = -1."""
+    return single_cloth(n=32, side=1.0, seed=seed, pin_top_corners=True, ground=-1.0, height=0.05, vertical=True,
+                        device=device)
 
 
 def draped_cloth(n: int = 256, seed: int = 0, device="cuda:0", offset: tuple = (0.0, 0.0), height: float = 1.1):

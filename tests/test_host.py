@@ -177,7 +177,12 @@ def test_cloth_grid_counts_masses_and_rest_data():
     np.testing.assert_allclose(model.edge_rest_angle, 0.0, atol=1e-7)  # flat rest shape
     interior = (model.edge_indices[:, 0] >= 0) & (model.edge_indices[:, 1] >= 0)
     assert interior.sum() == 2945 - 4 * 31
-    assert np.abs(q0[:, 2] - model.particle_q[:, 2]).max() <= 1e-3
+    # hanging in the XZ plane from the two top corners, noise only normal to the cloth (y)
+    np.testing.assert_allclose(model.particle_q[:, 1], 0.0, atol=1e-7)
+    assert abs(model.particle_q[:, 2].max() - 0.05) < 1e-6 and abs(model.particle_q[:, 2].min() + 0.95) < 1e-6
+    np.testing.assert_allclose(model.particle_q[pinned, 2], 0.05, atol=1e-6)
+    assert np.abs(q0[:, 1]).max() <= 1e-3 and np.abs(q0[:, 1]).max() > 0
+    np.testing.assert_array_equal(q0[:, [0, 2]], model.particle_q[:, [0, 2]])
     # DmInv maps the rest edges to the 2D rest frame: D * DmInv = I
     t = model.tri_indices[0]
     x = model.particle_q[t].astype(np.float64)

@@ -5,7 +5,9 @@ host callbacks or real-time loops where an allocation could block or synchronize
 embedders whose device memory belongs to a framework allocator): it runs the step with scratch
 from a static device array instead of a VbdSolver's allocations.  This test calls it through the
 C ABI twice in a row and compares each result with the solver entry point (vbd_step) on the same
-inputs.  The file is named so that pytest collects it last.
+inputs: within the parity tolerance, and bit for bit (both read the same packed contact table).
+It also checks that the calls after the first leave the device memory in use unchanged.  The
+file is named so that pytest collects it last.
 """
 
 import ctypes
@@ -56,6 +58,13 @@ def test_static_step_matches_solver_step_twice():
     b0, b1 = model.state(), model.state()
     b0.particle_q.copy_(torch.from_numpy(q0).to(dev))
     cb = pipe.contacts()
+    # a warm-up call on scratch states: the first call on a device looks up the array's address
+    w0, w1 = model.state(), model.state()
+    pipe.collide(w0, cb)
+    _static_step(model, w0, w1, cb, 1)
+    torch.cuda.synchronize()
+    reserved = torch.cuda.memory_reserved(dev)
+    free0 = torch.cuda.mem_get_info(dev)[0]
     for k in range(2):
         pipe.collide(b0, cb)
         _static_step(model, b0, b1, cb, 10)
@@ -64,8 +73,16 @@ def test_static_step_matches_solver_step_twice():
         assert cb.count() > 0
         assert np.abs(q - ref[k][0]).max() <= TOL
         assert np.abs(qd - ref[k][1]).max() <= TOL / DT
+        assert np.array_equal(q, ref[k][0]) and np.array_equal(qd, ref[k][1])
         assert np.array_equal(qin, q)  # state_in.particle_q holds the solved positions, as in vbd_step
+        status = _lib.VbdStatus()
+        _lib.check(_lib.load().vbd_step_static_status(ctypes.byref(status)))
+        assert status.nonfinite_updates == 0 and status.singular_blocks == 0 and status.contact_overflow == 0
         b0, b1 = b1, b0
+    # nothing was allocated by the two calls: torch's pool and the device's free memory are unchanged
+    # (the free-memory check allows the driver's 2 MiB page granularity for unrelated bookkeeping)
+    assert torch.cuda.memory_reserved(dev) == reserved
+    assert torch.cuda.mem_get_info(dev)[0] >= free0 - (2 << 20)
 
 
 def test_static_step_rejects_models_beyond_its_scratch():
