@@ -181,6 +181,20 @@ typedef struct VbdStatus {
     int32_t reserved;
 } VbdStatus;
 
+/* Statistics of residual-gated steps (vbd_set_residual_gate), since the gate was first enabled
+ * or last reset.  Residuals are in the gate's norm (max or mean of |f_i| / (m_i |g|)). */
+typedef struct VbdGateStats {
+    int64_t steps;                  /* gated steps finished */
+    int64_t iterations;             /* iterations summed over those steps */
+    int64_t capped_steps;           /* steps that stopped at max_iterations above the tolerance */
+    int32_t last_iterations;        /* iterations of the last step */
+    int32_t body_kernels;           /* kernel launches of one loop round (last capture; -1 unknown) */
+    float last_residual;            /* final residual norm of the last step */
+    float last_start_residual;      /* residual where the last step's iterations started */
+    float last_reference_residual;  /* relative mode: residual at the inertia target y */
+    float reserved;
+} VbdGateStats;
+
 typedef struct VbdModel VbdModel;
 typedef struct VbdSolver VbdSolver;
 
@@ -252,6 +266,29 @@ int vbd_step_static(const VbdModel* model, float* q_in, const float* qd_in, cons
  * `steps` and `self_contact_overflow` are 0).  Copies from the static array without allocating;
  * synchronize the stream of the step first.  The next vbd_step_static clears the counters. */
 int vbd_step_static_status(VbdStatus* out);
+
+/* Residual-gated iteration count (no counterpart in the reference, whose step runs the fixed
+ * `for iter_num in range(self.iterations)` loop of solver_vbd.py:1817-1819).  With tolerance > 0,
+ * vbd_step evaluates the Jacobi force residual r_i = |f_i| / (m_i |g|) of every solved vertex at
+ * the iterate the iterations start from and after every `check_every` iterations (the same
+ * evaluation as vbd_residual: inertia + elastic + contact force at the current positions), and
+ * keeps iterating while the residual norm exceeds the tolerance and fewer than max_iterations (at
+ * most 100000) have run.  The norm is max_i r_i, or with VBD_GATE_MEAN the mean of r_i over the
+ * solved vertices (summed in fixed point, 1/256 m|g| resolution, so the sum is deterministic).
+ * VBD_GATE_RELATIVE makes the tolerance relative to the norm at the inertia target y, the plain
+ * start (also with a warm start, so that both starts are held to the same absolute residual).  The
+ * loop runs on the device as a conditional (while) node of the step's CUDA graph: no host round
+ * trip; a gated vbd_step always runs from a graph (use_graph is implied), and inside a caller's
+ * stream capture it adds the loop to the caller's graph.  tolerance <= 0 turns the gate off (the
+ * vbd_step `iterations` argument applies again); while it is on, `iterations` is ignored.  Not
+ * available with self-contact (VBD_ERR_UNSUPPORTED).  The iteration count of each step is
+ * reported by vbd_gate_stats. */
+#define VBD_GATE_RELATIVE 1
+#define VBD_GATE_MEAN 2
+int vbd_set_residual_gate(VbdSolver* solver, float tolerance, int32_t max_iterations, int32_t check_every,
+                          int32_t mode);
+/* Gate statistics (synchronizes the device); reset != 0 zeroes the step / iteration sums. */
+int vbd_gate_stats(VbdSolver* solver, VbdGateStats* out, int32_t reset);
 
 /* Staged pieces of vbd_step, for parity tests against a staged oracle. */
 int vbd_forward(VbdSolver* solver, const float* q_in, const float* qd_in, const float* f_ext,

@@ -129,6 +129,20 @@ class VbdStatus(ctypes.Structure):
     ]
 
 
+class VbdGateStats(ctypes.Structure):
+    _fields_ = [
+        ("steps", ctypes.c_int64),
+        ("iterations", ctypes.c_int64),
+        ("capped_steps", ctypes.c_int64),
+        ("last_iterations", ctypes.c_int32),
+        ("body_kernels", ctypes.c_int32),
+        ("last_residual", ctypes.c_float),
+        ("last_start_residual", ctypes.c_float),
+        ("last_reference_residual", ctypes.c_float),
+        ("reserved", ctypes.c_float),
+    ]
+
+
 # (name, restype, argtypes) of every exported entry point declared in include/vbd_b200.h
 _VP = ctypes.c_void_p
 SIGNATURES = {
@@ -179,6 +193,8 @@ SIGNATURES = {
     "vbd_set_warm_start": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, ctypes.c_int32]),
     "vbd_residual": (ctypes.c_int, [_VP, ctypes.POINTER(VbdContacts), ctypes.c_float, _VP, _VP, _VP]),
     "vbd_status": (ctypes.c_int, [_VP, ctypes.POINTER(VbdStatus), ctypes.c_int32]),
+    "vbd_set_residual_gate": (ctypes.c_int, [_VP, ctypes.c_float, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+    "vbd_gate_stats": (ctypes.c_int, [_VP, ctypes.POINTER(VbdGateStats), ctypes.c_int32]),
     "vbd_solver_info": (ctypes.c_int, [_VP, c_int32_p, c_int32_p, c_int32_p]),
     "vbd_set_launch": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),
     "vbd_solver_step_kernel": (ctypes.c_int, [_VP, c_int32_p, c_int32_p, c_int32_p]),

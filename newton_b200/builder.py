@@ -548,6 +548,10 @@ class ModelBuilder:
             other = [(size, [(g, off + start) for g, off in chunks]) for size, chunks in builder._color_plan]
             self._color_plan = combine_independent_coloring_plan(self._color_plan, other)
 
+    def add_world(self, builder: "ModelBuilder") -> None:
+        """``ModelBuilder.add_world`` (``builder.py:4016``): append ``builder`` as a new world."""
+        self.add_builder(builder, world=None)
+
     # ---------------------------------------------------------------- finalize
     def finalize(self, device="cuda:0", requires_grad: bool = False) -> Model:
         p = self._flush_particles()

@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -30,6 +31,23 @@
 namespace vbd {
 
 enum StatusSlot { kNonfinite = 0, kSingular = 1, kOverflow = 2, kTimeout = 3, kStatusSlots = 4 };
+
+constexpr int kGateMaxIterations = 100000;  // upper bound of a gated step's iteration cap
+
+// Device-side state of the residual gate (vbd_set_residual_gate), one per solver.
+struct GateState {
+    unsigned long long resid_sum;  // fixed-point sum of the current evaluation's residuals
+    unsigned resid_cnt;      // vertices in that sum
+    unsigned resid_bits;     // max residual of the current evaluation (float bits; atomicMax target)
+    float ref;               // relative mode: max residual at the inertia target y of this step
+    int iters;               // iterations run so far in this step
+    int last_iters;          // iterations of the last finished step
+    float last_resid;        // final max residual of the last finished step
+    float start_resid;       // max residual where the last step's iterations started
+    unsigned long long steps;     // gated steps finished (since creation or the last reset)
+    unsigned long long iter_sum;  // iterations summed over those steps
+    unsigned long long capped;    // steps that stopped at the iteration cap above the tolerance
+};
 
 struct GraphEntry {
     float* q_in;
@@ -83,6 +101,16 @@ struct SolverImpl {
     float* ws_work = nullptr;        // [V][70] features, prediction, displacement
     // particle self-contact (particle_enable_self_contact)
     SelfContact sc;
+    // residual gate (vbd_set_residual_gate): iterate until max_i |f_i| / (m_i |g|) <= tolerance
+    float gate_tol = 0.f;            // <= 0: off (fixed iteration count)
+    int gate_max = 0;                // iteration cap
+    int gate_every = 1;              // iterations between residual checks
+    int gate_relative = 0;           // 1: tolerance relative to the residual at the inertia target y
+    int gate_mean = 0;               // 1: mean residual over the solved vertices instead of the max
+    GateState* gate = nullptr;       // device
+    cudaStream_t body_stream = nullptr;  // capture stream of the gate's loop body
+    int gate_body_kernels = -1;      // kernel nodes of one loop body (last capture)
+    bool pdl = true;                 // programmatic dependent launch of the sweeps
 };
 
 }  // namespace vbd
@@ -248,8 +276,11 @@ struct SweepArgs {
     int prefetch_records;    // 1: prefetch the vertices' element records into L2 (first iteration of a step)
     float* resid_out;        // residual mode: per-vertex residual (original order) or NULL
     float* resid_max;        // residual mode: max residual (float bits, atomicMax)
+    unsigned long long* resid_sum;  // residual mode: sum of the residuals, fixed point (resid_fixed)
+    unsigned* resid_cnt;     // residual mode: number of residuals summed
     const int* perm;
     float inv_g;             // 1/|g| (0 when g = 0)
+    int no_pdl;              // host side: launch without the programmatic-dependent-launch attribute
 };
 
 template <bool kDamp>
@@ -402,6 +433,71 @@ __device__ __forceinline__ float warp_sum(float v, int L) {
     return v;
 }
 
+// Contacts (packed table or records), self-contact, and inertia added to a vertex's summed
+// elastic force / Hessian, in the reference's order: elastic + inertia + contact
+// (solve_elasticity_tile, particle_vbd_kernels.py:2546-2565).
+__device__ __forceinline__ void add_vertex_terms(const SweepArgs& a, int i, float4 pi, float4 pv, float3 x, float4 yv,
+                                                 float3& f, Sym3& h) {
+    const float mass = yv.w;
+    float3 fc = f3(0.f, 0.f, 0.f);
+    Sym3 hc = zero_sym();
+    if (a.ctab) {
+        // the step's packed contacts, already in record order
+        const int nc = min(a.ccount[i], a.K);
+        const float4* e = a.ctab + static_cast<size_t>(i) * a.K * 4;
+        for (int k = 0; k < nc; ++k, e += 4) {
+            const float4 e0 = e[0], e1 = e[1], e2 = e[2], e3 = e[3];
+            contact_eval(x, xyz(pv), xyz(e0), xyz(e1), xyz(e2), pi.z, make_float4(e0.w, e1.w, e2.w, e3.x), a.dt,
+                         a.eps_u, fc, hc);
+        }
+    } else if (a.ccount) {
+        accumulate_contacts(a, i, x, xyz(pv), pi.z, fc, hc);
+    }
+    if (a.sc_f) {
+        const float4 s0 = a.sc_f[i], s1 = a.sc_h0[i], s2 = a.sc_h1[i];
+        fc = fc + xyz(s0);
+        hc.xx += s1.x;
+        hc.xy += s1.y;
+        hc.xz += s1.z;
+        hc.yy += s1.w;
+        hc.yz += s2.x;
+        hc.zz += s2.y;
+    }
+    // h_total = h_elastic + m/dt^2 I + h_contact ; f_total = f_elastic + m (y - x)/dt^2 + f_contact
+    add_diag(h, mass * a.dt_sqr_recip);
+    add(h, hc);
+    const float3 fi = (mass * (xyz(yv) - x)) * a.dt_sqr_recip;
+    f = f + fi + fc;
+}
+
+// Fixed-point scale of the residual sums (units of m|g|): r is rounded to 1/256 and clamped at
+// kResidSumClamp, so 2^64 holds the sum of ~7e7 clamped residuals
+constexpr float kResidSumScale = 256.0f;
+constexpr float kResidSumClamp = 1.0e9f;
+
+__device__ __forceinline__ unsigned long long resid_fixed(float r) {
+    // NaN and values beyond the clamp count as the clamp
+    const float c = (r <= kResidSumClamp) ? r : kResidSumClamp;
+    return static_cast<unsigned long long>(c * kResidSumScale + 0.5f);
+}
+
+// Warp-collective: every thread of the warp calls it (r = 0 and counted = false where the thread
+// holds no vertex).  Max (float bits as unsigned: exact for r >= 0; NaN bits exceed +inf), fixed-
+// point sum and count go to the accumulators with one atomic each per warp.
+__device__ __forceinline__ void reduce_residual(const SweepArgs& a, float r, bool counted) {
+    const unsigned full = 0xffffffffu;
+    const unsigned mx = __reduce_max_sync(full, __float_as_uint(r));
+    const unsigned cnt = __popc(__ballot_sync(full, counted));
+    unsigned long long sum = counted ? resid_fixed(r) : 0ull;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(full, sum, off);
+    if ((threadIdx.x & 31) == 0 && cnt) {
+        if (a.resid_max) atomicMax(reinterpret_cast<unsigned*>(a.resid_max), mx);
+        if (a.resid_sum) atomicAdd(a.resid_sum, sum);
+        if (a.resid_cnt) atomicAdd(a.resid_cnt, cnt);
+    }
+}
+
 // One Gauss-Seidel color (kResidual = false) or a Jacobi residual evaluation over a vertex range
 // (kResidual = true).  L lanes cooperate on one vertex: each lane takes every L-th element record
 // (triangles, then hinges, as the reference's 16-thread tile does), then the partial force and
@@ -471,56 +567,32 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
         h.yz = warp_sum(h.yz, L);
         h.zz = warp_sum(h.zz, L);
     }
+    if (kResidual) {
+        // Jacobi residual: lane 0 of each vertex forms r_i, then the warp reduces max, sum and
+        // count before one atomic per warp (fixed shuffle tree + integer atomics: deterministic)
+        float r = 0.0f;
+        bool counted = false;
+        if (valid && lane == 0) {
+            if (solve) {
+                const float4 pv = a.prev[i];
+                const float4 yv = a.y[i];
+                add_vertex_terms(a, i, pi, pv, xyz(a.pos[i]), yv, f, h);
+                r = length(f) / yv.w * a.inv_g;
+                counted = true;
+            }
+            if (a.resid_out) a.resid_out[a.perm[i]] = r;
+        }
+        reduce_residual(a, r, counted);
+        return;
+    }
     if (!valid || lane != 0) return;
     const float4 pv = a.prev[i];
     if (!solve) {
-        if (kResidual) {
-            if (a.resid_out) a.resid_out[a.perm[i]] = 0.0f;
-        } else {
-            a.disp[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (a.write_pos) a.pos[i] = pv;
-        }
+        a.disp[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (a.write_pos) a.pos[i] = pv;
         return;
     }
-    const float4 xv = a.pos[i];
-    const float3 x = xyz(xv);
-    const float4 yv = a.y[i];
-    const float mass = yv.w;
-    float3 fc = f3(0.f, 0.f, 0.f);
-    Sym3 hc = zero_sym();
-    if (a.ctab) {
-        // the step's packed contacts, already in record order
-        const int nc = min(a.ccount[i], a.K);
-        const float4* e = a.ctab + static_cast<size_t>(i) * a.K * 4;
-        for (int k = 0; k < nc; ++k, e += 4) {
-            const float4 e0 = e[0], e1 = e[1], e2 = e[2], e3 = e[3];
-            contact_eval(x, xyz(pv), xyz(e0), xyz(e1), xyz(e2), pi.z, make_float4(e0.w, e1.w, e2.w, e3.x), a.dt,
-                         a.eps_u, fc, hc);
-        }
-    } else if (a.ccount) {
-        accumulate_contacts(a, i, x, xyz(pv), pi.z, fc, hc);
-    }
-    if (a.sc_f) {
-        const float4 s0 = a.sc_f[i], s1 = a.sc_h0[i], s2 = a.sc_h1[i];
-        fc = fc + xyz(s0);
-        hc.xx += s1.x;
-        hc.xy += s1.y;
-        hc.xz += s1.z;
-        hc.yy += s1.w;
-        hc.yz += s2.x;
-        hc.zz += s2.y;
-    }
-    // h_total = h_elastic + m/dt^2 I + h_contact ; f_total = f_elastic + m (y - x)/dt^2 + f_contact
-    add_diag(h, mass * a.dt_sqr_recip);
-    add(h, hc);
-    const float3 fi = (mass * (xyz(yv) - x)) * a.dt_sqr_recip;
-    f = f + fi + fc;
-    if (kResidual) {
-        const float r = length(f) / mass * a.inv_g;
-        if (a.resid_out) a.resid_out[a.perm[i]] = r;
-        if (a.resid_max) atomicMax(reinterpret_cast<int*>(a.resid_max), __float_as_int(r));
-        return;
-    }
+    add_vertex_terms(a, i, pi, pv, xyz(a.pos[i]), a.y[i], f, h);
     float3 dx;
     float4 d = a.disp[i];
     if (solve3(h, f, dx)) {
@@ -686,7 +758,10 @@ __global__ void __launch_bounds__(TB) tile_kernel(SweepArgs a) {
     if (kResidual) {
         const float r = length(f) / pi.x * a.inv_g;
         if (a.resid_out) a.resid_out[a.perm[i]] = r;
-        if (a.resid_max) atomicMax(reinterpret_cast<int*>(a.resid_max), __float_as_int(r));
+        // one vertex per thread here: plain per-vertex atomics (integer, so still deterministic)
+        if (a.resid_max) atomicMax(reinterpret_cast<unsigned*>(a.resid_max), __float_as_uint(r));
+        if (a.resid_sum) atomicAdd(a.resid_sum, resid_fixed(r));
+        if (a.resid_cnt) atomicAdd(a.resid_cnt, 1u);
         return;
     }
     float3 dx;
@@ -789,6 +864,51 @@ __global__ void gather_positions_kernel(const int* perm, const float4* pos, floa
     q[3 * o + 2] = p.z;
 }
 
+// the gate's residual norm of the current evaluation: the max or the mean over the solved vertices
+__device__ __forceinline__ float gate_value(const GateState* g, int mean) {
+    if (!mean) return __uint_as_float(g->resid_bits);
+    if (g->resid_cnt == 0u) return 0.0f;
+    return static_cast<float>(static_cast<double>(g->resid_sum) / kResidSumScale / static_cast<double>(g->resid_cnt));
+}
+
+// Residual gate: after an evaluation of the Jacobi residual (a kResidual sweep over every solved
+// vertex, max_i |f_i| / (m_i |g|) accumulated into g->resid_bits), decide whether the loop runs
+// another round of iterations and set the while node's condition.  `first`: the evaluation at the
+// iterate the iterations start from (no iteration counted yet); `set_ref`: that evaluation is also
+// the relative mode's reference (the plain start y).  `add` iterations ran since the last check.
+__global__ void gate_check_kernel(GateState* g, cudaGraphConditionalHandle handle, float tol, int max_iters,
+                                  int relative, int mean, int first, int set_ref, int add) {
+    const float r = gate_value(g, mean);
+    if (first) {
+        g->iters = 0;
+        g->start_resid = r;
+        if (set_ref) g->ref = r;
+    } else {
+        g->iters += add;
+    }
+    const float thresh = relative ? tol * g->ref : tol;
+    const bool more = (r > thresh) && (g->iters < max_iters);
+    if (!more) {
+        g->last_iters = g->iters;
+        g->last_resid = r;
+        g->steps += 1ull;
+        g->iter_sum += static_cast<unsigned long long>(g->iters);
+        if (r > thresh) g->capped += 1ull;
+    }
+    g->resid_bits = 0u;
+    g->resid_sum = 0ull;
+    g->resid_cnt = 0u;
+    cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
+// relative mode with a warm start: the residual at the plain start y becomes the reference
+__global__ void gate_ref_kernel(GateState* g, int mean) {
+    g->ref = gate_value(g, mean);
+    g->resid_bits = 0u;
+    g->resid_sum = 0ull;
+    g->resid_cnt = 0u;
+}
+
 // ---------------------------------------------------------------------------------------------
 // host orchestration
 // ---------------------------------------------------------------------------------------------
@@ -833,6 +953,7 @@ static SweepArgs make_sweep_args(const SolverImpl& s, const VbdContacts* c, floa
     }
     a.perm = m.perm;
     a.inv_g = m.gravity_norm > 0.f ? 1.0f / m.gravity_norm : 0.f;
+    a.no_pdl = s.pdl ? 0 : 1;
     return a;
 }
 
@@ -867,7 +988,7 @@ static void launch_dependent(Kernel kernel, int grid, int block, cudaStream_t st
     attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr.val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = &attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = a.no_pdl ? 0 : 1;
     cudaLaunchKernelEx(&cfg, kernel, a);
 }
 
@@ -1035,6 +1156,77 @@ static int self_contact_start(SolverImpl& s, cudaStream_t st) {
     return rc;
 }
 
+// kernel nodes of a captured graph (memset and other nodes excluded); -1 if it cannot be read
+static int kernel_nodes(cudaGraph_t graph) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(graph, nullptr, &n) != cudaSuccess) return -1;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n > 0 && cudaGraphGetNodes(graph, nodes.data(), &n) != cudaSuccess) return -1;
+    int k = 0;
+    for (size_t j = 0; j < n; ++j) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[j], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+    }
+    return k;
+}
+
+// Jacobi residual of the current iterate into the gate's accumulator
+static void enqueue_gate_residual(SolverImpl& s, const VbdContacts* c, float dt, cudaStream_t st) {
+    const VbdModelImpl& m = *s.m;
+    SweepArgs a = make_sweep_args(s, c, dt);
+    a.v_begin = 0;
+    a.v_end = m.swept;
+    a.resid_out = nullptr;
+    a.resid_max = reinterpret_cast<float*>(&s.gate->resid_bits);
+    a.resid_sum = &s.gate->resid_sum;
+    a.resid_cnt = &s.gate->resid_cnt;
+    launch_sweep(a, s.lanes, m.any_tri_damping || m.any_edge_damping, true, s.block, st);
+}
+
+// The gated iterations of one step, recorded into the graph that `st` is capturing:
+//   residual at the start -> check (sets the condition) -> while (condition) {
+//       gate_every iterations of all colors -> residual -> check }
+// The loop is a conditional WHILE node; its body is captured on the solver's body stream into
+// the node's body graph.  Only valid while `st` is capturing.
+static int enqueue_gated_iterations(SolverImpl& s, const VbdContacts* c, float dt, cudaStream_t st, bool set_ref) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    VBD_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
+    if (cs != cudaStreamCaptureStatusActive || !graph)
+        return fail(VBD_ERR_UNSUPPORTED, "residual-gated step: the stream is not capturing");
+    cudaGraphConditionalHandle handle;
+    VBD_CUDA_TRY(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
+    enqueue_gate_residual(s, c, dt, st);
+    gate_check_kernel<<<1, 1, 0, st>>>(s.gate, handle, s.gate_tol, s.gate_max, s.gate_relative, s.gate_mean, 1,
+                                       set_ref ? 1 : 0, 0);
+    VBD_CUDA_TRY(cudaGetLastError());
+    VBD_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
+    cudaGraphNodeParams params = {cudaGraphNodeTypeConditional};  // the union has no default constructor
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = handle;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    cudaGraphNode_t node;
+    VBD_CUDA_TRY(cudaGraphAddNode(&node, graph, deps, ndeps, &params));
+    cudaGraph_t body = params.conditional.phGraph_out[0];
+    VBD_CUDA_TRY(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    VBD_CUDA_TRY(cudaStreamBeginCaptureToGraph(s.body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < s.gate_every; ++k)
+        for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, s.body_stream, false);
+    enqueue_gate_residual(s, c, dt, s.body_stream);
+    gate_check_kernel<<<1, 1, 0, s.body_stream>>>(s.gate, handle, s.gate_tol, s.gate_max, s.gate_relative,
+                                                 s.gate_mean, 0, 0, s.gate_every);
+    const cudaError_t e1 = cudaGetLastError();
+    cudaGraph_t captured = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(s.body_stream, &captured);
+    if (e1 != cudaSuccess) return cuda_fail(e1, "residual-gated loop body");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture (residual-gated loop body)");
+    s.gate_body_kernels = kernel_nodes(body);
+    return VBD_OK;
+}
+
 static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const float* f_ext, float* q_out,
                         float* qd_out, const VbdContacts* c, float dt, int iterations, cudaStream_t st) {
     enqueue_forward(s, q_in, qd_in, f_ext, c, dt, st);
@@ -1044,19 +1236,33 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
         float* feats = s.ws_work;
         float* pred = feats + static_cast<size_t>(V) * 64;
         float* delta = pred + static_cast<size_t>(V) * 3;
+        const bool gated = s.gate_tol > 0.f;
+        if (gated) {
+            VBD_CUDA_TRY(cudaMemsetAsync(s.gate, 0, offsetof(GateState, ref), st));
+            if (s.gate_relative) {
+                // the relative tolerance refers to the plain start y, before the warm start moves it
+                enqueue_gate_residual(s, c, dt, st);
+                gate_ref_kernel<<<1, 1, 0, st>>>(s.gate, s.gate_mean);
+            }
+        }
         int rc = mlp_features_launch(*s.m, s.prev, s.y, c ? s.ccount : nullptr, s.ws_corr, s.ws_mean, s.ws_inv_std,
                                      feats, st);
         if (!rc) rc = vbd_mlp_forward(s.ws_params, s.ws_w16, feats, V, pred, st);
         if (!rc) rc = mlp_scale_launch(*s.m, pred, delta, st);
         if (rc) return rc;
         warm_start_kernel<<<(V + 255) / 256, 256, 0, st>>>(s.m->perm, s.m->pinfo, s.prev, s.disp, s.pos, delta, V);
-        for (int it = 0; it < s.ws_iterations; ++it)
-            for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st, it == 0);
+        if (gated) {
+            rc = enqueue_gated_iterations(s, c, dt, st, false);
+            if (rc) return rc;
+        } else {
+            for (int it = 0; it < s.ws_iterations; ++it)
+                for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st, it == 0);
+        }
         correction_kernel<<<(V + 255) / 256, 256, 0, st>>>(s.m->perm, s.m->pinfo, s.pos, s.y, s.ws_corr, V);
         enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
         return VBD_OK;
     }
-    if (s.resident_on && s.resident.ready && iterations > 0) {
+    if (s.resident_on && s.resident.ready && iterations > 0 && !(s.gate_tol > 0.f)) {
         const VbdModelImpl& m = *s.m;
         ResidentLaunch L;
         std::memset(&L, 0, sizeof(L));
@@ -1094,24 +1300,17 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
         enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
         return VBD_OK;
     }
+    if (s.gate_tol > 0.f) {
+        VBD_CUDA_TRY(cudaMemsetAsync(s.gate, 0, offsetof(GateState, ref), st));
+        const int rc = enqueue_gated_iterations(s, c, dt, st, true);
+        if (rc) return rc;
+        enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
+        return VBD_OK;
+    }
     for (int it = 0; it < iterations; ++it)
         for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st, it == 0);
     enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
     return VBD_OK;
-}
-
-// kernel nodes of a captured graph (memset and other nodes excluded); -1 if it cannot be read
-static int kernel_nodes(cudaGraph_t graph) {
-    size_t n = 0;
-    if (cudaGraphGetNodes(graph, nullptr, &n) != cudaSuccess) return -1;
-    std::vector<cudaGraphNode_t> nodes(n);
-    if (n > 0 && cudaGraphGetNodes(graph, nodes.data(), &n) != cudaSuccess) return -1;
-    int k = 0;
-    for (size_t j = 0; j < n; ++j) {
-        cudaGraphNodeType t;
-        if (cudaGraphNodeGetType(nodes[j], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
-    }
-    return k;
 }
 
 static void free_solver(SolverImpl& s) {
@@ -1126,6 +1325,10 @@ static void free_solver(SolverImpl& s) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s.capture_stream) cudaStreamDestroy(s.capture_stream);
+    if (s.body_stream) cudaStreamDestroy(s.body_stream);
+    if (s.gate) cudaFree(s.gate);
+    s.gate = nullptr;
+    s.body_stream = nullptr;
     s.pos = s.prev = s.y = s.disp = nullptr;
     s.ccount = s.cslot = nullptr;
     s.ctab = nullptr;
@@ -1270,8 +1473,11 @@ extern "C" int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, cons
     s.steps++;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     VBD_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
-    if (!s.use_graph || cs != cudaStreamCaptureStatusNone) {
-        // plain launches (also the path taken inside a caller's own stream capture)
+    const bool gated = s.gate_tol > 0.f;
+    if ((!s.use_graph && !gated) || cs != cudaStreamCaptureStatusNone) {
+        // plain launches (also the path taken inside a caller's own stream capture, where a
+        // residual-gated step adds its conditional loop to the caller's graph); a gated step
+        // outside a capture always runs from a graph, since its loop is a conditional graph node
         s.last_step_kernels = -1;
         rc = enqueue_step(s, q_in, qd_in, f_ext, q_out, qd_out, contacts, dt, iters, st);
         if (rc) return rc;
@@ -1291,7 +1497,9 @@ extern "C" int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, cons
         }
     }
     // capture the step on the private stream, instantiate, replay on the caller's stream; if the
-    // resident kernel cannot be captured on this driver, fall back to per-color launches
+    // resident kernel cannot be captured on this driver, fall back to per-color launches; if a
+    // gated loop body with programmatic dependent launches does not instantiate, fall back to
+    // plain launches inside the loop
     cudaGraphExec_t exec = nullptr;
     int kernels = -1;
     for (int attempt = 0; attempt < 2 && !exec; ++attempt) {
@@ -1307,12 +1515,17 @@ extern "C" int vbd_step(VbdSolver* solver, float* q_in, const float* qd_in, cons
         if (e3 == cudaSuccess) break;
         exec = nullptr;
         cudaGetLastError();
+        if (gated && s.pdl && !erc) {
+            s.pdl = false;  // retry the gated step without programmatic dependent launch
+            continue;
+        }
         if (!s.resident.ready || !s.resident_on) {
             if (erc) return erc;
             return cuda_fail(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3), "vbd_step graph capture");
         }
         s.resident_on = false;  // retry with one launch per color
     }
+    if (!exec) return fail(VBD_ERR_CUDA, "vbd_step: the step graph could not be instantiated");
     if (s.graphs.size() >= 8) {
         cudaGraphExecDestroy(s.graphs.front().exec);
         s.graphs.erase(s.graphs.begin());
@@ -1543,6 +1756,62 @@ extern "C" int vbd_residual(VbdSolver* solver, const VbdContacts* contacts, floa
     a.resid_max = mx;
     launch_sweep(a, s.lanes, m.any_tri_damping || m.any_edge_damping, true, s.block, st);
     VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+extern "C" int vbd_set_residual_gate(VbdSolver* solver, float tolerance, int32_t max_iterations, int32_t check_every,
+                                     int32_t mode) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_residual_gate: solver is NULL");
+    SolverImpl& s = solver->s;
+    if (!(tolerance > 0.f)) {
+        s.gate_tol = 0.f;  // off: back to the fixed iteration count
+    } else {
+        // the cap bounds the device-side loop: every step ends after at most max_iterations
+        if (max_iterations < 0 || max_iterations > kGateMaxIterations || check_every < 1 || check_every > 64)
+            return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_residual_gate: max_iterations must be in [0, " +
+                                                      std::to_string(kGateMaxIterations) +
+                                                      "] and check_every in [1, 64]");
+        if (s.sc.on) return fail(VBD_ERR_UNSUPPORTED, "vbd_set_residual_gate: not available with self-contact");
+        if (!(s.m->gravity_norm > 0.f))
+            return fail(VBD_ERR_UNSUPPORTED, "vbd_set_residual_gate: the residual is in units of m|g|; gravity is zero");
+        if (!s.gate) {
+            VBD_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&s.gate), sizeof(GateState)));
+            VBD_CUDA_TRY(cudaMemset(s.gate, 0, sizeof(GateState)));
+        }
+        if (!s.body_stream) VBD_CUDA_TRY(cudaStreamCreateWithFlags(&s.body_stream, cudaStreamNonBlocking));
+        s.gate_tol = tolerance;
+        s.gate_max = max_iterations;
+        s.gate_every = check_every;
+        if (mode & ~(VBD_GATE_RELATIVE | VBD_GATE_MEAN))
+            return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_residual_gate: unknown mode bits");
+        s.gate_relative = (mode & VBD_GATE_RELATIVE) ? 1 : 0;
+        s.gate_mean = (mode & VBD_GATE_MEAN) ? 1 : 0;
+    }
+    for (auto& g : s.graphs) cudaGraphExecDestroy(g.exec);  // captured steps change
+    s.graphs.clear();
+    return VBD_OK;
+}
+
+extern "C" int vbd_gate_stats(VbdSolver* solver, VbdGateStats* out, int32_t reset) {
+    if (!solver || !out) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_gate_stats: NULL argument");
+    SolverImpl& s = solver->s;
+    std::memset(out, 0, sizeof(*out));
+    out->body_kernels = s.gate_body_kernels;
+    if (!s.gate) return VBD_OK;
+    GateState g;
+    VBD_CUDA_TRY(cudaDeviceSynchronize());
+    VBD_CUDA_TRY(cudaMemcpy(&g, s.gate, sizeof(g), cudaMemcpyDeviceToHost));
+    out->steps = static_cast<int64_t>(g.steps);
+    out->iterations = static_cast<int64_t>(g.iter_sum);
+    out->capped_steps = static_cast<int64_t>(g.capped);
+    out->last_iterations = g.last_iters;
+    out->last_residual = g.last_resid;
+    out->last_start_residual = g.start_resid;
+    out->last_reference_residual = g.ref;
+    if (reset) {
+        g.steps = g.iter_sum = g.capped = 0ull;
+        VBD_CUDA_TRY(cudaMemcpy(s.gate, &g, sizeof(g), cudaMemcpyHostToDevice));
+    }
     return VBD_OK;
 }
 

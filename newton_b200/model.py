@@ -261,6 +261,28 @@ class Model:
             self._device_model = DeviceModel(self)
         return self._device_model
 
+    def set_gravity(self, gravity, world: int | None = None) -> None:
+        """``Model.set_gravity`` (``model.py:1958-1991``): one vector for every world, a per-world
+        [world_count, 3] array, or one world's vector.  As in the reference, call the solver's
+        ``notify_model_changed(ModelFlags.MODEL_PROPERTIES)`` afterwards when a solver exists (the
+        device copy of the model is rebuilt on its next use either way)."""
+        g = np.asarray(gravity, dtype=np.float32)
+        cur = np.array(np.asarray(self.gravity, dtype=np.float32).reshape(-1, 3))
+        if world is not None:
+            if g.shape != (3,):
+                raise ValueError("Expected single gravity vector (3,) when world is specified")
+            if world < 0 or world >= self.world_count:
+                raise IndexError(f"world {world} out of range [0, {self.world_count})")
+            cur[world] = g
+        elif g.ndim == 1:
+            cur[:] = g
+        else:
+            if len(g) != self.world_count:
+                raise ValueError(f"Expected {self.world_count} gravity vectors, got {len(g)}")
+            cur = g.reshape(-1, 3).copy()
+        self.gravity = cur
+        self._device_model = None
+
     def notify_model_changed(self) -> None:
         """Drop the device copy so the next solver/pipeline use rebuilds it from the host arrays."""
         self._device_model = None

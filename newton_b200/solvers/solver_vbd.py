@@ -122,6 +122,7 @@ class SolverVBD(SolverBase):
                 setattr(opts, list_name, flat.ctypes.data)
         self._opts = opts
         self._warm = None
+        self._gate = None
         self._create()
 
     def _create(self) -> None:
@@ -346,6 +347,40 @@ class SolverVBD(SolverBase):
         _lib.check(self._lib.vbd_set_warm_start(self._handle, _lib.ptr(mlp.params), _lib.ptr(mlp.w16),
                                                 _lib.ptr(mlp.mean), _lib.ptr(mlp.inv_std), int(iterations)))
 
+    def set_residual_gate(self, tolerance: float | None, max_iterations: int = 100, check_every: int = 1,
+                          relative: bool = False, norm: str = "max") -> None:
+        """Residual-gated steps (no reference counterpart; the reference runs a fixed iteration count,
+        ``solver_vbd.py:1817-1819``): each ``step`` iterates until the Jacobi force residual norm --
+        ``max_i |f_i| / (m_i |g|)`` (``norm="max"``) or its mean over the solved vertices
+        (``norm="mean"``) -- is at most ``tolerance`` (relative to the norm at the inertia target
+        when ``relative``), checked every ``check_every`` iterations, at most ``max_iterations``.
+        The loop runs on the device (a conditional node of the step's CUDA graph).
+        ``tolerance=None`` turns the gate off."""
+        if norm not in ("max", "mean"):
+            raise ValueError("norm must be 'max' or 'mean'")
+        self._gate = None if tolerance is None else (float(tolerance), int(max_iterations), int(check_every),
+                                                     bool(relative), norm)
+        tol = 0.0 if tolerance is None else float(tolerance)
+        mode = (1 if relative else 0) | (2 if norm == "mean" else 0)
+        _lib.check(self._lib.vbd_set_residual_gate(self._handle, ctypes.c_float(tol), int(max_iterations),
+                                                   int(check_every), mode))
+
+    def gate_stats(self, reset: bool = False) -> dict:
+        """Iterations and residuals of the gated steps since the gate was enabled (or last reset)."""
+        g = _lib.VbdGateStats()
+        _lib.check(self._lib.vbd_gate_stats(self._handle, ctypes.byref(g), 1 if reset else 0))
+        return {
+            "steps": g.steps,
+            "iterations": g.iterations,
+            "mean_iterations": (g.iterations / g.steps) if g.steps else None,
+            "capped_steps": g.capped_steps,
+            "last_iterations": g.last_iterations,
+            "body_kernels": g.body_kernels,
+            "last_residual": g.last_residual,
+            "last_start_residual": g.last_start_residual,
+            "last_reference_residual": g.last_reference_residual,
+        }
+
     def set_spin_limit(self, spins: int) -> None:
         _lib.check(self._lib.vbd_set_spin_limit(self._handle, int(spins)))
 
@@ -370,6 +405,8 @@ class SolverVBD(SolverBase):
         self._lib.vbd_solver_destroy(old)
         if self._warm is not None:
             self.set_warm_start(self._warm, self._warm_iterations)
+        if getattr(self, "_gate", None) is not None:
+            self.set_residual_gate(*self._gate)
 
     def rebuild_bvh(self, state: State) -> None:
         """``SolverVBD.rebuild_bvh`` (``solver_vbd.py:3239``): the reference rebuilds its self-contact

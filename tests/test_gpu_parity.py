@@ -1,8 +1,11 @@
 """GPU parity of the VBD cloth step against the CPU oracle (FP32 and FP64).
 
 Parity criterion (per step, from identical states): max |x_gpu - x_oracle| <= 1e-5 m after one
-``SolverVBD.step`` with the same inputs; the FP64 re-evaluation of the same step is reported
-alongside.  All calls go through the C-ABI library (``libvbd_b200.so``).
+``SolverVBD.step`` with the same inputs, against the FP32 oracle and against the FP64
+re-evaluation of the same step (both asserted).  Every parity result also states the force
+residual of the GPU's result, max_i |f_i| / (m_i |g|) and its mean, evaluated by the FP64 oracle
+at the GPU positions with the step's inertia targets and contacts.  All calls go through the
+C-ABI library (``libvbd_b200.so``).
 """
 
 import numpy as np
@@ -40,49 +43,66 @@ def _oracle_step(model, orc, q, qd, margin, dt, iterations):
     return orc.step(q, qd, None, dt, iterations)
 
 
+def _residual_of(orc64, q_gpu):
+    """Force residual (max, mean over solvable vertices; units of m|g|) of the GPU's positions,
+    evaluated by the FP64 oracle right after its own step from the same state (same inertia
+    targets, anchors and contacts)."""
+    orc64.set_positions(q_gpu)
+    r = orc64.residual(DT)
+    m = orc64.model
+    solvable = ((m.particle_flags & 1) != 0) & (m.particle_mass != 0)
+    return float(r.max()), float(r[solvable].mean()) if solvable.any() else 0.0
+
+
+def _report(name, err, err64, resid):
+    print(f"{name}: max |dx| vs FP32 oracle {err:.3e} m, vs FP64 {err64:.3e} m; "
+          f"force residual of the GPU result max {resid[0]:.4g} / mean {resid[1]:.4g} m|g|")
+
+
 def _trajectory_parity(model, q0, steps, iterations, margin=5e-3, check_every=1):
     orc32 = oracle.VBDOracle(model, "f32", threads=8)
     orc64 = oracle.VBDOracle(model, "f64", threads=8)
     solver = SolverVBD(model, iterations=iterations)
     pipe = CollisionPipeline(model, soft_contact_margin=margin) if model.shape_count else None
     q, qd = q0.astype(np.float32), np.zeros_like(q0, dtype=np.float32)
-    worst, worst64 = 0.0, 0.0
+    worst, worst64, resid = 0.0, 0.0, (0.0, 0.0)
     for k in range(steps):
-        q_next, qd_next = None, None
         qin_o, q_o, qd_o = _oracle_step(model, orc32, q, qd, margin, DT, iterations)
         if k % check_every == 0:
             qin_g, q_g, qd_g, _ = _gpu_step(model, solver, q, qd, pipe, DT)
             _, q_64, _ = _oracle_step(model, orc64, q, qd, margin, DT, iterations)
             err = float(np.abs(q_g - q_o).max())
             err64 = float(np.abs(q_g - q_64).max())
+            r = _residual_of(orc64, q_g)
+            resid = max(resid, r)
             # aliasing: state_in.particle_q holds the solved positions, like the reference
             assert np.array_equal(qin_g, q_g)
             assert np.abs(qd_g - qd_o).max() <= 2.0 * TOL_STEP / DT
             worst, worst64 = max(worst, err), max(worst64, err64)
             assert err <= TOL_STEP, f"step {k}: max |dx| = {err:.3e} m vs FP32 oracle"
+            assert err64 <= TOL_STEP, f"step {k}: max |dx| = {err64:.3e} m vs FP64 re-evaluation"
+            assert np.isfinite(r[0])
         q, qd = q_o, qd_o
-    return worst, worst64
+    return worst, worst64, resid
 
 
 def test_hanging_cloth_single_step():
     model, q0 = scenes.hanging_cloth(seed=0)
-    worst, worst64 = _trajectory_parity(model, q0, steps=1, iterations=10)
-    print(f"hanging 32x32: max |dx| vs FP32 oracle {worst:.3e} m, vs FP64 {worst64:.3e} m")
+    _report("hanging 32x32, 1 step", *_trajectory_parity(model, q0, steps=1, iterations=10))
 
 
 def test_hanging_cloth_trajectory_per_step():
     """30 substeps (3 frames): every step from the oracle's own state stays within 1e-5 m."""
     model, q0 = scenes.hanging_cloth(seed=1)
-    worst, worst64 = _trajectory_parity(model, q0, steps=30, iterations=10, check_every=3)
-    print(f"hanging 32x32 x30: max |dx| {worst:.3e} m (FP64 {worst64:.3e} m)")
+    _report("hanging 32x32, 30 steps", *_trajectory_parity(model, q0, steps=30, iterations=10, check_every=3))
 
 
 def test_draped_cloth_contacts_per_step():
     """Sphere + ground contacts: cloth released just above the sphere so contacts are active."""
     model, q0 = scenes.single_cloth(n=48, side=1.0, seed=2, pin_top_corners=False, ground=0.0,
                                     sphere=((0.0, 0.0, 0.5), 0.4), height=0.905)
-    worst, worst64 = _trajectory_parity(model, q0, steps=12, iterations=10, check_every=2)
-    print(f"draped 48x48: max |dx| {worst:.3e} m (FP64 {worst64:.3e} m)")
+    _report("draped 48x48 on sphere + ground, 12 steps",
+            *_trajectory_parity(model, q0, steps=12, iterations=10, check_every=2))
 
 
 def test_collide_matches_oracle():
@@ -196,8 +216,7 @@ def test_residual_matches_oracle():
 
 def test_batched_worlds_per_step():
     model, q0 = scenes.batched_worlds(num_worlds=6, seed=8, n_range=(8, 20))
-    worst, _ = _trajectory_parity(model, q0, steps=4, iterations=10, check_every=1)
-    print(f"batched 6 worlds: max |dx| {worst:.3e} m")
+    _report("batched 6 worlds, 4 steps", *_trajectory_parity(model, q0, steps=4, iterations=10, check_every=1))
 
 
 def test_invalid_state_is_rejected():
@@ -301,9 +320,12 @@ def test_full_size_draped_cloth_step_matches_oracle():
     assert contacts.count() > 1000, "the cloth should rest on the sphere"
     orc = oracle.VBDOracle(model, "f32", threads=os.cpu_count() or 1)
     _, q_o, qd_o = _oracle_step(model, orc, q, qd, 5e-3, DT, 10)
+    orc64 = oracle.VBDOracle(model, "f64", threads=os.cpu_count() or 1)
+    _, q_64, _ = _oracle_step(model, orc64, q, qd, 5e-3, DT, 10)
     err = float(np.abs(q_g - q_o).max())
-    print(f"full-size draped cloth, {contacts.count()} contacts: max |dx| GPU vs oracle {err:.3e} m")
-    assert err <= TOL_STEP
+    err64 = float(np.abs(q_g - q_64).max())
+    _report(f"full-size draped cloth 256x256, {contacts.count()} contacts", err, err64, _residual_of(orc64, q_g))
+    assert err <= TOL_STEP and err64 <= TOL_STEP
     assert np.abs(qd_g - qd_o).max() <= 2.0 * TOL_STEP / DT
 
 
@@ -331,7 +353,11 @@ def test_full_size_batched_worlds_step_matches_oracle():
     assert contacts.count() > 10000, "the cloths should lie on their ground planes"
     orc = oracle.VBDOracle(model, "f32", threads=os.cpu_count() or 1)
     _, q_o, _ = _oracle_step(model, orc, q, qd, 5e-3, DT, 10)
+    del orc
+    orc64 = oracle.VBDOracle(model, "f64", threads=os.cpu_count() or 1)
+    _, q_64, _ = _oracle_step(model, orc64, q, qd, 5e-3, DT, 10)
     err = float(np.abs(q_g - q_o).max())
-    print(f"full-size batched worlds ({model.particle_count} vertices, {contacts.count()} contacts): "
-          f"max |dx| GPU vs oracle {err:.3e} m")
-    assert err <= TOL_STEP
+    err64 = float(np.abs(q_g - q_64).max())
+    _report(f"full-size batched worlds ({model.particle_count} vertices, {contacts.count()} contacts)", err, err64,
+            _residual_of(orc64, q_g))
+    assert err <= TOL_STEP and err64 <= TOL_STEP
