@@ -1156,16 +1156,29 @@ static int self_contact_start(SolverImpl& s, cudaStream_t st) {
     return rc;
 }
 
-// kernel nodes of a captured graph (memset and other nodes excluded); -1 if it cannot be read
+// kernel nodes of a captured graph (memset and other nodes excluded); -1 if it cannot be read.
+// The type query of a conditional node fails on this runtime (cudaErrorUnknown) even though the
+// graph instantiates and runs: such nodes are skipped, and the error the failed query leaves in
+// the runtime's last-error slot is cleared so that it is not reported by an unrelated later call.
 static int kernel_nodes(cudaGraph_t graph) {
     size_t n = 0;
-    if (cudaGraphGetNodes(graph, nullptr, &n) != cudaSuccess) return -1;
+    if (cudaGraphGetNodes(graph, nullptr, &n) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
     std::vector<cudaGraphNode_t> nodes(n);
-    if (n > 0 && cudaGraphGetNodes(graph, nodes.data(), &n) != cudaSuccess) return -1;
+    if (n > 0 && cudaGraphGetNodes(graph, nodes.data(), &n) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
     int k = 0;
     for (size_t j = 0; j < n; ++j) {
         cudaGraphNodeType t;
-        if (cudaGraphNodeGetType(nodes[j], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+        if (cudaGraphNodeGetType(nodes[j], &t) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        if (t == cudaGraphNodeTypeKernel) ++k;
     }
     return k;
 }
