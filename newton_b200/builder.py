@@ -386,8 +386,7 @@ class ModelBuilder:
         np.add.at(mass, inds.reshape(-1), np.repeat(density * areas / 3.0, 3))
         end_tri = self.tri_count
         if end_tri > start_tri:
-            local = MeshAdjacency(self.tri_indices[start_tri:end_tri])
-            e = local.edge_indices
+            e = self._edge_table(self.tri_indices[start_tri:end_tri])
             if e.shape[0]:
                 self.add_edges(e[:, 0], e[:, 1], e[:, 2], e[:, 3], edge_ke=edge_ke, edge_kd=edge_kd)
 
@@ -471,7 +470,26 @@ class ModelBuilder:
         xform = ((0.0, 0.0, 0.0), (0.0, 0.0, 0.0, 1.0)) if xform is None else xform
         return self._add_shape(GeoType.BOX, xform, (hx, hy, hz), cfg, body)
 
-    # ---------------------------------------------------------------- coloring
+    # ---------------------------------------------------------------- connectivity and coloring
+    # The four steps below run in the library's native host code (mesh.py, coloring.py).  They are
+    # methods so that a subclass can supply the same tables another way; the model data the rest
+    # of the builder produces does not depend on how.
+    def _edge_table(self, tri_indices) -> np.ndarray:
+        """Bending-edge table ``[o0, o1, v0, v1]`` of one mesh (``utils/mesh.py:465-531``)."""
+        return MeshAdjacency(tri_indices).edge_indices
+
+    def _vertex_adjacency(self, tri_indices, edge_indices, particle_count: int) -> MeshAdjacency:
+        """Per-vertex element CSR of the finalized model (``utils/mesh.py:595-926``)."""
+        return MeshAdjacency(tri_indices, edge_indices).init_vertex_adjacency(particle_count)
+
+    def _conflict_edges(self, tri_indices, tri_mask, bend_indices, bend_mask) -> np.ndarray:
+        """Canonical conflict-graph edges (``graph_coloring.py:99-197``)."""
+        return construct_trimesh_graph_edges(tri_indices, tri_mask, bend_indices, bend_mask)
+
+    def _color_graph(self, num_nodes, edges, balance_colors, target_ratio, algorithm) -> list[np.ndarray]:
+        """Color groups of the conflict graph (``graph_coloring.py:243-311``)."""
+        return color_graph(num_nodes, edges, balance_colors, target_ratio, algorithm)
+
     def set_coloring(self, particle_color_groups) -> None:
         self.particle_color_groups = [np.asarray(g, dtype=np.int32) for g in particle_color_groups]
 
@@ -484,7 +502,7 @@ class ModelBuilder:
             bend = self.edge_indices
             props = self.edge_bending_properties
             bend_mask = (props[:, 0] != 0.0) | (props[:, 1] != 0.0)
-        return construct_trimesh_graph_edges(self.tri_indices if self.tri_count else None, tri_mask, bend, bend_mask)
+        return self._conflict_edges(self.tri_indices if self.tri_count else None, tri_mask, bend, bend_mask)
 
     def color(self, include_bending: bool = False, balance_colors: bool = True, target_max_min_color_ratio: float = 1.1,
               coloring_algorithm: ColoringAlgorithm = ColoringAlgorithm.MCS) -> None:
@@ -493,7 +511,7 @@ class ModelBuilder:
             return
         edges = self.coloring_graph_edges(include_bending)
         if len(edges) > 0:
-            self.particle_color_groups = color_graph(self.particle_count, edges, balance_colors,
+            self.particle_color_groups = self._color_graph(self.particle_count, edges, balance_colors,
                                                      target_max_min_color_ratio, coloring_algorithm)
         else:
             self.particle_color_groups = [np.arange(self.particle_count, dtype=np.int32)]
@@ -582,9 +600,7 @@ class ModelBuilder:
         m.edge_rest_angle = self.edge_rest_angle.astype(np.float32)
         m.edge_rest_length = self.edge_rest_length.astype(np.float32)
         m.edge_bending_properties = self.edge_bending_properties.astype(np.float32).reshape(-1, 2)
-        adj = MeshAdjacency(m.tri_indices, m.edge_indices)
-        adj.init_vertex_adjacency(V)
-        m.soft_mesh_adjacency = adj
+        m.soft_mesh_adjacency = self._vertex_adjacency(m.tri_indices, m.edge_indices, V)
         S = self.shape_count
         m.shape_count = S
         m.shape_type = np.asarray(self.shape_type, dtype=np.int32)

@@ -1,5 +1,8 @@
 """Seeded synthetic cloth scenes with the shapes, sizes and materials of the VBD cloth workloads.
 
+Every scene takes ``builder_cls`` (default ``ModelBuilder``): a subclass that computes the
+connectivity and coloring another way builds the same scene.
+
 * ``single_cloth``   one square cloth, horizontal (XY plane, Z up) with U(-1 mm, 1 mm) z-noise
                      on the initial positions (rest shape flat), optional pinned corners, ground
                      plane and sphere collider.  Materials default to the cloth workload:
@@ -56,12 +59,13 @@ def _pin(builder: ModelBuilder, indices) -> None:
 def single_cloth(n: int = 32, side: float = 1.0, seed: int = 0, pin_top_corners: bool = True, ground: float | None = -1.0,
                  sphere: tuple | None = None, height: float = 0.0, particle_radius: float = 5.0e-3,
                  density: float = 0.1, material: dict | None = None, contact_ke: float = 1.0e4,
-                 include_bending: bool = True, z_noise: float = 1.0e-3, vertical: bool = False, device="cuda:0"):
+                 include_bending: bool = True, z_noise: float = 1.0e-3, vertical: bool = False, device="cuda:0",
+                 builder_cls=ModelBuilder):
     """Returns (model, initial particle_q float32 [V,3] with U(-z_noise, z_noise) noise normal to the
     cloth: along z for a horizontal cloth, along y for a ``vertical`` one (XZ plane, top edge at
     z = ``height``))."""
     material = dict(CLOTH_MATERIAL if material is None else material)
-    b = ModelBuilder()
+    b = builder_cls()
     start = _cloth(b, n, side, height, density, particle_radius, material, vertical=vertical)
     if pin_top_corners:
         _pin(b, [start + (n - 1) * n, start + n * n - 1])
@@ -81,25 +85,27 @@ def single_cloth(n: int = 32, side: float = 1.0, seed: int = 0, pin_top_corners:
     return m, q0
 
 
-def hanging_cloth(seed: int = 0, device="cuda:0"):
+def hanging_cloth(seed: int = 0, device="cuda:0", builder_cls=ModelBuilder):
     """32 x 32 vertices (1,922 triangles), 1 m side, hanging in the XZ plane from its two pinned top
     corners (top edge at z = 0.05), ground at z = -1."""
     return single_cloth(n=32, side=1.0, seed=seed, pin_top_corners=True, ground=-1.0, height=0.05, vertical=True,
-                        device=device)
+                        device=device, builder_cls=builder_cls)
 
 
-def draped_cloth(n: int = 256, seed: int = 0, device="cuda:0", offset: tuple = (0.0, 0.0), height: float = 1.1):
+def draped_cloth(n: int = 256, seed: int = 0, device="cuda:0", offset: tuple = (0.0, 0.0), height: float = 1.1,
+                 builder_cls=ModelBuilder):
     """256 x 256 vertices (130,050 triangles), 2 m side, flat and at rest 0.2 m above a static
     sphere of radius 0.4 m (centre offset by ``offset`` in x, y), and the ground plane."""
     return single_cloth(n=n, side=2.0, seed=seed, pin_top_corners=False, ground=0.0,
-                        sphere=((offset[0], offset[1], 0.5), 0.4), height=height, z_noise=0.0, device=device)
+                        sphere=((offset[0], offset[1], 0.5), 0.4), height=height, z_noise=0.0, device=device,
+                        builder_cls=builder_cls)
 
 
 def cloth_on_boxes(n: int = 1024, side: float = 4.0, boxes: int = 16, seed: int = 0, height: float = 0.8,
-                   device="cuda:0"):
+                   device="cuda:0", builder_cls=ModelBuilder):
     """Large cloth falling onto seeded static boxes on the ground (self-contact workload)."""
     rng = np.random.default_rng(seed)
-    b = ModelBuilder()
+    b = builder_cls()
     _cloth(b, n, side, height, 0.1, 1.0e-3, dict(CLOTH_MATERIAL))
     cfg = ModelBuilder.ShapeConfig(ke=1.0e4)
     b.add_ground_plane(height=0.0, cfg=cfg)
@@ -116,17 +122,18 @@ def cloth_on_boxes(n: int = 1024, side: float = 4.0, boxes: int = 16, seed: int 
     return m, m.particle_q.copy()
 
 
-def batched_worlds(num_worlds: int = 512, seed: int = 0, n_range=(16, 96), device="cuda:0", include_bending=True):
+def batched_worlds(num_worlds: int = 512, seed: int = 0, n_range=(16, 96), device="cuda:0", include_bending=True,
+                   builder_cls=ModelBuilder):
     """Independent cloth worlds of uneven size merged into one model (colors combined per world)."""
     rng = np.random.default_rng(seed)
-    top = ModelBuilder()
+    top = builder_cls()
     for w in range(num_worlds):
         n = int(rng.integers(n_range[0], n_range[1] + 1))
         side = float(rng.uniform(0.5, 2.0))
         ke = float(10.0 ** rng.uniform(3.0, 5.0))
         eke = float(10.0 ** rng.uniform(-3.0, -1.0))
         npin = int(rng.integers(0, 5))
-        b = ModelBuilder()
+        b = builder_cls()
         mat = dict(tri_ke=ke, tri_ka=ke, tri_kd=1.0e-3, edge_ke=eke, edge_kd=0.0)
         _cloth(b, n, side, 0.5, 0.1, 5.0e-3, mat)
         if npin:

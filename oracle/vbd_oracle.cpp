@@ -44,6 +44,8 @@
 #include <cstdint>
 #include <cstring>
 #include <vector>
+#include <tuple>
+#include <queue>
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -1689,4 +1691,132 @@ int oracle_collide(int V, const float* q, const float* radius, const int32_t* fl
     return n;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Model set-up restated for the checker (independent of the library's host code): the bending-
+// edge table and the conflict-graph coloring.  Used by oracle/setup.py to build scenes without the
+// CUDA library (the CPU-baseline leg) and to cross-check the library's set-up tables.
+// ---------------------------------------------------------------------------------------------
+
+// Edge table [o0, o1, v0, v1] of MeshAdjacency._compute_edge_adjacency (utils/mesh.py:465-531),
+// by sorting: every triangle slot (t, k) names the undirected edge {tris[t][k], tris[t][k+1]}
+// with opposite vertex tris[t][k+2]; slots are sorted by (edge key, slot index), each group is one
+// edge whose first slot fills [o0, -1, v0, v1] and whose second fills o1 (later ones are ignored,
+// as the reference does for non-manifold edges); edges are numbered in the order of their first
+// slot.  edges_out holds room for 3 nt rows; returns the edge count.
+int oracle_edge_table(const int32_t* tris, int nt, int32_t* edges_out) {
+    const int64_t ns = 3 * static_cast<int64_t>(nt);
+    std::vector<int64_t> slot(ns);
+    std::vector<uint64_t> key(ns);
+    for (int64_t j = 0; j < ns; ++j) {
+        const int64_t t = j / 3;
+        const int k = static_cast<int>(j % 3);
+        const uint32_t a = static_cast<uint32_t>(tris[3 * t + k]), b = static_cast<uint32_t>(tris[3 * t + (k + 1) % 3]);
+        key[j] = (static_cast<uint64_t>(std::min(a, b)) << 32) | std::max(a, b);
+        slot[j] = j;
+    }
+    std::sort(slot.begin(), slot.end(), [&](int64_t x, int64_t y) { return key[x] != key[y] ? key[x] < key[y] : x < y; });
+    // groups: (first slot, second slot or -1)
+    std::vector<std::pair<int64_t, int64_t>> groups;
+    for (int64_t i = 0; i < ns;) {
+        int64_t j = i + 1;
+        while (j < ns && key[slot[j]] == key[slot[i]]) ++j;
+        groups.push_back({slot[i], j - i > 1 ? slot[i + 1] : -1});
+        i = j;
+    }
+    std::sort(groups.begin(), groups.end());
+    for (size_t e = 0; e < groups.size(); ++e) {
+        const int64_t f = groups[e].first, g = groups[e].second;
+        const int64_t t = f / 3;
+        const int k = static_cast<int>(f % 3);
+        int32_t* row = edges_out + 4 * e;
+        row[0] = tris[3 * t + (k + 2) % 3];
+        row[1] = -1;
+        row[2] = tris[3 * t + k];
+        row[3] = tris[3 * t + (k + 1) % 3];
+        if (g >= 0) row[1] = tris[3 * (g / 3) + (g % 3 + 2) % 3];
+    }
+    return static_cast<int>(groups.size());
+}
+
+// Coloring of a canonical edge list (unique (min, max) pairs in lexicographic order), the
+// algorithm the library states: an ordering, first-fit colors in that order, then balancing.
+//   algorithm 0 (MCS, Pereira & Palsberg 2005): repeatedly take the unvisited vertex with the
+//     most visited neighbours; ties go to the vertex whose count was raised last (initially
+//     vertex 0 first, then 1, 2, ...).  Restated here with a priority queue keyed by (count,
+//     time of the last raise).
+//   algorithm 1 (GREEDY): decreasing degree, ties by index.
+//   balance: while max/min color size > target, move the lowest-index vertices of the largest
+//     color that have no neighbour in the smallest color into it; stop when a pass moves nothing
+//     (or after 64 passes per color).
+// Neighbour lists are in edge-list order.  Returns the number of colors (before balancing).
+int oracle_color_graph(int n, int64_t m, const int32_t* edges, int algorithm, int do_balance, float target,
+                       int32_t* colors) {
+    std::vector<std::vector<int>> nb(n);
+    for (int64_t e = 0; e < m; ++e) {
+        const int a = edges[2 * e], b = edges[2 * e + 1];
+        if (a == b) continue;
+        nb[a].push_back(b);
+        nb[b].push_back(a);
+    }
+    std::vector<int> order;
+    order.reserve(n);
+    if (algorithm == 0) {
+        using Entry = std::tuple<int, int64_t, int>;  // (count, raise time, vertex)
+        std::priority_queue<Entry> pq;
+        std::vector<int> count(n, 0);
+        std::vector<char> done(n, 0);
+        int64_t clock = 0;
+        for (int v = n - 1; v >= 0; --v) pq.emplace(0, clock++, v);
+        while (!pq.empty()) {
+            const auto [c, tm, v] = pq.top();
+            pq.pop();
+            if (done[v] || c != count[v]) continue;
+            done[v] = 1;
+            order.push_back(v);
+            for (int u : nb[v]) {
+                if (done[u]) continue;
+                pq.emplace(++count[u], clock++, u);
+            }
+        }
+    } else {
+        for (int v = 0; v < n; ++v) order.push_back(v);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return nb[a].size() > nb[b].size(); });
+    }
+    std::vector<int> col(n, -1);
+    int nc = 0;
+    for (int v : order) {
+        std::vector<char> used(nb[v].size() + 1, 0);
+        for (int u : nb[v])
+            if (col[u] >= 0 && col[u] <= static_cast<int>(nb[v].size())) used[col[u]] = 1;
+        int c = 0;
+        while (used[c]) ++c;
+        col[v] = c;
+        nc = std::max(nc, c + 1);
+    }
+    if (do_balance && nc >= 2) {
+        std::vector<int64_t> size(nc, 0);
+        for (int v = 0; v < n; ++v) size[col[v]]++;
+        auto ratio_ok = [&](int hi, int lo) { return size[lo] > 0 && double(size[hi]) / double(size[lo]) <= target; };
+        for (int pass = 0; pass < 64 * nc; ++pass) {
+            const int hi = static_cast<int>(std::max_element(size.begin(), size.end()) - size.begin());
+            const int lo = static_cast<int>(std::min_element(size.begin(), size.end()) - size.begin());
+            if (ratio_ok(hi, lo)) break;
+            bool moved = false;
+            for (int v = 0; v < n && size[hi] > size[lo] + 1; ++v) {
+                if (col[v] != hi) continue;
+                if (std::any_of(nb[v].begin(), nb[v].end(), [&](int u) { return col[u] == lo; })) continue;
+                col[v] = lo;
+                size[hi]--;
+                size[lo]++;
+                moved = true;
+                if (ratio_ok(hi, lo)) break;
+            }
+            if (!moved) break;
+        }
+    }
+    for (int v = 0; v < n; ++v) colors[v] = col[v];
+    return nc;
+}
+
 }  // extern "C"
+
