@@ -275,8 +275,14 @@ int vbd_step_static_status(VbdStatus* out);
  * keeps iterating while the residual norm exceeds the tolerance and fewer than max_iterations (at
  * most 100000) have run.  The norm is max_i r_i, or with VBD_GATE_MEAN the mean of r_i over the
  * solved vertices (summed in fixed point, 1/256 m|g| resolution, so the sum is deterministic).
- * VBD_GATE_RELATIVE makes the tolerance relative to the norm at the inertia target y, the plain
- * start (also with a warm start, so that both starts are held to the same absolute residual).  The
+ * VBD_GATE_SWEEP replaces the Jacobi evaluations by the Gauss-Seidel residual the sweeps form
+ * anyway: each vertex's force norm when its color is solved, accumulated by the last iteration
+ * before a check (no extra launch; the first check follows the first iteration, whose residual is
+ * that of the start iterate as each color meets it; at least one iteration runs unless
+ * max_iterations is 0).  VBD_GATE_RELATIVE makes the tolerance relative to the norm at the
+ * inertia target y, the plain start (with a warm start that norm is a Jacobi evaluation at y, so
+ * that both starts are held to the same absolute residual).  The iteration count is a multiple of
+ * check_every (the cap is rounded up to one).  The
  * loop runs on the device as a conditional (while) node of the step's CUDA graph: no host round
  * trip; a gated vbd_step always runs from a graph (use_graph is implied), and inside a caller's
  * stream capture it adds the loop to the caller's graph.  tolerance <= 0 turns the gate off (the
@@ -285,6 +291,7 @@ int vbd_step_static_status(VbdStatus* out);
  * reported by vbd_gate_stats. */
 #define VBD_GATE_RELATIVE 1
 #define VBD_GATE_MEAN 2
+#define VBD_GATE_SWEEP 4
 int vbd_set_residual_gate(VbdSolver* solver, float tolerance, int32_t max_iterations, int32_t check_every,
                           int32_t mode);
 /* Gate statistics (synchronizes the device); reset != 0 zeroes the step / iteration sums. */

@@ -34,16 +34,18 @@ enum StatusSlot { kNonfinite = 0, kSingular = 1, kOverflow = 2, kTimeout = 3, kS
 
 constexpr int kGateMaxIterations = 100000;  // upper bound of a gated step's iteration cap
 
-// Device-side state of the residual gate (vbd_set_residual_gate), one per solver.
+// Device-side state of the residual gate (vbd_set_residual_gate), one per solver.  The head, up
+// to `ref`, is zeroed at the start of every gated step.
 struct GateState {
     unsigned long long resid_sum;  // fixed-point sum of the current evaluation's residuals
     unsigned resid_cnt;      // vertices in that sum
     unsigned resid_bits;     // max residual of the current evaluation (float bits; atomicMax target)
-    float ref;               // relative mode: max residual at the inertia target y of this step
     int iters;               // iterations run so far in this step
+    int pad;
+    float ref;               // relative mode: the step's reference residual
     int last_iters;          // iterations of the last finished step
-    float last_resid;        // final max residual of the last finished step
-    float start_resid;       // max residual where the last step's iterations started
+    float last_resid;        // final residual of the last finished step
+    float start_resid;       // residual where the last step's iterations started
     unsigned long long steps;     // gated steps finished (since creation or the last reset)
     unsigned long long iter_sum;  // iterations summed over those steps
     unsigned long long capped;    // steps that stopped at the iteration cap above the tolerance
@@ -107,6 +109,7 @@ struct SolverImpl {
     int gate_every = 1;              // iterations between residual checks
     int gate_relative = 0;           // 1: tolerance relative to the residual at the inertia target y
     int gate_mean = 0;               // 1: mean residual over the solved vertices instead of the max
+    int gate_sweep = 0;              // 1: the Gauss-Seidel residual the sweeps accumulate (no Jacobi launch)
     GateState* gate = nullptr;       // device
     cudaStream_t body_stream = nullptr;  // capture stream of the gate's loop body
     int gate_body_kernels = -1;      // kernel nodes of one loop body (last capture)
@@ -470,6 +473,25 @@ __device__ __forceinline__ void add_vertex_terms(const SweepArgs& a, int i, floa
     f = f + fi + fc;
 }
 
+// The vertex's Newton step on its 3x3 block: disp += H^-1 f when |det H| > 1e-8 and the result is
+// finite (else counted and skipped, as the reference skips it), then q = prev + disp when the
+// color commits in place (solve_elasticity(_tile) + apply_truncation_ts without self-contact).
+__device__ __forceinline__ void solve_and_commit(const SweepArgs& a, int i, float4 pv, const Sym3& h, float3 f) {
+    float3 dx;
+    float4 d = a.disp[i];
+    if (solve3(h, f, dx)) {
+        if (isfinite(dx.x) && isfinite(dx.y) && isfinite(dx.z)) {
+            d = make_float4(d.x + dx.x, d.y + dx.y, d.z + dx.z, 0.f);
+            a.disp[i] = d;
+        } else {
+            atomicAdd(&a.status[kNonfinite], 1u);
+        }
+    } else {
+        atomicAdd(&a.status[kSingular], 1u);
+    }
+    if (a.write_pos) a.pos[i] = make_float4(pv.x + d.x, pv.y + d.y, pv.z + d.z, 0.f);
+}
+
 // Fixed-point scale of the residual sums (units of m|g|): r is rounded to 1/256 and clamped at
 // kResidSumClamp, so 2^64 holds the sum of ~7e7 clamped residuals
 constexpr float kResidSumScale = 256.0f;
@@ -504,7 +526,7 @@ __device__ __forceinline__ void reduce_residual(const SweepArgs& a, float r, boo
 // Hessian are summed across the L lanes with xor shuffles and lane 0 adds the contacts and solves.
 // kCap: the same kernel limited to 64 registers per thread (4 blocks of 256 per SM), used when the
 // uncapped kernel would need more than one wave of blocks (large colors, many lanes per vertex)
-template <int L, bool kDamp, bool kResidual, bool kCap>
+template <int L, bool kDamp, bool kResidual, bool kCap, bool kGate = false>
 __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = a.v_begin + tid / L;
@@ -585,6 +607,27 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
         reduce_residual(a, r, counted);
         return;
     }
+    if (kGate) {
+        // the same update, and the vertex's force norm before it (the Gauss-Seidel residual of
+        // the sweep) reduced per warp into the residual gate's accumulators
+        float rg = 0.0f;
+        bool counted = false;
+        if (valid && lane == 0) {
+            const float4 pv = a.prev[i];
+            if (!solve) {
+                a.disp[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (a.write_pos) a.pos[i] = pv;
+            } else {
+                const float4 yv = a.y[i];
+                add_vertex_terms(a, i, pi, pv, xyz(a.pos[i]), yv, f, h);
+                rg = length(f) / yv.w * a.inv_g;
+                counted = true;
+                solve_and_commit(a, i, pv, h, f);
+            }
+        }
+        reduce_residual(a, rg, counted);
+        return;
+    }
     if (!valid || lane != 0) return;
     const float4 pv = a.prev[i];
     if (!solve) {
@@ -593,19 +636,7 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
         return;
     }
     add_vertex_terms(a, i, pi, pv, xyz(a.pos[i]), a.y[i], f, h);
-    float3 dx;
-    float4 d = a.disp[i];
-    if (solve3(h, f, dx)) {
-        if (isfinite(dx.x) && isfinite(dx.y) && isfinite(dx.z)) {
-            d = make_float4(d.x + dx.x, d.y + dx.y, d.z + dx.z, 0.f);
-            a.disp[i] = d;
-        } else {
-            atomicAdd(&a.status[kNonfinite], 1u);
-        }
-    } else {
-        atomicAdd(&a.status[kSingular], 1u);
-    }
-    if (a.write_pos) a.pos[i] = make_float4(pv.x + d.x, pv.y + d.y, pv.z + d.z, 0.f);
+    solve_and_commit(a, i, pv, h, f);
 }
 
 // Record-parallel variant of the same color update (lanes_per_vertex == 0).  A block owns
@@ -871,21 +902,23 @@ __device__ __forceinline__ float gate_value(const GateState* g, int mean) {
     return static_cast<float>(static_cast<double>(g->resid_sum) / kResidSumScale / static_cast<double>(g->resid_cnt));
 }
 
-// Residual gate: after an evaluation of the Jacobi residual (a kResidual sweep over every solved
-// vertex, max_i |f_i| / (m_i |g|) accumulated into g->resid_bits), decide whether the loop runs
-// another round of iterations and set the while node's condition.  `first`: the evaluation at the
-// iterate the iterations start from (no iteration counted yet); `set_ref`: that evaluation is also
-// the relative mode's reference (the plain start y).  `add` iterations ran since the last check.
+// Residual gate: after an evaluation of the residual -- a Jacobi evaluation (a kResidual sweep
+// over every solved vertex) or the Gauss-Seidel residual the last iteration's sweeps accumulated
+// -- decide whether the loop runs another round and set the while node's condition.
+//   first = 1: the Jacobi evaluation at the iterate the iterations start from (nothing counted
+//              yet); first = 0: a later check; first = -1: sweep residuals, the first check of the
+//              step (iters == 0) is the one of the first iteration, which starts at the start iterate
+//   set_ref:   the first check also sets the relative mode's reference
+//   add:       iterations run since the last check
 __global__ void gate_check_kernel(GateState* g, cudaGraphConditionalHandle handle, float tol, int max_iters,
                                   int relative, int mean, int first, int set_ref, int add) {
     const float r = gate_value(g, mean);
-    if (first) {
-        g->iters = 0;
+    const bool is_first = first == 1 || (first == -1 && g->iters == 0);
+    if (is_first) {
         g->start_resid = r;
         if (set_ref) g->ref = r;
-    } else {
-        g->iters += add;
     }
+    if (first != 1) g->iters += add;
     const float thresh = relative ? tol * g->ref : tol;
     const bool more = (r > thresh) && (g->iters < max_iters);
     if (!more) {
@@ -992,11 +1025,13 @@ static void launch_dependent(Kernel kernel, int grid, int block, cudaStream_t st
     cudaLaunchKernelEx(&cfg, kernel, a);
 }
 
-template <int L, bool kDamp, bool kResidual>
+template <int L, bool kDamp, bool kResidual, bool kGate = false>
 static void launch_sweep_LDR(const SweepArgs& a, int grid, int block, cudaStream_t st) {
-    const void* uncapped = reinterpret_cast<const void*>(&sweep_kernel<L, kDamp, kResidual, false>);
-    if (grid > resident_blocks(uncapped, block)) launch_dependent(sweep_kernel<L, kDamp, kResidual, true>, grid, block, st, a);
-    else launch_dependent(sweep_kernel<L, kDamp, kResidual, false>, grid, block, st, a);
+    const void* uncapped = reinterpret_cast<const void*>(&sweep_kernel<L, kDamp, kResidual, false, kGate>);
+    if (grid > resident_blocks(uncapped, block))
+        launch_dependent(sweep_kernel<L, kDamp, kResidual, true, kGate>, grid, block, st, a);
+    else
+        launch_dependent(sweep_kernel<L, kDamp, kResidual, false, kGate>, grid, block, st, a);
 }
 
 // occupancy queries happen here, outside any stream capture (solver creation, vbd_set_launch)
@@ -1006,6 +1041,8 @@ static void prime_occupancy_L(int block) {
     resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, false, true, false>), block);
     resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, true, false, false>), block);
     resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, false, false, false>), block);
+    resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, true, false, false, true>), block);
+    resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, false, false, false, true>), block);
 }
 
 static void prime_occupancy(int lanes, int block) {
@@ -1020,10 +1057,15 @@ static void prime_occupancy(int lanes, int block) {
 }
 
 template <int L>
-static void launch_sweep_L(const SweepArgs& a, bool damp, bool residual, int block, cudaStream_t st) {
+static void launch_sweep_L(const SweepArgs& a, bool damp, bool residual, int block, cudaStream_t st, bool gate) {
     const long long threads = static_cast<long long>(a.v_end - a.v_begin) * L;
     const int grid = static_cast<int>((threads + block - 1) / block);
     if (grid <= 0) return;
+    if (gate && !residual) {
+        if (damp) launch_sweep_LDR<L, true, false, true>(a, grid, block, st);
+        else launch_sweep_LDR<L, false, false, true>(a, grid, block, st);
+        return;
+    }
     if (residual) {
         if (damp) launch_sweep_LDR<L, true, true>(a, grid, block, st);
         else launch_sweep_LDR<L, false, true>(a, grid, block, st);
@@ -1047,7 +1089,9 @@ static void launch_tile_TB(const SweepArgs& a, bool damp, bool residual, cudaStr
     }
 }
 
-static void launch_sweep(const SweepArgs& a, int lanes, bool damp, bool residual, int block, cudaStream_t st) {
+// gate: a Gauss-Seidel color that also accumulates its residual into a.resid_* (lanes > 0 only)
+static void launch_sweep(const SweepArgs& a, int lanes, bool damp, bool residual, int block, cudaStream_t st,
+                         bool gate = false) {
     if (lanes == 0) {
         if (block <= 64) launch_tile_TB<64>(a, damp, residual, st);
         else if (block <= 128) launch_tile_TB<128>(a, damp, residual, st);
@@ -1055,11 +1099,11 @@ static void launch_sweep(const SweepArgs& a, int lanes, bool damp, bool residual
         return;
     }
     switch (lanes) {
-        case 1: launch_sweep_L<1>(a, damp, residual, block, st); break;
-        case 2: launch_sweep_L<2>(a, damp, residual, block, st); break;
-        case 8: launch_sweep_L<8>(a, damp, residual, block, st); break;
-        case 16: launch_sweep_L<16>(a, damp, residual, block, st); break;
-        default: launch_sweep_L<4>(a, damp, residual, block, st); break;
+        case 1: launch_sweep_L<1>(a, damp, residual, block, st, gate); break;
+        case 2: launch_sweep_L<2>(a, damp, residual, block, st, gate); break;
+        case 8: launch_sweep_L<8>(a, damp, residual, block, st, gate); break;
+        case 16: launch_sweep_L<16>(a, damp, residual, block, st, gate); break;
+        default: launch_sweep_L<4>(a, damp, residual, block, st, gate); break;
     }
 }
 
@@ -1111,11 +1155,17 @@ static int enqueue_forward(SolverImpl& s, const float* q_in, const float* qd_in,
     return VBD_OK;
 }
 
+// gate: also accumulate the color's Gauss-Seidel residual into the residual gate (sweep mode)
 static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float dt, cudaStream_t st,
-                          bool first_iteration = true) {
+                          bool first_iteration = true, bool gate = false) {
     const VbdModelImpl& m = *s.m;
     SweepArgs a = make_sweep_args(s, c, dt);
     a.prefetch_records = first_iteration ? 1 : 0;
+    if (gate) {
+        a.resid_max = reinterpret_cast<float*>(&s.gate->resid_bits);
+        a.resid_sum = &s.gate->resid_sum;
+        a.resid_cnt = &s.gate->resid_cnt;
+    }
     a.v_begin = m.color_start[color];
     a.v_end = m.color_start[color + 1];
     if (a.v_end <= a.v_begin) return;
@@ -1125,7 +1175,7 @@ static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float 
         self_contact_truncate(m, s.sc, s.pos, s.disp, st);
         return;
     }
-    launch_sweep(a, s.lanes, m.any_tri_damping || m.any_edge_damping, false, s.block, st);
+    launch_sweep(a, s.lanes, m.any_tri_damping || m.any_edge_damping, false, s.block, st, gate);
     if (!m.fused_commit) {
         const int n = a.v_end - a.v_begin;
         commit_kernel<<<(n + 255) / 256, 256, 0, st>>>(s.pos, s.prev, s.disp, a.v_begin, a.v_end);
@@ -1209,13 +1259,21 @@ static int enqueue_gated_iterations(SolverImpl& s, const VbdContacts* c, float d
     VBD_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
     if (cs != cudaStreamCaptureStatusActive || !graph)
         return fail(VBD_ERR_UNSUPPORTED, "residual-gated step: the stream is not capturing");
+    // sweep residuals need the lane-parallel sweep; the record-parallel one is checked by Jacobi
+    const bool sweep = s.gate_sweep && s.lanes > 0;
     cudaGraphConditionalHandle handle;
-    VBD_CUDA_TRY(cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
-    enqueue_gate_residual(s, c, dt, st);
-    gate_check_kernel<<<1, 1, 0, st>>>(s.gate, handle, s.gate_tol, s.gate_max, s.gate_relative, s.gate_mean, 1,
-                                       set_ref ? 1 : 0, 0);
-    VBD_CUDA_TRY(cudaGetLastError());
-    VBD_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
+    // the loop runs at least once in sweep mode (its first check follows the first iteration)
+    const unsigned enter = (sweep && s.gate_max > 0) ? 1u : 0u;
+    VBD_CUDA_TRY(cudaGraphConditionalHandleCreate(&handle, graph, enter, cudaGraphCondAssignDefault));
+    if (!sweep || s.gate_max == 0) {
+        // the Jacobi residual at the start iterate (in sweep mode only when no iteration may run,
+        // so that the step is still recorded)
+        enqueue_gate_residual(s, c, dt, st);
+        gate_check_kernel<<<1, 1, 0, st>>>(s.gate, handle, s.gate_tol, s.gate_max, s.gate_relative, s.gate_mean, 1,
+                                           set_ref ? 1 : 0, 0);
+        VBD_CUDA_TRY(cudaGetLastError());
+        VBD_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
+    }
     cudaGraphNodeParams params = {cudaGraphNodeTypeConditional};  // the union has no default constructor
     params.type = cudaGraphNodeTypeConditional;
     params.conditional.handle = handle;
@@ -1226,11 +1284,14 @@ static int enqueue_gated_iterations(SolverImpl& s, const VbdContacts* c, float d
     cudaGraph_t body = params.conditional.phGraph_out[0];
     VBD_CUDA_TRY(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
     VBD_CUDA_TRY(cudaStreamBeginCaptureToGraph(s.body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < s.gate_every; ++k)
-        for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, s.body_stream, false);
-    enqueue_gate_residual(s, c, dt, s.body_stream);
+    for (int k = 0; k < s.gate_every; ++k) {
+        const bool last = k == s.gate_every - 1;
+        for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, s.body_stream, false, sweep && last);
+    }
+    if (!sweep) enqueue_gate_residual(s, c, dt, s.body_stream);
     gate_check_kernel<<<1, 1, 0, s.body_stream>>>(s.gate, handle, s.gate_tol, s.gate_max, s.gate_relative,
-                                                 s.gate_mean, 0, 0, s.gate_every);
+                                                 s.gate_mean, sweep ? -1 : 0, (sweep && set_ref) ? 1 : 0,
+                                                 s.gate_every);
     const cudaError_t e1 = cudaGetLastError();
     cudaGraph_t captured = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(s.body_stream, &captured);
@@ -1795,10 +1856,11 @@ extern "C" int vbd_set_residual_gate(VbdSolver* solver, float tolerance, int32_t
         s.gate_tol = tolerance;
         s.gate_max = max_iterations;
         s.gate_every = check_every;
-        if (mode & ~(VBD_GATE_RELATIVE | VBD_GATE_MEAN))
+        if (mode & ~(VBD_GATE_RELATIVE | VBD_GATE_MEAN | VBD_GATE_SWEEP))
             return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_residual_gate: unknown mode bits");
         s.gate_relative = (mode & VBD_GATE_RELATIVE) ? 1 : 0;
         s.gate_mean = (mode & VBD_GATE_MEAN) ? 1 : 0;
+        s.gate_sweep = (mode & VBD_GATE_SWEEP) ? 1 : 0;
     }
     for (auto& g : s.graphs) cudaGraphExecDestroy(g.exec);  // captured steps change
     s.graphs.clear();

@@ -348,20 +348,25 @@ class SolverVBD(SolverBase):
                                                 _lib.ptr(mlp.mean), _lib.ptr(mlp.inv_std), int(iterations)))
 
     def set_residual_gate(self, tolerance: float | None, max_iterations: int = 100, check_every: int = 1,
-                          relative: bool = False, norm: str = "max") -> None:
+                          relative: bool = False, norm: str = "max", residual: str = "jacobi") -> None:
         """Residual-gated steps (no reference counterpart; the reference runs a fixed iteration count,
         ``solver_vbd.py:1817-1819``): each ``step`` iterates until the Jacobi force residual norm --
         ``max_i |f_i| / (m_i |g|)`` (``norm="max"``) or its mean over the solved vertices
         (``norm="mean"``) -- is at most ``tolerance`` (relative to the norm at the inertia target
         when ``relative``), checked every ``check_every`` iterations, at most ``max_iterations``.
-        The loop runs on the device (a conditional node of the step's CUDA graph).
-        ``tolerance=None`` turns the gate off."""
+        ``residual="jacobi"`` evaluates the residual at the current iterate (one extra sweep-sized
+        launch per check); ``residual="sweep"`` uses the Gauss-Seidel residual the sweeps form
+        anyway (each vertex's force when its color is solved; no extra launch).  The loop runs on
+        the device (a conditional node of the step's CUDA graph).  ``tolerance=None`` turns the
+        gate off."""
         if norm not in ("max", "mean"):
             raise ValueError("norm must be 'max' or 'mean'")
+        if residual not in ("jacobi", "sweep"):
+            raise ValueError("residual must be 'jacobi' or 'sweep'")
         self._gate = None if tolerance is None else (float(tolerance), int(max_iterations), int(check_every),
-                                                     bool(relative), norm)
+                                                     bool(relative), norm, residual)
         tol = 0.0 if tolerance is None else float(tolerance)
-        mode = (1 if relative else 0) | (2 if norm == "mean" else 0)
+        mode = (1 if relative else 0) | (2 if norm == "mean" else 0) | (4 if residual == "sweep" else 0)
         _lib.check(self._lib.vbd_set_residual_gate(self._handle, ctypes.c_float(tol), int(max_iterations),
                                                    int(check_every), mode))
 

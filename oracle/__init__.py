@@ -124,6 +124,7 @@ def load():
         lib.oracle_get_positions.argtypes = [vp, c_double_p]
         lib.oracle_residual.argtypes = [vp, ctypes.c_float, c_float_p]
         lib.oracle_set_positions.argtypes = [vp, c_float_p]
+        lib.oracle_sweep_residual.argtypes = [vp, c_float_p]
         d = ctypes.c_double
         lib.oracle_membrane.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_double_p, c_double_p, c_int32_p,
                                         c_double_p, d, d, d, d, d, ctypes.c_int, c_double_p, c_double_p]
@@ -351,6 +352,40 @@ class VBDOracle:
         out = np.zeros(self.V, np.float32)
         self._lib.oracle_residual(self._h, float(dt), out.ctypes.data_as(c_float_p))
         return out
+
+    def sweep_residual(self) -> np.ndarray:
+        """|f_i| / (m_i |g|) of every vertex at its last Gauss-Seidel visit (0 if never solved)."""
+        out = np.zeros(self.V, np.float32)
+        self._lib.oracle_sweep_residual(self._h, out.ctypes.data_as(c_float_p))
+        return out
+
+    def gated_step(self, q_in, qd_in, f_ext, dt: float, tolerance: float, max_iterations: int,
+                   check_every: int = 1, norm: str = "mean"):
+        """The residual gate with sweep residuals (the library's VBD_GATE_SWEEP): forward, then
+        iterations until the norm of the last iteration's Gauss-Seidel residuals is <= tolerance
+        (checked every ``check_every`` iterations, at least one iteration, at most
+        ``max_iterations`` rounded up to a multiple of ``check_every``).  Returns
+        (q_in_after, q_out, qd_out, iterations, final norm)."""
+        self.forward(q_in, qd_in, f_ext, dt)
+        m = self.model
+        solvable = ((np.asarray(m.particle_flags) & 1) != 0) & (np.asarray(m.particle_mass) != 0)
+        k, r = 0, 0.0
+        while max_iterations > 0:
+            for _ in range(check_every):
+                self.begin_iteration()
+                for c in range(len(m.particle_color_groups)):
+                    self.sweep_color(c, dt)
+            k += check_every
+            pv = self.sweep_residual()[solvable]
+            if norm == "max":
+                r = float(pv.max()) if pv.size else 0.0
+            else:
+                fixed = np.floor(np.minimum(pv, np.float32(1e9)) * np.float32(256.0) + np.float32(0.5))
+                r = float(np.float32(float(fixed.astype(np.uint64).sum()) / 256.0 / max(pv.size, 1)))
+            if r <= tolerance or k >= max_iterations:
+                break
+        q_in_after, q_out, qd_out = self.finalize(dt)
+        return q_in_after, q_out, qd_out, k, r
 
 
 def collide(model, q: np.ndarray, margin: float):

@@ -474,6 +474,8 @@ struct Oracle {
     float soft_ke = 0.f, soft_kd = 0.f, soft_mu = 0.f;  // model.soft_contact_* (self-contact material)
     // scratch
     std::vector<T> q, q_prev, inertia, disp, pos_prev_cd, pf, ph;
+    // Gauss-Seidel residual of the last sweep of each vertex: |f| / (m |g|) at its visit
+    std::vector<float> gs_r;
     // contacts (reference record layout, per step)
     int ncontacts = 0;
     std::vector<int32_t> c_particle, c_shape;
@@ -553,6 +555,7 @@ void init_oracle(Oracle<T>& o, const OracleModelDesc* d) {
     o.disp = o.q;
     o.pos_prev_cd = o.q;
     o.pf = o.q;
+    o.gs_r.assign(static_cast<size_t>(o.V), 0.f);
     o.ph.assign(9 * V, T(0));
 }
 
@@ -1278,6 +1281,8 @@ void sweep_color(Oracle<T>& o, int color, T dt) {
         V3<T> f;
         M3<T> h;
         vertex_force(o, p, dt, f, h);
+        const T gn = std::sqrt(o.g[0] * o.g[0] + o.g[1] * o.g[1] + o.g[2] * o.g[2]);
+        o.gs_r[p] = float(len(f) / (o.mass[p] * gn));
         if (std::fabs(det3(h)) > T(1.0e-8)) {
             const M3<T> hi = inverse3(h);
             store3(o.disp.data(), p, load3(o.disp.data(), p) + hi * f);
@@ -1460,6 +1465,12 @@ void oracle_set_positions(OracleHandle* h, const float* q) {
 }
 
 void oracle_residual(OracleHandle* h, float dt, float* per_vertex) { ORACLE_DISPATCH(h, residual(o, T(dt), per_vertex)); }
+
+// Gauss-Seidel residual of each vertex's last sweep (0 for vertices never solved): the residual
+// the library's sweep-residual gate accumulates
+void oracle_sweep_residual(OracleHandle* h, float* per_vertex) {
+    ORACLE_DISPATCH(h, std::copy(o.gs_r.begin(), o.gs_r.end(), per_vertex));
+}
 
 // Self-contact (particle_enable_self_contact=True path): parameters, and detection alone.
 void oracle_set_self_contact(OracleHandle* h, const OracleSelfContact* p) {

@@ -254,3 +254,40 @@ def test_gate_rejects_self_contact_and_bad_arguments():
     plain = SolverVBD(model, iterations=4)
     with pytest.raises(VbdError, match="check_every"):
         plain.set_residual_gate(1.0, max_iterations=10, check_every=0)
+
+
+@pytest.mark.parametrize("norm", ["mean", "max"])
+def test_sweep_residual_gate(norm):
+    """residual="sweep": the check after iteration k reads the Gauss-Seidel residual R_k the
+    sweeps of iteration k accumulated (each vertex's force when its color was solved); the step
+    stops at the first k with R_k <= tolerance and equals the fixed-count step with k iterations."""
+    model, q, qd = _hanging_state()
+    solver = SolverVBD(model, iterations=10)
+    curve = [float("inf")]  # R_k for k = 1..16, each from a step capped at k
+    for k in range(1, 17):
+        solver.set_residual_gate(1e-30, max_iterations=k, norm=norm, residual="sweep")
+        _run(model, solver, q, qd)
+        st = solver.gate_stats(reset=True)
+        assert st["last_iterations"] == k and st["capped_steps"] == 1
+        curve.append(st["last_residual"])
+    assert all(np.isfinite(curve[1:])) and st["body_kernels"] == len(model.particle_color_groups) + 1
+    kd, tol = _clear_drop(curve, start=3, gap=0.99 if norm == "max" else 0.9995)
+    solver.set_residual_gate(tol, max_iterations=40, norm=norm, residual="sweep")
+    qg, qdg, _ = _run(model, solver, q, qd)
+    st = solver.gate_stats()
+    assert st["last_iterations"] == kd and st["last_residual"] == curve[kd] and st["capped_steps"] == 0
+    qf, qdf, _ = _run(model, SolverVBD(model, iterations=kd), q, qd)
+    assert np.array_equal(qg, qf) and np.array_equal(qdg, qdf)
+    # the oracle's restatement of the sweep gate picks the same count
+    orc = oracle.VBDOracle(model, "f32", threads=8)
+    orc.set_contacts(*oracle.collide(model, q, 5e-3))
+    _, qo, _, ko, ro = orc.gated_step(q, qd, None, DT, tol, 40, norm=norm)
+    assert ko == kd, (ko, kd)
+    assert float(np.abs(qg - qo).max()) <= TOL_STEP
+    # every 2 iterations: the first even k whose R_k meets the tolerance
+    solver.set_residual_gate(tol, max_iterations=40, check_every=2, norm=norm, residual="sweep")
+    _run(model, solver, q, qd)
+    k2 = solver.gate_stats()["last_iterations"]
+    assert k2 == min(k for k in range(2, 17, 2) if curve[k] <= tol)
+    print(f"sweep residual ({norm}): R_1..R_6 {[round(x, 3) for x in curve[1:7]]}, tolerance {tol:.5g} -> "
+          f"{kd} iterations (every 2: {k2})")
