@@ -36,10 +36,16 @@ constexpr int kGateMaxIterations = 100000;  // upper bound of a gated step's ite
 
 // Device-side state of the residual gate (vbd_set_residual_gate), one per solver.  The head, up
 // to `ref`, is zeroed at the start of every gated step.
+// The accumulators of one evaluation are spread over kGateSlots slots, each on its own 128-byte
+// line (warp w adds into slot w mod kGateSlots), so that the atomics of a large sweep do not all
+// queue on one line.
+constexpr int kGateSlots = 64;
+constexpr int kSumStride = 16;  // unsigned long long per 128-byte line
+constexpr int kMaxStride = 32;  // unsigned per 128-byte line
+
 struct GateState {
-    unsigned long long resid_sum;  // fixed-point sum of the current evaluation's residuals
-    unsigned resid_cnt;      // vertices in that sum
-    unsigned resid_bits;     // max residual of the current evaluation (float bits; atomicMax target)
+    unsigned long long sum[kGateSlots * kSumStride];  // fixed-point sums of the residuals (resid_fixed)
+    unsigned maxv[kGateSlots * kMaxStride];  // max residual (float bits; atomicMax target)
     int iters;               // iterations run so far in this step
     int pad;
     float ref;               // relative mode: the step's reference residual
@@ -110,6 +116,7 @@ struct SolverImpl {
     int gate_relative = 0;           // 1: tolerance relative to the residual at the inertia target y
     int gate_mean = 0;               // 1: mean residual over the solved vertices instead of the max
     int gate_sweep = 0;              // 1: the Gauss-Seidel residual the sweeps accumulate (no Jacobi launch)
+    int gate_count = 0;              // solved vertices (the mean's divisor)
     GateState* gate = nullptr;       // device
     cudaStream_t body_stream = nullptr;  // capture stream of the gate's loop body
     int gate_body_kernels = -1;      // kernel nodes of one loop body (last capture)
@@ -279,8 +286,8 @@ struct SweepArgs {
     int prefetch_records;    // 1: prefetch the vertices' element records into L2 (first iteration of a step)
     float* resid_out;        // residual mode: per-vertex residual (original order) or NULL
     float* resid_max;        // residual mode: max residual (float bits, atomicMax)
-    unsigned long long* resid_sum;  // residual mode: sum of the residuals, fixed point (resid_fixed)
-    unsigned* resid_cnt;     // residual mode: number of residuals summed
+    unsigned long long* gate_sum;   // residual gate: slotted fixed-point sums (GateState::sum) or NULL
+    unsigned* gate_max;      // residual gate: slotted max (GateState::maxv) or NULL
     const int* perm;
     float inv_g;             // 1/|g| (0 when g = 0)
     int no_pdl;              // host side: launch without the programmatic-dependent-launch attribute
@@ -504,19 +511,24 @@ __device__ __forceinline__ unsigned long long resid_fixed(float r) {
 }
 
 // Warp-collective: every thread of the warp calls it (r = 0 and counted = false where the thread
-// holds no vertex).  Max (float bits as unsigned: exact for r >= 0; NaN bits exceed +inf), fixed-
-// point sum and count go to the accumulators with one atomic each per warp.
+// holds no vertex).  Max (float bits as unsigned: exact for r >= 0; NaN bits exceed +inf) and the
+// fixed-point sum go to the accumulators with one atomic each per warp: the single max of
+// vbd_residual, and the residual gate's slots (slot = global warp index mod kGateSlots).
 __device__ __forceinline__ void reduce_residual(const SweepArgs& a, float r, bool counted) {
     const unsigned full = 0xffffffffu;
     const unsigned mx = __reduce_max_sync(full, __float_as_uint(r));
-    const unsigned cnt = __popc(__ballot_sync(full, counted));
-    unsigned long long sum = counted ? resid_fixed(r) : 0ull;
+    const bool any = __any_sync(full, counted);
+    unsigned long long sum = 0ull;
+    if (a.gate_sum) {
+        sum = counted ? resid_fixed(r) : 0ull;
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(full, sum, off);
-    if ((threadIdx.x & 31) == 0 && cnt) {
+        for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(full, sum, off);
+    }
+    if ((threadIdx.x & 31) == 0 && any) {
+        const int slot = static_cast<int>(((blockIdx.x * blockDim.x + threadIdx.x) >> 5) & (kGateSlots - 1));
         if (a.resid_max) atomicMax(reinterpret_cast<unsigned*>(a.resid_max), mx);
-        if (a.resid_sum) atomicAdd(a.resid_sum, sum);
-        if (a.resid_cnt) atomicAdd(a.resid_cnt, cnt);
+        if (a.gate_max) atomicMax(a.gate_max + slot * kMaxStride, mx);
+        if (a.gate_sum) atomicAdd(a.gate_sum + slot * kSumStride, sum);
     }
 }
 
@@ -791,8 +803,9 @@ __global__ void __launch_bounds__(TB) tile_kernel(SweepArgs a) {
         if (a.resid_out) a.resid_out[a.perm[i]] = r;
         // one vertex per thread here: plain per-vertex atomics (integer, so still deterministic)
         if (a.resid_max) atomicMax(reinterpret_cast<unsigned*>(a.resid_max), __float_as_uint(r));
-        if (a.resid_sum) atomicAdd(a.resid_sum, resid_fixed(r));
-        if (a.resid_cnt) atomicAdd(a.resid_cnt, 1u);
+        const int slot = static_cast<int>(i & (kGateSlots - 1));
+        if (a.gate_max) atomicMax(a.gate_max + slot * kMaxStride, __float_as_uint(r));
+        if (a.gate_sum) atomicAdd(a.gate_sum + slot * kSumStride, resid_fixed(r));
         return;
     }
     float3 dx;
@@ -895,11 +908,21 @@ __global__ void gather_positions_kernel(const int* perm, const float4* pos, floa
     q[3 * o + 2] = p.z;
 }
 
-// the gate's residual norm of the current evaluation: the max or the mean over the solved vertices
-__device__ __forceinline__ float gate_value(const GateState* g, int mean) {
-    if (!mean) return __uint_as_float(g->resid_bits);
-    if (g->resid_cnt == 0u) return 0.0f;
-    return static_cast<float>(static_cast<double>(g->resid_sum) / kResidSumScale / static_cast<double>(g->resid_cnt));
+// the gate's residual norm of the current evaluation -- the max, or the sum over the solved
+// vertices divided by their number `count` -- read from the slots, which are cleared for the next
+// evaluation (one thread)
+__device__ __forceinline__ float gate_take(GateState* g, int mean, int count) {
+    unsigned long long sum = 0ull;
+    unsigned mx = 0u;
+    for (int k = 0; k < kGateSlots; ++k) {
+        sum += g->sum[k * kSumStride];
+        mx = max(mx, g->maxv[k * kMaxStride]);
+        g->sum[k * kSumStride] = 0ull;
+        g->maxv[k * kMaxStride] = 0u;
+    }
+    if (!mean) return __uint_as_float(mx);
+    if (count <= 0) return 0.0f;
+    return static_cast<float>(static_cast<double>(sum) / kResidSumScale / static_cast<double>(count));
 }
 
 // Residual gate: after an evaluation of the residual -- a Jacobi evaluation (a kResidual sweep
@@ -911,8 +934,8 @@ __device__ __forceinline__ float gate_value(const GateState* g, int mean) {
 //   set_ref:   the first check also sets the relative mode's reference
 //   add:       iterations run since the last check
 __global__ void gate_check_kernel(GateState* g, cudaGraphConditionalHandle handle, float tol, int max_iters,
-                                  int relative, int mean, int first, int set_ref, int add) {
-    const float r = gate_value(g, mean);
+                                  int relative, int mean, int count, int first, int set_ref, int add) {
+    const float r = gate_take(g, mean, count);
     const bool is_first = first == 1 || (first == -1 && g->iters == 0);
     if (is_first) {
         g->start_resid = r;
@@ -928,19 +951,11 @@ __global__ void gate_check_kernel(GateState* g, cudaGraphConditionalHandle handl
         g->iter_sum += static_cast<unsigned long long>(g->iters);
         if (r > thresh) g->capped += 1ull;
     }
-    g->resid_bits = 0u;
-    g->resid_sum = 0ull;
-    g->resid_cnt = 0u;
     cudaGraphSetConditional(handle, more ? 1u : 0u);
 }
 
 // relative mode with a warm start: the residual at the plain start y becomes the reference
-__global__ void gate_ref_kernel(GateState* g, int mean) {
-    g->ref = gate_value(g, mean);
-    g->resid_bits = 0u;
-    g->resid_sum = 0ull;
-    g->resid_cnt = 0u;
-}
+__global__ void gate_ref_kernel(GateState* g, int mean, int count) { g->ref = gate_take(g, mean, count); }
 
 // ---------------------------------------------------------------------------------------------
 // host orchestration
@@ -1162,9 +1177,8 @@ static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float 
     SweepArgs a = make_sweep_args(s, c, dt);
     a.prefetch_records = first_iteration ? 1 : 0;
     if (gate) {
-        a.resid_max = reinterpret_cast<float*>(&s.gate->resid_bits);
-        a.resid_sum = &s.gate->resid_sum;
-        a.resid_cnt = &s.gate->resid_cnt;
+        a.gate_max = s.gate_mean ? nullptr : s.gate->maxv;
+        a.gate_sum = s.gate_mean ? s.gate->sum : nullptr;
     }
     a.v_begin = m.color_start[color];
     a.v_end = m.color_start[color + 1];
@@ -1240,9 +1254,8 @@ static void enqueue_gate_residual(SolverImpl& s, const VbdContacts* c, float dt,
     a.v_begin = 0;
     a.v_end = m.swept;
     a.resid_out = nullptr;
-    a.resid_max = reinterpret_cast<float*>(&s.gate->resid_bits);
-    a.resid_sum = &s.gate->resid_sum;
-    a.resid_cnt = &s.gate->resid_cnt;
+    a.gate_max = s.gate_mean ? nullptr : s.gate->maxv;
+    a.gate_sum = s.gate_mean ? s.gate->sum : nullptr;
     launch_sweep(a, s.lanes, m.any_tri_damping || m.any_edge_damping, true, s.block, st);
 }
 
@@ -1269,8 +1282,8 @@ static int enqueue_gated_iterations(SolverImpl& s, const VbdContacts* c, float d
         // the Jacobi residual at the start iterate (in sweep mode only when no iteration may run,
         // so that the step is still recorded)
         enqueue_gate_residual(s, c, dt, st);
-        gate_check_kernel<<<1, 1, 0, st>>>(s.gate, handle, s.gate_tol, s.gate_max, s.gate_relative, s.gate_mean, 1,
-                                           set_ref ? 1 : 0, 0);
+        gate_check_kernel<<<1, 1, 0, st>>>(s.gate, handle, s.gate_tol, s.gate_max, s.gate_relative, s.gate_mean,
+                                           s.gate_count, 1, set_ref ? 1 : 0, 0);
         VBD_CUDA_TRY(cudaGetLastError());
         VBD_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
     }
@@ -1290,8 +1303,8 @@ static int enqueue_gated_iterations(SolverImpl& s, const VbdContacts* c, float d
     }
     if (!sweep) enqueue_gate_residual(s, c, dt, s.body_stream);
     gate_check_kernel<<<1, 1, 0, s.body_stream>>>(s.gate, handle, s.gate_tol, s.gate_max, s.gate_relative,
-                                                 s.gate_mean, sweep ? -1 : 0, (sweep && set_ref) ? 1 : 0,
-                                                 s.gate_every);
+                                                 s.gate_mean, s.gate_count, sweep ? -1 : 0,
+                                                 (sweep && set_ref) ? 1 : 0, s.gate_every);
     const cudaError_t e1 = cudaGetLastError();
     cudaGraph_t captured = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(s.body_stream, &captured);
@@ -1312,11 +1325,11 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
         float* delta = pred + static_cast<size_t>(V) * 3;
         const bool gated = s.gate_tol > 0.f;
         if (gated) {
-            VBD_CUDA_TRY(cudaMemsetAsync(s.gate, 0, offsetof(GateState, ref), st));
+            VBD_CUDA_TRY(cudaMemsetAsync(s.gate, 0, offsetof(GateState, pad), st));
             if (s.gate_relative) {
                 // the relative tolerance refers to the plain start y, before the warm start moves it
                 enqueue_gate_residual(s, c, dt, st);
-                gate_ref_kernel<<<1, 1, 0, st>>>(s.gate, s.gate_mean);
+                gate_ref_kernel<<<1, 1, 0, st>>>(s.gate, s.gate_mean, s.gate_count);
             }
         }
         int rc = mlp_features_launch(*s.m, s.prev, s.y, c ? s.ccount : nullptr, s.ws_corr, s.ws_mean, s.ws_inv_std,
@@ -1375,7 +1388,7 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
         return VBD_OK;
     }
     if (s.gate_tol > 0.f) {
-        VBD_CUDA_TRY(cudaMemsetAsync(s.gate, 0, offsetof(GateState, ref), st));
+        VBD_CUDA_TRY(cudaMemsetAsync(s.gate, 0, offsetof(GateState, pad), st));
         const int rc = enqueue_gated_iterations(s, c, dt, st, true);
         if (rc) return rc;
         enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
@@ -1861,6 +1874,15 @@ extern "C" int vbd_set_residual_gate(VbdSolver* solver, float tolerance, int32_t
         s.gate_relative = (mode & VBD_GATE_RELATIVE) ? 1 : 0;
         s.gate_mean = (mode & VBD_GATE_MEAN) ? 1 : 0;
         s.gate_sweep = (mode & VBD_GATE_SWEEP) ? 1 : 0;
+        // every vertex a color solves is counted once per evaluation
+        int count = 0;
+        for (int i = 0; i < s.m->swept; ++i) {
+            const float4 pi = s.m->pinfo_h[i];
+            int flags = 0;
+            std::memcpy(&flags, &pi.w, sizeof(flags));
+            if ((flags & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f) ++count;
+        }
+        s.gate_count = count;
     }
     for (auto& g : s.graphs) cudaGraphExecDestroy(g.exec);  // captured steps change
     s.graphs.clear();

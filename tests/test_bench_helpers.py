@@ -12,6 +12,20 @@ import bench
 from newton_b200 import scenes
 
 
+def test_gate_configs_and_workload_configs():
+    """Every gated workload has a tolerance; the config object is the same for both arms."""
+    for wl in bench.WORKLOADS:
+        g = bench.gate_config(wl)
+        if wl == "cloth-on-boxes":
+            assert g is None  # the gate is not available with self-contact
+        else:
+            assert g["tolerance"] > 0 and g["max_iterations"] == bench.GATE_CAP and g["residual"] == "sweep"
+    model, _ = scenes.draped_cloth(n=16, device="cpu", height=0.904)
+    cfg = bench.workload_config("draped-cloth", model, bench.gate_config("draped-cloth"))
+    assert cfg["vertices"] == 256 and cfg["settle_steps"] == bench.SETTLE and cfg["residual_gate"]["norm"] == "mean"
+    json.dumps(cfg)
+
+
 def test_algorithmic_bytes_follow_the_per_element_formula():
     model, _ = scenes.hanging_cloth(seed=0, device="cpu")
     adj = model.soft_mesh_adjacency
@@ -80,10 +94,3 @@ def test_measured_peaks_read_the_file_or_fall_back(tmp_path, monkeypatch):
     # the fallback when the file cannot be read
     monkeypatch.setattr(bench.os.path, "abspath", lambda _p: str(tmp_path / "bench.py"))
     assert bench.measured_peaks() == {"hbm_gbs": 6650.0, "source": "fallback"}
-
-
-def test_sweep_traffic_summary_is_per_vertex_iteration():
-    t = bench.sweep_traffic_per_vertex_iteration()
-    assert t is not None and np.isfinite(t)
-    # 14.18 MB of cold-cache DRAM per color launch of 16,384 vertices (profiles/)
-    assert abs(t - 14.18e6 / 16384) < 5.0
