@@ -11,11 +11,14 @@ timed steps start from a state in contact.
 
 The metric is steps/s to a force-residual tolerance: every step iterates until the residual
 gate (``SolverVBD.set_residual_gate``) is met -- the mean over the vertices of the Gauss-Seidel
-residual |f_i| / (m_i |g|) that the sweeps form, at most ``GATE_CAP`` iterations.  The spec's
-1e-3 of the gravity load (max over the vertices) is unreachable for Gauss-Seidel VBD on these
-cloths, in FP32 and in FP64 alike, so the tolerance is set per workload to the residual that plain
-VBD reaches in about the reference's default 10 iterations over the timed steps (``GATE_TOL``).
-``fixed_iterations`` reports the reference's own loop (10 iterations per step) beside it.
+residual |f_i| / (m_i |g|) that the sweeps form must fall to ``GATE_RHO`` times the mean Jacobi
+residual at the step's inertia target y (the plain start), at most ``GATE_CAP`` iterations.  The
+spec's 1e-3 of the gravity load (max over the vertices) is unreachable for Gauss-Seidel VBD on
+these cloths, in FP32 and in FP64 alike, so the tolerance is the residual level the reference's
+default 10 iterations reach: on the settled states the mean residual after 10 plain iterations is
+0.87 (draped cloth) and 0.94 (batched worlds) of the residual at y (medians over 40 steps),
+rounded up to GATE_RHO.  ``fixed_iterations`` reports the reference's own loop (10 iterations per
+step) beside it.
 
 ``value`` is steps/s with inputs resident on the device (L2 flushed between timed steps);
 ``e2e`` is the same loop through the public API with the step's inputs copied from pinned host
@@ -54,9 +57,9 @@ ITERATIONS = 10
 MARGIN = 5.0e-3
 SETTLE = 150      # untimed steps before the warm-up: the cloth settles into contact
 GATE_CAP = 100    # iteration cap of a gated step
-# mean Gauss-Seidel residual tolerance per workload, in units of the vertex's gravity load m|g|:
-# plain VBD needs about 10 iterations per step to reach it over the timed steps
-GATE_TOL = {"draped-cloth": 5000.0, "batched-worlds": 3500.0}
+# relative tolerance per workload: the mean Gauss-Seidel residual must fall to GATE_RHO x the mean
+# Jacobi residual at y (plain VBD needs about 10 iterations for it on the settled states)
+GATE_RHO = {"draped-cloth": 0.9, "batched-worlds": 0.95}
 WORKLOADS = {
     "draped-cloth": ("draped cloth 256x256 (65,536 vertices, 130,050 triangles, 195,585 hinges) released 4 mm above "
                      "a static sphere on the ground, 150 settling steps, plain VBD to the residual gate, dt=1/600, "
@@ -71,10 +74,11 @@ WORKLOADS = {
 
 
 def gate_config(workload: str) -> dict | None:
-    tol = GATE_TOL.get(workload)
-    if tol is None:
+    rho = GATE_RHO.get(workload)
+    if rho is None:
         return None
-    return {"tolerance": tol, "max_iterations": GATE_CAP, "check_every": 1, "norm": "mean", "residual": "sweep"}
+    return {"tolerance": rho, "max_iterations": GATE_CAP, "check_every": 1, "relative": True, "norm": "mean",
+            "residual": "sweep"}
 
 
 def build_scene(workload: str, device, builder_cls=None, n: int = 0, rank: int = 0, world: int = 1):
@@ -189,7 +193,7 @@ def _oracle_step(orc, model, q, qd, gate):
         _, q, qd = orc.step(q, qd, None, DT, ITERATIONS)
         return q, qd, ITERATIONS
     _, q, qd, k, _ = orc.gated_step(q, qd, None, DT, gate["tolerance"], gate["max_iterations"],
-                                    gate["check_every"], gate["norm"])
+                                    gate["check_every"], gate["norm"], gate["relative"])
     return q, qd, k
 
 

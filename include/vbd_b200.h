@@ -279,9 +279,10 @@ int vbd_step_static_status(VbdStatus* out);
  * anyway: each vertex's force norm when its color is solved, accumulated by the last iteration
  * before a check (no extra launch; the first check follows the first iteration, whose residual is
  * that of the start iterate as each color meets it; at least one iteration runs unless
- * max_iterations is 0).  VBD_GATE_RELATIVE makes the tolerance relative to the norm at the
- * inertia target y, the plain start (with a warm start that norm is a Jacobi evaluation at y, so
- * that both starts are held to the same absolute residual).  The iteration count is a multiple of
+ * max_iterations is 0).  VBD_GATE_RELATIVE makes the tolerance relative to the norm of the
+ * Jacobi residual at the inertia target y, the plain start (one evaluation per step where the
+ * gate does not evaluate it anyway; with a warm start it is still taken at y, so that both starts
+ * are held to the same absolute residual).  The iteration count is a multiple of
  * check_every (the cap is rounded up to one).  The
  * loop runs on the device as a conditional (while) node of the step's CUDA graph: no host round
  * trip; a gated vbd_step always runs from a graph (use_graph is implied), and inside a caller's

@@ -1389,7 +1389,14 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
     }
     if (s.gate_tol > 0.f) {
         VBD_CUDA_TRY(cudaMemsetAsync(s.gate, 0, offsetof(GateState, pad), st));
-        const int rc = enqueue_gated_iterations(s, c, dt, st, true);
+        // relative mode: the reference is the Jacobi residual at the plain start y -- the Jacobi
+        // check at the start iterate when the gate evaluates one anyway, else one evaluation here
+        const bool sweep = s.gate_sweep && s.lanes > 0;
+        if (s.gate_relative && sweep) {
+            enqueue_gate_residual(s, c, dt, st);
+            gate_ref_kernel<<<1, 1, 0, st>>>(s.gate, s.gate_mean, s.gate_count);
+        }
+        const int rc = enqueue_gated_iterations(s, c, dt, st, !sweep);
         if (rc) return rc;
         enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
         return VBD_OK;

@@ -359,16 +359,27 @@ class VBDOracle:
         self._lib.oracle_sweep_residual(self._h, out.ctypes.data_as(c_float_p))
         return out
 
+    @staticmethod
+    def _norm(pv, norm):
+        if norm == "max":
+            return float(pv.max()) if pv.size else 0.0
+        fixed = np.floor(np.minimum(pv, np.float32(1e9)) * np.float32(256.0) + np.float32(0.5))
+        return float(np.float32(float(fixed.astype(np.uint64).sum()) / 256.0 / max(pv.size, 1)))
+
     def gated_step(self, q_in, qd_in, f_ext, dt: float, tolerance: float, max_iterations: int,
-                   check_every: int = 1, norm: str = "mean"):
+                   check_every: int = 1, norm: str = "mean", relative: bool = False):
         """The residual gate with sweep residuals (the library's VBD_GATE_SWEEP): forward, then
         iterations until the norm of the last iteration's Gauss-Seidel residuals is <= tolerance
-        (checked every ``check_every`` iterations, at least one iteration, at most
-        ``max_iterations`` rounded up to a multiple of ``check_every``).  Returns
+        (``relative``: tolerance x the norm of the Jacobi residual at the inertia target y),
+        checked every ``check_every`` iterations, at least one iteration, at most
+        ``max_iterations`` rounded up to a multiple of ``check_every``.  Returns
         (q_in_after, q_out, qd_out, iterations, final norm)."""
         self.forward(q_in, qd_in, f_ext, dt)
         m = self.model
         solvable = ((np.asarray(m.particle_flags) & 1) != 0) & (np.asarray(m.particle_mass) != 0)
+        thresh = float(np.float32(tolerance))
+        if relative:
+            thresh = float(np.float32(tolerance) * np.float32(self._norm(self.residual(dt)[solvable], norm)))
         k, r = 0, 0.0
         while max_iterations > 0:
             for _ in range(check_every):
@@ -376,13 +387,8 @@ class VBDOracle:
                 for c in range(len(m.particle_color_groups)):
                     self.sweep_color(c, dt)
             k += check_every
-            pv = self.sweep_residual()[solvable]
-            if norm == "max":
-                r = float(pv.max()) if pv.size else 0.0
-            else:
-                fixed = np.floor(np.minimum(pv, np.float32(1e9)) * np.float32(256.0) + np.float32(0.5))
-                r = float(np.float32(float(fixed.astype(np.uint64).sum()) / 256.0 / max(pv.size, 1)))
-            if r <= tolerance or k >= max_iterations:
+            r = self._norm(self.sweep_residual()[solvable], norm)
+            if r <= thresh or k >= max_iterations:
                 break
         q_in_after, q_out, qd_out = self.finalize(dt)
         return q_in_after, q_out, qd_out, k, r

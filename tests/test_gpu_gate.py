@@ -291,3 +291,31 @@ def test_sweep_residual_gate(norm):
     assert k2 == min(k for k in range(2, 17, 2) if curve[k] <= tol)
     print(f"sweep residual ({norm}): R_1..R_6 {[round(x, 3) for x in curve[1:7]]}, tolerance {tol:.5g} -> "
           f"{kd} iterations (every 2: {k2})")
+
+
+def test_relative_sweep_gate_refers_to_the_jacobi_residual_at_y():
+    """Relative sweep mode (the benchmark's gate): the reference is the mean Jacobi residual at the
+    inertia target y, the stop is the first k whose mean sweep residual R_k <= rho x reference."""
+    model, q, qd = _hanging_state(steps=45, seed=3)
+    jac = _jacobi_residuals(model, q, qd, 0, norm="mean")
+    solver = SolverVBD(model, iterations=10)
+    curve = [float("inf")]
+    for k in range(1, 13):
+        solver.set_residual_gate(1e-30, max_iterations=k, relative=True, norm="mean", residual="sweep")
+        _run(model, solver, q, qd)
+        st = solver.gate_stats(reset=True)
+        assert st["last_reference_residual"] == jac[0]
+        curve.append(st["last_residual"])
+    kd, _ = _clear_drop(curve, start=3, gap=0.9995)
+    rho = float(np.float32(0.5 * (curve[kd] + min(curve[:kd])) / jac[0]))
+    thresh = float(np.float32(rho) * np.float32(jac[0]))
+    expect = _first_at_or_below(curve, thresh)
+    solver.set_residual_gate(rho, max_iterations=40, relative=True, norm="mean", residual="sweep")
+    qg, _, _ = _run(model, solver, q, qd)
+    assert solver.gate_stats()["last_iterations"] == expect
+    qf, _, _ = _run(model, SolverVBD(model, iterations=expect), q, qd)
+    assert np.array_equal(qg, qf)
+    orc = oracle.VBDOracle(model, "f32", threads=8)
+    orc.set_contacts(*oracle.collide(model, q, 5e-3))
+    _, qo, _, ko, _ = orc.gated_step(q, qd, None, DT, rho, 40, norm="mean", relative=True)
+    assert ko == expect and float(np.abs(qg - qo).max()) <= TOL_STEP

@@ -27,3 +27,18 @@ def test_oracle_gated_step_bounds_and_identity():
     r = orc.sweep_residual()
     solvable = ((model.particle_flags & 1) != 0) & (model.particle_mass != 0)
     assert (r[~solvable] == 0).all() and (r[solvable] > 0).all()
+
+
+def test_oracle_relative_gate_refers_to_the_residual_at_the_inertia_target():
+    model, q0 = scenes.hanging_cloth(seed=4, device="cpu")
+    qd = np.zeros_like(q0)
+    orc = oracle.VBDOracle(model, "f32", threads=4)
+    orc.forward(q0, qd, None, DT)
+    solvable = ((model.particle_flags & 1) != 0) & (model.particle_mass != 0)
+    r_y = orc._norm(orc.residual(DT)[solvable], "mean")
+    _, _, _, k, r = orc.gated_step(q0, qd, None, DT, 0.5, 200, relative=True)
+    assert r <= np.float32(0.5) * np.float32(r_y) or k == 200
+    # one iteration earlier the tolerance was not met
+    if k > 1:
+        _, _, _, k2, r2 = orc.gated_step(q0, qd, None, DT, 1e-30, k - 1, relative=True)
+        assert k2 == k - 1 and r2 > np.float32(0.5) * np.float32(r_y)
