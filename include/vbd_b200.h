@@ -338,8 +338,17 @@ int vbd_mlp_sizes(int32_t* params, int32_t* weights16, int32_t* in_features, int
  * standardise them (both NULL = raw). */
 int vbd_mlp_features(VbdSolver* solver, const float* corr_prev, const float* mean, const float* inv_std, float* out,
                      void* stream);
-/* Y [n][3] = MLP(X [n][64]). */
+/* Y [n][3] = MLP(X [n][64]) on the 5th-generation tensor cores (tcgen05.mma, BF16 operands in
+ * shared memory, FP32 accumulators in tensor memory; SiLU with the hardware tanh approximation).
+ * X must be 16-byte aligned.  A wait that gives up is counted (vbd_mlp_timeouts). */
 int vbd_mlp_forward(const float* params, const uint16_t* w16, const float* X, int32_t n, float* Y, void* stream);
+/* The same inference on the previous tensor-core path (mma.sync m16n8k16 fragments, exact SiLU),
+ * kept to cross-check the tcgen05 kernel. */
+int vbd_mlp_forward_mma_sync(const float* params, const uint16_t* w16, const float* X, int32_t n, float* Y,
+                             void* stream);
+/* Waits of the tcgen05 inference kernel that gave up since the last reset (0 in normal operation);
+ * reset != 0 zeroes the counter.  Synchronizes with the device. */
+int vbd_mlp_timeouts(uint32_t* count, int32_t reset);
 /* Workspace bytes vbd_mlp_backward needs for n samples. */
 int vbd_mlp_workspace_bytes(int32_t n, int64_t* bytes);
 /* Gradients of L = grad_scale * sum |MLP(X) - T|^2 into grads (FP32 blob layout); loss (device

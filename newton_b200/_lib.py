@@ -179,6 +179,8 @@ SIGNATURES = {
     "vbd_mlp_sizes": (ctypes.c_int, [c_int32_p, c_int32_p, c_int32_p, c_int32_p, c_int32_p]),
     "vbd_mlp_features": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     "vbd_mlp_forward": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int32, _VP, _VP]),
+    "vbd_mlp_forward_mma_sync": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int32, _VP, _VP]),
+    "vbd_mlp_timeouts": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.c_int32]),
     "vbd_mlp_workspace_bytes": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
     "vbd_mlp_backward": (
         ctypes.c_int,

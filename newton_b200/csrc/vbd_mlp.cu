@@ -3,7 +3,9 @@
 // A per-vertex MLP 64 -> 128 -> 128 -> 3 with SiLU activations predicts the step's correction
 // to the inertia target (x_solved - y) from one-ring features; the Gauss-Seidel iterations then
 // start from y + prediction instead of y.  Weights are BF16, every product accumulates in FP32
-// on the tensor cores (mma.sync m16n8k16 bf16).  Training is hand-written too:
+// on the tensor cores.  Inference (vbd_mlp_forward, the step's warm start) runs on tcgen05.mma
+// with TMEM accumulators (vbd_mlp_tc.cuh).  Training is hand-written too, on mma.sync
+// m16n8k16 tiles:
 //   * mlp_tile_kernel: per warp, 16 samples through the three layers with the activations handed
 //     from one layer's accumulator fragments to the next layer's A fragments in registers; in
 //     training mode it continues with the backward pass (dY, dH2 = dY W3^T, dZ2, dH1 = dZ2 W2^T,
@@ -24,6 +26,7 @@
 
 #include "vbd_internal.h"
 #include "vbd_math.cuh"
+#include "vbd_mlp_tc.cuh"
 
 namespace vbd {
 
@@ -415,6 +418,9 @@ __global__ void to_bf16_kernel(const float* p, uint16_t* w16) {
 std::mutex g_attr_mutex;
 bool g_attr_done[64] = {};
 
+// waits of the tensor-core inference kernel that gave up (read by vbd_mlp_timeouts)
+__device__ unsigned g_mlp_tc_timeouts;
+
 int ensure_tile_smem() {
     int dev = 0;
     VBD_CUDA_TRY(cudaGetDevice(&dev));
@@ -425,9 +431,20 @@ int ensure_tile_smem() {
                                           static_cast<int>(kTileSmem)));
         VBD_CUDA_TRY(cudaFuncSetAttribute(mlp_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           static_cast<int>(kTileSmem)));
+        VBD_CUDA_TRY(cudaFuncSetAttribute(tc::mlp_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          tc::kSmemBytes));
         g_attr_done[dev] = true;
     }
     return VBD_OK;
+}
+
+// persistent grid of the tensor-core inference kernel: two CTAs per SM, at most one per tile
+int tc_grid(int n) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tiles = (n + tc::kRows - 1) / tc::kRows;
+    return std::max(1, std::min(2 * sms, tiles));
 }
 
 int tile_grid(int n) {
@@ -579,6 +596,32 @@ extern "C" int vbd_mlp_workspace_bytes(int32_t n, int64_t* bytes) {
 extern "C" int vbd_mlp_forward(const float* params, const uint16_t* w16, const float* X, int32_t n, float* Y,
                                void* stream) {
     if (!params || !w16 || (n > 0 && (!X || !Y))) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_forward: NULL argument");
+    if ((reinterpret_cast<uintptr_t>(X) & 15u) || (reinterpret_cast<uintptr_t>(w16) & 1u))
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_forward: X must be 16-byte aligned");
+    int rc = ensure_tile_smem();
+    if (rc) return rc;
+    if (n == 0) return VBD_OK;
+    tc::TcArgs a;
+    a.n = n;
+    a.params = params;
+    a.w16 = w16;
+    a.X = X;
+    a.Y = Y;
+    unsigned* counter = nullptr;
+    VBD_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&counter), g_mlp_tc_timeouts));
+    a.status = counter;
+    a.off_b1 = kOffB1;
+    a.off_b2 = kOffB2;
+    a.off_b3 = kOffB3;
+    tc::mlp_infer_tc_kernel<<<tc_grid(n), tc::kThreads, tc::kSmemBytes, static_cast<cudaStream_t>(stream)>>>(a);
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+extern "C" int vbd_mlp_forward_mma_sync(const float* params, const uint16_t* w16, const float* X, int32_t n, float* Y,
+                                        void* stream) {
+    if (!params || !w16 || (n > 0 && (!X || !Y)))
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_forward_mma_sync: NULL argument");
     int rc = ensure_tile_smem();
     if (rc) return rc;
     if (n == 0) return VBD_OK;
@@ -591,6 +634,16 @@ extern "C" int vbd_mlp_forward(const float* params, const uint16_t* w16, const f
     a.Y = Y;
     mlp_tile_kernel<false><<<tile_grid(n), kThreads, kTileSmem, static_cast<cudaStream_t>(stream)>>>(a);
     VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
+
+extern "C" int vbd_mlp_timeouts(uint32_t* count, int32_t reset) {
+    if (!count) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_timeouts: count is NULL");
+    VBD_CUDA_TRY(cudaMemcpyFromSymbol(count, g_mlp_tc_timeouts, sizeof(uint32_t)));
+    if (reset) {
+        const uint32_t zero = 0;
+        VBD_CUDA_TRY(cudaMemcpyToSymbol(g_mlp_tc_timeouts, &zero, sizeof(uint32_t)));
+    }
     return VBD_OK;
 }
 

@@ -1150,6 +1150,10 @@ static int enqueue_forward(SolverImpl& s, const float* q_in, const float* qd_in,
         a.c_particle = c->soft_contact_particle;
         a.c_max = c->soft_contact_max;
         n = std::max(n, std::min(c->soft_contact_max, 148 * 2048));
+        // the scatter counts into ccount: start it from zero here rather than trusting the previous
+        // step's finalize (a staged sequence -- forward and sweeps without finalize, as the launch
+        // autotuner runs -- leaves it set)
+        VBD_CUDA_TRY(cudaMemsetAsync(s.ccount, 0, sizeof(int) * static_cast<size_t>(m.V), st));
     }
     const int block = 256;
     if (n > 0) forward_kernel<<<(n + block - 1) / block, block, 0, st>>>(a);

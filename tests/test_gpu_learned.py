@@ -59,6 +59,36 @@ def test_mlp_forward_matches_fp64_reference():
     assert _rel(y, y_ref) < 2e-2
 
 
+@pytest.mark.parametrize("n", [1, 127, 128, 1000, 4097, 300000])
+def test_tcgen05_inference_matches_the_mma_sync_path_and_fp64(n):
+    """The tcgen05 inference kernel (TMEM accumulators) against the mma.sync one and the FP64
+    restatement: partial tiles, one tile, many tiles per CTA; no wait gave up."""
+    import ctypes
+
+    from newton_b200 import _lib
+
+    lib = _lib.load()
+    cnt = ctypes.c_uint32()
+    _lib.check(lib.vbd_mlp_timeouts(ctypes.byref(cnt), 1))
+    mlp = L.WarmStartMLP("cuda:0", seed=7)
+    rng = np.random.default_rng(n)
+    X = torch.from_numpy(rng.normal(size=(n, L.IN)).astype(np.float32)).cuda()
+    y_tc = mlp.forward(X)
+    y_ms = torch.empty_like(y_tc)
+    _lib.check(lib.vbd_mlp_forward_mma_sync(_lib.ptr(mlp.params), _lib.ptr(mlp.w16), _lib.ptr(X), n, _lib.ptr(y_ms),
+                                            mlp._stream()))
+    torch.cuda.synchronize()
+    a, b = y_tc.cpu().numpy(), y_ms.cpu().numpy()
+    assert np.isfinite(a).all()
+    # both round the activations to BF16; SiLU differs (hardware tanh vs exact), ~1e-3 relative
+    assert _rel(a, b) < 2e-2, _rel(a, b)
+    if n <= 4097:
+        y_ref, _ = _reference(mlp, X.cpu().numpy(), np.zeros((n, 3)))
+        assert _rel(a, y_ref) < 2e-2
+    _lib.check(lib.vbd_mlp_timeouts(ctypes.byref(cnt), 0))
+    assert cnt.value == 0
+
+
 def test_mlp_gradients_match_fp64_reference():
     mlp = L.WarmStartMLP("cuda:0", seed=2)
     rng = np.random.default_rng(1)

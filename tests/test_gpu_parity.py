@@ -361,3 +361,26 @@ def test_full_size_batched_worlds_step_matches_oracle():
     _report(f"full-size batched worlds ({model.particle_count} vertices, {contacts.count()} contacts)", err, err64,
             _residual_of(orc64, q_g))
     assert err <= TOL_STEP and err64 <= TOL_STEP
+
+
+def test_step_after_an_unfinished_staged_sequence_is_unaffected():
+    """A staged forward + sweeps without finalize (what the launch autotuner runs) must not leave
+    contact-table state behind: the next step equals a fresh solver's step bit for bit."""
+    model, q0 = scenes.single_cloth(n=32, side=1.0, seed=12, pin_top_corners=False, ground=0.0,
+                                    sphere=((0.0, 0.0, 0.5), 0.4), height=0.903)
+    pipe = CollisionPipeline(model, soft_contact_margin=5e-3)
+    outs = []
+    for staged_first in (False, True):
+        solver = SolverVBD(model, iterations=5)
+        c = pipe.contacts()
+        s0, s1 = model.state(), model.state()
+        s0.particle_q.copy_(torch.from_numpy(q0).cuda())
+        pipe.collide(s0, c)
+        assert c.count() > 0
+        if staged_first:
+            solver.forward(s0, c, DT)
+            solver.iterate(c, DT, 2)
+        solver.step(s0, s1, None, c, DT)
+        torch.cuda.synchronize()
+        outs.append(s1.particle_q.cpu().numpy())
+    np.testing.assert_array_equal(outs[0], outs[1])
