@@ -585,6 +585,60 @@ def learned_ab(dev, plain: dict, K: int, W: int) -> dict:
     }
 
 
+def mlp_kernels(rows: int, repeats: int) -> dict:
+    """Device time of the warm-start MLP kernels on random rows (the profile harness): tcgen05
+    inference, the mma.sync inference it replaced, and one training pass (forward + backward +
+    weight-gradient GEMMs)."""
+    import ctypes
+
+    import torch
+
+    from newton_b200 import _lib
+    from newton_b200 import learned as L
+
+    dev = torch.device("cuda:0")
+    lib = _lib.load()
+    mlp = L.WarmStartMLP(dev, seed=0)
+    gen = torch.Generator(device=dev).manual_seed(0)
+    X = torch.randn(rows, L.IN, device=dev, generator=gen)
+    T = torch.randn(rows, L.OUT, device=dev, generator=gen)
+    Y = torch.empty(rows, L.OUT, device=dev)
+    flops = 2 * (L.IN * L.HID + L.HID * L.HID + L.HID * L.OUT) * rows
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn) -> float:
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(repeats):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / repeats
+
+    t_tc = timed(lambda: _lib.check(lib.vbd_mlp_forward(_lib.ptr(mlp.params), _lib.ptr(mlp.w16), _lib.ptr(X), rows,
+                                                        _lib.ptr(Y), mlp._stream())))
+    t_ms = timed(lambda: _lib.check(lib.vbd_mlp_forward_mma_sync(_lib.ptr(mlp.params), _lib.ptr(mlp.w16), _lib.ptr(X),
+                                                                 rows, _lib.ptr(Y), mlp._stream())))
+    t_tr = timed(lambda: mlp.gradients(X, T))
+    peak = 1628.3
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["bf16_tflops"])
+    except Exception:
+        pass
+    cnt = ctypes.c_uint32()
+    _lib.check(lib.vbd_mlp_timeouts(ctypes.byref(cnt), 0))
+    return {"rows": rows, "flop_per_row": flops // rows,
+            "tcgen05_inference_ms": t_tc, "tcgen05_inference_tflops": flops / (t_tc * 1e-3) / 1e12,
+            "tcgen05_frac_of_bf16_peak": flops / (t_tc * 1e-3) / 1e12 / peak,
+            "mma_sync_inference_ms": t_ms, "mma_sync_inference_tflops": flops / (t_ms * 1e-3) / 1e12,
+            "training_pass_ms": t_tr, "training_tflops": 3 * flops / (t_tr * 1e-3) / 1e12,
+            "input_gbs_tcgen05": rows * L.IN * 4 / (t_tc * 1e-3) / 1e9, "timeouts": cnt.value}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -597,7 +651,12 @@ def main() -> None:
     ap.add_argument("--no-workloads", action="store_true", help="skip the batched-worlds and cloth-on-boxes entries")
     ap.add_argument("--n", type=int, default=0, help="grid vertices per side (default: the workload's)")
     ap.add_argument("--workload", default="draped-cloth", choices=sorted(WORKLOADS))
+    ap.add_argument("--mlp-kernels", type=int, default=0, metavar="ROWS",
+                    help="only time the warm-start MLP kernels on ROWS random rows and print their JSON")
     args = ap.parse_args()
+    if args.mlp_kernels:
+        print(json.dumps(mlp_kernels(args.mlp_kernels, max(args.steps, 5))), flush=True)
+        return
     if args.impl == "reference":
         run_reference(args)
         return

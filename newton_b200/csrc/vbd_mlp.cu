@@ -438,13 +438,13 @@ int ensure_tile_smem() {
     return VBD_OK;
 }
 
-// persistent grid of the tensor-core inference kernel: two CTAs per SM, at most one per tile
+// persistent grid of the tensor-core inference kernel: one CTA (four tile pipelines) per SM
 int tc_grid(int n) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int tiles = (n + tc::kRows - 1) / tc::kRows;
-    return std::max(1, std::min(2 * sms, tiles));
+    return std::max(1, std::min(sms, (tiles + tc::kGroups - 1) / tc::kGroups));
 }
 
 int tile_grid(int n) {

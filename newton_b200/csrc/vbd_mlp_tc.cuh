@@ -2,17 +2,20 @@
 // generation tensor cores: tcgen05.mma with BF16 operands in shared memory and FP32 accumulators
 // in tensor memory (TMEM).  Included by vbd_mlp.cu only.
 //
-// Work split.  A persistent CTA of 128 threads owns one 128-row tile of samples at a time; thread
-// t owns row t (TMEM lane t).  Per tile:
-//   1. all threads stage the tile's features as BF16 in shared memory (A1, 128 x 64);
-//   2. thread 0 issues layer 1: D1[128 x 128] = A1 W1 (4 MMAs of K = 16) and commits to an
-//      mbarrier; every thread waits, reads its row of D1 from TMEM (tcgen05.ld), adds the bias,
-//      applies SiLU and writes the BF16 row into A2 (128 x 128);
-//   3. layer 2 likewise: D2 = A2 W2 (8 MMAs), epilogue back into A2 (its MMAs have completed);
-//   4. layer 3: D3[128 x 16] = A2 W3 (8 MMAs, N padded from 3 to 16, D3 reuses D1's columns);
-//      the epilogue adds the bias and stores the 3 outputs.
-// Two CTAs run per SM (about 100 KB of shared memory and 256 TMEM columns each), so one CTA's
-// MMAs run while the other works through an epilogue.
+// Work split.  One persistent CTA of 512 threads per SM runs four independent tile pipelines
+// ("groups" of 4 warps) over one shared copy of the weights.  A group owns one 128-row tile of
+// samples at a time; its warp q reads TMEM lanes [32 q, 32 q + 32), the rows of those samples, and
+// thread 32 q + l owns row 32 q + l.  Per tile, in the group's 32 KB operand buffer and its 128 TMEM
+// columns:
+//   1. the group stages the tile's features as BF16 (128 x 64, the first 16 KB of the buffer);
+//   2. the group's first thread issues layer 1, D[128 x 128] = X W1 (4 MMAs of K = 16), and
+//      commits to the group's mbarrier; each thread waits, reads its row of D (tcgen05.ld), adds
+//      the bias, applies SiLU and writes the BF16 row into the buffer (X is no longer needed);
+//   3. layer 2 likewise: D = H1 W2 (8 MMAs, D's columns reused), epilogue back into the buffer;
+//   4. layer 3: D[128 x 16] = H2 W3 (8 MMAs, N padded from 3 to 16); the epilogue adds the bias
+//      and stores the 3 outputs.
+// Each step of a tile waits on the previous one (MMA -> epilogue -> MMA); four tiles in flight per
+// SM keep the tensor core busy across those waits.
 //
 // Shared-memory operand layout: the canonical K-major layout without swizzle.  An operand of R
 // rows by K columns is cut into 8 x 8 "core matrices" (8 rows of 16 bytes, 128 contiguous bytes);
@@ -22,9 +25,9 @@
 // groups) is 128; the slice for MMA step s starts at byte s * 2 * (R / 8) * 128.  B operands are
 // the weights transposed to [N][K] (K-major), written once per CTA.
 //
-// Every wait on the mbarrier is bounded: after kTcSpinLimit polls the kernel records a timeout
-// (the whole CTA decides together), stops taking tiles, waits (bounded again) for the MMAs it has
-// issued, frees its TMEM and returns.
+// Every wait on an mbarrier is bounded: after kTcSpinLimit polls the group records a timeout (its
+// four warps decide together), stops taking tiles, waits (bounded again) for the MMAs it has
+// issued, and the CTA frees its TMEM and returns.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -34,25 +37,25 @@ namespace vbd {
 namespace tc {
 
 constexpr int kRows = 128;                   // samples per tile (MMA M, TMEM lanes)
-constexpr int kThreads = 128;
-constexpr int kN3 = 16;                      // layer-3 MMA N (3 outputs, padded)
-constexpr uint32_t kTmemCols = 256;          // D1 [0, 128), D2 [128, 256), D3 reuses [0, 16)
+constexpr int kGroups = 4;                   // tile pipelines per CTA
+constexpr int kGroupThreads = 128;           // 4 warps, one per TMEM lane quarter
+constexpr int kThreads = kGroups * kGroupThreads;
+constexpr uint32_t kTmemCols = 512;          // 128 per group: D of layer 1, then of layer 2, then 3
 constexpr unsigned kTcSpinLimit = 1u << 26;  // polls of one mbarrier wait before giving up
 
 // shared-memory carve-up (bytes, 1024-aligned blocks)
 constexpr int kSzW1 = 128 * 64 * 2;    // B of layer 1: [128][64]
 constexpr int kSzW2 = 128 * 128 * 2;   // B of layer 2: [128][128]
-constexpr int kSzW3 = kN3 * 128 * 2;   // B of layer 3: [16][128]
-constexpr int kSzA1 = kRows * 64 * 2;  // features
-constexpr int kSzA2 = kRows * 128 * 2; // hidden activations (layer 1 out, then layer 2 out)
+constexpr int kN3 = 16;                 // layer-3 MMA N (3 outputs, padded)
+constexpr int kSzW3 = kN3 * 128 * 2;    // B of layer 3: [16][128]
+constexpr int kSzBuf = kRows * 128 * 2;  // per group: features (16 KB), then hidden activations
 constexpr int kOffW1 = 0;
 constexpr int kOffW2 = kOffW1 + kSzW1;
 constexpr int kOffW3 = kOffW2 + kSzW2;
-constexpr int kOffA1 = kOffW3 + kSzW3;
-constexpr int kOffA2 = kOffA1 + kSzA1;
-constexpr int kOffBias = kOffA2 + kSzA2;             // b1[128] b2[128] b3[16] (float)
-constexpr int kOffBar = kOffBias + (128 + 128 + 16) * 4;  // mbarrier (8 B), TMEM address (4 B)
-constexpr int kSmemBytes = kOffBar + 16 + 1024;      // + slack for aligning the base to 1024 B
+constexpr int kOffBuf = kOffW3 + kSzW3;
+constexpr int kOffBias = kOffBuf + kGroups * kSzBuf;  // b1, b2 as BF16 pairs [64] each, b3[16] float
+constexpr int kOffBar = kOffBias + (128 + 128 + 16) * 4;  // kGroups mbarriers (8 B), TMEM address
+constexpr int kSmemBytes = kOffBar + 8 * kGroups + 16 + 1024;  // + slack for aligning the base
 
 // byte offset of element (r, k) in an R-row K-major no-swizzle operand
 __device__ __forceinline__ uint32_t kmajor_offset(int r, int k, int R) {
@@ -118,25 +121,86 @@ __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
-// 32 consecutive FP32 columns of this thread's TMEM lane (the load and its wait in one statement,
-// so that no use of the registers can be scheduled before the wait)
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
+// barrier of one group's 128 threads (named barrier 1 + group; 0 is the CTA-wide __syncthreads)
+__device__ __forceinline__ void group_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+
+// the group's threads agree: true only if `v` is true in all 128
+__device__ __forceinline__ bool group_all(int id, bool v) {
+    uint32_t r;
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"(v ? 1u : 0u), "r"(id)
+        : "memory");
+    return r != 0;
+}
+
+// 64 consecutive FP32 columns of this thread's TMEM lane (one load, one wait)
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
+    uint32_t r[64];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
+        "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
+        "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n\t"
         "tcgen05.wait::ld.sync.aligned;"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
         : "r"(taddr)
         : "memory");
 #pragma unroll
-    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+    for (int j = 0; j < 64; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-// 16 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+// SiLU(z + b) of two accumulator columns in packed BF16x2 arithmetic: z is rounded to BF16 first,
+// then bias add, z / 2, tanh (hardware approximation), 1/2 + t / 2 and the product run two lanes
+// per instruction.  Each step rounds to BF16 (relative 2^-9), about the size of the rounding the
+// activation gets anyway; the SIMT work of this epilogue, not the MMAs, bounds the kernel.
+__device__ __forceinline__ uint32_t silu2_bias_bf16(float z0, float z1, uint32_t bias2) {
+    const __nv_bfloat162 half2 = __floats2bfloat162_rn(0.5f, 0.5f);
+    uint32_t zb = pack_bf16(z0, z1);
+    __nv_bfloat162 z = __hadd2(*reinterpret_cast<__nv_bfloat162*>(&zb), *reinterpret_cast<__nv_bfloat162*>(&bias2));
+    __nv_bfloat162 h = __hmul2(z, half2);
+    uint32_t hu = *reinterpret_cast<uint32_t*>(&h), tu;
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(tu) : "r"(hu));
+    __nv_bfloat162 sg = __hfma2(*reinterpret_cast<__nv_bfloat162*>(&tu), half2, half2);
+    __nv_bfloat162 out = __hmul2(z, sg);
+    return *reinterpret_cast<uint32_t*>(&out);
+}
+
+// bias + SiLU of 64 accumulator columns [c0, c0 + 64) of row r, stored as BF16 into an R = 128 row
+// K-major operand (8 stores of 16 bytes); the bias is read 4 floats at a time (a broadcast: every
+// thread of the warp reads the same address)
+__device__ __forceinline__ void store_hidden64(unsigned char* A, int r, int c0, const float (&acc)[64],
+                                               const uint32_t* bias2) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const uint4 b = *reinterpret_cast<const uint4*>(bias2 + (c0 + q * 8) / 2);  // 8 biases, BF16 pairs
+        const float* x = acc + q * 8;
+        uint4 w;
+        w.x = silu2_bias_bf16(x[0], x[1], b.x);
+        w.y = silu2_bias_bf16(x[2], x[3], b.y);
+        w.z = silu2_bias_bf16(x[4], x[5], b.z);
+        w.w = silu2_bias_bf16(x[6], x[7], b.w);
+        *reinterpret_cast<uint4*>(A + kmajor_offset(r, c0 + q * 8, kRows)) = w;
+    }
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane (one load, one wait)
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     uint32_t r[16];
     asm volatile(
@@ -150,36 +214,6 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-// SiLU(z) = z * sigmoid(z), sigmoid(z) = 1/2 + tanh(z / 2) / 2 with the hardware tanh approximation
-// (relative error ~2^-11, below the BF16 rounding the activations get next)
-__device__ __forceinline__ float silu_fast(float z) {
-    float t;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(0.5f * z));
-    return z * fmaf(0.5f, t, 0.5f);
-}
-
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
-    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-    return *reinterpret_cast<uint32_t*>(&v);
-}
-
-// bias + SiLU of 32 accumulator columns [c0, c0 + 32) of row r, stored as BF16 into an R = 128 row
-// K-major operand (4 stores of 16 bytes)
-__device__ __forceinline__ void store_hidden32(unsigned char* A, int r, int c0, const float (&acc)[32],
-                                               const float* bias) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        uint4 w;
-        uint32_t* wp = reinterpret_cast<uint32_t*>(&w);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int c = q * 8 + 2 * j;
-            wp[j] = pack_bf16(silu_fast(acc[c] + bias[c0 + c]), silu_fast(acc[c + 1] + bias[c0 + c + 1]));
-        }
-        *reinterpret_cast<uint4*>(A + kmajor_offset(r, c0 + q * 8, kRows)) = w;
-    }
-}
-
 struct TcArgs {
     int n;
     const float* params;  // FP32 blob (biases)
@@ -190,45 +224,47 @@ struct TcArgs {
     int off_b1, off_b2, off_b3;
 };
 
-__global__ void __launch_bounds__(kThreads, 2) mlp_infer_tc_kernel(TcArgs a) {
+__global__ void __launch_bounds__(kThreads, 1) mlp_infer_tc_kernel(TcArgs a) {
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned char* sW1 = smem + kOffW1;
     unsigned char* sW2 = smem + kOffW2;
     unsigned char* sW3 = smem + kOffW3;
-    unsigned char* sA1 = smem + kOffA1;
-    unsigned char* sA2 = smem + kOffA2;
-    float* sB1 = reinterpret_cast<float*>(smem + kOffBias);
-    float* sB2 = sB1 + 128;
-    float* sB3 = sB2 + 128;
-    uint64_t* bar_p = reinterpret_cast<uint64_t*>(smem + kOffBar);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kOffBar + 8);
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const uint32_t bar = smem_u32(bar_p);
+    uint32_t* sB1 = reinterpret_cast<uint32_t*>(smem + kOffBias);  // BF16 pairs
+    uint32_t* sB2 = sB1 + 64;
+    float* sB3 = reinterpret_cast<float*>(sB2 + 64);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kOffBar + 8 * kGroups);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int group = warp >> 2, quarter = warp & 3, gtid = tid & (kGroupThreads - 1);
+    const int bar_id = 1 + group;
+    unsigned char* buf = smem + kOffBuf + group * kSzBuf;
+    const uint32_t bar = smem_u32(bars + group);
 
-    // ---- set-up: weights transposed into the B layouts, biases, mbarrier, TMEM -----------------
-    for (int i = tid; i < 64 * 128; i += kThreads) {  // W1[k][n] -> B1[n][k]
-        const int k = i / 128, nn = i % 128;
-        *reinterpret_cast<uint16_t*>(sW1 + kmajor_offset(nn, k, 128)) = a.w16[i];
-    }
-    for (int i = tid; i < 128 * 128; i += kThreads) {  // W2[k][n] -> B2[n][k]
-        const int k = i / 128, nn = i % 128;
-        *reinterpret_cast<uint16_t*>(sW2 + kmajor_offset(nn, k, 128)) = a.w16[64 * 128 + i];
-    }
-    for (int i = tid; i < kN3 * 128; i += kThreads) {  // W3[k][n] (8 columns) -> B3[n][k], rows 8..15 zero
-        const int nn = i / 128, k = i % 128;
-        const uint16_t w = nn < 8 ? a.w16[64 * 128 + 128 * 128 + k * 8 + nn] : uint16_t(0);
-        *reinterpret_cast<uint16_t*>(sW3 + kmajor_offset(nn, k, kN3)) = w;
-    }
-    for (int i = tid; i < 128; i += kThreads) {
-        sB1[i] = a.params[a.off_b1 + i];
-        sB2[i] = a.params[a.off_b2 + i];
+    // ---- set-up: weights transposed into the B layouts, biases, mbarriers, TMEM ---------------
+    // weights [K][N] -> B operands [N][K]: a thread gathers 8 consecutive k of one column n (each
+    // load instruction reads 32 consecutive n of one row: coalesced) and stores them as one 16-byte
+    // chunk of a core matrix (a warp fills 512 contiguous bytes)
+    auto transpose_in = [&](unsigned char* dst, const uint16_t* src, int K, int N, int ld, int R) {
+        for (int i = tid; i < (K / 8) * R; i += kThreads) {
+            const int nn = i % R, kg = i / R;
+            uint4 w;
+            uint16_t* wh = reinterpret_cast<uint16_t*>(&w);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) wh[j] = nn < N ? src[(kg * 8 + j) * ld + nn] : uint16_t(0);
+            *reinterpret_cast<uint4*>(dst + kmajor_offset(nn, kg * 8, R)) = w;
+        }
+    };
+    transpose_in(sW1, a.w16, 64, 128, 128, 128);
+    transpose_in(sW2, a.w16 + 64 * 128, 128, 128, 128, 128);
+    transpose_in(sW3, a.w16 + 64 * 128 + 128 * 128, 128, 8, 8, kN3);  // rows 8..15 zero
+    for (int i = tid; i < 64; i += kThreads) {
+        sB1[i] = pack_bf16(a.params[a.off_b1 + 2 * i], a.params[a.off_b1 + 2 * i + 1]);
+        sB2[i] = pack_bf16(a.params[a.off_b2 + 2 * i], a.params[a.off_b2 + 2 * i + 1]);
     }
     if (tid < kN3) sB3[tid] = tid < 8 ? a.params[a.off_b3 + tid] : 0.f;
-    if (tid == 0) {
-        bar_init(bar, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
+    if (tid < kGroups) bar_init(smem_u32(bars + tid), 1);
+    if (tid == 0) asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                      "r"(kTmemCols));
@@ -238,98 +274,106 @@ __global__ void __launch_bounds__(kThreads, 2) mlp_infer_tc_kernel(TcArgs a) {
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = *tmem_slot;
-    const uint32_t d1 = tmem, d2 = tmem + 128, d3 = tmem;
-    const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;  // this warp's TMEM lanes
+    const uint32_t d = *tmem_slot + static_cast<uint32_t>(group * 128);   // this group's columns
+    const uint32_t lane_base = static_cast<uint32_t>(quarter * 32) << 16;  // this warp's TMEM lanes
     const uint32_t idesc128 = instr_desc(128, 128), idesc16 = instr_desc(128, kN3);
-    const uint32_t a1 = smem_u32(sA1), a2 = smem_u32(sA2), w1 = smem_u32(sW1), w2 = smem_u32(sW2),
-                   w3 = smem_u32(sW3);
+    const uint32_t ab = smem_u32(buf), w1 = smem_u32(sW1), w2 = smem_u32(sW2), w3 = smem_u32(sW3);
+    const bool issuer = gtid == 0;
+    const int r_own = quarter * 32 + lane;  // this thread's row of the tile
     uint32_t phase = 0;
     bool ok = true;
     const int ntiles = (a.n + kRows - 1) / kRows;
 
-    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    for (int tile = blockIdx.x * kGroups + group; tile < ntiles; tile += gridDim.x * kGroups) {
         const int row0 = tile * kRows;
-        // ---- 1. features -> A1 (BF16), 16 threads per row, coalesced float4 loads ----
-        for (int f = tid; f < kRows * 16; f += kThreads) {
-            const int r = f >> 4, c4 = f & 15;
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (row0 + r < a.n) v = __ldg(reinterpret_cast<const float4*>(a.X + static_cast<size_t>(row0 + r) * 64) + c4);
-            uint2 w;
-            w.x = pack_bf16(v.x, v.y);
-            w.y = pack_bf16(v.z, v.w);
-            *reinterpret_cast<uint2*>(sA1 + kmajor_offset(r, 4 * c4, kRows)) = w;
+        // ---- 1. features -> the buffer as BF16.  Warp q stages rows [32 q, 32 q + 32): in pass j
+        // a lane takes row 32 q + 8 (j / 4) + lane % 8 and float4 column 4 (j % 4) + lane / 8, so each
+        // load reads 8 rows x 64 contiguous bytes and each store fills whole core-matrix rows; the
+        // 16 loads are in flight together (the other groups' work covers their latency) ----
+        {
+            float4 v[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int r = quarter * 32 + 8 * (j >> 2) + (lane & 7);
+                const int c4 = 4 * (j & 3) + (lane >> 3);
+                v[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (row0 + r < a.n)
+                    v[j] = __ldg(reinterpret_cast<const float4*>(a.X + static_cast<size_t>(row0 + r) * 64) + c4);
+            }
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int r = quarter * 32 + 8 * (j >> 2) + (lane & 7);
+                const int c4 = 4 * (j & 3) + (lane >> 3);
+                uint2 w;
+                w.x = pack_bf16(v[j].x, v[j].y);
+                w.y = pack_bf16(v[j].z, v[j].w);
+                *reinterpret_cast<uint2*>(buf + kmajor_offset(r, 4 * c4, kRows)) = w;
+            }
         }
         fence_proxy_async();
         fence_before();
-        __syncthreads();
+        group_sync(bar_id);
         // ---- 2. layer 1 ----
-        if (tid == 0) {
+        if (issuer) {
             fence_after();
 #pragma unroll
             for (int s = 0; s < 4; ++s)
-                mma_bf16(d1, smem_desc(a1 + s * 2 * 2048, 2048, 128), smem_desc(w1 + s * 2 * 2048, 2048, 128),
-                         idesc128, s > 0 ? 1u : 0u);
+                mma_bf16(d, smem_desc(ab + s * 2 * 2048, 2048, 128), smem_desc(w1 + s * 2 * 2048, 2048, 128), idesc128,
+                         s > 0 ? 1u : 0u);
             mma_commit(bar);
         }
-        ok = __syncthreads_and(bar_wait(bar, phase) ? 1 : 0) != 0;  // one decision for the whole CTA
+        ok = group_all(bar_id, bar_wait(bar, phase));  // one decision for the whole group
         if (!ok) break;
         phase ^= 1u;
         fence_after();
-        {
-            const int r = tid;
 #pragma unroll 1
-            for (int c0 = 0; c0 < 128; c0 += 32) {
-                float acc[32];
-                tmem_ld32(d1 + lane_base + c0, acc);
-                store_hidden32(sA2, r, c0, acc, sB1);
-            }
+        for (int c0 = 0; c0 < 128; c0 += 64) {
+            float acc[64];
+            tmem_ld64(d + lane_base + c0, acc);
+            store_hidden64(buf, r_own, c0, acc, sB1);  // layer 1's MMAs have completed: X is free
         }
         fence_proxy_async();
         fence_before();
-        __syncthreads();
-        // ---- 3. layer 2 ----
-        if (tid == 0) {
+        group_sync(bar_id);
+        // ---- 3. layer 2 (D's columns reused: layer 1's epilogue has read them) ----
+        if (issuer) {
             fence_after();
 #pragma unroll
             for (int s = 0; s < 8; ++s)
-                mma_bf16(d2, smem_desc(a2 + s * 2 * 2048, 2048, 128), smem_desc(w2 + s * 2 * 2048, 2048, 128),
-                         idesc128, s > 0 ? 1u : 0u);
+                mma_bf16(d, smem_desc(ab + s * 2 * 2048, 2048, 128), smem_desc(w2 + s * 2 * 2048, 2048, 128), idesc128,
+                         s > 0 ? 1u : 0u);
             mma_commit(bar);
         }
-        ok = __syncthreads_and(bar_wait(bar, phase) ? 1 : 0) != 0;  // one decision for the whole CTA
+        ok = group_all(bar_id, bar_wait(bar, phase));
         if (!ok) break;
         phase ^= 1u;
         fence_after();
-        {
-            const int r = tid;
 #pragma unroll 1
-            for (int c0 = 0; c0 < 128; c0 += 32) {
-                float acc[32];
-                tmem_ld32(d2 + lane_base + c0, acc);
-                store_hidden32(sA2, r, c0, acc, sB2);  // layer 2's MMAs have completed: A2 is free
-            }
+        for (int c0 = 0; c0 < 128; c0 += 64) {
+            float acc[64];
+            tmem_ld64(d + lane_base + c0, acc);
+            store_hidden64(buf, r_own, c0, acc, sB2);  // layer 2's MMAs have completed: H1 is free
         }
         fence_proxy_async();
         fence_before();
-        __syncthreads();
+        group_sync(bar_id);
         // ---- 4. layer 3 ----
-        if (tid == 0) {
+        if (issuer) {
             fence_after();
 #pragma unroll
             for (int s = 0; s < 8; ++s)
-                mma_bf16(d3, smem_desc(a2 + s * 2 * 2048, 2048, 128), smem_desc(w3 + s * 2 * 256, 256, 128),
-                         idesc16, s > 0 ? 1u : 0u);
+                mma_bf16(d, smem_desc(ab + s * 2 * 2048, 2048, 128), smem_desc(w3 + s * 2 * 256, 256, 128), idesc16,
+                         s > 0 ? 1u : 0u);
             mma_commit(bar);
         }
-        ok = __syncthreads_and(bar_wait(bar, phase) ? 1 : 0) != 0;  // one decision for the whole CTA
+        ok = group_all(bar_id, bar_wait(bar, phase));
         if (!ok) break;
         phase ^= 1u;
         fence_after();
         {
             float y[16];
-            tmem_ld16(d3 + lane_base, y);
-            const int r = row0 + tid;
+            tmem_ld16(d + lane_base, y);
+            const int r = row0 + r_own;
             if (r < a.n) {
                 float* out = a.Y + static_cast<size_t>(r) * 3;
                 out[0] = y[0] + sB3[0];
@@ -338,19 +382,19 @@ __global__ void __launch_bounds__(kThreads, 2) mlp_infer_tc_kernel(TcArgs a) {
             }
         }
         fence_before();
-        __syncthreads();  // D1..D3 and A1/A2 are free for the next tile
+        group_sync(bar_id);  // the buffer and D are free for the group's next tile
     }
     if (!ok) {
-        // a wait gave up: record it, then wait (bounded) for the MMAs this CTA issued before freeing
-        // their TMEM (the last commit tracks all of them)
-        if (tid == 0 && a.status) atomicAdd(a.status, 1u);
+        // a wait gave up: record it, then wait (bounded) for the MMAs the group issued before the
+        // CTA frees the TMEM (the last commit tracks all of them)
+        if (issuer && a.status) atomicAdd(a.status, 1u);
         bar_wait(bar, phase);
     }
     fence_before();
     __syncthreads();
     if (warp == 0) {
         fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot), "r"(kTmemCols));
     }
 }
 

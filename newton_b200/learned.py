@@ -281,42 +281,3 @@ def calibrate_iterations(model, q0, solver, pipe, mlp: WarmStartMLP, steps: int,
         corr = s1.particle_q - y
         s0, s1 = s1, s0
     return int(np.ceil(np.percentile(need, 90))), records
-
-
-def _main() -> None:
-    """Time the warm-start network's inference and training passes on random rows."""
-    import argparse
-
-    ap = argparse.ArgumentParser(description="time the warm-start MLP kernels")
-    ap.add_argument("--rows", type=int, default=262144)
-    ap.add_argument("--repeats", type=int, default=20)
-    args = ap.parse_args()
-    dev = torch.device("cuda:0")
-    mlp = WarmStartMLP(dev, seed=0)
-    gen = torch.Generator(device=dev).manual_seed(0)
-    X = torch.randn(args.rows, IN, device=dev, generator=gen)
-    T = torch.randn(args.rows, OUT, device=dev, generator=gen)
-    for _ in range(3):
-        mlp.forward(X)
-        mlp.gradients(X, T)
-    torch.cuda.synchronize()
-    flops = 2 * (IN * HID + HID * HID + HID * OUT) * args.rows
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.repeats):
-        mlp.forward(X)
-    e1.record()
-    e1.synchronize()
-    ms = e0.elapsed_time(e1) / args.repeats
-    print(f"forward  {args.rows} rows: {ms * 1e3:8.1f} us  {flops / ms / 1e9:6.1f} TFLOP/s")
-    e0.record()
-    for _ in range(args.repeats):
-        mlp.gradients(X, T)
-    e1.record()
-    e1.synchronize()
-    ms = e0.elapsed_time(e1) / args.repeats
-    print(f"gradients {args.rows} rows: {ms * 1e3:8.1f} us  {3 * flops / ms / 1e9:6.1f} TFLOP/s (3x forward flops)")
-
-
-if __name__ == "__main__":
-    _main()
