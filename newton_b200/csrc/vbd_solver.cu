@@ -47,6 +47,7 @@ struct GateState {
     unsigned long long sum[kGateSlots * kSumStride];  // fixed-point sums of the residuals (resid_fixed)
     unsigned maxv[kGateSlots * kMaxStride];  // max residual (float bits; atomicMax target)
     int iters;               // iterations run so far in this step
+    unsigned done;           // blocks of the deciding sweep that have finished (last-block election)
     int pad;
     float ref;               // relative mode: the step's reference residual
     int last_iters;          // iterations of the last finished step
@@ -251,6 +252,18 @@ __global__ void pack_contacts_kernel(PackArgs a) {
     }
 }
 
+// What a residual check needs besides the state (baked into the step graph).
+struct GateParams {
+    float tol;
+    int max_iters;
+    int relative;
+    int mean;
+    int count;    // solved vertices (the mean's divisor)
+    int first;    // 1: the start evaluation; 0: a later one; -1: sweep residuals (first iff iters == 0)
+    int set_ref;  // the first evaluation is also the relative mode's reference
+    int add;      // iterations since the last check
+};
+
 struct SweepArgs {
     float4* pos;
     const float4* prev;
@@ -291,6 +304,10 @@ struct SweepArgs {
     const int* perm;
     float inv_g;             // 1/|g| (0 when g = 0)
     int no_pdl;              // host side: launch without the programmatic-dependent-launch attribute
+    // residual gate, sweep mode: the round's last color also decides (last block to finish)
+    GateState* gate_state;   // NULL: this sweep does not decide
+    cudaGraphConditionalHandle gate_handle;
+    GateParams gate_params;
 };
 
 template <bool kDamp>
@@ -510,6 +527,47 @@ __device__ __forceinline__ unsigned long long resid_fixed(float r) {
     return static_cast<unsigned long long>(c * kResidSumScale + 0.5f);
 }
 
+// Warp-collective (one full warp): the gate's residual norm of the current evaluation -- the max,
+// or the sum over the solved vertices divided by their number -- from the slots, which are
+// cleared for the next evaluation.  Every lane returns the norm.
+__device__ __forceinline__ float gate_take_warp(GateState* g, int mean, int count) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    unsigned long long sum = g->sum[lane * kSumStride] + g->sum[(lane + 32) * kSumStride];
+    const unsigned mx0 = max(g->maxv[lane * kMaxStride], g->maxv[(lane + 32) * kMaxStride]);
+    g->sum[lane * kSumStride] = 0ull;
+    g->sum[(lane + 32) * kSumStride] = 0ull;
+    g->maxv[lane * kMaxStride] = 0u;
+    g->maxv[(lane + 32) * kMaxStride] = 0u;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(full, sum, off);
+    const unsigned mx = __reduce_max_sync(full, mx0);
+    if (!mean) return __uint_as_float(mx);
+    if (count <= 0) return 0.0f;
+    return static_cast<float>(static_cast<double>(sum) / kResidSumScale / static_cast<double>(count));
+}
+
+// One thread: record the check of residual norm r and set the while node's condition.
+__device__ __forceinline__ void gate_decide(GateState* g, cudaGraphConditionalHandle handle, float r,
+                                            const GateParams& p) {
+    const bool is_first = p.first == 1 || (p.first == -1 && g->iters == 0);
+    if (is_first) {
+        g->start_resid = r;
+        if (p.set_ref) g->ref = r;
+    }
+    if (p.first != 1) g->iters += p.add;
+    const float thresh = p.relative ? p.tol * g->ref : p.tol;
+    const bool more = (r > thresh) && (g->iters < p.max_iters);
+    if (!more) {
+        g->last_iters = g->iters;
+        g->last_resid = r;
+        g->steps += 1ull;
+        g->iter_sum += static_cast<unsigned long long>(g->iters);
+        if (r > thresh) g->capped += 1ull;
+    }
+    cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
 // Warp-collective: every thread of the warp calls it (r = 0 and counted = false where the thread
 // holds no vertex).  Max (float bits as unsigned: exact for r >= 0; NaN bits exceed +inf) and the
 // fixed-point sum go to the accumulators with one atomic each per warp: the single max of
@@ -638,6 +696,25 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
             }
         }
         reduce_residual(a, rg, counted);
+        if (a.gate_state) {
+            // the round's last color: the last block to finish reduces the slots and decides (every
+            // block's slot atomics are fenced before it counts itself done)
+            __shared__ unsigned s_last;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                s_last = (atomicAdd(&a.gate_state->done, 1u) == gridDim.x - 1) ? 1u : 0u;
+            }
+            __syncthreads();
+            if (s_last && threadIdx.x < 32) {
+                __threadfence();
+                const float r = gate_take_warp(a.gate_state, a.gate_params.mean, a.gate_params.count);
+                if (threadIdx.x == 0) {
+                    gate_decide(a.gate_state, a.gate_handle, r, a.gate_params);
+                    a.gate_state->done = 0u;
+                }
+            }
+        }
         return;
     }
     if (!valid || lane != 0) return;
@@ -908,54 +985,19 @@ __global__ void gather_positions_kernel(const int* perm, const float4* pos, floa
     q[3 * o + 2] = p.z;
 }
 
-// the gate's residual norm of the current evaluation -- the max, or the sum over the solved
-// vertices divided by their number `count` -- read from the slots, which are cleared for the next
-// evaluation (one thread)
-__device__ __forceinline__ float gate_take(GateState* g, int mean, int count) {
-    unsigned long long sum = 0ull;
-    unsigned mx = 0u;
-    for (int k = 0; k < kGateSlots; ++k) {
-        sum += g->sum[k * kSumStride];
-        mx = max(mx, g->maxv[k * kMaxStride]);
-        g->sum[k * kSumStride] = 0ull;
-        g->maxv[k * kMaxStride] = 0u;
-    }
-    if (!mean) return __uint_as_float(mx);
-    if (count <= 0) return 0.0f;
-    return static_cast<float>(static_cast<double>(sum) / kResidSumScale / static_cast<double>(count));
-}
-
-// Residual gate: after an evaluation of the residual -- a Jacobi evaluation (a kResidual sweep
-// over every solved vertex) or the Gauss-Seidel residual the last iteration's sweeps accumulated
-// -- decide whether the loop runs another round and set the while node's condition.
-//   first = 1: the Jacobi evaluation at the iterate the iterations start from (nothing counted
-//              yet); first = 0: a later check; first = -1: sweep residuals, the first check of the
-//              step (iters == 0) is the one of the first iteration, which starts at the start iterate
-//   set_ref:   the first check also sets the relative mode's reference
-//   add:       iterations run since the last check
-__global__ void gate_check_kernel(GateState* g, cudaGraphConditionalHandle handle, float tol, int max_iters,
-                                  int relative, int mean, int count, int first, int set_ref, int add) {
-    const float r = gate_take(g, mean, count);
-    const bool is_first = first == 1 || (first == -1 && g->iters == 0);
-    if (is_first) {
-        g->start_resid = r;
-        if (set_ref) g->ref = r;
-    }
-    if (first != 1) g->iters += add;
-    const float thresh = relative ? tol * g->ref : tol;
-    const bool more = (r > thresh) && (g->iters < max_iters);
-    if (!more) {
-        g->last_iters = g->iters;
-        g->last_resid = r;
-        g->steps += 1ull;
-        g->iter_sum += static_cast<unsigned long long>(g->iters);
-        if (r > thresh) g->capped += 1ull;
-    }
-    cudaGraphSetConditional(handle, more ? 1u : 0u);
+// Residual gate: after an evaluation of the residual (a Jacobi evaluation, a kResidual sweep over
+// every solved vertex; or the Gauss-Seidel residual the last round's sweeps accumulated) decide
+// whether the loop runs another round.  One warp.
+__global__ void gate_check_kernel(GateState* g, cudaGraphConditionalHandle handle, GateParams p) {
+    const float r = gate_take_warp(g, p.mean, p.count);
+    if (threadIdx.x == 0) gate_decide(g, handle, r, p);
 }
 
 // relative mode with a warm start: the residual at the plain start y becomes the reference
-__global__ void gate_ref_kernel(GateState* g, int mean, int count) { g->ref = gate_take(g, mean, count); }
+__global__ void gate_ref_kernel(GateState* g, int mean, int count) {
+    const float r = gate_take_warp(g, mean, count);
+    if (threadIdx.x == 0) g->ref = r;
+}
 
 // ---------------------------------------------------------------------------------------------
 // host orchestration
@@ -1003,6 +1045,19 @@ static SweepArgs make_sweep_args(const SolverImpl& s, const VbdContacts* c, floa
     a.inv_g = m.gravity_norm > 0.f ? 1.0f / m.gravity_norm : 0.f;
     a.no_pdl = s.pdl ? 0 : 1;
     return a;
+}
+
+static GateParams gate_params(const SolverImpl& s, int first, int set_ref, int add) {
+    GateParams p;
+    p.tol = s.gate_tol;
+    p.max_iters = s.gate_max;
+    p.relative = s.gate_relative;
+    p.mean = s.gate_mean;
+    p.count = s.gate_count;
+    p.first = first;
+    p.set_ref = set_ref;
+    p.add = add;
+    return p;
 }
 
 // blocks of `kernel` resident on the whole device at `block` threads (cached per kernel / block)
@@ -1174,15 +1229,28 @@ static int enqueue_forward(SolverImpl& s, const float* q_in, const float* qd_in,
     return VBD_OK;
 }
 
-// gate: also accumulate the color's Gauss-Seidel residual into the residual gate (sweep mode)
+// The decision a round's last sweep makes in sweep mode (GateState, while-node handle, params).
+struct GateCheck {
+    GateState* state;
+    cudaGraphConditionalHandle handle;
+    GateParams params;
+};
+
+// gate: also accumulate the color's Gauss-Seidel residual into the residual gate (sweep mode);
+// check: this sweep also takes the round's decision
 static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float dt, cudaStream_t st,
-                          bool first_iteration = true, bool gate = false) {
+                          bool first_iteration = true, bool gate = false, const GateCheck* check = nullptr) {
     const VbdModelImpl& m = *s.m;
     SweepArgs a = make_sweep_args(s, c, dt);
     a.prefetch_records = first_iteration ? 1 : 0;
     if (gate) {
         a.gate_max = s.gate_mean ? nullptr : s.gate->maxv;
         a.gate_sum = s.gate_mean ? s.gate->sum : nullptr;
+    }
+    if (check) {
+        a.gate_state = check->state;
+        a.gate_handle = check->handle;
+        a.gate_params = check->params;
     }
     a.v_begin = m.color_start[color];
     a.v_end = m.color_start[color + 1];
@@ -1286,8 +1354,7 @@ static int enqueue_gated_iterations(SolverImpl& s, const VbdContacts* c, float d
         // the Jacobi residual at the start iterate (in sweep mode only when no iteration may run,
         // so that the step is still recorded)
         enqueue_gate_residual(s, c, dt, st);
-        gate_check_kernel<<<1, 1, 0, st>>>(s.gate, handle, s.gate_tol, s.gate_max, s.gate_relative, s.gate_mean,
-                                           s.gate_count, 1, set_ref ? 1 : 0, 0);
+        gate_check_kernel<<<1, 32, 0, st>>>(s.gate, handle, gate_params(s, 1, set_ref ? 1 : 0, 0));
         VBD_CUDA_TRY(cudaGetLastError());
         VBD_CUDA_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps));
     }
@@ -1303,12 +1370,18 @@ static int enqueue_gated_iterations(SolverImpl& s, const VbdContacts* c, float d
     VBD_CUDA_TRY(cudaStreamBeginCaptureToGraph(s.body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < s.gate_every; ++k) {
         const bool last = k == s.gate_every - 1;
-        for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, s.body_stream, false, sweep && last);
+        for (int color = 0; color < s.m->C; ++color) {
+            // sweep mode: the round's last sweep also decides (no separate check kernel)
+            const bool decides = sweep && last && color == s.m->C - 1;
+            GateCheck chk{decides ? s.gate : nullptr, handle,
+                          gate_params(s, -1, (sweep && set_ref) ? 1 : 0, s.gate_every)};
+            enqueue_color(s, color, c, dt, s.body_stream, false, sweep && last, decides ? &chk : nullptr);
+        }
     }
-    if (!sweep) enqueue_gate_residual(s, c, dt, s.body_stream);
-    gate_check_kernel<<<1, 1, 0, s.body_stream>>>(s.gate, handle, s.gate_tol, s.gate_max, s.gate_relative,
-                                                 s.gate_mean, s.gate_count, sweep ? -1 : 0,
-                                                 (sweep && set_ref) ? 1 : 0, s.gate_every);
+    if (!sweep) {
+        enqueue_gate_residual(s, c, dt, s.body_stream);
+        gate_check_kernel<<<1, 32, 0, s.body_stream>>>(s.gate, handle, gate_params(s, 0, 0, s.gate_every));
+    }
     const cudaError_t e1 = cudaGetLastError();
     cudaGraph_t captured = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(s.body_stream, &captured);
@@ -1333,7 +1406,7 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
             if (s.gate_relative) {
                 // the relative tolerance refers to the plain start y, before the warm start moves it
                 enqueue_gate_residual(s, c, dt, st);
-                gate_ref_kernel<<<1, 1, 0, st>>>(s.gate, s.gate_mean, s.gate_count);
+                gate_ref_kernel<<<1, 32, 0, st>>>(s.gate, s.gate_mean, s.gate_count);
             }
         }
         int rc = mlp_features_launch(*s.m, s.prev, s.y, c ? s.ccount : nullptr, s.ws_corr, s.ws_mean, s.ws_inv_std,
@@ -1398,7 +1471,7 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
         const bool sweep = s.gate_sweep && s.lanes > 0;
         if (s.gate_relative && sweep) {
             enqueue_gate_residual(s, c, dt, st);
-            gate_ref_kernel<<<1, 1, 0, st>>>(s.gate, s.gate_mean, s.gate_count);
+            gate_ref_kernel<<<1, 32, 0, st>>>(s.gate, s.gate_mean, s.gate_count);
         }
         const int rc = enqueue_gated_iterations(s, c, dt, st, !sweep);
         if (rc) return rc;
