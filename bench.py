@@ -28,8 +28,14 @@ the cloth (a single cloth does not shard), so per-GPU work is fixed ("weak" scal
 At N = 1 the line also carries ``workloads``: the batched-worlds workload (512 independent cloth
 worlds, 1.89 M vertices, one launch per color for all worlds) and the cloth-on-boxes workload
 (1024 x 1024 cloth, 1.05 M vertices, on 16 boxes with self-contact; the gate is not available
-with self-contact, so it runs the reference's fixed 10 iterations), each with the same fields,
-and ``learned``: the learned warm start against plain VBD at the same residual tolerance.
+with self-contact, so it runs the reference's fixed 10 iterations), each with the same fields.
+``learned`` (on the line and on the batched-worlds entry) is the learned warm start against
+plain VBD at the same residual, one network per feature set ("kinematic", the headline, and
+"corrections"), trained on plain-VBD trajectories of other seeds: two drapes of 300 steps, and
+256 batched worlds for 800 steps (204,800 cloth steps).  "Same residual" is made exact by
+stepping both arms from the same recorded plain-VBD states (the relative gate then fixes the
+same absolute tolerance for both); the learned solver on its own trajectory is reported beside
+it, with the residual at y its states reach.
 
 ``--impl reference`` times the CPU oracle (the reference's VBD step restated in C++, OpenMP over
 the vertices of a color) on the host cores, on the same workload, gate and trajectory; the scene
@@ -290,14 +296,15 @@ def workload_config(workload: str, model, gate) -> dict:
 # ------------------------------------------------------------------------------------------------
 # GPU arm
 # ------------------------------------------------------------------------------------------------
-def _launches_per_step(solver, gate_stats, steps: int, colors: int) -> int:
+def _launches_per_step(solver, gate_stats, steps: int, colors: int) -> float:
     """Kernels one step launched: the collide kernel + the step graph's top-level kernel nodes +
-    (gated) the loop body's kernels per round."""
+    (gated) the loop body's kernels per pass of the body (sweeps of a body pass that return at
+    once after the gate's decision count as launches)."""
     top = solver.step_kernel_count()
     if gate_stats is None:
         return 1 + (top if top >= 0 else 3 + ITERATIONS * colors)
-    rounds = gate_stats["iterations"] / max(gate_stats["steps"], 1)  # check_every = 1
-    return int(round(1 + top + rounds * gate_stats["body_kernels"])) if top >= 0 else -1
+    passes = gate_stats["body_passes"] / max(gate_stats["steps"], 1)
+    return 1 + top + passes * gate_stats["body_kernels"] if top >= 0 else -1
 
 
 def measure_workload(workload: str, dev, W: int, K: int, world: int, rank: int, local: int, args, cpu: bool) -> dict:
@@ -464,7 +471,7 @@ def measure_workload(workload: str, dev, W: int, K: int, world: int, rank: int, 
         "roofline": roofline,
         "e2e": {"value": (1e3 if batched else world * 1e3) / e2e_ms, "unit": "steps/s",
                 "h2d_bytes_per_step": 2 * V * 12, "d2h_bytes_per_step": 2 * V * 12},
-        "gpu_launches": K * launches if launches >= 0 else None,
+        "gpu_launches": int(round(K * launches)) if launches >= 0 else None,
         "clocks": clocks,
         "autotune": tune,
         "status": solver.status(),
@@ -507,81 +514,178 @@ def cpu_boxes_sample(dev, args) -> dict:
     return cb
 
 
-def learned_ab(dev, plain: dict, K: int, W: int) -> dict:
-    """The learned warm start against plain VBD at the same residual tolerance (the BASELINE metric):
-    trains the warm-start network on plain-VBD trajectories of the draped-cloth distribution, then
-    steps the held-out headline trajectory from the same start state with the learned step mode
-    under the same residual gate, and compares steps/s and iterations per step."""
+# training trajectories of the learned warm start (held out from the timed scenes: other seeds)
+FEATURE_SETS = ("kinematic", "corrections")  # the first is the headline arm
+LEARN_TRAIN = {
+    # two 256x256 drapes (other seeds and sphere offsets), 300 plain-VBD steps each
+    "draped-cloth": {"steps": 300, "samples_per_step": 2048},
+    # 256 worlds of the batched distribution (seed 1) for 800 steps: 204,800 cloth steps
+    "batched-worlds": {"steps": 800, "samples_per_step": 2048, "worlds": 256},
+}
+
+
+def learned_training_data(workload: str, dev):
+    """Plain-VBD trajectories of the workload's distribution (other seeds than the timed scene):
+    features of every feature set on the same samples, and the 20-iteration targets."""
     import torch
 
     from newton_b200 import CollisionPipeline, scenes
     from newton_b200 import learned as L
     from newton_b200.solvers import SolverVBD
 
-    t0 = time.time()
-    Xs, Ts = [], []
-    for seed, off in ((1, (0.2, -0.1)), (4, (-0.15, 0.25))):
-        model, q0 = scenes.draped_cloth(n=256, seed=seed, device=dev, offset=off, height=0.904)
+    cfg = LEARN_TRAIN[workload]
+    if workload == "draped-cloth":
+        runs = [scenes.draped_cloth(n=256, seed=seed, device=dev, offset=off, height=0.904)
+                for seed, off in ((1, (0.2, -0.1)), (4, (-0.15, 0.25)))]
+    else:
+        runs = [scenes.batched_worlds(cfg["worlds"], seed=1, device=dev)]
+    Xs, Ts = {fs: [] for fs in FEATURE_SETS}, []
+    cloth_steps = 0
+    vertices = 0
+    for i, (model, q0) in enumerate(runs):
         solver = SolverVBD(model, iterations=ITERATIONS)
         pipe = CollisionPipeline(model, soft_contact_margin=MARGIN)
-        X, T = L.generate_dataset(model, q0, solver, pipe, steps=300, dt=DT, target_iterations=20,
-                                  samples_per_step=2048, seed=seed, trajectory_iterations=ITERATIONS)
-        Xs.append(X)
+        X, T = L.generate_dataset(model, q0, solver, pipe, steps=cfg["steps"], dt=DT, target_iterations=20,
+                                  samples_per_step=cfg["samples_per_step"], seed=1 + i,
+                                  trajectory_iterations=ITERATIONS, feature_set=FEATURE_SETS)
+        for fs in FEATURE_SETS:
+            Xs[fs].append(X[fs])
         Ts.append(T)
-    X, T = torch.cat(Xs), torch.cat(Ts)
-    t_data = time.time() - t0
-    mlp = L.WarmStartMLP(dev, seed=0)
-    mlp.set_standardization(X)
-    t1 = time.time()
-    hist = mlp.train(mlp.standardize(X), T, epochs=20, batch=32768, lr=2e-3)
-    torch.cuda.synchronize()
-    t_train = time.time() - t1
+        cloth_steps += cfg["steps"] * (cfg.get("worlds", 1))
+        vertices = model.particle_count
+    X = {fs: torch.cat(Xs[fs]) for fs in FEATURE_SETS}
+    T = torch.cat(Ts)
+    info = {"cloth_steps": cloth_steps, "trajectory_steps": cfg["steps"] * len(runs),
+            "samples": int(T.shape[0]), "samples_per_step": cfg["samples_per_step"],
+            "sample_rate": cfg["samples_per_step"] / vertices,
+            "target": "x after 20 plain iterations from y, minus y, over L; trajectories advance with 10"}
+    return X, T, info
 
-    model, q_start, qd_start = plain["_states_start"]
-    gate = gate_config("draped-cloth")
-    solver = SolverVBD(model, iterations=ITERATIONS)
-    solver.set_warm_start(mlp, ITERATIONS)
-    solver.set_residual_gate(**gate)
+
+class _StepTimer:
+    """CUDA events around each step, L2 flushed before each (the timed loops' protocol)."""
+
+    def __init__(self, dev, flush):
+        import torch
+
+        self.torch, self.stream, self.flush, self.evs = torch, torch.cuda.current_stream(dev), flush, []
+
+    def before(self):
+        self.flush.zero_()
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record(self.stream)
+        self.evs.append([e])
+
+    def after(self):
+        e = self.torch.cuda.Event(enable_timing=True)
+        e.record(self.stream)
+        self.evs[-1].append(e)
+
+    def ms(self) -> float:
+        self.torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in self.evs) / max(len(self.evs), 1)
+
+
+def learned_ab(dev, workload: str, plain: dict, start_state, K: int) -> dict:
+    """The learned warm start against plain VBD at the same residual tolerance (the BASELINE metric).
+
+    One warm-start network per feature set is trained on plain-VBD trajectories of the workload's
+    distribution (other seeds).  Then, from the plain arm's start state, the plain gated
+    trajectory is recorded (3 + K steps), and every arm takes one gated step from each recorded
+    state ("teacher forced"): both start each step from the same state, so the relative gate holds
+    them to the same absolute force residual, and the iterations and times of the last K steps
+    are compared.  The learned solver running its own trajectory ("free_running") is reported
+    beside it with the residual at y its states end with (the relative gate refers to it)."""
+    import torch
+
+    from newton_b200 import CollisionPipeline
+    from newton_b200 import learned as L
+    from newton_b200.solvers import SolverVBD
+
+    t0 = time.time()
+    X, T, info = learned_training_data(workload, dev)
+    info["data_s"] = time.time() - t0
+    model, q_start, qd_start = start_state
+    gate = gate_config(workload)
+    launch = plain["launch"]
+    batched = workload == "batched-worlds"
     pipe = CollisionPipeline(model, soft_contact_margin=MARGIN)
-    c = pipe.contacts()
-    s0, s1 = model.state(), model.state()
-    stream = torch.cuda.current_stream(dev)
-    for _ in range(2):  # capture the learned step graph, untimed
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    W = 3
+    states = L.record_plain_states(model, q_start, qd_start, pipe, gate, W + K, DT, launch)
+    tp = _StepTimer(dev, flush)
+    plain_tf = L.teacher_forced_steps(model, states, pipe, gate, DT, None, launch, warm=W, timer=tp)
+    plain_ms = tp.ms()
+    arms = {}
+    for fs in FEATURE_SETS:
+        mlp = L.WarmStartMLP(dev, seed=0, feature_set=fs)
+        mlp.set_standardization(X[fs])
+        t1 = time.time()
+        hist = mlp.train(mlp.standardize(X[fs]), T, epochs=20, batch=32768, lr=2e-3)
+        torch.cuda.synchronize()
+        t_train = time.time() - t1
+        tl = _StepTimer(dev, flush)
+        tf = L.teacher_forced_steps(model, states, pipe, gate, DT, mlp, launch, warm=W, timer=tl)
+        ms = tl.ms()
+        # free running: the learned solver along its own trajectory from the same start
+        solver = SolverVBD(model, iterations=ITERATIONS)
+        solver.set_launch(launch["lanes_per_vertex"], launch["block_size"])
+        solver.set_warm_start(mlp, ITERATIONS)
+        solver.set_residual_gate(**gate)
+        c = pipe.contacts()
+        s0, s1 = model.state(), model.state()
         s0.particle_q.copy_(q_start)
         s0.particle_qd.copy_(qd_start)
-        pipe.collide(s0, c)
-        solver.step(s0, s1, None, c, DT)
-    s0.particle_q.copy_(q_start)
-    s0.particle_qd.copy_(qd_start)
-    torch.cuda.synchronize()
-    solver.gate_stats(reset=True)
-    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-    for k in range(K):
-        flush.zero_()
-        evs[k][0].record(stream)
-        pipe.collide(s0, c)
-        solver.step(s0, s1, None, c, DT)
-        s0, s1 = s1, s0
-        evs[k][1].record(stream)
-    torch.cuda.synchronize()
-    ms = sum(a.elapsed_time(b) for a, b in evs) / K
-    gs = solver.gate_stats()
-    learned_sps = 1e3 / ms
+        tfr = _StepTimer(dev, flush)
+        for k in range(W + K):
+            if k == W:
+                solver.gate_stats(reset=True)
+            if k >= W:
+                tfr.before()
+            pipe.collide(s0, c)
+            solver.step(s0, s1, None, c, DT)
+            if k >= W:
+                tfr.after()
+            s0, s1 = s1, s0
+        fr_ms = tfr.ms()
+        fr = solver.gate_stats()
+        arms[fs] = {
+            "steps_per_s": 1e3 / ms,
+            "ms_per_step": ms,
+            "mean_iterations": tf["mean_iterations"],
+            "capped_steps": tf["capped_steps"],
+            "speedup_at_equal_residual": plain_ms / ms,
+            "iteration_ratio": tf["mean_iterations"] / plain_tf["mean_iterations"],
+            "status": tf["status"],
+            "free_running": {"steps_per_s": 1e3 / fr_ms, "mean_iterations": fr["mean_iterations"],
+                             "capped_steps": fr["capped_steps"],
+                             "last_reference_residual": fr["last_reference_residual"],
+                             "status": solver.status()},
+            "train": {"train_s": t_train, "epochs": 20, "mse_first_epoch": hist[0], "mse_last_epoch": hist[-1],
+                      "target_variance": float(T.var(0).mean())},
+        }
+        del solver
+    head = arms[FEATURE_SETS[0]]
     flops = 2 * (64 * 128 + 128 * 128 + 128 * 3) * model.particle_count
     return {
         "tolerance": gate,
-        "plain_steps_per_s": plain["value"],
-        "plain_mean_iterations": plain["mean_iterations"],
-        "learned_steps_per_s": learned_sps,
-        "learned_mean_iterations": gs["mean_iterations"],
-        "learned_capped_steps": gs["capped_steps"],
-        "speedup_at_equal_residual": learned_sps / plain["value"],
-        "learned_status": solver.status(),
-        "train": {"samples": int(X.shape[0]), "data_s": t_data, "train_s": t_train, "epochs": 20,
-                  "mse_first_epoch": hist[0], "mse_last_epoch": hist[-1], "target_variance": float(T.var(0).mean())},
+        "protocol": "teacher forced: both arms step from the same recorded plain-VBD states (same y, same "
+                    "absolute tolerance); last K of 3 + K steps, L2 flushed before each",
+        "feature_set": FEATURE_SETS[0],
+        "plain_steps_per_s": 1e3 / plain_ms,
+        "plain_mean_iterations": plain_tf["mean_iterations"],
+        "plain_capped_steps": plain_tf["capped_steps"],
+        "plain_last_reference_residual": plain_tf["last_reference_residual"],
+        "learned_steps_per_s": head["steps_per_s"],
+        "learned_mean_iterations": head["mean_iterations"],
+        "learned_capped_steps": head["capped_steps"],
+        "speedup_at_equal_residual": head["speedup_at_equal_residual"],
+        "learned_status": head["status"],
+        "feature_sets": arms,
+        "training_data": info,
         "mlp_flop_per_step": flops,
-        "note": "both arms start from the same state and iterate until the same mean Gauss-Seidel residual",
+        "unit": "batch steps/s" if batched else "steps/s",
+        "note": "the networks never saw the timed scene",
     }
 
 
@@ -696,19 +800,23 @@ def main() -> None:
         "config": dict(head["config"], parallelism=parallelism),
     }
     line.update({k: v for k, v in head.items() if k not in ("metric", "value", "unit", "ms_per_step", "config")})
+    if rank == 0 and world == 1 and not args.no_learned and args.workload in LEARN_TRAIN:
+        # the learned arm starts where the plain arm's timed steps started
+        line["learned"] = learned_ab(dev, args.workload, head, start_state, K)
+    del start_state
+    torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.no_workloads:
         line["workloads"] = {}
         for wl in ("batched-worlds", "cloth-on-boxes"):
             if wl == args.workload:
                 continue
             r = measure_workload(wl, dev, W, K, 1, 0, local, args, cpu)
-            r.pop("_states")
+            st = r.pop("_states")
+            if not args.no_learned and wl in LEARN_TRAIN:
+                r["learned"] = learned_ab(dev, wl, r, st, K)
+            del st
             line["workloads"][wl] = r
             torch.cuda.empty_cache()
-    if rank == 0 and world == 1 and not args.no_learned and args.workload == "draped-cloth":
-        # the learned arm starts where the plain arm's timed steps started
-        head["_states_start"] = start_state
-        line["learned"] = learned_ab(dev, head, K, W)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -192,7 +192,9 @@ typedef struct VbdGateStats {
     float last_residual;            /* final residual norm of the last step */
     float last_start_residual;      /* residual where the last step's iterations started */
     float last_reference_residual;  /* relative mode: residual at the inertia target y */
-    float reserved;
+    int32_t body_programmatic_edges; /* programmatic-dependent-launch edges of one loop body (last
+                                        capture; 0 after the step fell back to plain launches) */
+    int64_t body_passes;            /* passes of the device-side loop body summed over the steps */
 } VbdGateStats;
 
 typedef struct VbdModel VbdModel;
@@ -289,10 +291,15 @@ int vbd_step_static_status(VbdStatus* out);
  * stream capture it adds the loop to the caller's graph.  tolerance <= 0 turns the gate off (the
  * vbd_step `iterations` argument applies again); while it is on, `iterations` is ignored.  Not
  * available with self-contact (VBD_ERR_UNSUPPORTED).  The iteration count of each step is
- * reported by vbd_gate_stats. */
+ * reported by vbd_gate_stats.  In VBD_GATE_SWEEP mode one pass of the loop body holds R check
+ * rounds (R * check_every iterations, a decision after each round; the sweeps of the rounds after
+ * the decision return at once), because every pass of the body costs a pipeline drain between
+ * its last and first sweep; R is (mode >> VBD_GATE_ROUNDS_SHIFT) & 15, 0 = 4. */
 #define VBD_GATE_RELATIVE 1
 #define VBD_GATE_MEAN 2
 #define VBD_GATE_SWEEP 4
+#define VBD_GATE_ROUNDS_SHIFT 8
+#define VBD_GATE_ROUNDS_MASK 0xF00
 int vbd_set_residual_gate(VbdSolver* solver, float tolerance, int32_t max_iterations, int32_t check_every,
                           int32_t mode);
 /* Gate statistics (synchronizes the device); reset != 0 zeroes the step / iteration sums. */
@@ -325,17 +332,28 @@ int vbd_warm_start(VbdSolver* solver, const float* delta, void* stream);
 
 /* ---- learned warm start (no reference counterpart) -----------------------------------------
  * A per-vertex MLP 64 -> 128 -> 128 -> 3 (SiLU) with BF16 weights and FP32 accumulation on the
- * tensor cores predicts how the coming step's correction x_solved - y differs from the previous
- * step's, in units of the vertex's characteristic element length; the warm start is
- * y + previous correction + prediction * length.  Parameters: an FP32 blob of vbd_mlp_sizes()->params floats
+ * tensor cores predicts the coming step's correction x_solved - y, in units of the vertex's
+ * characteristic element length L; the warm start is y + prediction * L (a zero network leaves
+ * the start at y, plain VBD).  Parameters: an FP32 blob of vbd_mlp_sizes()->params floats
  * (W1 [64][128], b1, W2 [128][128], b2, W3 [128][8] with columns 3..7 zero, b3 [8]) and its BF16
  * copy of the three weight matrices (vbd_mlp_sizes()->weights16 values, refreshed by
  * vbd_mlp_adam or vbd_mlp_pack_weights).  All pointers are DEVICE pointers. */
 int vbd_mlp_sizes(int32_t* params, int32_t* weights16, int32_t* in_features, int32_t* hidden, int32_t* out_features);
-/* Per-vertex features [V][64] (model particle order) of the step prepared by vbd_forward: inertia
- * offset, the previous step's correction corr_prev [V][3] (may be NULL), 8 one-ring edge vectors
- * and their corrections, log-stiffnesses, mass, contact and pin flags.  mean / inv_std [64]
- * standardise them (both NULL = raw). */
+/* Feature sets of the network's input (vbd_set_feature_set).
+ * VBD_FEATURES_CORRECTIONS (default): inertia offset (y - x) / L, the previous step's correction
+ *   corr_prev of the vertex and of 8 one-ring neighbours / L, the 8 one-ring edge vectors / L,
+ *   log-stiffnesses, log10 mass, contact flag, one-ring size, solvable flag.
+ * VBD_FEATURES_KINEMATIC: the vertex's motion only -- previous step's displacement v dt / L,
+ *   velocity v (m/s), inertia offset (y - x) / L -- with the same one-ring edge vectors,
+ *   log-stiffnesses, mass and flags; corr_prev is not read. */
+#define VBD_FEATURES_CORRECTIONS 0
+#define VBD_FEATURES_KINEMATIC 1
+/* Select the feature set of vbd_mlp_features, vbd_mlp_warm_start and the warm-start step mode
+ * (a network is trained on one set and must run with it). */
+int vbd_set_feature_set(VbdSolver* solver, int32_t feature_set);
+/* Per-vertex features [V][64] (model particle order) of the step prepared by vbd_forward, in the
+ * solver's feature set; corr_prev [V][3] (the previous step's correction, model order) may be
+ * NULL.  mean / inv_std [64] standardise them (both NULL = raw). */
 int vbd_mlp_features(VbdSolver* solver, const float* corr_prev, const float* mean, const float* inv_std, float* out,
                      void* stream);
 /* Y [n][3] = MLP(X [n][64]) on the 5th-generation tensor cores (tcgen05.mma, BF16 operands in
@@ -450,6 +468,20 @@ int vbd_mesh_edge_adjacency(const int32_t* tris, int32_t nt, int32_t* edge_indic
  * element order.  values receives 2 ints per record; offsets [particle_count + 1] counts ints. */
 int vbd_mesh_vertex_csr(const int32_t* entries, int32_t n_elements, int32_t per_element, const int32_t* slot_of,
                         int32_t particle_count, int32_t* values, int32_t* offsets);
+
+/* The three set-up tables above on the GPU: the same rules and the same tables, element for
+ * element, from DEVICE arrays (inputs and outputs, same layouts and capacities as the host
+ * versions) on `stream`; counts are returned to host variables (the call synchronizes the
+ * stream).  Temporary memory is allocated (cudaMalloc) and freed within the call.
+ * vbd_mesh_vertex_csr_device: slot_of is a HOST array; n_elements * per_element <= 2^30; values
+ * needs 2 ints per record; num_records (may be NULL) receives the record count. */
+int vbd_mesh_edge_adjacency_device(const int32_t* tris, int32_t nt, int32_t* edge_indices, int32_t* edge_tri,
+                                   int32_t* tri_edge, int32_t* num_edges, int32_t* nonmanifold, void* stream);
+int vbd_mesh_vertex_csr_device(const int32_t* entries, int32_t n_elements, int32_t per_element,
+                               const int32_t* slot_of, int32_t particle_count, int32_t* values, int32_t* offsets,
+                               int32_t* num_records, void* stream);
+int vbd_trimesh_graph_edges_device(int32_t num_nodes, const int32_t* tris, int64_t nt, const int32_t* bend,
+                                   int64_t nb, int32_t* edges_out, int64_t* num_edges_out, void* stream);
 
 #ifdef __cplusplus
 }

@@ -139,7 +139,8 @@ class VbdGateStats(ctypes.Structure):
         ("last_residual", ctypes.c_float),
         ("last_start_residual", ctypes.c_float),
         ("last_reference_residual", ctypes.c_float),
-        ("reserved", ctypes.c_float),
+        ("body_programmatic_edges", ctypes.c_int32),
+        ("body_passes", ctypes.c_int64),
     ]
 
 
@@ -178,6 +179,7 @@ SIGNATURES = {
     "vbd_warm_start": (ctypes.c_int, [_VP, _VP, _VP]),
     "vbd_mlp_sizes": (ctypes.c_int, [c_int32_p, c_int32_p, c_int32_p, c_int32_p, c_int32_p]),
     "vbd_mlp_features": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
+    "vbd_set_feature_set": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "vbd_mlp_forward": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int32, _VP, _VP]),
     "vbd_mlp_forward_mma_sync": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int32, _VP, _VP]),
     "vbd_mlp_timeouts": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.c_int32]),
@@ -222,6 +224,18 @@ SIGNATURES = {
     "vbd_mesh_vertex_csr": (
         ctypes.c_int,
         [c_int32_p, ctypes.c_int32, ctypes.c_int32, c_int32_p, ctypes.c_int32, c_int32_p, c_int32_p],
+    ),
+    "vbd_mesh_edge_adjacency_device": (
+        ctypes.c_int,
+        [_VP, ctypes.c_int32, _VP, _VP, _VP, c_int32_p, c_int32_p, _VP],
+    ),
+    "vbd_mesh_vertex_csr_device": (
+        ctypes.c_int,
+        [_VP, ctypes.c_int32, ctypes.c_int32, c_int32_p, ctypes.c_int32, _VP, _VP, c_int32_p, _VP],
+    ),
+    "vbd_trimesh_graph_edges_device": (
+        ctypes.c_int,
+        [ctypes.c_int32, _VP, ctypes.c_int64, _VP, ctypes.c_int64, _VP, ctypes.POINTER(ctypes.c_int64), _VP],
     ),
 }
 
@@ -359,3 +373,65 @@ def canonical_edges(num_nodes: int, pairs: np.ndarray) -> np.ndarray:
         return out
     check(lib.vbd_coloring_graph_edges(int(num_nodes), pairs.shape[0], as_i32p(pairs), as_i32p(out), ctypes.byref(n)))
     return out[: n.value].copy()
+
+
+# ---- the set-up tables on the GPU (same tables as the host functions above) ----------------------
+def _dev_call(device):
+    import torch
+
+    dev = torch.device(device)
+    return torch, dev, ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+
+def mesh_edge_adjacency_device(tris: np.ndarray, device) -> tuple[np.ndarray, np.ndarray, np.ndarray, int]:
+    """mesh_edge_adjacency computed on ``device`` (vbd_mesh_edge_adjacency_device)."""
+    lib = load()
+    torch, dev, st = _dev_call(device)
+    tris = np.ascontiguousarray(np.asarray(tris, dtype=np.int32).reshape(-1, 3))
+    nt = tris.shape[0]
+    if nt == 0:
+        return np.empty((0, 4), np.int32), np.empty((0, 2), np.int32), np.empty((0, 3), np.int32), 0
+    d_tris = torch.from_numpy(tris).to(dev)
+    d_edges = torch.empty((3 * nt, 4), dtype=torch.int32, device=dev)
+    d_edge_tri = torch.empty((3 * nt, 2), dtype=torch.int32, device=dev)
+    d_tri_edge = torch.empty((nt, 3), dtype=torch.int32, device=dev)
+    ne, bad = ctypes.c_int32(0), ctypes.c_int32(0)
+    check(lib.vbd_mesh_edge_adjacency_device(ptr(d_tris), nt, ptr(d_edges), ptr(d_edge_tri), ptr(d_tri_edge),
+                                             ctypes.byref(ne), ctypes.byref(bad), st))
+    n = ne.value
+    return d_edges[:n].cpu().numpy(), d_edge_tri[:n].cpu().numpy(), d_tri_edge.cpu().numpy(), bad.value
+
+
+def mesh_vertex_csr_device(entries: np.ndarray, slot_of, particle_count: int, device) -> tuple[np.ndarray, np.ndarray]:
+    """mesh_vertex_csr computed on ``device`` (vbd_mesh_vertex_csr_device)."""
+    lib = load()
+    torch, dev, st = _dev_call(device)
+    entries = np.ascontiguousarray(np.asarray(entries, dtype=np.int32))
+    n_el, per = entries.shape
+    slots = np.ascontiguousarray(np.asarray(slot_of, dtype=np.int32).reshape(-1))
+    d_entries = torch.from_numpy(entries).to(dev)
+    d_values = torch.empty(max(2 * n_el * per, 2), dtype=torch.int32, device=dev)
+    d_offsets = torch.empty(particle_count + 1, dtype=torch.int32, device=dev)
+    n_rec = ctypes.c_int32(0)
+    check(lib.vbd_mesh_vertex_csr_device(ptr(d_entries), n_el, per, as_i32p(slots), int(particle_count),
+                                         ptr(d_values), ptr(d_offsets), ctypes.byref(n_rec), st))
+    return d_values[: 2 * n_rec.value].cpu().numpy(), d_offsets.cpu().numpy()
+
+
+def trimesh_graph_edges_device(num_nodes: int, tris: np.ndarray, bend: np.ndarray | None, device) -> np.ndarray:
+    """trimesh_graph_edges computed on ``device`` (vbd_trimesh_graph_edges_device)."""
+    lib = load()
+    torch, dev, st = _dev_call(device)
+    tris = np.ascontiguousarray(np.asarray(tris, dtype=np.int32).reshape(-1, 3))
+    bend = np.ascontiguousarray(np.asarray(bend if bend is not None else np.empty((0, 4)), dtype=np.int32)
+                                .reshape(-1, 4))
+    cap = 3 * tris.shape[0] + 6 * bend.shape[0]
+    if cap == 0:
+        return np.empty((0, 2), np.int32)
+    d_tris = torch.from_numpy(tris).to(dev) if tris.size else None
+    d_bend = torch.from_numpy(bend).to(dev) if bend.size else None
+    d_out = torch.empty((cap, 2), dtype=torch.int32, device=dev)
+    n = ctypes.c_int64(0)
+    check(lib.vbd_trimesh_graph_edges_device(int(num_nodes), ptr(d_tris), tris.shape[0], ptr(d_bend),
+                                             bend.shape[0], ptr(d_out), ctypes.byref(n), st))
+    return d_out[: n.value].cpu().numpy()

@@ -471,20 +471,40 @@ class ModelBuilder:
         return self._add_shape(GeoType.BOX, xform, (hx, hy, hz), cfg, body)
 
     # ---------------------------------------------------------------- connectivity and coloring
-    # The four steps below run in the library's native host code (mesh.py, coloring.py).  They are
-    # methods so that a subclass can supply the same tables another way; the model data the rest
-    # of the builder produces does not depend on how.
+    # The four steps below run in the library's native code (mesh.py, coloring.py): the first three
+    # on the GPU for large meshes (``setup_device``), the coloring on the host.  They are methods so
+    # that a subclass can supply the same tables another way; the model data the rest of the
+    # builder produces does not depend on how.
+
+    # Where the edge table, vertex CSR and conflict edges are computed: "auto" (the current CUDA
+    # device, when one is available, for meshes of at least SETUP_DEVICE_MIN_ELEMENTS elements;
+    # otherwise the host), None (always the host) or a CUDA device.  The tables are the same.
+    setup_device = "auto"
+    SETUP_DEVICE_MIN_ELEMENTS = 1 << 16
+
+    def _setup_dev(self, elements: int):
+        d = self.setup_device
+        if d != "auto":
+            return d
+        if elements < self.SETUP_DEVICE_MIN_ELEMENTS:
+            return None
+        import torch
+
+        return torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else None
+
     def _edge_table(self, tri_indices) -> np.ndarray:
         """Bending-edge table ``[o0, o1, v0, v1]`` of one mesh (``utils/mesh.py:465-531``)."""
-        return MeshAdjacency(tri_indices).edge_indices
+        return MeshAdjacency(tri_indices, device=self._setup_dev(len(tri_indices))).edge_indices
 
     def _vertex_adjacency(self, tri_indices, edge_indices, particle_count: int) -> MeshAdjacency:
         """Per-vertex element CSR of the finalized model (``utils/mesh.py:595-926``)."""
-        return MeshAdjacency(tri_indices, edge_indices).init_vertex_adjacency(particle_count)
+        dev = self._setup_dev(len(tri_indices) + len(edge_indices))
+        return MeshAdjacency(tri_indices, edge_indices, device=dev).init_vertex_adjacency(particle_count)
 
     def _conflict_edges(self, tri_indices, tri_mask, bend_indices, bend_mask) -> np.ndarray:
         """Canonical conflict-graph edges (``graph_coloring.py:99-197``)."""
-        return construct_trimesh_graph_edges(tri_indices, tri_mask, bend_indices, bend_mask)
+        n = (0 if tri_indices is None else len(tri_indices)) + (0 if bend_indices is None else len(bend_indices))
+        return construct_trimesh_graph_edges(tri_indices, tri_mask, bend_indices, bend_mask, device=self._setup_dev(n))
 
     def _color_graph(self, num_nodes, edges, balance_colors, target_ratio, algorithm) -> list[np.ndarray]:
         """Color groups of the conflict graph (``graph_coloring.py:243-311``)."""

@@ -32,7 +32,9 @@ def _canonicalize_edges(edges: np.ndarray) -> np.ndarray:
 
 
 def construct_trimesh_graph_edges(tri_indices, tri_active_mask=None, bending_edge_indices=None,
-                                  bending_edge_active_mask=None) -> np.ndarray:
+                                  bending_edge_active_mask=None, device=None) -> np.ndarray:
+    """The canonical conflict-graph edges; ``device`` (a CUDA device) computes the same edges on
+    the GPU (``vbd_trimesh_graph_edges_device``), None on the host."""
     tris = np.empty((0, 3), np.int32)
     bend = np.empty((0, 4), np.int32)
     if tri_indices is not None:
@@ -49,6 +51,8 @@ def construct_trimesh_graph_edges(tri_indices, tri_active_mask=None, bending_edg
         return np.empty((0, 2), dtype=np.int32)
     num_nodes = int(max(tris.max() if tris.size else -1, bend.max() if bend.size else -1)) + 1
     # the pairs are generated and canonicalised natively (no [3 nt + 6 nb, 2] intermediate)
+    if device is not None:
+        return _lib.trimesh_graph_edges_device(num_nodes, tris, bend, device)
     return _lib.trimesh_graph_edges(num_nodes, tris, bend)
 
 

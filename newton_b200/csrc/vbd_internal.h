@@ -83,8 +83,10 @@ struct VbdModelImpl {
 
 // learned warm start (vbd_mlp.cu): per-vertex features after the forward pass, and the warm-start
 // displacement = network output (in characteristic lengths) * length
+// mode: VBD_FEATURES_CORRECTIONS or VBD_FEATURES_KINEMATIC; dt: the step's (kinematic set)
 int mlp_features_launch(const VbdModelImpl& m, const float4* prev, const float4* y, const int* ccount,
-                        const float* corr_prev, const float* mean, const float* inv_std, float* out, cudaStream_t st);
+                        const float* corr_prev, const float* mean, const float* inv_std, float* out, int mode,
+                        float dt, cudaStream_t st);
 int mlp_scale_launch(const VbdModelImpl& m, const float* pred, float* delta, cudaStream_t st);
 
 }  // namespace vbd

@@ -469,7 +469,57 @@ struct FeatArgs {
     const float* mean;       // [64] or NULL
     const float* inv_std;    // [64] or NULL
     float* out;              // [V][64] model order
+    int mode;                // VBD_FEATURES_CORRECTIONS or VBD_FEATURES_KINEMATIC
+    float3 g_dt2;            // gravity * dt^2 (kinematic set)
+    float inv_dt;            // 1 / dt (kinematic set)
 };
+
+// The kinematic feature set: the vertex's own motion and its one-ring geometry, no solver history.
+//   f[0..2]   previous step's displacement x_n - x_(n-1) = v dt, over L (v dt = (y - x) - g dt^2)
+//   f[3..5]   velocity v (m/s)
+//   f[6..8]   inertia-target offset (y - x) / L
+//   f[9..32]  8 one-ring edge vectors (x_j - x_i) / L, zero-padded
+//   f[33..35] material log-stiffnesses;  f[36] log10 mass;  f[37] contact flag;
+//   f[38]     one-ring size / 8;  f[39] solvable flag;  f[63] 1
+__device__ void kinematic_features(const FeatArgs& a, int i, float (&f)[64]) {
+    const float4 pi = a.pinfo[i];
+    const bool solvable = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
+    const float4 vf = a.vfeat[i];
+    const float invL = 1.0f / fmaxf(vf.w, 1e-9f);
+    const float3 x = xyz(a.prev[i]);
+    const float3 yy = xyz(a.y[i]);
+    const float3 off = f3(yy.x - x.x, yy.y - x.y, yy.z - x.z);
+    if (solvable) {
+        const float3 vdt = f3(off.x - a.g_dt2.x, off.y - a.g_dt2.y, off.z - a.g_dt2.z);
+        f[0] = vdt.x * invL;
+        f[1] = vdt.y * invL;
+        f[2] = vdt.z * invL;
+        f[3] = vdt.x * a.inv_dt;
+        f[4] = vdt.y * a.inv_dt;
+        f[5] = vdt.z * a.inv_dt;
+    }
+    f[6] = off.x * invL;
+    f[7] = off.y * invL;
+    f[8] = off.z * invL;
+    int nn = 0;
+    for (int k = 0; k < 8; ++k) {
+        const int nb = a.nbr8[8 * i + k];
+        if (nb < 0) continue;
+        ++nn;
+        const float3 xn = xyz(a.prev[nb]);
+        f[9 + 3 * k] = (xn.x - x.x) * invL;
+        f[10 + 3 * k] = (xn.y - x.y) * invL;
+        f[11 + 3 * k] = (xn.z - x.z) * invL;
+    }
+    f[33] = vf.x;
+    f[34] = vf.y;
+    f[35] = vf.z;
+    f[36] = pi.x > 0.f ? log10f(pi.x) : 0.f;
+    f[37] = (a.ccount && a.ccount[i] > 0) ? 1.f : 0.f;
+    f[38] = nn * 0.125f;
+    f[39] = solvable ? 1.f : 0.f;
+    f[63] = 1.f;
+}
 
 __global__ void features_kernel(FeatArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -477,6 +527,16 @@ __global__ void features_kernel(FeatArgs a) {
     const int o = a.perm[i];
     float f[64];
     for (int k = 0; k < 64; ++k) f[k] = 0.f;
+    if (a.mode == VBD_FEATURES_KINEMATIC) {
+        kinematic_features(a, i, f);
+        float* out = a.out + (size_t)o * 64;
+        for (int k = 0; k < 64; ++k) {
+            float v = f[k];
+            if (a.mean) v = (v - a.mean[k]) * a.inv_std[k];
+            out[k] = v;
+        }
+        return;
+    }
     const float4 pi = a.pinfo[i];
     const bool solvable = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
     const float4 vf = a.vfeat[i];
@@ -523,9 +583,15 @@ __global__ void features_kernel(FeatArgs a) {
     }
 }
 
+// Largest warm-start move, in characteristic lengths.  Trained corrections are a few hundredths
+// of L; a prediction beyond this bound (an input unlike the training data) is shortened to it, so
+// that the start cannot fold an element over before the sweeps begin.
+constexpr float kMaxPrediction = 0.25f;
+
 // delta = prediction * characteristic length (solvable vertices, 0 elsewhere), model order: the
 // network predicts the step's correction x - y from the inertia target in units of the vertex's
-// mean rest edge length.  A zero network therefore leaves the solve exactly as plain VBD's.
+// mean rest edge length, |prediction| <= kMaxPrediction (a non-finite prediction gives 0).  A zero
+// network therefore leaves the solve exactly as plain VBD's.
 __global__ void scale_prediction_kernel(int V, const int* perm, const float4* pinfo, const float4* vfeat,
                                         const float* pred, float* delta) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -533,16 +599,30 @@ __global__ void scale_prediction_kernel(int V, const int* perm, const float4* pi
     const int o = perm[i];
     const float4 pi = pinfo[i];
     const bool solvable = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
-    const float L = vfeat[i].w;
-    for (int k = 0; k < 3; ++k) delta[3 * o + k] = solvable ? pred[3 * o + k] * L : 0.f;
+    const float p0 = pred[3 * o], p1 = pred[3 * o + 1], p2 = pred[3 * o + 2];
+    const float n2 = p0 * p0 + p1 * p1 + p2 * p2;
+    float s = vfeat[i].w;
+    if (!(n2 <= kMaxPrediction * kMaxPrediction)) s = s * kMaxPrediction * rsqrtf(n2);
+    const bool use = solvable && isfinite(n2);
+    delta[3 * o] = use ? p0 * s : 0.f;
+    delta[3 * o + 1] = use ? p1 * s : 0.f;
+    delta[3 * o + 2] = use ? p2 * s : 0.f;
 }
 
 }  // namespace
 
 int mlp_features_launch(const VbdModelImpl& m, const float4* prev, const float4* y, const int* ccount,
-                        const float* corr_prev, const float* mean, const float* inv_std, float* out, cudaStream_t st) {
+                        const float* corr_prev, const float* mean, const float* inv_std, float* out, int mode,
+                        float dt, cudaStream_t st) {
+    if (mode != VBD_FEATURES_CORRECTIONS && mode != VBD_FEATURES_KINEMATIC)
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_features: unknown feature set");
+    if (mode == VBD_FEATURES_KINEMATIC && !(dt > 0.f))
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_features: the kinematic set needs the step's dt (run vbd_forward first)");
     if (m.V == 0) return VBD_OK;
     FeatArgs f;
+    f.mode = mode;
+    f.g_dt2 = make_float3(m.gravity[0] * dt * dt, m.gravity[1] * dt * dt, m.gravity[2] * dt * dt);
+    f.inv_dt = dt > 0.f ? 1.0f / dt : 0.f;
     f.V = m.V;
     f.perm = m.perm;
     f.pinfo = m.pinfo;

@@ -3,10 +3,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "vbd_internal.h"
@@ -33,6 +35,25 @@ static int upload(T** dst, const std::vector<T>& src) {
     VBD_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(dst), src.size() * sizeof(T)));
     VBD_CUDA_TRY(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
     return VBD_OK;
+}
+
+// fn(begin, end) over [0, n) in contiguous chunks on the host's cores (serial for small n)
+template <typename Fn>
+static void parallel_chunks(int n, Fn&& fn) {
+    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    const int workers = std::min(std::min(hw, 32), std::max(1, n / 16384));
+    if (workers <= 1) {
+        fn(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    pool.reserve(workers);
+    for (int w = 0; w < workers; ++w) {
+        const int b = static_cast<int>(static_cast<long long>(n) * w / workers);
+        const int e = static_cast<int>(static_cast<long long>(n) * (w + 1) / workers);
+        pool.emplace_back([&fn, b, e] { fn(b, e); });
+    }
+    for (auto& t : pool) t.join();
 }
 
 static void free_model(VbdModelImpl& m) {
@@ -131,73 +152,136 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
     }
 
     // ---- per-vertex element records ----------------------------------------------------
+    // Two passes over the vertices, each split over the host's cores: count the records each
+    // vertex keeps, then (after a prefix sum) write them at their offsets.  The record order is
+    // the serial one: vertices in internal order, a vertex's records in its CSR order.
     std::vector<float4> pinfo(V);
     std::vector<int4> vadj(V);
-    std::vector<int4> tri_idx;
-    std::vector<float4> tri_D, tri_mat;
-    std::vector<int4> edge_idx;
-    std::vector<float4> edge_mat;
-    tri_idx.reserve(static_cast<size_t>(3) * T);
-    tri_D.reserve(static_cast<size_t>(3) * T);
-    tri_mat.reserve(static_cast<size_t>(3) * T);
-    edge_idx.reserve(static_cast<size_t>(4) * E);
-    edge_mat.reserve(static_cast<size_t>(4) * E);
-    m.any_tri_damping = false;
-    m.any_edge_damping = false;
-    for (int i = 0; i < V; ++i) {
-        const int o = perm[i];
-        int flags = d->particle_flags[o];
-        float fl;
-        std::memcpy(&fl, &flags, sizeof(float));
-        pinfo[i] = make_float4(d->particle_mass[o], d->particle_inv_mass[o], d->particle_radius[o], fl);
-        int4 a;
-        a.x = static_cast<int>(tri_idx.size());
-        // pinned / massless vertices are never solved (solve_elasticity returns early for them),
-        // so they own no element records
-        const bool solvable = (flags & VBD_PARTICLE_ACTIVE) && d->particle_mass[o] != 0.0f;
-        if (T > 0 && solvable) {
-            const int b = d->v_adj_tris_offsets[o], e = d->v_adj_tris_offsets[o + 1];
-            for (int k = b; k < e; k += 2) {
+    std::vector<int> n_tri_keep(static_cast<size_t>(V) + 1, 0), n_edge_keep(static_cast<size_t>(V) + 1, 0);
+    std::atomic<int> bad_record{-1};  // smallest internal vertex with an invalid record, or -1
+    auto solvable_of = [&](int o) {
+        return (d->particle_flags[o] & VBD_PARTICLE_ACTIVE) && d->particle_mass[o] != 0.0f;
+    };
+    auto tri_kept = [&](int t) {
+        const float* mat = d->tri_materials + 5 * t;
+        return mat[0] > 0.0f || mat[1] > 0.0f;  // the reference skips the others
+    };
+    auto edge_kept = [&](int ed) {
+        const int* ei = d->edge_indices + 4 * ed;
+        // ke <= 0: not evaluated by the reference; boundary hinge: exact zero in the reference
+        return d->edge_bending_properties[2 * ed] > 0.0f && ei[0] != -1 && ei[1] != -1;
+    };
+    auto note_bad = [&](int i) {
+        int cur = bad_record.load();
+        while ((cur == -1 || i < cur) && !bad_record.compare_exchange_weak(cur, i)) {
+        }
+    };
+    parallel_chunks(V, [&](int b, int e) {
+        for (int i = b; i < e; ++i) {
+            const int o = perm[i];
+            // pinned / massless vertices are never solved (solve_elasticity returns early for
+            // them), so they own no element records
+            if (!solvable_of(o)) continue;
+            int nt = 0, ne = 0;
+            if (T > 0) {
+                for (int k = d->v_adj_tris_offsets[o]; k < d->v_adj_tris_offsets[o + 1]; k += 2) {
+                    const int t = d->v_adj_tris[k], slot = d->v_adj_tris[k + 1];
+                    if (t < 0 || t >= T || slot < 0 || slot > 2) {
+                        note_bad(i);
+                        break;
+                    }
+                    nt += tri_kept(t) ? 1 : 0;
+                }
+            }
+            if (E > 0) {
+                for (int k = d->v_adj_edges_offsets[o]; k < d->v_adj_edges_offsets[o + 1]; k += 2) {
+                    const int ed = d->v_adj_edges[k], slot = d->v_adj_edges[k + 1];
+                    if (ed < 0 || ed >= E || slot < 0 || slot > 3) {
+                        note_bad(i);
+                        break;
+                    }
+                    ne += edge_kept(ed) ? 1 : 0;
+                }
+            }
+            n_tri_keep[i + 1] = nt;
+            n_edge_keep[i + 1] = ne;
+        }
+    });
+    if (bad_record.load() >= 0) {
+        // report the first invalid record the serial walk would meet
+        const int o = perm[bad_record.load()];
+        bool tri_bad = false;
+        if (T > 0)
+            for (int k = d->v_adj_tris_offsets[o]; k < d->v_adj_tris_offsets[o + 1]; k += 2) {
                 const int t = d->v_adj_tris[k], slot = d->v_adj_tris[k + 1];
-                if (t < 0 || t >= T || slot < 0 || slot > 2)
-                    return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_model_create: bad triangle adjacency record");
-                const float* mat = d->tri_materials + 5 * t;
-                if (!(mat[0] > 0.0f || mat[1] > 0.0f)) continue;  // the reference skips such triangles
-                const int* ti = d->tri_indices + 3 * t;
-                tri_idx.push_back(make_int4(inv[ti[0]], inv[ti[1]], inv[ti[2]], slot));
-                m.tri_elem_h.push_back(t);
-                const float* P = d->tri_poses + 4 * t;
-                tri_D.push_back(make_float4(P[0], P[1], P[2], P[3]));
-                // (area*mu, area*lambda_nh, alpha, area*kd) with lambda_nh = lambda + mu and
-                // alpha = 1 + mu / lambda_nh (particle_vbd_kernels.py:561-565), in float32
-                const float area = d->tri_areas[t], mu = mat[0], lnh = mat[1] + mat[0];
-                const float lsafe = (lnh < 0.0f ? -1.0f : 1.0f) * std::max(std::fabs(lnh), 1.0e-6f);
-                const float alpha = 1.0f + mu / lsafe;
-                tri_mat.push_back(make_float4(area * mu, area * lnh, alpha, area * mat[2]));
-                if (mat[2] > 0.0f) m.any_tri_damping = true;
+                tri_bad |= t < 0 || t >= T || slot < 0 || slot > 2;
             }
-        }
-        a.y = static_cast<int>(tri_idx.size());
-        a.z = static_cast<int>(edge_idx.size());
-        if (E > 0 && solvable) {
-            const int b = d->v_adj_edges_offsets[o], e = d->v_adj_edges_offsets[o + 1];
-            for (int k = b; k < e; k += 2) {
-                const int ed = d->v_adj_edges[k], slot = d->v_adj_edges[k + 1];
-                if (ed < 0 || ed >= E || slot < 0 || slot > 3)
-                    return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_model_create: bad edge adjacency record");
-                const int* ei = d->edge_indices + 4 * ed;
-                const float ke = d->edge_bending_properties[2 * ed], kd = d->edge_bending_properties[2 * ed + 1];
-                if (!(ke > 0.0f)) continue;                 // not evaluated by the reference
-                if (ei[0] == -1 || ei[1] == -1) continue;   // boundary hinge: exact zero in the reference
-                edge_idx.push_back(make_int4(inv[ei[0]] | (slot << 30), inv[ei[1]], inv[ei[2]], inv[ei[3]]));
-                m.edge_elem_h.push_back(ed);
-                edge_mat.push_back(make_float4(d->edge_rest_angle[ed], d->edge_rest_length[ed], ke, kd));
-                if (kd > 0.0f) m.any_edge_damping = true;
-            }
-        }
-        a.w = static_cast<int>(edge_idx.size());
-        vadj[i] = a;
+        return fail(VBD_ERR_INVALID_ARGUMENT, tri_bad ? "vbd_model_create: bad triangle adjacency record"
+                                                      : "vbd_model_create: bad edge adjacency record");
     }
+    for (int i = 0; i < V; ++i) {
+        n_tri_keep[i + 1] += n_tri_keep[i];
+        n_edge_keep[i + 1] += n_edge_keep[i];
+    }
+    const size_t n_tri_rec = static_cast<size_t>(n_tri_keep[V]), n_edge_rec = static_cast<size_t>(n_edge_keep[V]);
+    std::vector<int4> tri_idx(n_tri_rec);
+    std::vector<float4> tri_D(n_tri_rec), tri_mat(n_tri_rec);
+    std::vector<int4> edge_idx(n_edge_rec);
+    std::vector<float4> edge_mat(n_edge_rec);
+    m.tri_elem_h.assign(n_tri_rec, 0);
+    m.edge_elem_h.assign(n_edge_rec, 0);
+    std::atomic<bool> any_tri_damp{false}, any_edge_damp{false};
+    parallel_chunks(V, [&](int b, int e) {
+        bool tdamp = false, edamp = false;
+        for (int i = b; i < e; ++i) {
+            const int o = perm[i];
+            int flags = d->particle_flags[o];
+            float fl;
+            std::memcpy(&fl, &flags, sizeof(float));
+            pinfo[i] = make_float4(d->particle_mass[o], d->particle_inv_mass[o], d->particle_radius[o], fl);
+            vadj[i] = make_int4(n_tri_keep[i], n_tri_keep[i + 1], n_edge_keep[i], n_edge_keep[i + 1]);
+            if (!solvable_of(o)) continue;
+            int r = n_tri_keep[i];
+            if (T > 0) {
+                for (int k = d->v_adj_tris_offsets[o]; k < d->v_adj_tris_offsets[o + 1]; k += 2) {
+                    const int t = d->v_adj_tris[k], slot = d->v_adj_tris[k + 1];
+                    if (!tri_kept(t)) continue;
+                    const float* mat = d->tri_materials + 5 * t;
+                    const int* ti = d->tri_indices + 3 * t;
+                    tri_idx[r] = make_int4(inv[ti[0]], inv[ti[1]], inv[ti[2]], slot);
+                    m.tri_elem_h[r] = t;
+                    const float* P = d->tri_poses + 4 * t;
+                    tri_D[r] = make_float4(P[0], P[1], P[2], P[3]);
+                    // (area*mu, area*lambda_nh, alpha, area*kd) with lambda_nh = lambda + mu and
+                    // alpha = 1 + mu / lambda_nh (particle_vbd_kernels.py:561-565), in float32
+                    const float area = d->tri_areas[t], mu = mat[0], lnh = mat[1] + mat[0];
+                    const float lsafe = (lnh < 0.0f ? -1.0f : 1.0f) * std::max(std::fabs(lnh), 1.0e-6f);
+                    const float alpha = 1.0f + mu / lsafe;
+                    tri_mat[r] = make_float4(area * mu, area * lnh, alpha, area * mat[2]);
+                    tdamp |= mat[2] > 0.0f;
+                    ++r;
+                }
+            }
+            r = n_edge_keep[i];
+            if (E > 0) {
+                for (int k = d->v_adj_edges_offsets[o]; k < d->v_adj_edges_offsets[o + 1]; k += 2) {
+                    const int ed = d->v_adj_edges[k], slot = d->v_adj_edges[k + 1];
+                    if (!edge_kept(ed)) continue;
+                    const int* ei = d->edge_indices + 4 * ed;
+                    const float ke = d->edge_bending_properties[2 * ed], kd = d->edge_bending_properties[2 * ed + 1];
+                    edge_idx[r] = make_int4(inv[ei[0]] | (slot << 30), inv[ei[1]], inv[ei[2]], inv[ei[3]]);
+                    m.edge_elem_h[r] = ed;
+                    edge_mat[r] = make_float4(d->edge_rest_angle[ed], d->edge_rest_length[ed], ke, kd);
+                    edamp |= kd > 0.0f;
+                    ++r;
+                }
+            }
+        }
+        if (tdamp) any_tri_damp = true;
+        if (edamp) any_edge_damp = true;
+    });
+    m.any_tri_damping = any_tri_damp.load();
+    m.any_edge_damping = any_edge_damp.load();
     m.n_tri_rec = static_cast<int>(tri_idx.size());
     m.n_edge_rec = static_cast<int>(edge_idx.size());
 
@@ -224,39 +308,43 @@ static int build_model(const VbdModelDesc* d, VbdModelImpl& m) {
     // learned-warm-start inputs: one-ring neighbours and material features per vertex
     std::vector<int> nbr8(static_cast<size_t>(V) * 8, -1);
     std::vector<float4> vfeat(V);
-    for (int i = 0; i < V; ++i) {
-        const int o = perm[i];
-        int nn = 0;
-        double lke = 0, lka = 0, larea = 0, lek = 0;
-        int nt = 0, ne = 0;
-        if (T > 0) {
-            for (int k = d->v_adj_tris_offsets[o]; k < d->v_adj_tris_offsets[o + 1]; k += 2) {
-                const int t = d->v_adj_tris[k];
-                const int* ti = d->tri_indices + 3 * t;
-                const float* mat = d->tri_materials + 5 * t;
-                lke += std::log10(std::max(mat[0], 1e-12f));
-                lka += std::log10(std::max(mat[1], 1e-12f));
-                larea += std::sqrt(2.0 * std::max(d->tri_areas[t], 0.0f));
-                ++nt;
-                for (int c = 0; c < 3; ++c) {
-                    const int nb = inv[ti[c]];
-                    if (ti[c] == o || nn >= 8) continue;
-                    bool seen = false;
-                    for (int q = 0; q < nn; ++q) seen |= nbr8[8 * i + q] == nb;
-                    if (!seen) nbr8[8 * i + nn++] = nb;
+    parallel_chunks(V, [&](int ib, int ie) {
+        for (int i = ib; i < ie; ++i) {
+            const int o = perm[i];
+            int nn = 0;
+            double lke = 0, lka = 0, larea = 0, lek = 0;
+            int nt = 0, ne = 0;
+            if (T > 0) {
+                for (int k = d->v_adj_tris_offsets[o]; k < d->v_adj_tris_offsets[o + 1]; k += 2) {
+                    const int t = d->v_adj_tris[k];
+                    if (t < 0 || t >= T) continue;  // (records of unsolved vertices are not validated above)
+                    const int* ti = d->tri_indices + 3 * t;
+                    const float* mat = d->tri_materials + 5 * t;
+                    lke += std::log10(std::max(mat[0], 1e-12f));
+                    lka += std::log10(std::max(mat[1], 1e-12f));
+                    larea += std::sqrt(2.0 * std::max(d->tri_areas[t], 0.0f));
+                    ++nt;
+                    for (int c = 0; c < 3; ++c) {
+                        const int nb = inv[ti[c]];
+                        if (ti[c] == o || nn >= 8) continue;
+                        bool seen = false;
+                        for (int q = 0; q < nn; ++q) seen |= nbr8[8 * i + q] == nb;
+                        if (!seen) nbr8[8 * i + nn++] = nb;
+                    }
                 }
             }
-        }
-        if (E > 0) {
-            for (int k = d->v_adj_edges_offsets[o]; k < d->v_adj_edges_offsets[o + 1]; k += 2) {
-                const int e = d->v_adj_edges[k];
-                lek += std::log10(std::max(d->edge_bending_properties[2 * e], 1e-12f));
-                ++ne;
+            if (E > 0) {
+                for (int k = d->v_adj_edges_offsets[o]; k < d->v_adj_edges_offsets[o + 1]; k += 2) {
+                    const int e = d->v_adj_edges[k];
+                    if (e < 0 || e >= E) continue;
+                    lek += std::log10(std::max(d->edge_bending_properties[2 * e], 1e-12f));
+                    ++ne;
+                }
             }
+            vfeat[i] = make_float4(nt ? float(lke / nt) : 0.f, nt ? float(lka / nt) : 0.f, ne ? float(lek / ne) : 0.f,
+                                   nt ? float(larea / nt) : 1.f);
         }
-        vfeat[i] = make_float4(nt ? float(lke / nt) : 0.f, nt ? float(lka / nt) : 0.f, ne ? float(lek / ne) : 0.f,
-                               nt ? float(larea / nt) : 1.f);
-    }
+    });
 
     std::vector<int> pworld(V, -1), pflags(V);
     std::vector<float> pradius(V);

@@ -33,21 +33,26 @@ namespace vbd {
 enum StatusSlot { kNonfinite = 0, kSingular = 1, kOverflow = 2, kTimeout = 3, kStatusSlots = 4 };
 
 constexpr int kGateMaxIterations = 100000;  // upper bound of a gated step's iteration cap
+constexpr int kGateDefaultRounds = 4;        // sweep mode: check rounds per loop body by default
 
 // Device-side state of the residual gate (vbd_set_residual_gate), one per solver.  The head, up
 // to `ref`, is zeroed at the start of every gated step.
 // The accumulators of one evaluation are spread over kGateSlots slots, each on its own 128-byte
-// line (warp w adds into slot w mod kGateSlots), so that the atomics of a large sweep do not all
-// queue on one line.
-constexpr int kGateSlots = 64;
+// line (a sweep's block b adds its block total into slot b mod kGateSlots; the Jacobi evaluation's
+// warp w into slot w mod kGateSlots), so that the atomics of a large sweep do not queue on a few
+// lines: atomics on one address serialize at the L2.
+constexpr int kGateSlots = 256;
+constexpr int kElectGroups = 64;  // first-level counters of the deciding sweep's last-block election
 constexpr int kSumStride = 16;  // unsigned long long per 128-byte line
 constexpr int kMaxStride = 32;  // unsigned per 128-byte line
 
 struct GateState {
     unsigned long long sum[kGateSlots * kSumStride];  // fixed-point sums of the residuals (resid_fixed)
     unsigned maxv[kGateSlots * kMaxStride];  // max residual (float bits; atomicMax target)
+    unsigned done_sub[kElectGroups * kMaxStride];  // last-block election, first level (one line per group)
     int iters;               // iterations run so far in this step
-    unsigned done;           // blocks of the deciding sweep that have finished (last-block election)
+    unsigned done;           // groups of the deciding sweep's blocks that have finished (second level)
+    unsigned stop;           // 1 once this step's gate has decided: later sweeps of the loop body return
     int pad;
     float ref;               // relative mode: the step's reference residual
     int last_iters;          // iterations of the last finished step
@@ -56,6 +61,7 @@ struct GateState {
     unsigned long long steps;     // gated steps finished (since creation or the last reset)
     unsigned long long iter_sum;  // iterations summed over those steps
     unsigned long long capped;    // steps that stopped at the iteration cap above the tolerance
+    unsigned long long passes;    // passes of the loop body summed over those steps
 };
 
 struct GraphEntry {
@@ -108,6 +114,8 @@ struct SolverImpl {
     int ws_iterations = 0;
     float* ws_corr = nullptr;        // [V][3] previous step's correction x_solved - y (model order)
     float* ws_work = nullptr;        // [V][70] features, prediction, displacement
+    int feature_set = VBD_FEATURES_CORRECTIONS;  // vbd_set_feature_set
+    float last_dt = 0.f;             // dt of the last vbd_forward (the kinematic features need it)
     // particle self-contact (particle_enable_self_contact)
     SelfContact sc;
     // residual gate (vbd_set_residual_gate): iterate until max_i |f_i| / (m_i |g|) <= tolerance
@@ -118,9 +126,11 @@ struct SolverImpl {
     int gate_mean = 0;               // 1: mean residual over the solved vertices instead of the max
     int gate_sweep = 0;              // 1: the Gauss-Seidel residual the sweeps accumulate (no Jacobi launch)
     int gate_count = 0;              // solved vertices (the mean's divisor)
+    int gate_rounds = 4;             // sweep mode: check rounds per body of the device-side loop
     GateState* gate = nullptr;       // device
     cudaStream_t body_stream = nullptr;  // capture stream of the gate's loop body
     int gate_body_kernels = -1;      // kernel nodes of one loop body (last capture)
+    int gate_body_pdl_edges = -1;    // programmatic edges of that body
     bool pdl = true;                 // programmatic dependent launch of the sweeps
 };
 
@@ -262,6 +272,7 @@ struct GateParams {
     int first;    // 1: the start evaluation; 0: a later one; -1: sweep residuals (first iff iters == 0)
     int set_ref;  // the first evaluation is also the relative mode's reference
     int add;      // iterations since the last check
+    int rounds;   // check rounds per pass of the loop body (sweep mode), else 1
 };
 
 struct SweepArgs {
@@ -308,6 +319,9 @@ struct SweepArgs {
     GateState* gate_state;   // NULL: this sweep does not decide
     cudaGraphConditionalHandle gate_handle;
     GateParams gate_params;
+    // residual gate, later rounds of an unrolled loop body: return at once when the step's gate
+    // has already decided (GateState::stop); NULL otherwise
+    const unsigned* gate_stop;
 };
 
 template <bool kDamp>
@@ -533,12 +547,15 @@ __device__ __forceinline__ unsigned long long resid_fixed(float r) {
 __device__ __forceinline__ float gate_take_warp(GateState* g, int mean, int count) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    unsigned long long sum = g->sum[lane * kSumStride] + g->sum[(lane + 32) * kSumStride];
-    const unsigned mx0 = max(g->maxv[lane * kMaxStride], g->maxv[(lane + 32) * kMaxStride]);
-    g->sum[lane * kSumStride] = 0ull;
-    g->sum[(lane + 32) * kSumStride] = 0ull;
-    g->maxv[lane * kMaxStride] = 0u;
-    g->maxv[(lane + 32) * kMaxStride] = 0u;
+    unsigned long long sum = 0ull;
+    unsigned mx0 = 0u;
+#pragma unroll
+    for (int k = lane; k < kGateSlots; k += 32) {
+        sum += g->sum[k * kSumStride];
+        mx0 = max(mx0, g->maxv[k * kMaxStride]);
+        g->sum[k * kSumStride] = 0ull;
+        g->maxv[k * kMaxStride] = 0u;
+    }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(full, sum, off);
     const unsigned mx = __reduce_max_sync(full, mx0);
@@ -559,13 +576,20 @@ __device__ __forceinline__ void gate_decide(GateState* g, cudaGraphConditionalHa
     const float thresh = p.relative ? p.tol * g->ref : p.tol;
     const bool more = (r > thresh) && (g->iters < p.max_iters);
     if (!more) {
+        g->stop = 1u;
         g->last_iters = g->iters;
         g->last_resid = r;
         g->steps += 1ull;
         g->iter_sum += static_cast<unsigned long long>(g->iters);
         if (r > thresh) g->capped += 1ull;
+        if (p.first != 1) {
+            const int checks = p.add > 0 ? (g->iters + p.add - 1) / p.add : 0;
+            g->passes += static_cast<unsigned long long>((checks + p.rounds - 1) / p.rounds);
+        }
     }
-    cudaGraphSetConditional(handle, more ? 1u : 0u);
+    // the condition keeps its value between loop passes: write it only where it changes (the
+    // start evaluation of Jacobi mode, whose default is 0; the stop)
+    if (!more || p.first == 1) cudaGraphSetConditional(handle, more ? 1u : 0u);
 }
 
 // Warp-collective: every thread of the warp calls it (r = 0 and counted = false where the thread
@@ -590,14 +614,51 @@ __device__ __forceinline__ void reduce_residual(const SweepArgs& a, float r, boo
     }
 }
 
+// Block-collective (every thread of the block calls it; blockDim a multiple of 32, at most 256):
+// the same reduction, with the warps' results combined in shared memory so that one thread adds
+// the block's max and sum to slot (block mod kGateSlots) -- one atomic per block, not per warp.
+__device__ __forceinline__ void reduce_residual_block(const SweepArgs& a, float r, bool counted) {
+    __shared__ unsigned long long s_sum[8];
+    __shared__ unsigned s_max[8];
+    __shared__ int s_any[8];
+    const unsigned full = 0xffffffffu;
+    const int w = threadIdx.x >> 5;
+    const unsigned mx = __reduce_max_sync(full, __float_as_uint(r));
+    const bool any = __any_sync(full, counted);
+    unsigned long long sum = counted ? resid_fixed(r) : 0ull;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(full, sum, off);
+    if ((threadIdx.x & 31) == 0) {
+        s_sum[w] = sum;
+        s_max[w] = mx;
+        s_any[w] = any ? 1 : 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long bs = 0ull;
+        unsigned bm = 0u;
+        int ba = 0;
+        for (int k = 0; k < static_cast<int>(blockDim.x >> 5); ++k) {
+            bs += s_sum[k];
+            bm = max(bm, s_max[k]);
+            ba |= s_any[k];
+        }
+        if (ba) {
+            const int slot = static_cast<int>(blockIdx.x & (kGateSlots - 1));
+            if (a.gate_max) atomicMax(a.gate_max + slot * kMaxStride, bm);
+            if (a.gate_sum) atomicAdd(a.gate_sum + slot * kSumStride, bs);
+        }
+    }
+}
+
 // One Gauss-Seidel color (kResidual = false) or a Jacobi residual evaluation over a vertex range
 // (kResidual = true).  L lanes cooperate on one vertex: each lane takes every L-th element record
 // (triangles, then hinges, as the reference's 16-thread tile does), then the partial force and
 // Hessian are summed across the L lanes with xor shuffles and lane 0 adds the contacts and solves.
 // kCap: the same kernel limited to 64 registers per thread (4 blocks of 256 per SM), used when the
 // uncapped kernel would need more than one wave of blocks (large colors, many lanes per vertex)
-template <int L, bool kDamp, bool kResidual, bool kCap, bool kGate = false>
-__global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
+template <int L, bool kDamp, bool kResidual, bool kCap, bool kGate>
+__device__ __forceinline__ void sweep_body(const SweepArgs& a) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = a.v_begin + tid / L;
     const int lane = tid & (L - 1);
@@ -627,6 +688,9 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
     }
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;");
+    // a round of the gate's loop body after the decision: nothing to do (the flag was written by
+    // an earlier kernel of the stream and is the same for every thread of the grid)
+    if (a.gate_stop && *reinterpret_cast<const volatile unsigned*>(a.gate_stop) != 0u) return;
     if (valid && solve && lane == 0) {
         // Warm L1 with what lane 0 reads after the element walk (the vertex's own state, its
         // contact count, its self-contact terms): a prefetch holds no register, so the walk keeps
@@ -695,15 +759,29 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
                 solve_and_commit(a, i, pv, h, f);
             }
         }
-        reduce_residual(a, rg, counted);
+        reduce_residual_block(a, rg, counted);
         if (a.gate_state) {
-            // the round's last color: the last block to finish reduces the slots and decides (every
-            // block's slot atomics are fenced before it counts itself done)
+            // the round's last color: the last block to finish reduces the slots and decides.  The
+            // election has two levels so that no counter takes more than ~grid/64 atomics: block
+            // b counts itself done in group b mod G (G = min(kElectGroups, grid) counters on
+            // separate lines);
+            // the last block of a group counts the group done; the last group's last block
+            // decides.  Every block's slot atomics are fenced before it counts itself, and every
+            // group's count before the group is counted (the fences order the chain).
             __shared__ unsigned s_last;
             __syncthreads();
             if (threadIdx.x == 0) {
+                const unsigned groups = min(gridDim.x, static_cast<unsigned>(kElectGroups));
+                const unsigned g = blockIdx.x % groups;
+                const unsigned members = (gridDim.x - g + groups - 1) / groups;
+                unsigned* sub = &a.gate_state->done_sub[g * kMaxStride];
+                s_last = 0u;
                 __threadfence();
-                s_last = (atomicAdd(&a.gate_state->done, 1u) == gridDim.x - 1) ? 1u : 0u;
+                if (atomicAdd(sub, 1u) == members - 1) {
+                    *sub = 0u;  // the group's last block: no other block touches it in this launch
+                    __threadfence();
+                    s_last = (atomicAdd(&a.gate_state->done, 1u) == groups - 1) ? 1u : 0u;
+                }
             }
             __syncthreads();
             if (s_last && threadIdx.x < 32) {
@@ -726,6 +804,20 @@ __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
     }
     add_vertex_terms(a, i, pi, pv, xyz(a.pos[i]), a.y[i], f, h);
     solve_and_commit(a, i, pv, h, f);
+}
+
+template <int L, bool kDamp, bool kResidual, bool kCap, bool kGate = false>
+__global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
+    sweep_body<L, kDamp, kResidual, kCap, kGate>(a);
+}
+
+// The gate's accumulating sweep with 4 or more lanes per vertex, held to the 72 registers of the
+// plain sweep: at 74 (what the compiler picks for the extra reduction) the allocation rounds up
+// to 80 registers per thread, two color grids no longer fit on an SM together, and each launch
+// loses its overlap with the previous one.
+template <int L, bool kDamp>
+__global__ void __maxnreg__(72) sweep_gate_kernel(SweepArgs a) {
+    sweep_body<L, kDamp, false, false, true>(a);
 }
 
 // Record-parallel variant of the same color update (lanes_per_vertex == 0).  A block owns
@@ -1057,6 +1149,7 @@ static GateParams gate_params(const SolverImpl& s, int first, int set_ref, int a
     p.first = first;
     p.set_ref = set_ref;
     p.add = add;
+    p.rounds = (s.gate_sweep && s.lanes > 0) ? s.gate_rounds : 1;
     return p;
 }
 
@@ -1097,11 +1190,18 @@ static void launch_dependent(Kernel kernel, int grid, int block, cudaStream_t st
 
 template <int L, bool kDamp, bool kResidual, bool kGate = false>
 static void launch_sweep_LDR(const SweepArgs& a, int grid, int block, cudaStream_t st) {
-    const void* uncapped = reinterpret_cast<const void*>(&sweep_kernel<L, kDamp, kResidual, false, kGate>);
-    if (grid > resident_blocks(uncapped, block))
-        launch_dependent(sweep_kernel<L, kDamp, kResidual, true, kGate>, grid, block, st, a);
-    else
-        launch_dependent(sweep_kernel<L, kDamp, kResidual, false, kGate>, grid, block, st, a);
+    if constexpr (kGate && !kResidual && L >= 4) {
+        if (grid > resident_blocks(reinterpret_cast<const void*>(&sweep_gate_kernel<L, kDamp>), block))
+            launch_dependent(sweep_kernel<L, kDamp, kResidual, true, kGate>, grid, block, st, a);
+        else
+            launch_dependent(sweep_gate_kernel<L, kDamp>, grid, block, st, a);
+    } else {
+        const void* uncapped = reinterpret_cast<const void*>(&sweep_kernel<L, kDamp, kResidual, false, kGate>);
+        if (grid > resident_blocks(uncapped, block))
+            launch_dependent(sweep_kernel<L, kDamp, kResidual, true, kGate>, grid, block, st, a);
+        else
+            launch_dependent(sweep_kernel<L, kDamp, kResidual, false, kGate>, grid, block, st, a);
+    }
 }
 
 // occupancy queries happen here, outside any stream capture (solver creation, vbd_set_launch)
@@ -1113,6 +1213,10 @@ static void prime_occupancy_L(int block) {
     resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, false, false, false>), block);
     resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, true, false, false, true>), block);
     resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, false, false, false, true>), block);
+    if constexpr (L >= 4) {
+        resident_blocks(reinterpret_cast<const void*>(&sweep_gate_kernel<L, true>), block);
+        resident_blocks(reinterpret_cast<const void*>(&sweep_gate_kernel<L, false>), block);
+    }
 }
 
 static void prime_occupancy(int lanes, int block) {
@@ -1180,6 +1284,7 @@ static void launch_sweep(const SweepArgs& a, int lanes, bool damp, bool residual
 static int enqueue_forward(SolverImpl& s, const float* q_in, const float* qd_in, const float* f_ext,
                            const VbdContacts* c, float dt, cudaStream_t st) {
     const VbdModelImpl& m = *s.m;
+    s.last_dt = dt;
     ForwardArgs a;
     std::memset(&a, 0, sizeof(a));
     a.perm = m.perm;
@@ -1239,10 +1344,12 @@ struct GateCheck {
 // gate: also accumulate the color's Gauss-Seidel residual into the residual gate (sweep mode);
 // check: this sweep also takes the round's decision
 static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float dt, cudaStream_t st,
-                          bool first_iteration = true, bool gate = false, const GateCheck* check = nullptr) {
+                          bool first_iteration = true, bool gate = false, const GateCheck* check = nullptr,
+                          bool skip_when_decided = false) {
     const VbdModelImpl& m = *s.m;
     SweepArgs a = make_sweep_args(s, c, dt);
     a.prefetch_records = first_iteration ? 1 : 0;
+    if (skip_when_decided) a.gate_stop = &s.gate->stop;
     if (gate) {
         a.gate_max = s.gate_mean ? nullptr : s.gate->maxv;
         a.gate_sum = s.gate_mean ? s.gate->sum : nullptr;
@@ -1319,6 +1426,24 @@ static int kernel_nodes(cudaGraph_t graph) {
     return k;
 }
 
+// programmatic (PDL) edges of a captured graph; -1 if they cannot be read
+static int programmatic_edges(cudaGraph_t graph) {
+    size_t n = 0;
+    if (cudaGraphGetEdges_v2(graph, nullptr, nullptr, nullptr, &n) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    std::vector<cudaGraphNode_t> from(n), to(n);
+    std::vector<cudaGraphEdgeData> data(n);
+    if (n > 0 && cudaGraphGetEdges_v2(graph, from.data(), to.data(), data.data(), &n) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    int k = 0;
+    for (size_t j = 0; j < n; ++j) k += data[j].type == cudaGraphDependencyTypeProgrammatic ? 1 : 0;
+    return k;
+}
+
 // Jacobi residual of the current iterate into the gate's accumulator
 static void enqueue_gate_residual(SolverImpl& s, const VbdContacts* c, float dt, cudaStream_t st) {
     const VbdModelImpl& m = *s.m;
@@ -1368,14 +1493,21 @@ static int enqueue_gated_iterations(SolverImpl& s, const VbdContacts* c, float d
     cudaGraph_t body = params.conditional.phGraph_out[0];
     VBD_CUDA_TRY(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
     VBD_CUDA_TRY(cudaStreamBeginCaptureToGraph(s.body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < s.gate_every; ++k) {
-        const bool last = k == s.gate_every - 1;
-        for (int color = 0; color < s.m->C; ++color) {
-            // sweep mode: the round's last sweep also decides (no separate check kernel)
-            const bool decides = sweep && last && color == s.m->C - 1;
-            GateCheck chk{decides ? s.gate : nullptr, handle,
-                          gate_params(s, -1, (sweep && set_ref) ? 1 : 0, s.gate_every)};
-            enqueue_color(s, color, c, dt, s.body_stream, false, sweep && last, decides ? &chk : nullptr);
+    // sweep mode: the body holds gate_rounds rounds, each deciding after its last sweep; the
+    // sweeps of a round after the decision return at once, so the loop's per-body cost (the body
+    // boundary, where consecutive sweeps cannot overlap) is paid once per gate_rounds rounds
+    const int rounds = sweep ? s.gate_rounds : 1;
+    for (int u = 0; u < rounds; ++u) {
+        for (int k = 0; k < s.gate_every; ++k) {
+            const bool last = k == s.gate_every - 1;
+            for (int color = 0; color < s.m->C; ++color) {
+                // sweep mode: the round's last sweep also decides (no separate check kernel)
+                const bool decides = sweep && last && color == s.m->C - 1;
+                GateCheck chk{decides ? s.gate : nullptr, handle,
+                              gate_params(s, -1, (sweep && set_ref) ? 1 : 0, s.gate_every)};
+                enqueue_color(s, color, c, dt, s.body_stream, false, sweep && last, decides ? &chk : nullptr,
+                              u > 0);
+            }
         }
     }
     if (!sweep) {
@@ -1388,6 +1520,7 @@ static int enqueue_gated_iterations(SolverImpl& s, const VbdContacts* c, float d
     if (e1 != cudaSuccess) return cuda_fail(e1, "residual-gated loop body");
     if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture (residual-gated loop body)");
     s.gate_body_kernels = kernel_nodes(body);
+    s.gate_body_pdl_edges = programmatic_edges(body);
     return VBD_OK;
 }
 
@@ -1410,7 +1543,7 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
             }
         }
         int rc = mlp_features_launch(*s.m, s.prev, s.y, c ? s.ccount : nullptr, s.ws_corr, s.ws_mean, s.ws_inv_std,
-                                     feats, st);
+                                     feats, s.feature_set, dt, st);
         if (!rc) rc = vbd_mlp_forward(s.ws_params, s.ws_w16, feats, V, pred, st);
         if (!rc) rc = mlp_scale_launch(*s.m, pred, delta, st);
         if (rc) return rc;
@@ -1837,8 +1970,21 @@ extern "C" int vbd_mlp_features(VbdSolver* solver, const float* corr_prev, const
     if (!solver || !out || ((mean == nullptr) != (inv_std == nullptr)))
         return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_features: bad arguments");
     SolverImpl& s = solver->s;
-    return mlp_features_launch(*s.m, s.prev, s.y, s.ccount, corr_prev, mean, inv_std, out,
+    return mlp_features_launch(*s.m, s.prev, s.y, s.ccount, corr_prev, mean, inv_std, out, s.feature_set, s.last_dt,
                                static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int vbd_set_feature_set(VbdSolver* solver, int32_t feature_set) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_feature_set: solver is NULL");
+    if (feature_set != VBD_FEATURES_CORRECTIONS && feature_set != VBD_FEATURES_KINEMATIC)
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_feature_set: unknown feature set");
+    SolverImpl& s = solver->s;
+    if (s.feature_set != feature_set) {
+        for (auto& g : s.graphs) cudaGraphExecDestroy(g.exec);  // captured steps change
+        s.graphs.clear();
+    }
+    s.feature_set = feature_set;
+    return VBD_OK;
 }
 
 extern "C" int vbd_set_warm_start(VbdSolver* solver, const float* params, const uint16_t* w16, const float* mean,
@@ -1886,7 +2032,8 @@ extern "C" int vbd_mlp_warm_start(VbdSolver* solver, const float* params, const 
     float* feats = workspace;
     float* pred = feats + static_cast<size_t>(V) * 64;
     float* delta = pred + static_cast<size_t>(V) * 3;
-    int rc = mlp_features_launch(*s.m, s.prev, s.y, s.ccount, corr_prev, mean, inv_std, feats, st);
+    int rc = mlp_features_launch(*s.m, s.prev, s.y, s.ccount, corr_prev, mean, inv_std, feats, s.feature_set,
+                                 s.last_dt, st);
     if (rc) return rc;
     rc = vbd_mlp_forward(params, w16, feats, V, pred, stream);
     if (rc) return rc;
@@ -1953,8 +2100,10 @@ extern "C" int vbd_set_residual_gate(VbdSolver* solver, float tolerance, int32_t
         s.gate_tol = tolerance;
         s.gate_max = max_iterations;
         s.gate_every = check_every;
-        if (mode & ~(VBD_GATE_RELATIVE | VBD_GATE_MEAN | VBD_GATE_SWEEP))
+        if (mode & ~(VBD_GATE_RELATIVE | VBD_GATE_MEAN | VBD_GATE_SWEEP | VBD_GATE_ROUNDS_MASK))
             return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_residual_gate: unknown mode bits");
+        const int rounds = (mode & VBD_GATE_ROUNDS_MASK) >> VBD_GATE_ROUNDS_SHIFT;
+        s.gate_rounds = rounds > 0 ? rounds : kGateDefaultRounds;
         s.gate_relative = (mode & VBD_GATE_RELATIVE) ? 1 : 0;
         s.gate_mean = (mode & VBD_GATE_MEAN) ? 1 : 0;
         s.gate_sweep = (mode & VBD_GATE_SWEEP) ? 1 : 0;
@@ -1978,6 +2127,7 @@ extern "C" int vbd_gate_stats(VbdSolver* solver, VbdGateStats* out, int32_t rese
     SolverImpl& s = solver->s;
     std::memset(out, 0, sizeof(*out));
     out->body_kernels = s.gate_body_kernels;
+    out->body_programmatic_edges = s.pdl ? s.gate_body_pdl_edges : 0;
     if (!s.gate) return VBD_OK;
     GateState g;
     VBD_CUDA_TRY(cudaDeviceSynchronize());
@@ -1989,8 +2139,9 @@ extern "C" int vbd_gate_stats(VbdSolver* solver, VbdGateStats* out, int32_t rese
     out->last_residual = g.last_resid;
     out->last_start_residual = g.start_resid;
     out->last_reference_residual = g.ref;
+    out->body_passes = static_cast<int64_t>(g.passes);
     if (reset) {
-        g.steps = g.iter_sum = g.capped = 0ull;
+        g.steps = g.iter_sum = g.capped = g.passes = 0ull;
         VBD_CUDA_TRY(cudaMemcpy(s.gate, &g, sizeof(g), cudaMemcpyHostToDevice));
     }
     return VBD_OK;

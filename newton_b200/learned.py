@@ -3,11 +3,13 @@
 A per-vertex MLP (64 -> 128 -> 128 -> 3, SiLU, BF16 weights, FP32 accumulation on the tensor
 cores) predicts the correction ``x_solved - y`` that the coming step applies to the inertia
 target ``y``, in units of the vertex's characteristic element length, from one-ring features
-(``vbd_mlp_features``): inertia offset, the previous step's correction of the vertex and of 8
-one-ring neighbours, the 8 one-ring edge vectors, log-stiffnesses, mass, contact and pin flags.
-The Gauss-Seidel iterations then start from ``y + prediction``; a zero network is plain VBD bit
-for bit.  The force residual after the iterations, against plain VBD's on the same state, is
-what decides whether the warm start pays (``calibrate_iterations``).
+(``vbd_mlp_features``).  Two feature sets: ``"kinematic"`` (default) -- previous step's
+displacement, velocity and inertia offset, the 8 one-ring edge vectors, log-stiffnesses, mass,
+contact and pin flags; ``"corrections"`` -- the inertia offset, the previous step's correction of
+the vertex and of 8 one-ring neighbours, with the same geometry, material and flags.  The Gauss-Seidel iterations then start from ``y + prediction``; a zero network is
+plain VBD bit for bit.  What decides whether the warm start pays is the residual-gated step
+(``SolverVBD.set_residual_gate``): from the same state, the learned and the plain solver iterate
+until the same force residual, and the iterations they need are compared (``gated_steps``).
 
 The previous correction is a feature and never the start itself: starting from
 ``y + (x_prev_solved - y_prev)`` counts the previous step's acceleration twice (it is already in
@@ -54,8 +56,9 @@ def characteristic_length(model) -> np.ndarray:
 class WarmStartMLP:
     """Parameters, optimiser state and feature standardisation of the warm-start network."""
 
-    def __init__(self, device, seed: int = 0):
+    def __init__(self, device, seed: int = 0, feature_set: str = "kinematic"):
         self.device = torch.device(device)
+        self.feature_set = feature_set  # the solver's feature set this network reads
         self.lib = _lib.load()
         sizes = [ctypes.c_int32() for _ in range(5)]
         _lib.check(self.lib.vbd_mlp_sizes(*[ctypes.byref(v) for v in sizes]))
@@ -150,9 +153,10 @@ class WarmStartMLP:
 
     def state_dict(self) -> dict:
         return {"params": self.params.cpu().numpy(), "mean": self.mean.cpu().numpy(),
-                "inv_std": self.inv_std.cpu().numpy()}
+                "inv_std": self.inv_std.cpu().numpy(), "feature_set": self.feature_set}
 
     def load_state_dict(self, d: dict) -> None:
+        self.feature_set = str(d.get("feature_set", "corrections"))
         self.params.copy_(torch.as_tensor(np.asarray(d["params"]), device=self.device))
         self.mean.copy_(torch.as_tensor(np.asarray(d["mean"]), device=self.device))
         self.inv_std.copy_(torch.as_tensor(np.asarray(d["inv_std"]), device=self.device))
@@ -168,13 +172,17 @@ def inertia_target(model, state, dt: float) -> torch.Tensor:
 
 
 def generate_dataset(model, q0, solver, pipe, steps: int, dt: float, target_iterations: int = 20,
-                     samples_per_step: int = 1024, seed: int = 0, trajectory_iterations: int | None = None):
+                     samples_per_step: int = 1024, seed: int = 0, trajectory_iterations: int | None = None,
+                     feature_set: str | tuple = "kinematic", record_every: int = 1):
     """Features and targets from a VBD trajectory.
 
-    At every step: collide, forward, features (with the previous step's correction), then
-    ``target_iterations`` sweeps give the target correction (x - y) / L.  The trajectory advances
-    with ``trajectory_iterations`` plain sweeps from y (default: the target solve itself).
-    Returns raw (unstandardised) features [N,64] and targets [N,3]."""
+    At every ``record_every``-th step: collide, forward, features of ``feature_set`` (with the
+    previous step's correction), then ``target_iterations`` sweeps give the target correction
+    (x - y) / L.  The trajectory advances every step with ``trajectory_iterations`` plain sweeps
+    from y (default: the target solve itself).  Returns raw (unstandardised) features [N,64] and
+    targets [N,3]; with a tuple of feature sets, the features are a dict {set: [N,64]} of the
+    same samples."""
+    sets = (feature_set,) if isinstance(feature_set, str) else tuple(feature_set)
     dev = model.device
     L = torch.from_numpy(characteristic_length(model)).to(dev)
     solvable = torch.from_numpy(((model.particle_flags & 1) != 0) & (model.particle_inv_mass != 0)).to(dev)
@@ -184,100 +192,131 @@ def generate_dataset(model, q0, solver, pipe, steps: int, dt: float, target_iter
     s0.particle_q.copy_(torch.as_tensor(q0, device=dev))
     c = pipe.contacts() if pipe is not None else None
     corr = torch.zeros_like(s0.particle_q)
-    feats = torch.empty((model.particle_count, IN), dtype=torch.float32, device=dev)
+    feats = {fs: torch.empty((model.particle_count, IN), dtype=torch.float32, device=dev) for fs in sets}
     lib = _lib.load()
-    Xs, Ts = [], []
+    Xs, Ts = {fs: [] for fs in sets}, []
     it_traj = target_iterations if trajectory_iterations is None else trajectory_iterations
-    for _ in range(steps):
-        if pipe is not None:
-            pipe.collide(s0, c)
-        y = inertia_target(model, s0, dt)
-        solver.forward(s0, c, dt)
-        _lib.check(lib.vbd_mlp_features(solver._handle, _lib.ptr(corr), None, None, _lib.ptr(feats), solver._stream()))
-        solver.iterate(c, dt, target_iterations)
-        x = solver.positions()
-        T = (x - y) / L[:, None]
-        idx = cand[torch.randint(0, cand.numel(), (min(samples_per_step, cand.numel()),), generator=gen, device=dev)]
-        Xs.append(feats[idx].clone())
-        Ts.append(T[idx].clone())
-        if it_traj != target_iterations:  # advance with the trajectory's own iteration count
-            solver.forward(s0, c, dt)
-            solver.iterate(c, dt, it_traj)
-        solver.finalize(s0, s1, dt)
-        corr = s1.particle_q - y
-        s0, s1 = s1, s0
-    return torch.cat(Xs), torch.cat(Ts)
-
-
-def mean_residual(solver, contacts, dt: float) -> float:
-    """Mean over solved vertices of |f_i| / (m_i |g|) at the current iterate."""
-    _, pv = solver.residual(contacts, dt, per_vertex=True)
-    m = solver.model
-    solvable = torch.from_numpy(((m.particle_flags & 1) != 0) & (m.particle_inv_mass != 0)).to(pv.device)
-    return float(pv[solvable].mean().item())
-
-
-def calibrate_iterations(model, q0, solver, pipe, mlp: WarmStartMLP, steps: int, dt: float,
-                         plain_iterations: int = 10, max_iterations: int = 10, check_every: int = 10,
-                         advance: str = "learned"):
-    """At every ``check_every``-th step, find the fewest warm-started iterations whose mean
-    residual matches plain VBD's after ``plain_iterations`` on the same step (same state).  The
-    trajectory advances with the learned solver (``advance="learned"``) or with plain VBD
-    (``advance="plain"``: teacher forcing, which isolates the per-step effect of the start from
-    the stability of a trajectory driven by it).  Returns (iterations, per-check records)."""
-    dev = model.device
-    lib = _lib.load()
-    s0, s1 = model.state(), model.state()
-    s0.particle_q.copy_(torch.as_tensor(q0, device=dev))
-    c = pipe.contacts() if pipe is not None else None
-    corr = torch.zeros_like(s0.particle_q)
-    work = torch.empty(model.particle_count * 70, dtype=torch.float32, device=dev)
-    need = []
-    records = []
     for step in range(steps):
         if pipe is not None:
             pipe.collide(s0, c)
         y = inertia_target(model, s0, dt)
-        if step % check_every == 0:
-            solver.forward(s0, c, dt)
-            r_plain_k = []
-            for k in range(1, plain_iterations + 1):
-                solver.iterate(c, dt, 1)
-                r_plain_k.append(mean_residual(solver, c, dt))
-            r_plain = r_plain_k[-1]
-            solver.forward(s0, c, dt)
-            _lib.check(lib.vbd_mlp_warm_start(solver._handle, _lib.ptr(mlp.params), _lib.ptr(mlp.w16), _lib.ptr(corr),
-                                              _lib.ptr(mlp.mean), _lib.ptr(mlp.inv_std), _lib.ptr(work), work.numel(),
-                                              solver._stream()))
-            r_k = []
-            k_hit = max_iterations + 1
-            for k in range(1, max_iterations + 1):
-                solver.iterate(c, dt, 1)
-                r = mean_residual(solver, c, dt)
-                r_k.append(r)
-                if r <= r_plain and k_hit > max_iterations:
-                    k_hit = k
-            # the same start without the network: previous correction only
-            solver.forward(s0, c, dt)
-            solver.warm_start(corr.contiguous())
-            k_prev = max_iterations + 1
-            for k in range(1, max_iterations + 1):
-                solver.iterate(c, dt, 1)
-                if mean_residual(solver, c, dt) <= r_plain:
-                    k_prev = k
-                    break
-            need.append(k_hit)
-            records.append({"step": step, "plain": r_plain, "plain_curve": r_plain_k, "warm": r_k, "k": k_hit,
-                            "k_previous_correction": k_prev})
         solver.forward(s0, c, dt)
-        if advance == "plain":
-            solver.iterate(c, dt, plain_iterations)
-        else:  # the learned solver at the current working point
-            _lib.check(lib.vbd_mlp_warm_start(solver._handle, _lib.ptr(mlp.params), _lib.ptr(mlp.w16), _lib.ptr(corr),
-                                              _lib.ptr(mlp.mean), _lib.ptr(mlp.inv_std), _lib.ptr(work), work.numel(),
-                                              solver._stream()))
-            solver.iterate(c, dt, max(1, int(np.percentile(need, 90))) if need else plain_iterations)
+        record = step % max(1, record_every) == 0
+        if record:
+            for fs in sets:
+                solver.set_feature_set(fs)
+                _lib.check(lib.vbd_mlp_features(solver._handle, _lib.ptr(corr), None, None, _lib.ptr(feats[fs]),
+                                                solver._stream()))
+            solver.iterate(c, dt, target_iterations)
+            x = solver.positions()
+            T = (x - y) / L[:, None]
+            idx = cand[torch.randint(0, cand.numel(), (min(samples_per_step, cand.numel()),), generator=gen,
+                                     device=dev)]
+            for fs in sets:
+                Xs[fs].append(feats[fs][idx].clone())
+            Ts.append(T[idx].clone())
+        if not record or it_traj != target_iterations:  # advance with the trajectory's own count
+            if record:
+                solver.forward(s0, c, dt)
+            solver.iterate(c, dt, it_traj)
         solver.finalize(s0, s1, dt)
         corr = s1.particle_q - y
         s0, s1 = s1, s0
-    return int(np.ceil(np.percentile(need, 90))), records
+    X = {fs: torch.cat(Xs[fs]) for fs in sets}
+    return (X[sets[0]] if isinstance(feature_set, str) else X), torch.cat(Ts)
+
+
+def record_plain_states(model, q_start, qd_start, pipe, gate: dict, steps: int, dt: float,
+                        launch: dict | None = None) -> list:
+    """The state before each of ``steps`` residual-gated plain-VBD steps from (q_start, qd_start):
+    [(particle_q, particle_qd)] as device tensors."""
+    from .solvers import SolverVBD
+
+    dev = model.device
+    solver = SolverVBD(model, iterations=10)
+    if launch is not None:
+        solver.set_launch(launch["lanes_per_vertex"], launch["block_size"])
+    solver.set_residual_gate(**gate)
+    c = pipe.contacts() if pipe is not None else None
+    s0, s1 = model.state(), model.state()
+    s0.particle_q.copy_(torch.as_tensor(q_start, device=dev))
+    s0.particle_qd.copy_(torch.as_tensor(qd_start, device=dev))
+    states = []
+    for _ in range(steps):
+        states.append((s0.particle_q.clone(), s0.particle_qd.clone()))
+        if pipe is not None:
+            pipe.collide(s0, c)
+        solver.step(s0, s1, None, c, dt)
+        s0, s1 = s1, s0
+    torch.cuda.synchronize(dev)
+    return states
+
+
+def teacher_forced_steps(model, states: list, pipe, gate: dict, dt: float, mlp: WarmStartMLP | None = None,
+                         launch: dict | None = None, warm: int = 0, timer=None) -> dict:
+    """One residual-gated step from every recorded state of a plain trajectory, by plain VBD
+    (``mlp=None``) or by the learned step mode.  Both arms start each step from the same state,
+    hence the same inertia target y and -- the gate being relative to the residual at y -- the same
+    absolute tolerance: the iterations they need are counted to the same force residual.  The
+    learned solver's correction feature carries over from its own previous step.  The first
+    ``warm`` states are stepped but not counted (the correction feature needs one step of
+    history).  ``timer`` (optional) has ``before()`` / ``after()``, called around each counted
+    collide + step.  Returns the gate statistics of the counted steps and the solver status."""
+    from .solvers import SolverVBD
+
+    solver = SolverVBD(model, iterations=10)
+    if launch is not None:
+        solver.set_launch(launch["lanes_per_vertex"], launch["block_size"])
+    if mlp is not None:
+        solver.set_warm_start(mlp, 10)
+    solver.set_residual_gate(**gate)
+    c = pipe.contacts() if pipe is not None else None
+    s0, s1 = model.state(), model.state()
+    for k, (q, qd) in enumerate(states):
+        if k == warm:
+            solver.gate_stats(reset=True)
+            solver.status(reset=True)
+        s0.particle_q.copy_(q)
+        s0.particle_qd.copy_(qd)
+        counted = k >= warm and timer is not None
+        if counted:
+            timer.before()
+        if pipe is not None:
+            pipe.collide(s0, c)
+        solver.step(s0, s1, None, c, dt)
+        if counted:
+            timer.after()
+    torch.cuda.synchronize(model.device)
+    out = solver.gate_stats()
+    out["status"] = solver.status()
+    return out
+
+
+def gated_steps(model, q_start, qd_start, pipe, gate: dict, steps: int, dt: float, mlp: WarmStartMLP | None = None,
+                launch: dict | None = None) -> dict:
+    """``steps`` residual-gated steps (``SolverVBD.set_residual_gate(**gate)``) from the state
+    (q_start, qd_start): plain VBD (``mlp=None``) or the learned step mode.  Returns the gate
+    statistics (mean iterations, capped steps, residuals), the solver status and the end state."""
+    from .solvers import SolverVBD
+
+    dev = model.device
+    solver = SolverVBD(model, iterations=10)
+    if launch is not None:
+        solver.set_launch(launch["lanes_per_vertex"], launch["block_size"])
+    if mlp is not None:
+        solver.set_warm_start(mlp, 10)
+    solver.set_residual_gate(**gate)
+    c = pipe.contacts() if pipe is not None else None
+    s0, s1 = model.state(), model.state()
+    s0.particle_q.copy_(torch.as_tensor(q_start, device=dev))
+    s0.particle_qd.copy_(torch.as_tensor(qd_start, device=dev))
+    for _ in range(steps):
+        if pipe is not None:
+            pipe.collide(s0, c)
+        solver.step(s0, s1, None, c, dt)
+        s0, s1 = s1, s0
+    torch.cuda.synchronize(dev)
+    out = solver.gate_stats()
+    out["status"] = solver.status()
+    out["q"] = s0.particle_q.clone()
+    return out

@@ -123,6 +123,7 @@ class SolverVBD(SolverBase):
         self._opts = opts
         self._warm = None
         self._gate = None
+        self._feature_set = "corrections"
         self._create()
 
     def _create(self) -> None:
@@ -336,19 +337,33 @@ class SolverVBD(SolverBase):
         _lib.check(self._lib.vbd_step_kernel_count(self._handle, ctypes.byref(k)))
         return k.value
 
+    FEATURE_SETS = {"corrections": 0, "kinematic": 1}
+
+    def set_feature_set(self, name: str) -> None:
+        """Input features of the learned warm start (``vbd_set_feature_set``): ``"corrections"``
+        (the previous step's solver correction of the vertex and its one-ring, the default) or
+        ``"kinematic"`` (previous displacement, velocity and inertia offset only)."""
+        if name not in self.FEATURE_SETS:
+            raise ValueError(f"feature set must be one of {sorted(self.FEATURE_SETS)}")
+        self._feature_set = name
+        _lib.check(self._lib.vbd_set_feature_set(self._handle, self.FEATURE_SETS[name]))
+
     def set_warm_start(self, mlp, iterations: int) -> None:
         """Learned warm start as the step mode: every ``step`` runs forward, the MLP's prediction,
-        ``iterations`` colour sweeps and finalize (``mlp=None`` turns it off)."""
+        ``iterations`` colour sweeps and finalize (``mlp=None`` turns it off).  The solver takes
+        the network's feature set (``mlp.feature_set``)."""
         self._warm = mlp  # keeps the network's buffers alive while the solver points at them
         self._warm_iterations = int(iterations)
         if mlp is None:
             _lib.check(self._lib.vbd_set_warm_start(self._handle, None, None, None, None, 0))
             return
+        self.set_feature_set(getattr(mlp, "feature_set", "corrections"))
         _lib.check(self._lib.vbd_set_warm_start(self._handle, _lib.ptr(mlp.params), _lib.ptr(mlp.w16),
                                                 _lib.ptr(mlp.mean), _lib.ptr(mlp.inv_std), int(iterations)))
 
     def set_residual_gate(self, tolerance: float | None, max_iterations: int = 100, check_every: int = 1,
-                          relative: bool = False, norm: str = "max", residual: str = "jacobi") -> None:
+                          relative: bool = False, norm: str = "max", residual: str = "jacobi",
+                          rounds_per_body: int = 0) -> None:
         """Residual-gated steps (no reference counterpart; the reference runs a fixed iteration count,
         ``solver_vbd.py:1817-1819``): each ``step`` iterates until the Jacobi force residual norm --
         ``max_i |f_i| / (m_i |g|)`` (``norm="max"``) or its mean over the solved vertices
@@ -357,16 +372,20 @@ class SolverVBD(SolverBase):
         ``residual="jacobi"`` evaluates the residual at the current iterate (one extra sweep-sized
         launch per check); ``residual="sweep"`` uses the Gauss-Seidel residual the sweeps form
         anyway (each vertex's force when its color is solved; no extra launch).  The loop runs on
-        the device (a conditional node of the step's CUDA graph).  ``tolerance=None`` turns the
-        gate off."""
+        the device (a conditional node of the step's CUDA graph); with ``residual="sweep"`` one
+        pass of its body runs ``rounds_per_body`` check rounds (0: the library's default, 4), the
+        rounds after the decision returning at once.  ``tolerance=None`` turns the gate off."""
         if norm not in ("max", "mean"):
             raise ValueError("norm must be 'max' or 'mean'")
         if residual not in ("jacobi", "sweep"):
             raise ValueError("residual must be 'jacobi' or 'sweep'")
+        if not 0 <= int(rounds_per_body) <= 15:
+            raise ValueError("rounds_per_body must be in [0, 15]")
         self._gate = None if tolerance is None else (float(tolerance), int(max_iterations), int(check_every),
-                                                     bool(relative), norm, residual)
+                                                     bool(relative), norm, residual, int(rounds_per_body))
         tol = 0.0 if tolerance is None else float(tolerance)
-        mode = (1 if relative else 0) | (2 if norm == "mean" else 0) | (4 if residual == "sweep" else 0)
+        mode = ((1 if relative else 0) | (2 if norm == "mean" else 0) | (4 if residual == "sweep" else 0)
+                | (int(rounds_per_body) << 8))
         _lib.check(self._lib.vbd_set_residual_gate(self._handle, ctypes.c_float(tol), int(max_iterations),
                                                    int(check_every), mode))
 
@@ -384,6 +403,8 @@ class SolverVBD(SolverBase):
             "last_residual": g.last_residual,
             "last_start_residual": g.last_start_residual,
             "last_reference_residual": g.last_reference_residual,
+            "body_programmatic_edges": g.body_programmatic_edges,
+            "body_passes": g.body_passes,
         }
 
     def set_spin_limit(self, spins: int) -> None:
@@ -408,6 +429,8 @@ class SolverVBD(SolverBase):
         self.model.notify_model_changed()
         self._create()
         self._lib.vbd_solver_destroy(old)
+        if self._feature_set != "corrections":
+            self.set_feature_set(self._feature_set)
         if self._warm is not None:
             self.set_warm_start(self._warm, self._warm_iterations)
         if getattr(self, "_gate", None) is not None:

@@ -270,8 +270,8 @@ def test_sweep_residual_gate(norm):
         st = solver.gate_stats(reset=True)
         assert st["last_iterations"] == k and st["capped_steps"] == 1
         curve.append(st["last_residual"])
-    # the loop body is the round's sweeps; the last of them also takes the decision
-    assert all(np.isfinite(curve[1:])) and st["body_kernels"] == len(model.particle_color_groups)
+    # one pass of the loop body is 4 check rounds of the sweeps; each round's last sweep decides
+    assert all(np.isfinite(curve[1:])) and st["body_kernels"] == 4 * len(model.particle_color_groups)
     kd, tol = _clear_drop(curve, start=3, gap=0.99 if norm == "max" else 0.9995)
     solver.set_residual_gate(tol, max_iterations=40, norm=norm, residual="sweep")
     qg, qdg, _ = _run(model, solver, q, qd)
@@ -292,6 +292,34 @@ def test_sweep_residual_gate(norm):
     assert k2 == min(k for k in range(2, 17, 2) if curve[k] <= tol)
     print(f"sweep residual ({norm}): R_1..R_6 {[round(x, 3) for x in curve[1:7]]}, tolerance {tol:.5g} -> "
           f"{kd} iterations (every 2: {k2})")
+
+
+def test_sweep_gate_rounds_per_body_do_not_change_the_step():
+    """The rounds per pass of the device-side loop body only change how the loop is launched: the
+    same stop, the same bits, ceil(iterations / rounds) passes, and the sweeps after the decision
+    change nothing."""
+    model, q, qd = _hanging_state(steps=45, seed=3)
+    colors = len(model.particle_color_groups)
+    qf, qdf, _ = _run(model, SolverVBD(model, iterations=5), q, qd)
+    for tol, cap in ((1e-30, 5), (0.9, 40)):  # stopped by the cap mid-body; by the tolerance
+        out = {}
+        for rounds in (1, 3, 4, 7):
+            solver = SolverVBD(model, iterations=10)
+            solver.set_residual_gate(tol, max_iterations=cap, relative=True, norm="mean", residual="sweep",
+                                     rounds_per_body=rounds)
+            qg, qdg, _ = _run(model, solver, q, qd)
+            st = solver.gate_stats()
+            k = st["last_iterations"]
+            assert st["steps"] == 1 and st["body_kernels"] == rounds * colors
+            assert st["body_passes"] == -(-k // rounds)
+            out[rounds] = (k, qg, qdg, st["last_residual"])
+        k1, q1, qd1, r1 = out[1]
+        for rounds, (k, qg, qdg, r) in out.items():
+            assert k == k1 and r == r1 and np.array_equal(qg, q1) and np.array_equal(qdg, qd1), rounds
+        if cap == 5:
+            assert k1 == 5 and np.array_equal(q1, qf) and np.array_equal(qd1, qdf)
+    with pytest.raises(ValueError):
+        SolverVBD(model, iterations=10).set_residual_gate(0.9, residual="sweep", rounds_per_body=16)
 
 
 def test_relative_sweep_gate_refers_to_the_jacobi_residual_at_y():

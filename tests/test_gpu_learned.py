@@ -146,30 +146,170 @@ def test_zero_network_warm_start_is_plain_vbd():
     assert torch.equal(out[0][1], out[1][1])
 
 
-def test_learned_warm_start_ab_measurement():
-    """A/B of the learned start against plain VBD on a held-out drape: the network trains, and the
-    calibration reports, per checked step, plain VBD's 10-iteration mean residual and the fewest
-    warm-started iterations that match it (11 = not reached within 10)."""
+def test_kinematic_features_match_a_restatement():
+    """Kinematic feature set: previous displacement v dt / L, velocity, inertia offset (y - x) / L,
+    one-ring size and solvable flag against a torch restatement from the state (pins included)."""
     dt = 1.0 / 600.0
-    model, q0 = scenes.single_cloth(n=48, side=1.0, seed=30, pin_top_corners=False, ground=0.0,
-                                    sphere=((0.0, 0.0, 0.5), 0.4), height=0.95, z_noise=0.0)
+    model, q0 = scenes.single_cloth(n=20, side=1.0, seed=8, pin_top_corners=True, ground=None, height=0.5)
+    solver = SolverVBD(model, iterations=4)
+    solver.set_feature_set("kinematic")
+    s = model.state()
+    dev = s.particle_q.device
+    s.particle_q.copy_(torch.from_numpy(q0).to(dev))
+    g = torch.Generator(device="cpu").manual_seed(3)
+    s.particle_qd.copy_((torch.randn(model.particle_count, 3, generator=g) * 0.3).to(dev))
+    solver.forward(s, None, dt)
+    feats = torch.empty(model.particle_count, 64, device=dev)
+    lib = L._lib.load()
+    L._lib.check(lib.vbd_mlp_features(solver._handle, None, None, None, L._lib.ptr(feats), solver._stream()))
+    f = feats.cpu().double()
+    Lc = torch.from_numpy(L.characteristic_length(model)).double()
+    solvable = torch.from_numpy(((model.particle_flags & 1) != 0) & (model.particle_inv_mass != 0))
+    v = s.particle_qd.cpu().double()
+    gvec = torch.tensor(np.asarray(model.gravity, dtype=np.float64).reshape(-1, 3)[0])
+    y_off = torch.where(solvable[:, None], (v + gvec * dt) * dt, torch.zeros_like(v))
+    vdt = torch.where(solvable[:, None], v * dt, torch.zeros_like(v))
+    tol = 1e-5
+    assert torch.allclose(f[:, 0:3], vdt / Lc[:, None], atol=tol * 10, rtol=1e-4)
+    assert torch.allclose(f[:, 3:6], torch.where(solvable[:, None], v, torch.zeros_like(v)), atol=1e-4, rtol=1e-4)
+    assert torch.allclose(f[:, 6:9], y_off / Lc[:, None], atol=tol * 10, rtol=1e-4)
+    assert torch.equal(f[:, 39], solvable.double())
+    assert int(solvable.sum()) == model.particle_count - 2
+    assert (f[:, 38] > 0).all() and (f[:, 38] <= 1).all()
+    assert (f[:, 40:63] == 0).all() and (f[:, 63] == 1).all()
+
+
+def test_warm_start_prediction_is_bounded():
+    """A prediction longer than 0.25 characteristic lengths moves the start by 0.25 L along it; a
+    non-finite prediction leaves the start at y."""
+    dt = 1.0 / 600.0
+    model, q0 = scenes.single_cloth(n=16, side=1.0, seed=2, pin_top_corners=True, ground=None, height=0.5)
+    solver = SolverVBD(model, iterations=4)
+    s = model.state()
+    dev = s.particle_q.device
+    s.particle_q.copy_(torch.from_numpy(q0).to(dev))
+    Lc = torch.from_numpy(L.characteristic_length(model)).to(dev)
+    solvable = torch.from_numpy(((model.particle_flags & 1) != 0) & (model.particle_inv_mass != 0)).to(dev)
+    y = L.inertia_target(model, s, dt)
+    lib = L._lib.load()
+    work = torch.empty(model.particle_count * 70, device=dev)
+    for b3, expect in (((3.0e3, 4.0e3, 0.0), (0.15, 0.2, 0.0)), ((float("nan"), 0.0, 0.0), (0.0, 0.0, 0.0))):
+        mlp = L.WarmStartMLP("cuda:0", seed=1)
+        mlp.params.zero_()
+        mlp.params[L.OFF_B3:L.OFF_B3 + 3] = torch.tensor(b3, device=dev)
+        mlp.pack()
+        solver.forward(s, None, dt)
+        L._lib.check(lib.vbd_mlp_warm_start(solver._handle, L._lib.ptr(mlp.params), L._lib.ptr(mlp.w16), None,
+                                            None, None, L._lib.ptr(work), work.numel(), solver._stream()))
+        x = solver.positions()
+        want = y + torch.tensor(expect, device=dev) * Lc[:, None] * solvable[:, None]
+        assert torch.allclose(x, want, atol=1e-6, rtol=0), float((x - want).abs().max())
+
+
+# The residual gate of the A/B: the mean Gauss-Seidel residual must fall to RHO x the mean Jacobi
+# residual at the step's inertia target (what plain VBD reaches in about 10 iterations here).
+DT = 1.0 / 600.0
+FEATURE_SETS = ("kinematic", "corrections")
+
+
+def _gate(rho):
+    return {"tolerance": rho, "max_iterations": 100, "check_every": 1, "relative": True, "norm": "mean",
+            "residual": "sweep"}
+
+
+def _settle(model, q0, pipe, steps):
     solver = SolverVBD(model, iterations=10)
+    c = pipe.contacts()
+    s0, s1 = model.state(), model.state()
+    s0.particle_q.copy_(torch.as_tensor(q0, device=model.device))
+    for _ in range(steps):
+        pipe.collide(s0, c)
+        solver.step(s0, s1, None, c, DT)
+        s0, s1 = s1, s0
+    return s0.particle_q.clone(), s0.particle_qd.clone()
+
+
+def _ab(train_scenes, test_scene, steps, samples, rho, counted=20, warm=3):
+    """Trains one network per feature set on plain-VBD trajectories of ``train_scenes``; records the
+    gated plain trajectory of the held-out ``test_scene`` (settled for 150 steps with the fixed
+    10-iteration loop) and steps every arm from each recorded state (the same state, hence the
+    same absolute tolerance); the last ``counted`` steps are compared."""
+    Xs, Ts = {fs: [] for fs in FEATURE_SETS}, []
+    for i, (model, q0) in enumerate(train_scenes):
+        X, T = L.generate_dataset(model, q0, SolverVBD(model, iterations=10),
+                                  CollisionPipeline(model, soft_contact_margin=5e-3), steps=steps, dt=DT,
+                                  target_iterations=20, samples_per_step=samples, seed=i, trajectory_iterations=10,
+                                  feature_set=FEATURE_SETS)
+        for fs in FEATURE_SETS:
+            Xs[fs].append(X[fs])
+        Ts.append(T)
+    T = torch.cat(Ts)
+    model, q0 = test_scene
     pipe = CollisionPipeline(model, soft_contact_margin=5e-3)
-    X, T = L.generate_dataset(model, q0, solver, pipe, steps=300, dt=dt, target_iterations=20, samples_per_step=1024,
-                              trajectory_iterations=10)
-    mlp = L.WarmStartMLP("cuda:0", seed=4)
-    mlp.set_standardization(X)
-    hist = mlp.train(mlp.standardize(X), T, epochs=40, batch=8192, lr=2e-3)
-    assert hist[-1] < hist[0]
-    model, q_test = scenes.single_cloth(n=48, side=1.0, seed=31, pin_top_corners=False, ground=0.0,
-                                        sphere=((0.1, 0.05, 0.5), 0.4), height=0.95, z_noise=0.0)
-    solver = SolverVBD(model, iterations=10)
-    pipe = CollisionPipeline(model, soft_contact_margin=5e-3)
-    k, records = L.calibrate_iterations(model, q_test, solver, pipe, mlp, steps=100, dt=dt, check_every=20)
-    print("iterations to reach plain-10 residual (learned):", [r["k"] for r in records])
-    print("iterations to reach plain-10 residual (previous correction only):", [r["k_previous_correction"] for r in records])
-    assert len(records) == 5
-    for r in records:
-        assert np.isfinite(r["plain"]) and len(r["plain_curve"]) == 10
-        assert 1 <= r["k"] <= 11 and 1 <= r["k_previous_correction"] <= 11
-    assert 1 <= k <= 11
+    q, qd = _settle(model, q0, pipe, 150)
+    states = L.record_plain_states(model, q, qd, pipe, _gate(rho), warm + counted, DT)
+    out = {"plain": L.teacher_forced_steps(model, states, pipe, _gate(rho), DT, warm=warm)}
+    for fs in FEATURE_SETS:
+        X = torch.cat(Xs[fs])
+        mlp = L.WarmStartMLP("cuda:0", seed=0, feature_set=fs)
+        mlp.set_standardization(X)
+        hist = mlp.train(mlp.standardize(X), T, epochs=20, batch=16384, lr=2e-3)
+        assert hist[-1] < hist[0]
+        out[fs] = L.teacher_forced_steps(model, states, pipe, _gate(rho), DT, mlp=mlp, warm=warm)
+        out[fs]["mse"] = (hist[0], hist[-1])
+    for k, v in out.items():
+        print(f"{k}: mean iterations {v['mean_iterations']:.2f}, capped {v['capped_steps']}, "
+              f"residual {v['last_residual']:.4g} (reference {v['last_reference_residual']:.4g}), "
+              f"status {v['status']}")
+    return out
+
+
+@pytest.fixture(scope="module")
+def drape_ab():
+    """The benchmark's draped cloth (256 x 256, 2 m, on a sphere), trained on two other drapes."""
+    train = [scenes.draped_cloth(n=256, seed=seed, offset=off, height=0.904)
+             for seed, off in ((1, (0.2, -0.1)), (4, (-0.15, 0.25)))]
+    return _ab(train, scenes.draped_cloth(n=256, seed=0, height=0.904), steps=300, samples=2048, rho=0.9)
+
+
+@pytest.fixture(scope="module")
+def batched_ab():
+    """128 worlds of the batched distribution, trained on 128 worlds of another seed."""
+    train = [scenes.batched_worlds(128, seed=1)]
+    return _ab(train, scenes.batched_worlds(128, seed=0), steps=400, samples=2048, rho=0.95)
+
+
+def _check_clean(r, plain=None):
+    """No rejected update, no timed-out wait; a learned arm caps no more steps than plain VBD on
+    the same states (a step that caps in both counts max_iterations in both)."""
+    assert r["status"]["nonfinite_updates"] == 0 and r["status"]["timeouts"] == 0
+    if plain is not None:
+        assert r["capped_steps"] <= plain["capped_steps"]
+
+
+def _ratios(r):
+    plain = r["plain"]
+    for fs in FEATURE_SETS:
+        _check_clean(r[fs], plain)
+    _check_clean(plain)
+    out = {fs: r[fs]["mean_iterations"] / plain["mean_iterations"] for fs in FEATURE_SETS}
+    print("iterations to the same residual, learned / plain:", {k: round(v, 3) for k, v in out.items()})
+    return out
+
+
+def test_learned_warm_start_at_equal_residual_on_a_held_out_drape(drape_ab):
+    """From the same states (so to the same absolute residual), the kinematic network needs at
+    most 0.95x the iterations of plain VBD (measured on a B200: 0.88); the network fed the previous
+    step's correction needs at least 1.5x (measured: 2.3) -- its feature, taken from its own
+    previous solve, carries that solve's smooth error into the start."""
+    ratio = _ratios(drape_ab)
+    assert ratio["kinematic"] <= 0.95
+    assert ratio["corrections"] >= 1.5
+
+
+def test_learned_warm_start_at_equal_residual_on_batched_worlds(batched_ab):
+    """The same on held-out batched worlds: no gain (kinematic within 1.05x of plain VBD's
+    iterations, measured 1.00), the corrections network at least 1.5x (measured 4.5)."""
+    ratio = _ratios(batched_ab)
+    assert ratio["kinematic"] <= 1.05
+    assert ratio["corrections"] >= 1.5
