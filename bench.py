@@ -120,8 +120,12 @@ def algorithmic_bytes_per_iteration(model) -> int:
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed region: through NVML
+    every millisecond from a thread (a timed region of a few milliseconds still gets samples);
+    where NVML is unavailable, nvidia-smi every 200 ms."""
 
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -130,8 +134,41 @@ class ClockSampler:
         self.gpu_index = gpu_index
         self.proc = None
         self.path = None
+        self.thread = None
+        self.samples = []
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:  # the NVML device of this process's CUDA device, by PCI bus id
+            props = torch.cuda.get_device_properties(self.gpu_index)
+            bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.gpu_index)
 
     def start(self):
+        import threading
+
+        try:
+            nv, h = self._nvml_handle()
+            reasons_fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self.stop_flag = False
+
+            def poll():
+                while not self.stop_flag:
+                    self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), reasons_fn(h)))
+                    time.sleep(0.001)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
@@ -143,6 +180,14 @@ class ClockSampler:
             self.proc = None
 
     def stop(self) -> dict | None:
+        if self.thread is not None:
+            self.stop_flag = True
+            self.thread.join(timeout=5)
+            if not self.samples:
+                return None
+            reasons = sorted({name for _, bits in self.samples for name, bit in self.REASONS if bits & bit})
+            return {"sm_mhz": statistics.median(c for c, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(self.samples), "source": "nvml, 1 ms"}
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -162,10 +207,10 @@ class ClockSampler:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = [n for n, _ in self.REASONS]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi, 200 ms"}
 
 
 def measured_peaks() -> dict:
