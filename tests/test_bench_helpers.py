@@ -66,7 +66,22 @@ def test_clock_samples_give_median_max_and_active_reasons():
         "garbage line",
     ]
     out = _sampler_with(rows).stop()
-    assert out == {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
+    assert out == {"sm_mhz": 1965.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3,
+                   "source": "nvidia-smi, 200 ms"}
+
+
+def test_nvml_clock_samples_give_median_max_and_active_reasons():
+    s = bench.ClockSampler(0)
+    s.thread, s.stop_flag, s.max_mhz = _FakeThread(), False, 1965
+    s.samples = [(1965, 0x0), (1950, 0x4), (1965, 0x0), (1200, 0x8 | 0x20)]
+    out = s.stop()
+    assert out == {"sm_mhz": 1957.5, "sm_max_mhz": 1965, "samples": 4, "source": "nvml, 1 ms",
+                   "reasons": ["hw_slowdown", "sw_power_cap", "sw_thermal_slowdown"]}
+
+
+class _FakeThread:
+    def join(self, timeout=None):
+        pass
 
 
 def test_clock_samples_flag_the_rejecting_reasons():
