@@ -16,8 +16,9 @@ package and Newton pipelines:
   :881-972), a ``cache_index``, and the payload as a ``"numpy.ndarray"`` entry whose ``data``
   is the JSON text of the nested list (``serialize_ndarray`` :281-346).
 
-Only ``.json`` is written here; ``.bin`` (CBOR2) needs the ``cbor2`` package, as in the
-reference.  The model part holds the cloth fields (particles, triangles, hinges, static shapes,
+``.json`` and ``.bin`` are written and read; ``.bin`` is the same tree in CBOR with every
+array's payload as its C-order bytes (the ``cbor2`` branch of ``serialize_ndarray``, :299-312)
+and needs the ``cbor2`` package, as in the reference.  The model part holds the cloth fields (particles, triangles, hinges, static shapes,
 colors, contact material, gravity); a Newton ``ViewerFile`` loads it field by field into a
 ``Model`` (its transfer is source-driven), and ``load_model`` here restores a ``Model`` of this
 package (adjacency and colors rebuilt).

@@ -43,9 +43,12 @@ def test_file_layout_matches_the_viewerfile_container(tmp_path):
     assert len(set(idx)) == len(idx)
 
 
-def test_round_trip_model_and_states(tmp_path):
+@pytest.mark.parametrize("ext", [".json", ".bin"])
+def test_round_trip_model_and_states(tmp_path, ext):
+    if ext == ".bin":
+        pytest.importorskip("cbor2")
     model, q0 = _scene()
-    rec = RecorderFile(str(tmp_path / "run.json"), auto_save=False)
+    rec = RecorderFile(str(tmp_path / ("run" + ext)), auto_save=False)
     rec.set_model(model)
     s = model.state()
     frames = []
@@ -57,7 +60,7 @@ def test_round_trip_model_and_states(tmp_path):
         frames.append(s.particle_q.clone())
     rec.save_recording()
 
-    back = RecorderFile(str(tmp_path / "run.json"))
+    back = RecorderFile(str(tmp_path / ("run" + ext)))
     back.load_recording()
     assert back.get_frame_count() == 4 and back.has_model()
     m2 = Model("cpu")
@@ -75,6 +78,25 @@ def test_round_trip_model_and_states(tmp_path):
         assert torch.allclose(s2.particle_qd, torch.full_like(s2.particle_qd, 0.1 * k))
     with pytest.raises(IndexError):
         back.load_state(s2, 4)
+
+
+def test_binary_file_holds_the_arrays_as_cbor_byte_strings(tmp_path):
+    """.bin: the same containers, each array's payload its C-order bytes with the numpy dtype
+    string (serialize_ndarray's cbor2 branch, viewer_file.py:299-312)."""
+    cbor2 = pytest.importorskip("cbor2")
+    model, q0 = _scene()
+    rec = RecorderFile(str(tmp_path / "cloth.bin"), auto_save=False)
+    rec.set_model(model)
+    rec.log_state(model.state())
+    rec.save_recording()
+    data = cbor2.loads((tmp_path / "cloth.bin").read_bytes())
+    pq = data["items"]["model"]["attributes"]["particle_q"]
+    assert pq["__type__"] == "warp.array" and pq["__dtype__"] == "<class 'warp.types.vec3f'>"
+    payload = pq["data"]
+    assert payload["__type__"] == "numpy.ndarray" and payload["dtype"] == "<f4" and payload["order"] == "C"
+    assert list(payload["shape"]) == [model.particle_count, 3]
+    got = np.frombuffer(payload["binary_data"], dtype=np.float32).reshape(model.particle_count, 3)
+    np.testing.assert_array_equal(got, model.particle_q)
 
 
 def test_binary_format_needs_cbor2(tmp_path):
