@@ -42,16 +42,13 @@ constexpr int kGateDefaultRounds = 4;        // sweep mode: check rounds per loo
 // warp w into slot w mod kGateSlots), so that the atomics of a large sweep do not queue on a few
 // lines: atomics on one address serialize at the L2.
 constexpr int kGateSlots = 256;
-constexpr int kElectGroups = 64;  // first-level counters of the deciding sweep's last-block election
 constexpr int kSumStride = 16;  // unsigned long long per 128-byte line
 constexpr int kMaxStride = 32;  // unsigned per 128-byte line
 
 struct GateState {
     unsigned long long sum[kGateSlots * kSumStride];  // fixed-point sums of the residuals (resid_fixed)
     unsigned maxv[kGateSlots * kMaxStride];  // max residual (float bits; atomicMax target)
-    unsigned done_sub[kElectGroups * kMaxStride];  // last-block election, first level (one line per group)
     int iters;               // iterations run so far in this step
-    unsigned done;           // groups of the deciding sweep's blocks that have finished (second level)
     unsigned stop;           // 1 once this step's gate has decided: later sweeps of the loop body return
     int pad;
     float ref;               // relative mode: the step's reference residual
@@ -315,10 +312,6 @@ struct SweepArgs {
     const int* perm;
     float inv_g;             // 1/|g| (0 when g = 0)
     int no_pdl;              // host side: launch without the programmatic-dependent-launch attribute
-    // residual gate, sweep mode: the round's last color also decides (last block to finish)
-    GateState* gate_state;   // NULL: this sweep does not decide
-    cudaGraphConditionalHandle gate_handle;
-    GateParams gate_params;
     // residual gate, later rounds of an unrolled loop body: return at once when the step's gate
     // has already decided (GateState::stop); NULL otherwise
     const unsigned* gate_stop;
@@ -615,39 +608,39 @@ __device__ __forceinline__ void reduce_residual(const SweepArgs& a, float r, boo
 }
 
 // Block-collective (every thread of the block calls it; blockDim a multiple of 32, at most 256):
-// the same reduction, with the warps' results combined in shared memory so that one thread adds
-// the block's max and sum to slot (block mod kGateSlots) -- one atomic per block, not per warp.
+// the same reduction for a sweep whose vertices are held by lanes 0, L, 2L, ... of each warp (the
+// others pass r = 0): the warp's values are combined over those lanes only, the warps' results in
+// shared memory, and one thread adds the block's sum (and max, in max mode) to slot (block mod
+// kGateSlots) -- one atomic per block.
+template <int L>
 __device__ __forceinline__ void reduce_residual_block(const SweepArgs& a, float r, bool counted) {
     __shared__ unsigned long long s_sum[8];
     __shared__ unsigned s_max[8];
-    __shared__ int s_any[8];
     const unsigned full = 0xffffffffu;
     const int w = threadIdx.x >> 5;
-    const unsigned mx = __reduce_max_sync(full, __float_as_uint(r));
-    const bool any = __any_sync(full, counted);
+    const bool want_max = a.gate_max != nullptr;
+    unsigned mx = __float_as_uint(r);
     unsigned long long sum = counted ? resid_fixed(r) : 0ull;
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(full, sum, off);
+    for (int off = 16; off >= L; off >>= 1) {
+        sum += __shfl_xor_sync(full, sum, off);
+        if (want_max) mx = max(mx, __shfl_xor_sync(full, mx, off));
+    }
     if ((threadIdx.x & 31) == 0) {
         s_sum[w] = sum;
         s_max[w] = mx;
-        s_any[w] = any ? 1 : 0;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long bs = 0ull;
         unsigned bm = 0u;
-        int ba = 0;
         for (int k = 0; k < static_cast<int>(blockDim.x >> 5); ++k) {
             bs += s_sum[k];
             bm = max(bm, s_max[k]);
-            ba |= s_any[k];
         }
-        if (ba) {
-            const int slot = static_cast<int>(blockIdx.x & (kGateSlots - 1));
-            if (a.gate_max) atomicMax(a.gate_max + slot * kMaxStride, bm);
-            if (a.gate_sum) atomicAdd(a.gate_sum + slot * kSumStride, bs);
-        }
+        const int slot = static_cast<int>(blockIdx.x & (kGateSlots - 1));
+        if (want_max) atomicMax(a.gate_max + slot * kMaxStride, bm);
+        if (a.gate_sum && bs) atomicAdd(a.gate_sum + slot * kSumStride, bs);
     }
 }
 
@@ -743,7 +736,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a) {
     }
     if (kGate) {
         // the same update, and the vertex's force norm before it (the Gauss-Seidel residual of
-        // the sweep) reduced per warp into the residual gate's accumulators
+        // the sweep) reduced per block into the residual gate's accumulators
         float rg = 0.0f;
         bool counted = false;
         if (valid && lane == 0) {
@@ -759,40 +752,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a) {
                 solve_and_commit(a, i, pv, h, f);
             }
         }
-        reduce_residual_block(a, rg, counted);
-        if (a.gate_state) {
-            // the round's last color: the last block to finish reduces the slots and decides.  The
-            // election has two levels so that no counter takes more than ~grid/64 atomics: block
-            // b counts itself done in group b mod G (G = min(kElectGroups, grid) counters on
-            // separate lines);
-            // the last block of a group counts the group done; the last group's last block
-            // decides.  Every block's slot atomics are fenced before it counts itself, and every
-            // group's count before the group is counted (the fences order the chain).
-            __shared__ unsigned s_last;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                const unsigned groups = min(gridDim.x, static_cast<unsigned>(kElectGroups));
-                const unsigned g = blockIdx.x % groups;
-                const unsigned members = (gridDim.x - g + groups - 1) / groups;
-                unsigned* sub = &a.gate_state->done_sub[g * kMaxStride];
-                s_last = 0u;
-                __threadfence();
-                if (atomicAdd(sub, 1u) == members - 1) {
-                    *sub = 0u;  // the group's last block: no other block touches it in this launch
-                    __threadfence();
-                    s_last = (atomicAdd(&a.gate_state->done, 1u) == groups - 1) ? 1u : 0u;
-                }
-            }
-            __syncthreads();
-            if (s_last && threadIdx.x < 32) {
-                __threadfence();
-                const float r = gate_take_warp(a.gate_state, a.gate_params.mean, a.gate_params.count);
-                if (threadIdx.x == 0) {
-                    gate_decide(a.gate_state, a.gate_handle, r, a.gate_params);
-                    a.gate_state->done = 0u;
-                }
-            }
-        }
+        reduce_residual_block<L>(a, rg, counted);
         return;
     }
     if (!valid || lane != 0) return;
@@ -1081,6 +1041,7 @@ __global__ void gather_positions_kernel(const int* perm, const float4* pos, floa
 // every solved vertex; or the Gauss-Seidel residual the last round's sweeps accumulated) decide
 // whether the loop runs another round.  One warp.
 __global__ void gate_check_kernel(GateState* g, cudaGraphConditionalHandle handle, GateParams p) {
+    if (p.first != 1 && g->stop) return;  // a later round of a loop body that has already decided
     const float r = gate_take_warp(g, p.mean, p.count);
     if (threadIdx.x == 0) gate_decide(g, handle, r, p);
 }
@@ -1334,18 +1295,10 @@ static int enqueue_forward(SolverImpl& s, const float* q_in, const float* qd_in,
     return VBD_OK;
 }
 
-// The decision a round's last sweep makes in sweep mode (GateState, while-node handle, params).
-struct GateCheck {
-    GateState* state;
-    cudaGraphConditionalHandle handle;
-    GateParams params;
-};
-
 // gate: also accumulate the color's Gauss-Seidel residual into the residual gate (sweep mode);
-// check: this sweep also takes the round's decision
+// skip_when_decided: return at once once the step's gate has decided (later rounds of a loop body)
 static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float dt, cudaStream_t st,
-                          bool first_iteration = true, bool gate = false, const GateCheck* check = nullptr,
-                          bool skip_when_decided = false) {
+                          bool first_iteration = true, bool gate = false, bool skip_when_decided = false) {
     const VbdModelImpl& m = *s.m;
     SweepArgs a = make_sweep_args(s, c, dt);
     a.prefetch_records = first_iteration ? 1 : 0;
@@ -1353,11 +1306,6 @@ static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float 
     if (gate) {
         a.gate_max = s.gate_mean ? nullptr : s.gate->maxv;
         a.gate_sum = s.gate_mean ? s.gate->sum : nullptr;
-    }
-    if (check) {
-        a.gate_state = check->state;
-        a.gate_handle = check->handle;
-        a.gate_params = check->params;
     }
     a.v_begin = m.color_start[color];
     a.v_end = m.color_start[color + 1];
@@ -1493,21 +1441,20 @@ static int enqueue_gated_iterations(SolverImpl& s, const VbdContacts* c, float d
     cudaGraph_t body = params.conditional.phGraph_out[0];
     VBD_CUDA_TRY(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
     VBD_CUDA_TRY(cudaStreamBeginCaptureToGraph(s.body_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    // sweep mode: the body holds gate_rounds rounds, each deciding after its last sweep; the
-    // sweeps of a round after the decision return at once, so the loop's per-body cost (the body
-    // boundary, where consecutive sweeps cannot overlap) is paid once per gate_rounds rounds
+    // sweep mode: the body holds gate_rounds rounds; the last iteration of a round accumulates
+    // the sweep residuals and a one-warp check kernel after it decides; once decided, the rest
+    // of the body returns at once.  (A decision taken by the round's last sweep itself -- its last
+    // block to finish, found by an election over atomic counters -- cost 14 us more per round at
+    // 1.89 M vertices: every block of that sweep had to take part.)
     const int rounds = sweep ? s.gate_rounds : 1;
     for (int u = 0; u < rounds; ++u) {
         for (int k = 0; k < s.gate_every; ++k) {
             const bool last = k == s.gate_every - 1;
-            for (int color = 0; color < s.m->C; ++color) {
-                // sweep mode: the round's last sweep also decides (no separate check kernel)
-                const bool decides = sweep && last && color == s.m->C - 1;
-                GateCheck chk{decides ? s.gate : nullptr, handle,
-                              gate_params(s, -1, (sweep && set_ref) ? 1 : 0, s.gate_every)};
-                enqueue_color(s, color, c, dt, s.body_stream, false, sweep && last, decides ? &chk : nullptr,
-                              u > 0);
-            }
+            for (int color = 0; color < s.m->C; ++color)
+                enqueue_color(s, color, c, dt, s.body_stream, false, sweep && last, u > 0);
+            if (sweep && last)
+                gate_check_kernel<<<1, 32, 0, s.body_stream>>>(
+                    s.gate, handle, gate_params(s, -1, set_ref ? 1 : 0, s.gate_every));
         }
     }
     if (!sweep) {

@@ -270,8 +270,8 @@ def test_sweep_residual_gate(norm):
         st = solver.gate_stats(reset=True)
         assert st["last_iterations"] == k and st["capped_steps"] == 1
         curve.append(st["last_residual"])
-    # one pass of the loop body is 4 check rounds of the sweeps; each round's last sweep decides
-    assert all(np.isfinite(curve[1:])) and st["body_kernels"] == 4 * len(model.particle_color_groups)
+    # one pass of the loop body is 4 check rounds: the colors' sweeps and a one-warp check kernel
+    assert all(np.isfinite(curve[1:])) and st["body_kernels"] == 4 * (len(model.particle_color_groups) + 1)
     kd, tol = _clear_drop(curve, start=3, gap=0.99 if norm == "max" else 0.9995)
     solver.set_residual_gate(tol, max_iterations=40, norm=norm, residual="sweep")
     qg, qdg, _ = _run(model, solver, q, qd)
@@ -310,7 +310,7 @@ def test_sweep_gate_rounds_per_body_do_not_change_the_step():
             qg, qdg, _ = _run(model, solver, q, qd)
             st = solver.gate_stats()
             k = st["last_iterations"]
-            assert st["steps"] == 1 and st["body_kernels"] == rounds * colors
+            assert st["steps"] == 1 and st["body_kernels"] == rounds * (colors + 1)
             assert st["body_passes"] == -(-k // rounds)
             out[rounds] = (k, qg, qdg, st["last_residual"])
         k1, q1, qd1, r1 = out[1]
