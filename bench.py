@@ -248,12 +248,39 @@ def _oracle_step(orc, model, q, qd, gate):
     return q, qd, k
 
 
-def cpu_sample(model, q, qd, gate, self_contact=None, max_seconds: float = 12.0, max_steps: int = 50) -> dict:
+def _parity_of_first_step(model, orc, q, qd, gate, gpu_first: dict) -> dict:
+    """The checker's view of the GPU's first timed step: the FP32 oracle takes the same gated step
+    from the same state, the FP64 oracle the same number of iterations; max |dx| against both and
+    the force residual of the GPU's positions (evaluated by the FP64 oracle after its own step)."""
+    import oracle
+
+    threads = os.cpu_count() or 1
+    q_o, _, k_o = _oracle_step(orc, model, q, qd, gate)
+    k_g = int(gpu_first["iterations"])
+    orc64 = oracle.VBDOracle(model, "f64", threads=threads)
+    if model.shape_count:
+        orc64.set_contacts(*oracle.collide(model, q, MARGIN))
+    _, q_64, _ = orc64.step(q, qd, None, DT, k_g)
+    q_g = gpu_first["q"]
+    orc64.set_positions(q_g)
+    r = orc64.residual(DT)
+    solvable = ((np.asarray(model.particle_flags) & 1) != 0) & (np.asarray(model.particle_mass) != 0)
+    return {"max_dx_vs_fp32_oracle_m": float(np.abs(q_g - q_o).max()),
+            "max_dx_vs_fp64_oracle_m": float(np.abs(q_g - q_64).max()),
+            "tolerance_m": 1.0e-5, "iterations_gpu": k_g, "iterations_fp32_oracle": int(k_o),
+            "residual_max_mg": float(r.max()), "residual_mean_mg": float(r[solvable].mean()) if solvable.any() else 0.0,
+            "note": "the first timed step; residual |f_i|/(m_i|g|) of the GPU's positions, Jacobi, FP64"}
+
+
+def cpu_sample(model, q, qd, gate, self_contact=None, max_seconds: float = 12.0, max_steps: int = 50,
+               gpu_first: dict | None = None) -> dict:
     """The oracle stepping the same workload from the given state, on all host cores, for a
-    bounded number of steps."""
+    bounded number of steps; with ``gpu_first`` (the GPU's first step from that state), also the
+    parity of that step (untimed, before the sample)."""
     threads = os.cpu_count() or 1
     orc = _oracle_stepper(model, threads, self_contact)
     q, qd = np.asarray(q, np.float32), np.asarray(qd, np.float32)
+    parity = _parity_of_first_step(model, orc, q, qd, gate, gpu_first) if gpu_first is not None else None
     t0 = time.perf_counter()
     steps, iters = 0, 0
     while True:
@@ -263,11 +290,14 @@ def cpu_sample(model, q, qd, gate, self_contact=None, max_seconds: float = 12.0,
         el = time.perf_counter() - t0
         if el >= max_seconds or steps >= max_steps:
             break
-    return {"value": steps / el, "unit": "steps/s", "cores": threads, "kind": "port",
+    out = {"value": steps / el, "unit": "steps/s", "cores": threads, "kind": "port",
             "vertex_iterations_per_s": model.particle_count * iters / el, "mean_iterations": iters / steps,
             "sample": f"{steps} steps of the same workload from the same state ({model.particle_count} vertices, "
                       f"collide + VBD step{' to the residual gate' if gate else ', 10 iterations'}), {el:.1f} s, "
                       f"oracle stand-in, not reference (Warp is not installed)"}
+    if parity is not None:
+        out["parity"] = parity
+    return out
 
 
 def run_reference(args) -> None:
@@ -528,9 +558,32 @@ def measure_workload(workload: str, dev, W: int, K: int, world: int, rank: int, 
             qs = q_start.cpu().numpy()
             qds = qd_start.cpu().numpy()
             out["cpu_baseline"] = cpu_sample(model, qs, qds, gate, max_steps=max(3, min(K, 50)),
-                                             max_seconds=20.0 if batched else 12.0)
+                                             max_seconds=20.0 if batched else 12.0,
+                                             gpu_first=_gpu_first_step(model, solver, pipe, q_start, qd_start, gate))
     out["_states"] = (model, q_start, qd_start)
     return out
+
+
+def _gpu_first_step(model, solver, pipe, q_start, qd_start, gate) -> dict:
+    """The gated step the timed loop began with, again from its start state (for the checker)."""
+    import torch
+
+    from newton_b200.solvers import SolverVBD
+
+    check = SolverVBD(model, iterations=ITERATIONS)
+    launch = solver.launch_info()
+    check.set_launch(launch["lanes_per_vertex"], launch["block_size"])
+    if gate:
+        check.set_residual_gate(**gate)
+    c = pipe.contacts()
+    a, b = model.state(), model.state()
+    a.particle_q.copy_(q_start)
+    a.particle_qd.copy_(qd_start)
+    pipe.collide(a, c)
+    check.step(a, b, None, c, DT)
+    torch.cuda.synchronize()
+    k = check.gate_stats()["last_iterations"] if gate else ITERATIONS
+    return {"q": a.particle_q.cpu().numpy(), "iterations": k}
 
 
 def cpu_boxes_sample(dev, args) -> dict:
