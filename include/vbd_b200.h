@@ -412,6 +412,19 @@ int vbd_status(VbdSolver* solver, VbdStatus* out, int32_t reset);
 int vbd_solver_info(const VbdSolver* solver, int32_t* color_count, int32_t* lanes_per_vertex,
                     int32_t* block_size);
 
+/* Staged sweep (no reference counterpart; the north_star's "adjacency staged into shared memory
+ * per color block"): on != 0 makes every color sweep load, per block, the positions its vertices'
+ * element records read (the block's one-ring "patch", built on the host for the current launch
+ * shape and rebuilt by vbd_set_launch) into shared memory once, and read them from there; the
+ * records carry 16-bit indices into the patch.  Same math in the same order: results are
+ * bit-identical to the unstaged sweep.  Not used with self-contact, for the record-parallel
+ * shape, or when a block's patch would exceed 1,536 positions (the sweep then stays unstaged).
+ * Allocates the patch tables when turned on.  vbd_staged_sweep_info: whether the sweeps of the
+ * next step are staged, the largest patch and the patch entries in total (out pointers may be
+ * NULL). */
+int vbd_set_staged_sweep(VbdSolver* solver, int32_t on);
+int vbd_staged_sweep_info(const VbdSolver* solver, int32_t* active, int32_t* max_patch, int64_t* patch_entries);
+
 /* How vbd_step runs the colors: resident = 1 when one persistent shared-memory-resident kernel
  * (cooperative launch, one CTA per patch, neighbour-only synchronisation) runs all colors of all
  * iterations; 0 when each color is its own launch.  patches / smem_bytes describe the resident

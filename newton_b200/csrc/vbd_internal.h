@@ -3,8 +3,10 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/vbd_b200.h"
@@ -14,6 +16,26 @@ namespace vbd {
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t err, const char* what);
+
+// fn(begin, end) over [0, n) in contiguous chunks on the host's cores, at least `grain` items per
+// chunk (serial for small n)
+template <typename Fn>
+inline void parallel_chunks(int n, Fn&& fn, int grain = 16384) {
+    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
+    const int workers = std::min(std::min(hw, 32), std::max(1, n / std::max(grain, 1)));
+    if (workers <= 1) {
+        fn(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    pool.reserve(workers);
+    for (int w = 0; w < workers; ++w) {
+        const int b = static_cast<int>(static_cast<long long>(n) * w / workers);
+        const int e = static_cast<int>(static_cast<long long>(n) * (w + 1) / workers);
+        pool.emplace_back([&fn, b, e] { fn(b, e); });
+    }
+    for (auto& t : pool) t.join();
+}
 
 #define VBD_CUDA_TRY(expr)                                       \
     do {                                                         \

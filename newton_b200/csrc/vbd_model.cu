@@ -37,25 +37,6 @@ static int upload(T** dst, const std::vector<T>& src) {
     return VBD_OK;
 }
 
-// fn(begin, end) over [0, n) in contiguous chunks on the host's cores (serial for small n)
-template <typename Fn>
-static void parallel_chunks(int n, Fn&& fn) {
-    const int hw = static_cast<int>(std::max(1u, std::thread::hardware_concurrency()));
-    const int workers = std::min(std::min(hw, 32), std::max(1, n / 16384));
-    if (workers <= 1) {
-        fn(0, n);
-        return;
-    }
-    std::vector<std::thread> pool;
-    pool.reserve(workers);
-    for (int w = 0; w < workers; ++w) {
-        const int b = static_cast<int>(static_cast<long long>(n) * w / workers);
-        const int e = static_cast<int>(static_cast<long long>(n) * (w + 1) / workers);
-        pool.emplace_back([&fn, b, e] { fn(b, e); });
-    }
-    for (auto& t : pool) t.join();
-}
-
 static void free_model(VbdModelImpl& m) {
     void* ptrs[] = {m.perm,       m.inv_perm, m.pinfo,          m.vadj,
                     m.tri_idx,    m.tri_D,    m.tri_mat,        m.edge_idx,

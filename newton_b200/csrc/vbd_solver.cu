@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstddef>
 #include <cstring>
@@ -126,6 +127,16 @@ struct SolverImpl {
     int gate_rounds = 4;             // sweep mode: check rounds per body of the device-side loop
     GateState* gate = nullptr;       // device
     cudaStream_t body_stream = nullptr;  // capture stream of the gate's loop body
+    // staged sweep (vbd_set_staged_sweep): per color block, the ids of the positions its records
+    // read (its patch), and each record's indices into the patch, for one launch shape
+    bool stage_on = false;
+    bool stage_ready = false;        // built for (stage_lanes, stage_block)
+    int stage_lanes = 0, stage_block = 0, stage_max_patch = 0;
+    std::vector<int> stage_color_base;  // first patch of each color
+    int* patch_off = nullptr;
+    int* patch_ids = nullptr;
+    uint2* tri_loc = nullptr;
+    uint2* edge_loc = nullptr;
     int gate_body_kernels = -1;      // kernel nodes of one loop body (last capture)
     int gate_body_pdl_edges = -1;    // programmatic edges of that body
     bool pdl = true;                 // programmatic dependent launch of the sweeps
@@ -315,7 +326,19 @@ struct SweepArgs {
     // residual gate, later rounds of an unrolled loop body: return at once when the step's gate
     // has already decided (GateState::stop); NULL otherwise
     const unsigned* gate_stop;
+    // staged sweep (vbd_set_staged_sweep): block b of this color reads the positions it needs from
+    // shared memory, loaded from patch patch_base + b (its vertices' one-ring, ascending internal
+    // ids); the records carry 14/16-bit indices into the patch.  NULL: unstaged.
+    const int* patch_off;
+    const int* patch_ids;
+    const uint2* tri_loc;    // per triangle record: (l0 | l1 << 16, l2 | slot << 16)
+    const uint2* edge_loc;   // per hinge record: (o0 | slot << 14 | o1 << 16, v0 | v1 << 16)
+    int patch_base;
 };
+
+// The staged positions of a block: [patch size] iterate positions, then (damping) [patch size]
+// step-start positions.
+extern __shared__ float4 s_stage[];
 
 template <bool kDamp>
 __device__ __forceinline__ void accumulate_elements(const SweepArgs& a, int i, int lane, int L, int4 adj, float3& f,
@@ -351,6 +374,117 @@ __device__ __forceinline__ void accumulate_elements(const SweepArgs& a, int i, i
             p3 = xyz(__ldg(&a.prev[ei.w]));
         }
         bending_eval<kDamp>(order, x0, x1, x2, x3, p0, p1, p2, p3, em, a.inv_dt, f, h);
+    }
+}
+
+// The staged walk: the same records and the same math, with every position read from the block's
+// shared-memory patch (s_pos, and s_prev for damping) through the record's local indices.
+template <bool kDamp>
+__device__ __forceinline__ void accumulate_elements_staged(const SweepArgs& a, int lane, int L, int4 adj,
+                                                           const float4* s_pos, const float4* s_prev, float3& f,
+                                                           Sym3& h) {
+    const int nt = adj.y - adj.x;
+    const int lane_e = (lane - nt % L + L) % L;
+    for (int r = adj.x + lane; r < adj.y; r += L) {
+        const uint2 tl = __ldg(&a.tri_loc[r]);
+        const float4 D = __ldg(&a.tri_D[r]);
+        const float4 mt = __ldg(&a.tri_mat[r]);
+        const int l0 = tl.x & 0xffff, l1 = tl.x >> 16, l2 = tl.y & 0xffff, slot = tl.y >> 16;
+        const float3 x0 = xyz(s_pos[l0]), x1 = xyz(s_pos[l1]), x2 = xyz(s_pos[l2]);
+        float3 p0 = x0, p1 = x1, p2 = x2;
+        if (kDamp && mt.w > 0.0f) {
+            p0 = xyz(s_prev[l0]);
+            p1 = xyz(s_prev[l1]);
+            p2 = xyz(s_prev[l2]);
+        }
+        membrane_eval<kDamp>(slot, x0, x1, x2, p0, p1, p2, D, mt, a.inv_dt, f, h);
+    }
+    for (int r = adj.z + lane_e; r < adj.w; r += L) {
+        const uint2 el = __ldg(&a.edge_loc[r]);
+        const float4 em = __ldg(&a.edge_mat[r]);
+        const int o0 = el.x & 0x3fff, order = (el.x >> 14) & 3, o1 = el.x >> 16, v0 = el.y & 0xffff, v1 = el.y >> 16;
+        const float3 x0 = xyz(s_pos[o0]), x1 = xyz(s_pos[o1]), x2 = xyz(s_pos[v0]), x3 = xyz(s_pos[v1]);
+        float3 p0 = x0, p1 = x1, p2 = x2, p3 = x3;
+        if (kDamp && em.w > 0.0f) {
+            p0 = xyz(s_prev[o0]);
+            p1 = xyz(s_prev[o1]);
+            p2 = xyz(s_prev[v0]);
+            p3 = xyz(s_prev[v1]);
+        }
+        bending_eval<kDamp>(order, x0, x1, x2, x3, p0, p1, p2, p3, em, a.inv_dt, f, h);
+    }
+}
+
+// The staged walk with two records in flight per lane: accumulate_elements_x2's order and math,
+// positions from the patch (used where the unstaged sweep uses the two-record walk, so that both
+// give the same bits).
+template <bool kDamp>
+__device__ __forceinline__ void accumulate_elements_staged_x2(const SweepArgs& a, int lane, int L, int4 adj,
+                                                              const float4* s_pos, const float4* s_prev, float3& f,
+                                                              Sym3& h) {
+    const int nt = adj.y - adj.x;
+    const int lane_e = (lane - nt % L + L) % L;
+    for (int r = adj.x + lane; r < adj.y; r += 2 * L) {
+        const bool two = r + L < adj.y;
+        const int rb = two ? r + L : r;
+        const uint2 ta = __ldg(&a.tri_loc[r]), tb = __ldg(&a.tri_loc[rb]);
+        const float4 Da = __ldg(&a.tri_D[r]), Db = __ldg(&a.tri_D[rb]);
+        const float4 ma = __ldg(&a.tri_mat[r]), mb = __ldg(&a.tri_mat[rb]);
+        const int a0 = ta.x & 0xffff, a1 = ta.x >> 16, a2 = ta.y & 0xffff, sa = ta.y >> 16;
+        const int b0 = tb.x & 0xffff, b1 = tb.x >> 16, b2 = tb.y & 0xffff, sb = tb.y >> 16;
+        const float3 xa0 = xyz(s_pos[a0]), xa1 = xyz(s_pos[a1]), xa2 = xyz(s_pos[a2]);
+        const float3 xb0 = xyz(s_pos[b0]), xb1 = xyz(s_pos[b1]), xb2 = xyz(s_pos[b2]);
+        float3 pa0 = xa0, pa1 = xa1, pa2 = xa2, pb0 = xb0, pb1 = xb1, pb2 = xb2;
+        if (kDamp && (ma.w > 0.0f || mb.w > 0.0f)) {
+            pa0 = xyz(s_prev[a0]);
+            pa1 = xyz(s_prev[a1]);
+            pa2 = xyz(s_prev[a2]);
+            pb0 = xyz(s_prev[b0]);
+            pb1 = xyz(s_prev[b1]);
+            pb2 = xyz(s_prev[b2]);
+        }
+        float3 fa = f3(0.f, 0.f, 0.f), fb = fa;
+        Sym3 ha = zero_sym(), hb = zero_sym();
+        membrane_eval<kDamp>(sa, xa0, xa1, xa2, pa0, pa1, pa2, Da, ma, a.inv_dt, fa, ha);
+        membrane_eval<kDamp>(sb, xb0, xb1, xb2, pb0, pb1, pb2, Db, mb, a.inv_dt, fb, hb);
+        f = f + fa;
+        add(h, ha);
+        if (two) {
+            f = f + fb;
+            add(h, hb);
+        }
+    }
+    for (int r = adj.z + lane_e; r < adj.w; r += 2 * L) {
+        const bool two = r + L < adj.w;
+        const int rb = two ? r + L : r;
+        const uint2 ea = __ldg(&a.edge_loc[r]), eb = __ldg(&a.edge_loc[rb]);
+        const float4 ma = __ldg(&a.edge_mat[r]), mb = __ldg(&a.edge_mat[rb]);
+        const int oa = (ea.x >> 14) & 3, ob = (eb.x >> 14) & 3;
+        const int a0 = ea.x & 0x3fff, a1 = ea.x >> 16, a2 = ea.y & 0xffff, a3 = ea.y >> 16;
+        const int b0 = eb.x & 0x3fff, b1 = eb.x >> 16, b2 = eb.y & 0xffff, b3 = eb.y >> 16;
+        const float3 xa0 = xyz(s_pos[a0]), xa1 = xyz(s_pos[a1]), xa2 = xyz(s_pos[a2]), xa3 = xyz(s_pos[a3]);
+        const float3 xb0 = xyz(s_pos[b0]), xb1 = xyz(s_pos[b1]), xb2 = xyz(s_pos[b2]), xb3 = xyz(s_pos[b3]);
+        float3 pa0 = xa0, pa1 = xa1, pa2 = xa2, pa3 = xa3, pb0 = xb0, pb1 = xb1, pb2 = xb2, pb3 = xb3;
+        if (kDamp && (ma.w > 0.0f || mb.w > 0.0f)) {
+            pa0 = xyz(s_prev[a0]);
+            pa1 = xyz(s_prev[a1]);
+            pa2 = xyz(s_prev[a2]);
+            pa3 = xyz(s_prev[a3]);
+            pb0 = xyz(s_prev[b0]);
+            pb1 = xyz(s_prev[b1]);
+            pb2 = xyz(s_prev[b2]);
+            pb3 = xyz(s_prev[b3]);
+        }
+        float3 fa = f3(0.f, 0.f, 0.f), fb = fa;
+        Sym3 ha = zero_sym(), hb = zero_sym();
+        bending_eval<kDamp, true>(oa, xa0, xa1, xa2, xa3, pa0, pa1, pa2, pa3, ma, a.inv_dt, fa, ha);
+        bending_eval<kDamp, true>(ob, xb0, xb1, xb2, xb3, pb0, pb1, pb2, pb3, mb, a.inv_dt, fb, hb);
+        f = f + fa;
+        add(h, ha);
+        if (two) {
+            f = f + fb;
+            add(h, hb);
+        }
     }
 }
 
@@ -650,7 +784,7 @@ __device__ __forceinline__ void reduce_residual_block(const SweepArgs& a, float 
 // Hessian are summed across the L lanes with xor shuffles and lane 0 adds the contacts and solves.
 // kCap: the same kernel limited to 64 registers per thread (4 blocks of 256 per SM), used when the
 // uncapped kernel would need more than one wave of blocks (large colors, many lanes per vertex)
-template <int L, bool kDamp, bool kResidual, bool kCap, bool kGate>
+template <int L, bool kDamp, bool kResidual, bool kCap, bool kGate, bool kStaged = false>
 __device__ __forceinline__ void sweep_body(const SweepArgs& a) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = a.v_begin + tid / L;
@@ -684,6 +818,24 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a) {
     // a round of the gate's loop body after the decision: nothing to do (the flag was written by
     // an earlier kernel of the stream and is the same for every thread of the grid)
     if (a.gate_stop && *reinterpret_cast<const volatile unsigned*>(a.gate_stop) != 0u) return;
+    const float4* s_pos = s_stage;
+    const float4* s_prev = s_stage;
+    if (kStaged) {
+        // the block's one-ring: one coalesced pass over the patch ids, one gather per position
+        // (the previous kernel's writes are visible after griddepcontrol.wait), then every record
+        // of the block reads its positions from shared memory
+        const int p = a.patch_base + static_cast<int>(blockIdx.x);
+        const int b0 = __ldg(&a.patch_off[p]), n = __ldg(&a.patch_off[p + 1]) - b0;
+        float4* sp = s_stage;
+        float4* sq = s_stage + n;
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const int g = __ldg(&a.patch_ids[b0 + j]);
+            sp[j] = a.pos[g];
+            if (kDamp) sq[j] = __ldg(&a.prev[g]);
+        }
+        s_prev = sq;
+        __syncthreads();
+    }
     if (valid && solve && lane == 0) {
         // Warm L1 with what lane 0 reads after the element walk (the vertex's own state, its
         // contact count, its self-contact terms): a prefetch holds no register, so the walk keeps
@@ -702,7 +854,9 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a) {
         }
     }
     if (valid && solve) {
-        if (L <= 2 && !kCap) accumulate_elements_x2<kDamp>(a, lane, L, adj, f, h);
+        if (kStaged && L <= 2 && !kCap) accumulate_elements_staged_x2<kDamp>(a, lane, L, adj, s_pos, s_prev, f, h);
+        else if (kStaged) accumulate_elements_staged<kDamp>(a, lane, L, adj, s_pos, s_prev, f, h);
+        else if (L <= 2 && !kCap) accumulate_elements_x2<kDamp>(a, lane, L, adj, f, h);
         else accumulate_elements<kDamp>(a, i, lane, L, adj, f, h);
     }
     if (L > 1) {
@@ -766,18 +920,25 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a) {
     solve_and_commit(a, i, pv, h, f);
 }
 
-template <int L, bool kDamp, bool kResidual, bool kCap, bool kGate = false>
+template <int L, bool kDamp, bool kResidual, bool kCap, bool kGate = false, bool kStaged = false>
 __global__ void __launch_bounds__(256, kCap ? 4 : 1) sweep_kernel(SweepArgs a) {
-    sweep_body<L, kDamp, kResidual, kCap, kGate>(a);
+    sweep_body<L, kDamp, kResidual, kCap, kGate, kStaged>(a);
 }
 
 // The gate's accumulating sweep with 4 or more lanes per vertex, held to the 72 registers of the
 // plain sweep: at 74 (what the compiler picks for the extra reduction) the allocation rounds up
 // to 80 registers per thread, two color grids no longer fit on an SM together, and each launch
 // loses its overlap with the previous one.
-template <int L, bool kDamp>
+template <int L, bool kDamp, bool kStaged = false>
 __global__ void __maxnreg__(72) sweep_gate_kernel(SweepArgs a) {
-    sweep_body<L, kDamp, false, false, true>(a);
+    sweep_body<L, kDamp, false, false, true, kStaged>(a);
+}
+
+// The staged sweep at 4 or more lanes, held to the same 72 registers (unbounded, the damping
+// build takes 79).
+template <int L, bool kDamp>
+__global__ void __maxnreg__(72) sweep_staged_kernel(SweepArgs a) {
+    sweep_body<L, kDamp, false, false, false, true>(a);
 }
 
 // Record-parallel variant of the same color update (lanes_per_vertex == 0).  A block owns
@@ -1115,17 +1276,17 @@ static GateParams gate_params(const SolverImpl& s, int first, int set_ref, int a
 }
 
 // blocks of `kernel` resident on the whole device at `block` threads (cached per kernel / block)
-static long long resident_blocks(const void* kernel, int block) {
+static long long resident_blocks(const void* kernel, int block, size_t smem = 0) {
     static std::mutex mu;
-    static std::map<std::pair<const void*, int>, long long> cache;
+    static std::map<std::pair<const void*, long long>, long long> cache;
     std::lock_guard<std::mutex> lock(mu);
-    const auto key = std::make_pair(kernel, block);
+    const auto key = std::make_pair(kernel, static_cast<long long>(block) | (static_cast<long long>(smem) << 16));
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem);
     const long long n = static_cast<long long>(std::max(per_sm, 1)) * std::max(sms, 1);
     cache[key] = n;
     return n;
@@ -1135,11 +1296,13 @@ static long long resident_blocks(const void* kernel, int block) {
 // blocks may start while that kernel drains and wait (griddepcontrol.wait) before reading any
 // position, so consecutive colors overlap launch latency instead of serialising it.
 template <typename Kernel>
-static void launch_dependent(Kernel kernel, int grid, int block, cudaStream_t st, const SweepArgs& a) {
+static void launch_dependent(Kernel kernel, int grid, int block, cudaStream_t st, const SweepArgs& a,
+                             size_t smem = 0) {
     cudaLaunchConfig_t cfg;
     std::memset(&cfg, 0, sizeof(cfg));
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr;
     attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1149,8 +1312,56 @@ static void launch_dependent(Kernel kernel, int grid, int block, cudaStream_t st
     cudaLaunchKernelEx(&cfg, kernel, a);
 }
 
+// the staged instantiations: the same choice between the uncapped (or 72-register gate) kernel
+// and the 64-register one, with the patch's shared memory counted in the occupancy
+template <int L, bool kDamp, bool kGate>
+static void launch_staged_LDG(const SweepArgs& a, int grid, int block, cudaStream_t st, size_t smem) {
+    if constexpr (kGate && L >= 4) {
+        if (grid > resident_blocks(reinterpret_cast<const void*>(&sweep_gate_kernel<L, kDamp, true>), block, smem))
+            launch_dependent(sweep_kernel<L, kDamp, false, true, kGate, true>, grid, block, st, a, smem);
+        else
+            launch_dependent(sweep_gate_kernel<L, kDamp, true>, grid, block, st, a, smem);
+    } else if constexpr (kGate || L <= 2) {
+        // (at 1-2 lanes the two-record walk needs more than 72 registers, as unstaged)
+        const void* uncapped = reinterpret_cast<const void*>(&sweep_kernel<L, kDamp, false, false, kGate, true>);
+        if (grid > resident_blocks(uncapped, block, smem))
+            launch_dependent(sweep_kernel<L, kDamp, false, true, kGate, true>, grid, block, st, a, smem);
+        else
+            launch_dependent(sweep_kernel<L, kDamp, false, false, kGate, true>, grid, block, st, a, smem);
+    } else {
+        if (grid > resident_blocks(reinterpret_cast<const void*>(&sweep_staged_kernel<L, kDamp>), block, smem))
+            launch_dependent(sweep_kernel<L, kDamp, false, true, false, true>, grid, block, st, a, smem);
+        else
+            launch_dependent(sweep_staged_kernel<L, kDamp>, grid, block, st, a, smem);
+    }
+}
+
+template <int L>
+static void prime_staged_occupancy_L(int block, size_t smem) {
+    if constexpr (L >= 4) {
+        resident_blocks(reinterpret_cast<const void*>(&sweep_staged_kernel<L, true>), block, smem);
+        resident_blocks(reinterpret_cast<const void*>(&sweep_staged_kernel<L, false>), block, smem);
+    } else {
+        resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, true, false, false, false, true>), block, smem);
+        resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, false, false, false, false, true>), block, smem);
+    }
+    if constexpr (L >= 4) {
+        resident_blocks(reinterpret_cast<const void*>(&sweep_gate_kernel<L, true, true>), block, smem);
+        resident_blocks(reinterpret_cast<const void*>(&sweep_gate_kernel<L, false, true>), block, smem);
+    } else {
+        resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, true, false, false, true, true>), block, smem);
+        resident_blocks(reinterpret_cast<const void*>(&sweep_kernel<L, false, false, false, true, true>), block, smem);
+    }
+}
+
 template <int L, bool kDamp, bool kResidual, bool kGate = false>
-static void launch_sweep_LDR(const SweepArgs& a, int grid, int block, cudaStream_t st) {
+static void launch_sweep_LDR(const SweepArgs& a, int grid, int block, cudaStream_t st, size_t smem = 0) {
+    if constexpr (!kResidual) {
+        if (a.patch_off) {
+            launch_staged_LDG<L, kDamp, kGate>(a, grid, block, st, smem);
+            return;
+        }
+    }
     if constexpr (kGate && !kResidual && L >= 4) {
         if (grid > resident_blocks(reinterpret_cast<const void*>(&sweep_gate_kernel<L, kDamp>), block))
             launch_dependent(sweep_kernel<L, kDamp, kResidual, true, kGate>, grid, block, st, a);
@@ -1192,21 +1403,22 @@ static void prime_occupancy(int lanes, int block) {
 }
 
 template <int L>
-static void launch_sweep_L(const SweepArgs& a, bool damp, bool residual, int block, cudaStream_t st, bool gate) {
+static void launch_sweep_L(const SweepArgs& a, bool damp, bool residual, int block, cudaStream_t st, bool gate,
+                           size_t smem) {
     const long long threads = static_cast<long long>(a.v_end - a.v_begin) * L;
     const int grid = static_cast<int>((threads + block - 1) / block);
     if (grid <= 0) return;
     if (gate && !residual) {
-        if (damp) launch_sweep_LDR<L, true, false, true>(a, grid, block, st);
-        else launch_sweep_LDR<L, false, false, true>(a, grid, block, st);
+        if (damp) launch_sweep_LDR<L, true, false, true>(a, grid, block, st, smem);
+        else launch_sweep_LDR<L, false, false, true>(a, grid, block, st, smem);
         return;
     }
     if (residual) {
         if (damp) launch_sweep_LDR<L, true, true>(a, grid, block, st);
         else launch_sweep_LDR<L, false, true>(a, grid, block, st);
     } else {
-        if (damp) launch_sweep_LDR<L, true, false>(a, grid, block, st);
-        else launch_sweep_LDR<L, false, false>(a, grid, block, st);
+        if (damp) launch_sweep_LDR<L, true, false>(a, grid, block, st, smem);
+        else launch_sweep_LDR<L, false, false>(a, grid, block, st, smem);
     }
 }
 
@@ -1226,7 +1438,7 @@ static void launch_tile_TB(const SweepArgs& a, bool damp, bool residual, cudaStr
 
 // gate: a Gauss-Seidel color that also accumulates its residual into a.resid_* (lanes > 0 only)
 static void launch_sweep(const SweepArgs& a, int lanes, bool damp, bool residual, int block, cudaStream_t st,
-                         bool gate = false) {
+                         bool gate = false, size_t smem = 0) {
     if (lanes == 0) {
         if (block <= 64) launch_tile_TB<64>(a, damp, residual, st);
         else if (block <= 128) launch_tile_TB<128>(a, damp, residual, st);
@@ -1234,11 +1446,11 @@ static void launch_sweep(const SweepArgs& a, int lanes, bool damp, bool residual
         return;
     }
     switch (lanes) {
-        case 1: launch_sweep_L<1>(a, damp, residual, block, st, gate); break;
-        case 2: launch_sweep_L<2>(a, damp, residual, block, st, gate); break;
-        case 8: launch_sweep_L<8>(a, damp, residual, block, st, gate); break;
-        case 16: launch_sweep_L<16>(a, damp, residual, block, st, gate); break;
-        default: launch_sweep_L<4>(a, damp, residual, block, st, gate); break;
+        case 1: launch_sweep_L<1>(a, damp, residual, block, st, gate, smem); break;
+        case 2: launch_sweep_L<2>(a, damp, residual, block, st, gate, smem); break;
+        case 8: launch_sweep_L<8>(a, damp, residual, block, st, gate, smem); break;
+        case 16: launch_sweep_L<16>(a, damp, residual, block, st, gate, smem); break;
+        default: launch_sweep_L<4>(a, damp, residual, block, st, gate, smem); break;
     }
 }
 
@@ -1310,13 +1522,23 @@ static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float 
     a.v_begin = m.color_start[color];
     a.v_end = m.color_start[color + 1];
     if (a.v_end <= a.v_begin) return;
+    size_t smem = 0;
+    const bool damp = m.any_tri_damping || m.any_edge_damping;
+    if (s.stage_on && s.stage_ready && !s.sc.on && s.lanes == s.stage_lanes && s.block == s.stage_block) {
+        a.patch_off = s.patch_off;
+        a.patch_ids = s.patch_ids;
+        a.tri_loc = s.tri_loc;
+        a.edge_loc = s.edge_loc;
+        a.patch_base = s.stage_color_base[color];
+        smem = static_cast<size_t>(s.stage_max_patch) * sizeof(float4) * (damp ? 2 : 1);
+    }
     if (s.sc.on) {
         self_contact_accumulate(m, s.sc, s.pos, s.prev, color, dt, s.friction_epsilon, st);
         launch_sweep(a, s.lanes, m.any_tri_damping || m.any_edge_damping, false, s.block, st);
         self_contact_truncate(m, s.sc, s.pos, s.disp, st);
         return;
     }
-    launch_sweep(a, s.lanes, m.any_tri_damping || m.any_edge_damping, false, s.block, st, gate);
+    launch_sweep(a, s.lanes, damp, false, s.block, st, gate, smem);
     if (!m.fused_commit) {
         const int n = a.v_end - a.v_begin;
         commit_kernel<<<(n + 255) / 256, 256, 0, st>>>(s.pos, s.prev, s.disp, a.v_begin, a.v_end);
@@ -1567,6 +1789,12 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
 static void free_solver(SolverImpl& s) {
     resident_free(s.resident);
     self_contact_free(s.sc);
+    cudaFree(s.patch_off);
+    cudaFree(s.patch_ids);
+    cudaFree(s.tri_loc);
+    cudaFree(s.edge_loc);
+    s.patch_off = s.patch_ids = nullptr;
+    s.tri_loc = s.edge_loc = nullptr;
     if (s.ws_corr) cudaFree(s.ws_corr);
     if (s.ws_work) cudaFree(s.ws_work);
     s.ws_corr = s.ws_work = nullptr;
@@ -2129,6 +2357,147 @@ extern "C" int vbd_solver_info(const VbdSolver* solver, int32_t* color_count, in
     return VBD_OK;
 }
 
+// ---- staged sweep ---------------------------------------------------------------------------
+constexpr int kMaxPatch = 1536;  // patch entries: local indices fit 14 bits; 2 x 16 B x 1536 = 48 KB
+
+static void free_staged(SolverImpl& s) {
+    cudaFree(s.patch_off);
+    cudaFree(s.patch_ids);
+    cudaFree(s.tri_loc);
+    cudaFree(s.edge_loc);
+    s.patch_off = s.patch_ids = nullptr;
+    s.tri_loc = s.edge_loc = nullptr;
+    s.stage_ready = false;
+    s.stage_max_patch = 0;
+    s.stage_color_base.clear();
+}
+
+// Patches of the staged sweep for the solver's launch shape: color c's block b (the vertices
+// [color_start[c] + b V_B, + V_B), V_B = block / lanes, as the sweep's grid maps them) gets the
+// sorted ids of every position its vertices' records read; each record's ids become indices into
+// its vertex's patch.  Built on the host's cores.  Leaves stage_ready false (unstaged sweeps) for
+// the record-parallel shape or when a patch would exceed kMaxPatch entries.
+static int build_staged(SolverImpl& s) {
+    free_staged(s);
+    const VbdModelImpl& m = *s.m;
+    if (s.lanes < 1 || m.C == 0) return VBD_OK;
+    const int VB = s.block / s.lanes;
+    std::vector<int> base(static_cast<size_t>(m.C) + 1, 0);
+    for (int c = 0; c < m.C; ++c) base[c + 1] = base[c] + (m.color_start[c + 1] - m.color_start[c] + VB - 1) / VB;
+    const int P = base[m.C];
+    std::vector<std::vector<int>> ids(P);
+    std::vector<uint2> tri_loc(std::max(m.n_tri_rec, 1)), edge_loc(std::max(m.n_edge_rec, 1));
+    std::atomic<bool> too_big{false};
+    parallel_chunks(
+        P,
+        [&](int pb, int pe) {
+            std::vector<int> buf;
+            for (int p = pb; p < pe; ++p) {
+                const int c = static_cast<int>(std::upper_bound(base.begin(), base.end(), p) - base.begin()) - 1;
+                const int v0 = m.color_start[c] + (p - base[c]) * VB;
+                const int v1 = std::min(v0 + VB, m.color_start[c + 1]);
+                buf.clear();
+                for (int i = v0; i < v1; ++i) {
+                    const int4 ad = m.vadj_h[i];
+                    for (int r = ad.x; r < ad.y; ++r) {
+                        const int4 t = m.tri_idx_h[r];
+                        buf.insert(buf.end(), {t.x, t.y, t.z});
+                    }
+                    for (int r = ad.z; r < ad.w; ++r) {
+                        const int4 e = m.edge_idx_h[r];
+                        buf.insert(buf.end(), {e.x & 0x3fffffff, e.y, e.z, e.w});
+                    }
+                }
+                std::sort(buf.begin(), buf.end());
+                buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+                if (static_cast<int>(buf.size()) > kMaxPatch) {
+                    too_big = true;
+                    continue;
+                }
+                auto loc = [&buf](int g) {
+                    return static_cast<unsigned>(std::lower_bound(buf.begin(), buf.end(), g) - buf.begin());
+                };
+                for (int i = v0; i < v1; ++i) {
+                    const int4 ad = m.vadj_h[i];
+                    for (int r = ad.x; r < ad.y; ++r) {
+                        const int4 t = m.tri_idx_h[r];
+                        tri_loc[r] = make_uint2(loc(t.x) | (loc(t.y) << 16), loc(t.z) | (static_cast<unsigned>(t.w) << 16));
+                    }
+                    for (int r = ad.z; r < ad.w; ++r) {
+                        const int4 e = m.edge_idx_h[r];
+                        const unsigned slot = static_cast<unsigned>(e.x) >> 30;
+                        edge_loc[r] = make_uint2(loc(e.x & 0x3fffffff) | (slot << 14) | (loc(e.y) << 16),
+                                                 loc(e.z) | (loc(e.w) << 16));
+                    }
+                }
+                ids[p] = buf;
+            }
+        },
+        64);
+    if (too_big) return VBD_OK;
+    std::vector<int> off(static_cast<size_t>(P) + 1, 0);
+    int maxp = 0;
+    for (int p = 0; p < P; ++p) {
+        off[p + 1] = off[p] + static_cast<int>(ids[p].size());
+        maxp = std::max(maxp, static_cast<int>(ids[p].size()));
+    }
+    std::vector<int> flat(std::max(off[P], 1));
+    for (int p = 0; p < P; ++p) std::copy(ids[p].begin(), ids[p].end(), flat.begin() + off[p]);
+    VBD_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&s.patch_off), off.size() * sizeof(int)));
+    VBD_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&s.patch_ids), flat.size() * sizeof(int)));
+    VBD_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&s.tri_loc), tri_loc.size() * sizeof(uint2)));
+    VBD_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&s.edge_loc), edge_loc.size() * sizeof(uint2)));
+    VBD_CUDA_TRY(cudaMemcpy(s.patch_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
+    VBD_CUDA_TRY(cudaMemcpy(s.patch_ids, flat.data(), flat.size() * sizeof(int), cudaMemcpyHostToDevice));
+    VBD_CUDA_TRY(cudaMemcpy(s.tri_loc, tri_loc.data(), tri_loc.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    VBD_CUDA_TRY(cudaMemcpy(s.edge_loc, edge_loc.data(), edge_loc.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+    s.stage_color_base = base;
+    s.stage_max_patch = maxp;
+    s.stage_lanes = s.lanes;
+    s.stage_block = s.block;
+    s.stage_ready = true;
+    // occupancy of the staged kernels with their shared memory, queried outside any capture
+    const bool damp = m.any_tri_damping || m.any_edge_damping;
+    const size_t smem = static_cast<size_t>(maxp) * sizeof(float4) * (damp ? 2 : 1);
+    switch (s.lanes) {
+        case 1: prime_staged_occupancy_L<1>(s.block, smem); break;
+        case 2: prime_staged_occupancy_L<2>(s.block, smem); break;
+        case 4: prime_staged_occupancy_L<4>(s.block, smem); break;
+        case 8: prime_staged_occupancy_L<8>(s.block, smem); break;
+        case 16: prime_staged_occupancy_L<16>(s.block, smem); break;
+        default: break;
+    }
+    return VBD_OK;
+}
+
+extern "C" int vbd_set_staged_sweep(VbdSolver* solver, int32_t on) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_staged_sweep: solver is NULL");
+    SolverImpl& s = solver->s;
+    for (auto& g : s.graphs) cudaGraphExecDestroy(g.exec);  // captured steps change
+    s.graphs.clear();
+    s.stage_on = on != 0;
+    if (s.stage_on && !(s.stage_ready && s.stage_lanes == s.lanes && s.stage_block == s.block)) return build_staged(s);
+    return VBD_OK;
+}
+
+extern "C" int vbd_staged_sweep_info(const VbdSolver* solver, int32_t* active, int32_t* max_patch,
+                                     int64_t* patch_entries) {
+    if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_staged_sweep_info: solver is NULL");
+    const SolverImpl& s = solver->s;
+    const bool act = s.stage_on && s.stage_ready && !s.sc.on && s.lanes == s.stage_lanes && s.block == s.stage_block;
+    if (active) *active = act ? 1 : 0;
+    if (max_patch) *max_patch = s.stage_ready ? s.stage_max_patch : 0;
+    if (patch_entries) {
+        *patch_entries = 0;
+        if (s.stage_ready && !s.stage_color_base.empty()) {
+            int last = 0;
+            cudaMemcpy(&last, s.patch_off + s.stage_color_base.back(), sizeof(int), cudaMemcpyDeviceToHost);
+            *patch_entries = last;
+        }
+    }
+    return VBD_OK;
+}
+
 extern "C" int vbd_set_launch(VbdSolver* solver, int32_t lanes_per_vertex, int32_t block_size) {
     if (!solver) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_launch: solver is NULL");
     if (const char* why = launch_shape_error(lanes_per_vertex, block_size))
@@ -2136,6 +2505,7 @@ extern "C" int vbd_set_launch(VbdSolver* solver, int32_t lanes_per_vertex, int32
     solver->s.lanes = lanes_per_vertex;
     solver->s.block = block_size;
     prime_occupancy(lanes_per_vertex, block_size);
+    if (solver->s.stage_on) return build_staged(solver->s);
     return VBD_OK;
 }
 

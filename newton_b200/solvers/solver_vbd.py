@@ -124,6 +124,7 @@ class SolverVBD(SolverBase):
         self._warm = None
         self._gate = None
         self._feature_set = "corrections"
+        self._staged = False
         self._create()
 
     def _create(self) -> None:
@@ -320,6 +321,17 @@ class SolverVBD(SolverBase):
     def set_launch(self, lanes_per_vertex: int, block_size: int) -> None:
         _lib.check(self._lib.vbd_set_launch(self._handle, int(lanes_per_vertex), int(block_size)))
 
+    def set_staged_sweep(self, on: bool = True) -> None:
+        """Sweeps read the one-ring positions from a per-block shared-memory patch
+        (``vbd_set_staged_sweep``); bit-identical results."""
+        self._staged = bool(on)
+        _lib.check(self._lib.vbd_set_staged_sweep(self._handle, 1 if on else 0))
+
+    def staged_sweep_info(self) -> dict:
+        a, mp, n = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        _lib.check(self._lib.vbd_staged_sweep_info(self._handle, ctypes.byref(a), ctypes.byref(mp), ctypes.byref(n)))
+        return {"active": bool(a.value), "max_patch": mp.value, "patch_entries": n.value}
+
     def launch_info(self) -> dict:
         c, l, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
         _lib.check(self._lib.vbd_solver_info(self._handle, ctypes.byref(c), ctypes.byref(l), ctypes.byref(b)))
@@ -431,6 +443,8 @@ class SolverVBD(SolverBase):
         self._lib.vbd_solver_destroy(old)
         if self._feature_set != "corrections":
             self.set_feature_set(self._feature_set)
+        if self._staged:
+            self.set_staged_sweep(True)
         if self._warm is not None:
             self.set_warm_start(self._warm, self._warm_iterations)
         if getattr(self, "_gate", None) is not None:
