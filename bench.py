@@ -787,6 +787,46 @@ def learned_ab(dev, workload: str, plain: dict, start_state, K: int) -> dict:
     }
 
 
+def sweep_profile(workload: str, n: int, worlds: int, steps: int) -> dict:
+    """The profile harness of the sweep: the workload's scene (``worlds`` batched worlds, or an
+    ``n`` x ``n`` cloth), a few plain 10-iteration steps, then ``steps`` steps inside an NVTX range
+    named ``sweep_profile`` (for ncu --nvtx-include); returns their mean device time."""
+    import torch
+
+    from newton_b200 import CollisionPipeline, scenes
+    from newton_b200.solvers import SolverVBD
+
+    dev = torch.device("cuda:0")
+    if workload == "batched-worlds" and worlds:
+        model, q0 = scenes.batched_worlds(worlds, seed=0, device=dev)
+        kw = {}
+    else:
+        model, q0, kw, _ = build_scene(workload, dev, n=n)
+    solver = SolverVBD(model, iterations=ITERATIONS, **kw)
+    pipe = CollisionPipeline(model, soft_contact_margin=MARGIN)
+    c = pipe.contacts()
+    a, b = model.state(), model.state()
+    a.particle_q.copy_(torch.from_numpy(q0).to(dev))
+    for _ in range(3):
+        pipe.collide(a, c)
+        solver.step(a, b, None, c, DT)
+        a, b = b, a
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("sweep_profile")
+    e0.record()
+    for _ in range(steps):
+        pipe.collide(a, c)
+        solver.step(a, b, None, c, DT)
+        a, b = b, a
+    e1.record()
+    torch.cuda.nvtx.range_pop()
+    e1.synchronize()
+    return {"workload": workload, "vertices": model.particle_count, "colors": len(model.particle_color_groups),
+            "launch": solver.launch_info(), "steps": steps, "ms_per_step": e0.elapsed_time(e1) / steps,
+            "algorithmic_bytes_per_iteration": algorithmic_bytes_per_iteration(model)}
+
+
 def mlp_kernels(rows: int, repeats: int) -> dict:
     """Device time of the warm-start MLP kernels on random rows (the profile harness): tcgen05
     inference, the mma.sync inference it replaced, and one training pass (forward + backward +
@@ -853,9 +893,15 @@ def main() -> None:
     ap.add_argument("--no-workloads", action="store_true", help="skip the batched-worlds and cloth-on-boxes entries")
     ap.add_argument("--n", type=int, default=0, help="grid vertices per side (default: the workload's)")
     ap.add_argument("--workload", default="draped-cloth", choices=sorted(WORKLOADS))
+    ap.add_argument("--sweep-profile", action="store_true",
+                    help="only run the sweep profile harness (--workload, --n, --worlds, --steps) and print its JSON")
+    ap.add_argument("--worlds", type=int, default=0, help="batched worlds of --sweep-profile (default 512)")
     ap.add_argument("--mlp-kernels", type=int, default=0, metavar="ROWS",
                     help="only time the warm-start MLP kernels on ROWS random rows and print their JSON")
     args = ap.parse_args()
+    if args.sweep_profile:
+        print(json.dumps(sweep_profile(args.workload, args.n, args.worlds, max(args.steps, 1))), flush=True)
+        return
     if args.mlp_kernels:
         print(json.dumps(mlp_kernels(args.mlp_kernels, max(args.steps, 5))), flush=True)
         return
