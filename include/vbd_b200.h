@@ -353,7 +353,7 @@ int vbd_mlp_sizes(int32_t* params, int32_t* weights16, int32_t* in_features, int
 int vbd_set_feature_set(VbdSolver* solver, int32_t feature_set);
 /* Per-vertex features [V][64] (model particle order) of the step prepared by vbd_forward, in the
  * solver's feature set; corr_prev [V][3] (the previous step's correction, model order) may be
- * NULL.  mean / inv_std [64] standardise them (both NULL = raw). */
+ * NULL.  mean / inv_std [64] standardise them (both NULL = raw).  out must be 16-byte aligned. */
 int vbd_mlp_features(VbdSolver* solver, const float* corr_prev, const float* mean, const float* inv_std, float* out,
                      void* stream);
 /* Y [n][3] = MLP(X [n][64]) on the 5th-generation tensor cores (tcgen05.mma, BF16 operands in
@@ -394,6 +394,12 @@ int vbd_mlp_warm_start(VbdSolver* solver, const float* params, const uint16_t* w
  * turns the mode off.  Allocates the solver's correction and workspace buffers on first use. */
 int vbd_set_warm_start(VbdSolver* solver, const float* params, const uint16_t* w16, const float* mean,
                        const float* inv_std, int32_t iterations);
+
+/* The previous step's correction x_solved - y that the warm-start step mode feeds to the next
+ * step's features (model order, DEVICE [V,3]); replaces the one the last step left.  For
+ * stepping the learned solver from states of another trajectory with that trajectory's history
+ * (the equal-residual A/B).  The warm start must be on. */
+int vbd_set_warm_start_correction(VbdSolver* solver, const float* corr, void* stream);
 
 /* Copy the solver's current Gauss-Seidel iterate (model particle order) into q_out [V,3] (DEVICE). */
 int vbd_get_positions(const VbdSolver* solver, float* q_out, void* stream);

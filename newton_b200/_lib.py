@@ -181,6 +181,7 @@ SIGNATURES = {
     "vbd_mlp_features": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     "vbd_set_feature_set": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "vbd_set_staged_sweep": (ctypes.c_int, [_VP, ctypes.c_int32]),
+    "vbd_set_warm_start_correction": (ctypes.c_int, [_VP, _VP, _VP]),
     "vbd_staged_sweep_info": (ctypes.c_int, [_VP, c_int32_p, c_int32_p, ctypes.POINTER(ctypes.c_int64)]),
     "vbd_mlp_forward": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int32, _VP, _VP]),
     "vbd_mlp_forward_mma_sync": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int32, _VP, _VP]),

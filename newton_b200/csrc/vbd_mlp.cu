@@ -431,7 +431,9 @@ int ensure_tile_smem() {
                                           static_cast<int>(kTileSmem)));
         VBD_CUDA_TRY(cudaFuncSetAttribute(mlp_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           static_cast<int>(kTileSmem)));
-        VBD_CUDA_TRY(cudaFuncSetAttribute(tc::mlp_infer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        VBD_CUDA_TRY(cudaFuncSetAttribute(tc::mlp_infer_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          tc::kSmemBytes));
+        VBD_CUDA_TRY(cudaFuncSetAttribute(tc::mlp_infer_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           tc::kSmemBytes));
         g_attr_done[dev] = true;
     }
@@ -465,122 +467,139 @@ struct FeatArgs {
     const int* nbr8;
     const float4* vfeat;
     const int* ccount;
-    const float* corr_prev;  // [V][3] model order, may be NULL
+    const float* corr_prev;  // [V][3] (model order; internal order when `internal`), may be NULL
     const float* mean;       // [64] or NULL
     const float* inv_std;    // [64] or NULL
-    float* out;              // [V][64] model order
+    float* out;              // [V][64]: row = model index, or internal index when `internal`
+    uint16_t* out16;         // instead of out: BF16 rows (rounded to nearest, as the inference rounds)
+    int internal;
     int mode;                // VBD_FEATURES_CORRECTIONS or VBD_FEATURES_KINEMATIC
     float3 g_dt2;            // gravity * dt^2 (kinematic set)
     float inv_dt;            // 1 / dt (kinematic set)
 };
 
-// The kinematic feature set: the vertex's own motion and its one-ring geometry, no solver history.
-//   f[0..2]   previous step's displacement x_n - x_(n-1) = v dt, over L (v dt = (y - x) - g dt^2)
-//   f[3..5]   velocity v (m/s)
-//   f[6..8]   inertia-target offset (y - x) / L
-//   f[9..32]  8 one-ring edge vectors (x_j - x_i) / L, zero-padded
+// Features, 8 lanes per vertex: lane j handles one-ring neighbour j (edge vector, and in the
+// corrections set its previous correction), lane 0 the vertex's own terms; the row is assembled in
+// shared memory and each lane writes 8 consecutive values (256 contiguous bytes per row), so no
+// per-thread 64-value array and no 4-byte stores 256 bytes apart.
+//
+// Corrections set (VBD_FEATURES_CORRECTIONS), lengths in units of the vertex's mean rest edge L:
+//   f[0..2] inertia offset (y - x);  f[3..5] the vertex's previous correction;
+//   f[6+3j..8+3j] edge vector to neighbour j;  f[30+3j..32+3j] neighbour j's previous correction;
+//   f[54..56] material log-stiffnesses;  f[57] log10 mass;  f[58] contact flag;
+//   f[59] one-ring size / 8;  f[60] solvable flag;  f[63] 1
+// Kinematic set (VBD_FEATURES_KINEMATIC): the vertex's own motion and its one-ring geometry, no
+// solver history:
+//   f[0..2] previous step's displacement v dt = (y - x) - g dt^2;  f[3..5] velocity v (m/s);
+//   f[6..8] inertia offset (y - x);  f[9+3j..11+3j] edge vector to neighbour j;
 //   f[33..35] material log-stiffnesses;  f[36] log10 mass;  f[37] contact flag;
-//   f[38]     one-ring size / 8;  f[39] solvable flag;  f[63] 1
-__device__ void kinematic_features(const FeatArgs& a, int i, float (&f)[64]) {
-    const float4 pi = a.pinfo[i];
-    const bool solvable = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
-    const float4 vf = a.vfeat[i];
-    const float invL = 1.0f / fmaxf(vf.w, 1e-9f);
-    const float3 x = xyz(a.prev[i]);
-    const float3 yy = xyz(a.y[i]);
-    const float3 off = f3(yy.x - x.x, yy.y - x.y, yy.z - x.z);
-    if (solvable) {
-        const float3 vdt = f3(off.x - a.g_dt2.x, off.y - a.g_dt2.y, off.z - a.g_dt2.z);
-        f[0] = vdt.x * invL;
-        f[1] = vdt.y * invL;
-        f[2] = vdt.z * invL;
-        f[3] = vdt.x * a.inv_dt;
-        f[4] = vdt.y * a.inv_dt;
-        f[5] = vdt.z * a.inv_dt;
-    }
-    f[6] = off.x * invL;
-    f[7] = off.y * invL;
-    f[8] = off.z * invL;
-    int nn = 0;
-    for (int k = 0; k < 8; ++k) {
-        const int nb = a.nbr8[8 * i + k];
-        if (nb < 0) continue;
-        ++nn;
-        const float3 xn = xyz(a.prev[nb]);
-        f[9 + 3 * k] = (xn.x - x.x) * invL;
-        f[10 + 3 * k] = (xn.y - x.y) * invL;
-        f[11 + 3 * k] = (xn.z - x.z) * invL;
-    }
-    f[33] = vf.x;
-    f[34] = vf.y;
-    f[35] = vf.z;
-    f[36] = pi.x > 0.f ? log10f(pi.x) : 0.f;
-    f[37] = (a.ccount && a.ccount[i] > 0) ? 1.f : 0.f;
-    f[38] = nn * 0.125f;
-    f[39] = solvable ? 1.f : 0.f;
-    f[63] = 1.f;
-}
+//   f[38] one-ring size / 8;  f[39] solvable flag;  f[63] 1
+constexpr int kFeatLanes = 8;
+constexpr int kFeatBlock = 128;
+constexpr int kFeatRows = kFeatBlock / kFeatLanes;
+constexpr int kFeatStride = 68;  // floats per shared row (16-byte aligned, rows 4 banks apart)
 
-__global__ void features_kernel(FeatArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.V) return;
-    const int o = a.perm[i];
-    float f[64];
-    for (int k = 0; k < 64; ++k) f[k] = 0.f;
-    if (a.mode == VBD_FEATURES_KINEMATIC) {
-        kinematic_features(a, i, f);
-        float* out = a.out + (size_t)o * 64;
-        for (int k = 0; k < 64; ++k) {
-            float v = f[k];
-            if (a.mean) v = (v - a.mean[k]) * a.inv_std[k];
-            out[k] = v;
+__global__ void __launch_bounds__(kFeatBlock) features_kernel(FeatArgs a) {
+    __shared__ __align__(16) float rows[kFeatRows * kFeatStride];
+    const int t = threadIdx.x, vr = t / kFeatLanes, j = t % kFeatLanes;
+    const int i = blockIdx.x * kFeatRows + vr;
+    const bool valid = i < a.V;
+    float* f = rows + vr * kFeatStride;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) f[8 * j + k] = 0.f;
+    __syncwarp();
+    const bool kin = a.mode == VBD_FEATURES_KINEMATIC;
+    int nb = -1;
+    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f), vf = make_float4(0.f, 0.f, 0.f, 1.f);
+    float3 x = f3(0.f, 0.f, 0.f);
+    float invL = 1.f;
+    if (valid) {
+        pi = a.pinfo[i];
+        vf = a.vfeat[i];
+        invL = 1.0f / fmaxf(vf.w, 1e-9f);
+        x = xyz(a.prev[i]);
+        nb = a.nbr8[kFeatLanes * i + j];
+        if (nb >= 0) {
+            const float3 xn = xyz(a.prev[nb]);
+            const int e = kin ? 9 + 3 * j : 6 + 3 * j;
+            f[e] = (xn.x - x.x) * invL;
+            f[e + 1] = (xn.y - x.y) * invL;
+            f[e + 2] = (xn.z - x.z) * invL;
+            if (!kin && a.corr_prev) {
+                const int on = a.internal ? nb : a.perm[nb];
+                f[30 + 3 * j] = a.corr_prev[3 * on] * invL;
+                f[31 + 3 * j] = a.corr_prev[3 * on + 1] * invL;
+                f[32 + 3 * j] = a.corr_prev[3 * on + 2] * invL;
+            }
         }
+    }
+    // one-ring size: the vertex's 8 lanes are consecutive lanes of one warp
+    const unsigned have = __ballot_sync(0xffffffffu, nb >= 0);
+    const int nn = __popc((have >> ((t & 31) & ~(kFeatLanes - 1))) & 0xffu);
+    if (valid && j == 0) {
+        const bool solvable = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
+        const float3 yy = xyz(a.y[i]);
+        const float3 off = f3(yy.x - x.x, yy.y - x.y, yy.z - x.z);
+        const float mass = pi.x > 0.f ? log10f(pi.x) : 0.f;
+        const float contact = (a.ccount && a.ccount[i] > 0) ? 1.f : 0.f;
+        if (kin) {
+            if (solvable) {
+                const float3 vdt = f3(off.x - a.g_dt2.x, off.y - a.g_dt2.y, off.z - a.g_dt2.z);
+                f[0] = vdt.x * invL;
+                f[1] = vdt.y * invL;
+                f[2] = vdt.z * invL;
+                f[3] = vdt.x * a.inv_dt;
+                f[4] = vdt.y * a.inv_dt;
+                f[5] = vdt.z * a.inv_dt;
+            }
+            f[6] = off.x * invL;
+            f[7] = off.y * invL;
+            f[8] = off.z * invL;
+            f[33] = vf.x;
+            f[34] = vf.y;
+            f[35] = vf.z;
+            f[36] = mass;
+            f[37] = contact;
+            f[38] = nn * 0.125f;
+            f[39] = solvable ? 1.f : 0.f;
+        } else {
+            f[0] = off.x * invL;
+            f[1] = off.y * invL;
+            f[2] = off.z * invL;
+            if (a.corr_prev) {
+                const int o = a.internal ? i : a.perm[i];
+                f[3] = a.corr_prev[3 * o] * invL;
+                f[4] = a.corr_prev[3 * o + 1] * invL;
+                f[5] = a.corr_prev[3 * o + 2] * invL;
+            }
+            f[54] = vf.x;
+            f[55] = vf.y;
+            f[56] = vf.z;
+            f[57] = mass;
+            f[58] = contact;
+            f[59] = nn * 0.125f;
+            f[60] = solvable ? 1.f : 0.f;
+        }
+        f[63] = 1.f;
+    }
+    __syncwarp();
+    if (!valid) return;
+    const int row = a.internal ? i : a.perm[i];
+    float v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int c = 8 * j + k;
+        v[k] = a.mean ? (f[c] - __ldg(&a.mean[c])) * __ldg(&a.inv_std[c]) : f[c];
+    }
+    if (a.out16) {
+        const uint4 w = make_uint4(tc::pack_bf16(v[0], v[1]), tc::pack_bf16(v[2], v[3]), tc::pack_bf16(v[4], v[5]),
+                                   tc::pack_bf16(v[6], v[7]));
+        *reinterpret_cast<uint4*>(a.out16 + static_cast<size_t>(row) * 64 + 8 * j) = w;
         return;
     }
-    const float4 pi = a.pinfo[i];
-    const bool solvable = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
-    const float4 vf = a.vfeat[i];
-    const float invL = 1.0f / fmaxf(vf.w, 1e-9f);
-    const float3 x = xyz(a.prev[i]);
-    const float3 yy = xyz(a.y[i]);
-    f[0] = (yy.x - x.x) * invL;
-    f[1] = (yy.y - x.y) * invL;
-    f[2] = (yy.z - x.z) * invL;
-    if (a.corr_prev) {
-        f[3] = a.corr_prev[3 * o] * invL;
-        f[4] = a.corr_prev[3 * o + 1] * invL;
-        f[5] = a.corr_prev[3 * o + 2] * invL;
-    }
-    int nn = 0;
-    for (int k = 0; k < 8; ++k) {
-        const int nb = a.nbr8[8 * i + k];
-        if (nb < 0) continue;
-        ++nn;
-        const float3 xn = xyz(a.prev[nb]);
-        f[6 + 3 * k] = (xn.x - x.x) * invL;
-        f[7 + 3 * k] = (xn.y - x.y) * invL;
-        f[8 + 3 * k] = (xn.z - x.z) * invL;
-        if (a.corr_prev) {
-            const int on = a.perm[nb];
-            f[30 + 3 * k] = a.corr_prev[3 * on] * invL;
-            f[31 + 3 * k] = a.corr_prev[3 * on + 1] * invL;
-            f[32 + 3 * k] = a.corr_prev[3 * on + 2] * invL;
-        }
-    }
-    f[54] = vf.x;
-    f[55] = vf.y;
-    f[56] = vf.z;
-    f[57] = pi.x > 0.f ? log10f(pi.x) : 0.f;
-    f[58] = (a.ccount && a.ccount[i] > 0) ? 1.f : 0.f;
-    f[59] = nn * 0.125f;
-    f[60] = solvable ? 1.f : 0.f;
-    f[63] = 1.f;
-    float* out = a.out + (size_t)o * 64;
-    for (int k = 0; k < 64; ++k) {
-        float v = f[k];
-        if (a.mean) v = (v - a.mean[k]) * a.inv_std[k];
-        out[k] = v;
-    }
+    float4* out = reinterpret_cast<float4*>(a.out + static_cast<size_t>(row) * 64 + 8 * j);
+    out[0] = make_float4(v[0], v[1], v[2], v[3]);
+    out[1] = make_float4(v[4], v[5], v[6], v[7]);
 }
 
 // Largest warm-start move, in characteristic lengths.  Trained corrections are a few hundredths
@@ -588,15 +607,16 @@ __global__ void features_kernel(FeatArgs a) {
 // that the start cannot fold an element over before the sweeps begin.
 constexpr float kMaxPrediction = 0.25f;
 
-// delta = prediction * characteristic length (solvable vertices, 0 elsewhere), model order: the
+// delta = prediction * characteristic length (solvable vertices, 0 elsewhere), in model order (or
+// internal order for the step mode's rows, `internal`): the
 // network predicts the step's correction x - y from the inertia target in units of the vertex's
 // mean rest edge length, |prediction| <= kMaxPrediction (a non-finite prediction gives 0).  A zero
 // network therefore leaves the solve exactly as plain VBD's.
 __global__ void scale_prediction_kernel(int V, const int* perm, const float4* pinfo, const float4* vfeat,
-                                        const float* pred, float* delta) {
+                                        const float* pred, float* delta, int internal) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= V) return;
-    const int o = perm[i];
+    const int o = internal ? i : perm[i];
     const float4 pi = pinfo[i];
     const bool solvable = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
     const float p0 = pred[3 * o], p1 = pred[3 * o + 1], p2 = pred[3 * o + 2];
@@ -609,18 +629,51 @@ __global__ void scale_prediction_kernel(int V, const int* perm, const float4* pi
     delta[3 * o + 2] = use ? p2 * s : 0.f;
 }
 
+// The step mode's start, in one pass over the internal rows: the bounded prediction scaled by L
+// (scale_prediction_kernel's arithmetic) added to the displacement and the iterate
+// (warm_start_kernel's), with the same roundings.
+__global__ void apply_prediction_kernel(int V, const float4* pinfo, const float4* vfeat, const float* pred,
+                                        const float4* prev, float4* disp, float4* pos) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V) return;
+    const float4 pi = pinfo[i];
+    if (!((__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f)) return;
+    const float p0 = pred[3 * i], p1 = pred[3 * i + 1], p2 = pred[3 * i + 2];
+    const float n2 = p0 * p0 + p1 * p1 + p2 * p2;
+    float s = vfeat[i].w;
+    if (!(n2 <= kMaxPrediction * kMaxPrediction)) s = s * kMaxPrediction * rsqrtf(n2);
+    const bool use = isfinite(n2);
+    const float d0 = use ? p0 * s : 0.f, d1 = use ? p1 * s : 0.f, d2 = use ? p2 * s : 0.f;
+    float4 d = disp[i];
+    d = make_float4(d.x + d0, d.y + d1, d.z + d2, 0.f);
+    disp[i] = d;
+    const float4 p = prev[i];
+    pos[i] = make_float4(__fadd_rn(p.x, d.x), __fadd_rn(p.y, d.y), __fadd_rn(p.z, d.z), 0.f);
+}
+
 }  // namespace
+
+int mlp_apply_launch(const VbdModelImpl& m, const float* pred, const float4* prev, float4* disp, float4* pos,
+                     cudaStream_t st) {
+    if (m.V == 0) return VBD_OK;
+    apply_prediction_kernel<<<(m.V + 255) / 256, 256, 0, st>>>(m.V, m.pinfo, m.vfeat, pred, prev, disp, pos);
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
+}
 
 int mlp_features_launch(const VbdModelImpl& m, const float4* prev, const float4* y, const int* ccount,
                         const float* corr_prev, const float* mean, const float* inv_std, float* out, int mode,
-                        float dt, cudaStream_t st) {
+                        float dt, cudaStream_t st, int internal, uint16_t* out16) {
     if (mode != VBD_FEATURES_CORRECTIONS && mode != VBD_FEATURES_KINEMATIC)
         return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_features: unknown feature set");
     if (mode == VBD_FEATURES_KINEMATIC && !(dt > 0.f))
         return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_features: the kinematic set needs the step's dt (run vbd_forward first)");
+    if ((reinterpret_cast<uintptr_t>(out) & 15u) || (reinterpret_cast<uintptr_t>(out16) & 15u))
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_features: out must be 16-byte aligned");
     if (m.V == 0) return VBD_OK;
     FeatArgs f;
     f.mode = mode;
+    f.internal = internal;
     f.g_dt2 = make_float3(m.gravity[0] * dt * dt, m.gravity[1] * dt * dt, m.gravity[2] * dt * dt);
     f.inv_dt = dt > 0.f ? 1.0f / dt : 0.f;
     f.V = m.V;
@@ -635,14 +688,16 @@ int mlp_features_launch(const VbdModelImpl& m, const float4* prev, const float4*
     f.mean = mean;
     f.inv_std = inv_std;
     f.out = out;
-    features_kernel<<<(m.V + 127) / 128, 128, 0, st>>>(f);
+    f.out16 = out16;
+    features_kernel<<<(m.V + kFeatRows - 1) / kFeatRows, kFeatBlock, 0, st>>>(f);
     VBD_CUDA_TRY(cudaGetLastError());
     return VBD_OK;
 }
 
-int mlp_scale_launch(const VbdModelImpl& m, const float* pred, float* delta, cudaStream_t st) {
+int mlp_scale_launch(const VbdModelImpl& m, const float* pred, float* delta, cudaStream_t st, int internal) {
     if (m.V == 0) return VBD_OK;
-    scale_prediction_kernel<<<(m.V + 255) / 256, 256, 0, st>>>(m.V, m.perm, m.pinfo, m.vfeat, pred, delta);
+    scale_prediction_kernel<<<(m.V + 255) / 256, 256, 0, st>>>(m.V, m.perm, m.pinfo, m.vfeat, pred, delta,
+                                                                internal);
     VBD_CUDA_TRY(cudaGetLastError());
     return VBD_OK;
 }
@@ -673,11 +728,10 @@ extern "C" int vbd_mlp_workspace_bytes(int32_t n, int64_t* bytes) {
     return VBD_OK;
 }
 
-extern "C" int vbd_mlp_forward(const float* params, const uint16_t* w16, const float* X, int32_t n, float* Y,
-                               void* stream) {
-    if (!params || !w16 || (n > 0 && (!X || !Y))) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_forward: NULL argument");
-    if ((reinterpret_cast<uintptr_t>(X) & 15u) || (reinterpret_cast<uintptr_t>(w16) & 1u))
-        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_forward: X must be 16-byte aligned");
+namespace vbd {
+// the tcgen05 inference on FP32 rows (X) or on BF16 rows (X16)
+static int tc_forward(const float* params, const uint16_t* w16, const float* X, const uint16_t* X16, int32_t n,
+                      float* Y, cudaStream_t st) {
     int rc = ensure_tile_smem();
     if (rc) return rc;
     if (n == 0) return VBD_OK;
@@ -686,6 +740,7 @@ extern "C" int vbd_mlp_forward(const float* params, const uint16_t* w16, const f
     a.params = params;
     a.w16 = w16;
     a.X = X;
+    a.X16 = X16;
     a.Y = Y;
     unsigned* counter = nullptr;
     VBD_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&counter), g_mlp_tc_timeouts));
@@ -693,9 +748,27 @@ extern "C" int vbd_mlp_forward(const float* params, const uint16_t* w16, const f
     a.off_b1 = kOffB1;
     a.off_b2 = kOffB2;
     a.off_b3 = kOffB3;
-    tc::mlp_infer_tc_kernel<<<tc_grid(n), tc::kThreads, tc::kSmemBytes, static_cast<cudaStream_t>(stream)>>>(a);
+    if (X16)
+        tc::mlp_infer_tc_kernel<true><<<tc_grid(n), tc::kThreads, tc::kSmemBytes, st>>>(a);
+    else
+        tc::mlp_infer_tc_kernel<false><<<tc_grid(n), tc::kThreads, tc::kSmemBytes, st>>>(a);
     VBD_CUDA_TRY(cudaGetLastError());
     return VBD_OK;
+}
+
+int mlp_forward_bf16(const float* params, const uint16_t* w16, const uint16_t* X16, int n, float* Y, cudaStream_t st) {
+    if ((reinterpret_cast<uintptr_t>(X16) & 15u) || (reinterpret_cast<uintptr_t>(w16) & 1u))
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp: BF16 rows must be 16-byte aligned");
+    return tc_forward(params, w16, nullptr, X16, n, Y, st);
+}
+}  // namespace vbd
+
+extern "C" int vbd_mlp_forward(const float* params, const uint16_t* w16, const float* X, int32_t n, float* Y,
+                               void* stream) {
+    if (!params || !w16 || (n > 0 && (!X || !Y))) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_forward: NULL argument");
+    if ((reinterpret_cast<uintptr_t>(X) & 15u) || (reinterpret_cast<uintptr_t>(w16) & 1u))
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_forward: X must be 16-byte aligned");
+    return tc_forward(params, w16, X, nullptr, n, Y, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int vbd_mlp_forward_mma_sync(const float* params, const uint16_t* w16, const float* X, int32_t n, float* Y,

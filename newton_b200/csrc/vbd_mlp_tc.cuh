@@ -218,12 +218,14 @@ struct TcArgs {
     int n;
     const float* params;  // FP32 blob (biases)
     const uint16_t* w16;  // BF16 weights: W1 [64][128] | W2 [128][128] | W3 [128][8]
-    const float* X;       // [n][64]
+    const float* X;       // [n][64] FP32, or NULL when X16 is given
+    const uint16_t* X16;  // [n][64] BF16 (16-byte aligned rows), already rounded as the FP32 path rounds
     float* Y;             // [n][3]
     unsigned* status;     // incremented on a wait that gave up (may be NULL)
     int off_b1, off_b2, off_b3;
 };
 
+template <bool kBf16In>
 __global__ void __launch_bounds__(kThreads, 1) mlp_infer_tc_kernel(TcArgs a) {
     extern __shared__ unsigned char smem_raw[];
     unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -290,7 +292,24 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_infer_tc_kernel(TcArgs a) {
         // a lane takes row 32 q + 8 (j / 4) + lane % 8 and float4 column 4 (j % 4) + lane / 8, so each
         // load reads 8 rows x 64 contiguous bytes and each store fills whole core-matrix rows; the
         // 16 loads are in flight together (the other groups' work covers their latency) ----
-        {
+        if (kBf16In) {
+            // BF16 rows: a 16-byte chunk is 8 consecutive k of one row, i.e. one core-matrix row;
+            // in pass j a lane takes row 32 q + 4 j + lane / 8 and chunk lane % 8 (each load reads
+            // 4 whole 128-byte rows)
+            uint4 v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int r = quarter * 32 + 4 * j + (lane >> 3);
+                v[j] = make_uint4(0u, 0u, 0u, 0u);
+                if (row0 + r < a.n)
+                    v[j] = __ldg(reinterpret_cast<const uint4*>(a.X16 + static_cast<size_t>(row0 + r) * 64) + (lane & 7));
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int r = quarter * 32 + 4 * j + (lane >> 3);
+                *reinterpret_cast<uint4*>(buf + kmajor_offset(r, 8 * (lane & 7), kRows)) = v[j];
+            }
+        } else {
             float4 v[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) {

@@ -1161,12 +1161,12 @@ __global__ void finalize_kernel(FinalizeArgs a) {
 // Warm start: the initial Gauss-Seidel iterate becomes inertia target + delta for every vertex the
 // sweep solves (pinned / massless vertices keep their position).
 __global__ void warm_start_kernel(const int* perm, const float4* pinfo, const float4* prev, float4* disp, float4* pos,
-                                  const float* delta, int V) {
+                                  const float* delta, int V, int internal = 0) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= V) return;
     const float4 pi = pinfo[i];
     if (!((__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f)) return;
-    const int o = perm[i];
+    const int o = internal ? i : perm[i];  // row of delta
     float4 d = disp[i];
     d = make_float4(d.x + delta[3 * o], d.y + delta[3 * o + 1], d.z + delta[3 * o + 2], 0.f);
     disp[i] = d;
@@ -1174,12 +1174,22 @@ __global__ void warm_start_kernel(const int* perm, const float4* pinfo, const fl
     pos[i] = make_float4(__fadd_rn(p.x, d.x), __fadd_rn(p.y, d.y), __fadd_rn(p.z, d.z), 0.f);
 }
 
-// correction of the finished step, x_solved - y (model order), the next step's warm-start feature
+// out[3 i + k] = in[3 perm[i] + k]: a [V,3] model-order array into the internal order
+__global__ void gather_rows3_kernel(const int* perm, const float* in, float* out, int V) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= V) return;
+    const int o = perm[i];
+    out[3 * i] = in[3 * o];
+    out[3 * i + 1] = in[3 * o + 1];
+    out[3 * i + 2] = in[3 * o + 2];
+}
+
+// correction of the finished step, x_solved - y, the next step's warm-start feature
 __global__ void correction_kernel(const int* perm, const float4* pinfo, const float4* pos, const float4* y,
                                   float* corr, int V) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= V) return;
-    const int o = perm[i];
+    const int o = perm ? perm[i] : i;  // NULL: internal order (the step mode's own buffer)
     const float4 pi = pinfo[i];
     const bool solvable = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
     const float4 p = pos[i], yy = y[i];
@@ -1701,7 +1711,6 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
         const int V = s.m->V;
         float* feats = s.ws_work;
         float* pred = feats + static_cast<size_t>(V) * 64;
-        float* delta = pred + static_cast<size_t>(V) * 3;
         const bool gated = s.gate_tol > 0.f;
         if (gated) {
             VBD_CUDA_TRY(cudaMemsetAsync(s.gate, 0, offsetof(GateState, pad), st));
@@ -1711,12 +1720,14 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
                 gate_ref_kernel<<<1, 32, 0, st>>>(s.gate, s.gate_mean, s.gate_count);
             }
         }
+        // rows in the internal vertex order (coalesced, no model-order scatter), as BF16 (the
+        // inference rounds its inputs to BF16 anyway: half the bytes written and read)
+        uint16_t* feats16 = reinterpret_cast<uint16_t*>(feats);
         int rc = mlp_features_launch(*s.m, s.prev, s.y, c ? s.ccount : nullptr, s.ws_corr, s.ws_mean, s.ws_inv_std,
-                                     feats, s.feature_set, dt, st);
-        if (!rc) rc = vbd_mlp_forward(s.ws_params, s.ws_w16, feats, V, pred, st);
-        if (!rc) rc = mlp_scale_launch(*s.m, pred, delta, st);
+                                     nullptr, s.feature_set, dt, st, 1, feats16);
+        if (!rc) rc = mlp_forward_bf16(s.ws_params, s.ws_w16, feats16, V, pred, st);
+        if (!rc) rc = mlp_apply_launch(*s.m, pred, s.prev, s.disp, s.pos, st);
         if (rc) return rc;
-        warm_start_kernel<<<(V + 255) / 256, 256, 0, st>>>(s.m->perm, s.m->pinfo, s.prev, s.disp, s.pos, delta, V);
         if (gated) {
             rc = enqueue_gated_iterations(s, c, dt, st, false);
             if (rc) return rc;
@@ -1724,7 +1735,7 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
             for (int it = 0; it < s.ws_iterations; ++it)
                 for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st, it == 0);
         }
-        correction_kernel<<<(V + 255) / 256, 256, 0, st>>>(s.m->perm, s.m->pinfo, s.pos, s.y, s.ws_corr, V);
+        correction_kernel<<<(V + 255) / 256, 256, 0, st>>>(nullptr, s.m->pinfo, s.pos, s.y, s.ws_corr, V);
         enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
         return VBD_OK;
     }
@@ -2190,6 +2201,18 @@ extern "C" int vbd_set_warm_start(VbdSolver* solver, const float* params, const 
     s.ws_mean = mean;
     s.ws_inv_std = inv_std;
     s.ws_iterations = iterations;
+    return VBD_OK;
+}
+
+extern "C" int vbd_set_warm_start_correction(VbdSolver* solver, const float* corr, void* stream) {
+    if (!solver || !corr) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_warm_start_correction: NULL argument");
+    SolverImpl& s = solver->s;
+    if (!s.ws_corr) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_set_warm_start_correction: the warm start is off");
+    const int V = s.m->V;
+    if (V == 0) return VBD_OK;
+    // the step mode keeps it in the internal vertex order
+    gather_rows3_kernel<<<(V + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(s.m->perm, corr, s.ws_corr, V);
+    VBD_CUDA_TRY(cudaGetLastError());
     return VBD_OK;
 }
 

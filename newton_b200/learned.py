@@ -3,10 +3,11 @@
 A per-vertex MLP (64 -> 128 -> 128 -> 3, SiLU, BF16 weights, FP32 accumulation on the tensor
 cores) predicts the correction ``x_solved - y`` that the coming step applies to the inertia
 target ``y``, in units of the vertex's characteristic element length, from one-ring features
-(``vbd_mlp_features``).  Two feature sets: ``"kinematic"`` (default) -- previous step's
-displacement, velocity and inertia offset, the 8 one-ring edge vectors, log-stiffnesses, mass,
-contact and pin flags; ``"corrections"`` -- the inertia offset, the previous step's correction of
-the vertex and of 8 one-ring neighbours, with the same geometry, material and flags.  The Gauss-Seidel iterations then start from ``y + prediction``; a zero network is
+(``vbd_mlp_features``).  Two feature sets: ``"corrections"`` (default) -- the inertia offset, the
+previous step's correction of the vertex and of 8 one-ring neighbours, the 8 one-ring edge
+vectors, log-stiffnesses, mass, contact and pin flags; ``"kinematic"`` -- previous step's
+displacement, velocity and inertia offset with the same geometry, material and flags, no solver
+history.  The Gauss-Seidel iterations then start from ``y + prediction``; a zero network is
 plain VBD bit for bit.  What decides whether the warm start pays is the residual-gated step
 (``SolverVBD.set_residual_gate``): from the same state, the learned and the plain solver iterate
 until the same force residual, and the iterations they need are compared (``gated_steps``).
@@ -56,7 +57,7 @@ def characteristic_length(model) -> np.ndarray:
 class WarmStartMLP:
     """Parameters, optimiser state and feature standardisation of the warm-start network."""
 
-    def __init__(self, device, seed: int = 0, feature_set: str = "kinematic"):
+    def __init__(self, device, seed: int = 0, feature_set: str = "corrections"):
         self.device = torch.device(device)
         self.feature_set = feature_set  # the solver's feature set this network reads
         self.lib = _lib.load()
@@ -173,7 +174,7 @@ def inertia_target(model, state, dt: float) -> torch.Tensor:
 
 def generate_dataset(model, q0, solver, pipe, steps: int, dt: float, target_iterations: int = 20,
                      samples_per_step: int = 1024, seed: int = 0, trajectory_iterations: int | None = None,
-                     feature_set: str | tuple = "kinematic", record_every: int = 1):
+                     feature_set: str | tuple = "corrections", record_every: int = 1):
     """Features and targets from a VBD trajectory.
 
     At every ``record_every``-th step: collide, forward, features of ``feature_set`` (with the
@@ -253,15 +254,17 @@ def record_plain_states(model, q_start, qd_start, pipe, gate: dict, steps: int, 
 
 
 def teacher_forced_steps(model, states: list, pipe, gate: dict, dt: float, mlp: WarmStartMLP | None = None,
-                         launch: dict | None = None, warm: int = 0, timer=None) -> dict:
+                         launch: dict | None = None, warm: int = 0, timer=None, history: bool = True) -> dict:
     """One residual-gated step from every recorded state of a plain trajectory, by plain VBD
     (``mlp=None``) or by the learned step mode.  Both arms start each step from the same state,
     hence the same inertia target y and -- the gate being relative to the residual at y -- the same
-    absolute tolerance: the iterations they need are counted to the same force residual.  The
-    learned solver's correction feature carries over from its own previous step.  The first
-    ``warm`` states are stepped but not counted (the correction feature needs one step of
-    history).  ``timer`` (optional) has ``before()`` / ``after()``, called around each counted
-    collide + step.  Returns the gate statistics of the counted steps and the solver status."""
+    absolute tolerance: the iterations they need are counted to the same force residual.  With
+    ``history`` the learned solver's previous-correction feature is the recorded trajectory's own
+    (x_k - y_(k-1), set before each step), as it is for a solver on its own trajectory; otherwise it
+    carries over from the learned solver's previous step from the previous recorded state.  The
+    first ``warm`` states are stepped but not counted.  ``timer`` (optional) has ``before()`` /
+    ``after()``, called around each counted collide + step.  Returns the gate statistics of the
+    counted steps and the solver status."""
     from .solvers import SolverVBD
 
     solver = SolverVBD(model, iterations=10)
@@ -276,6 +279,12 @@ def teacher_forced_steps(model, states: list, pipe, gate: dict, dt: float, mlp: 
         if k == warm:
             solver.gate_stats(reset=True)
             solver.status(reset=True)
+        if mlp is not None and history and k > 0:
+            # the recorded trajectory's correction of step k-1: its solved positions (state k)
+            # minus the inertia target of state k-1
+            s0.particle_q.copy_(states[k - 1][0])
+            s0.particle_qd.copy_(states[k - 1][1])
+            solver.set_warm_start_correction(q - inertia_target(model, s0, dt))
         s0.particle_q.copy_(q)
         s0.particle_qd.copy_(qd)
         counted = k >= warm and timer is not None

@@ -349,6 +349,12 @@ class SolverVBD(SolverBase):
         _lib.check(self._lib.vbd_step_kernel_count(self._handle, ctypes.byref(k)))
         return k.value
 
+    def set_warm_start_correction(self, corr: torch.Tensor) -> None:
+        """The previous step's correction ``x_solved - y`` ([V,3] model order, device) the warm-start
+        step mode feeds to the next step's features (``vbd_set_warm_start_correction``)."""
+        corr = corr.contiguous()
+        _lib.check(self._lib.vbd_set_warm_start_correction(self._handle, _lib.ptr(corr), self._stream()))
+
     FEATURE_SETS = {"corrections": 0, "kinematic": 1}
 
     def set_feature_set(self, name: str) -> None:
