@@ -356,9 +356,11 @@ int vbd_set_feature_set(VbdSolver* solver, int32_t feature_set);
  * NULL.  mean / inv_std [64] standardise them (both NULL = raw).  out must be 16-byte aligned. */
 int vbd_mlp_features(VbdSolver* solver, const float* corr_prev, const float* mean, const float* inv_std, float* out,
                      void* stream);
-/* Y [n][3] = MLP(X [n][64]) on the 5th-generation tensor cores (tcgen05.mma, BF16 operands in
- * shared memory, FP32 accumulators in tensor memory; SiLU with the hardware tanh approximation).
- * X must be 16-byte aligned.  A wait that gives up is counted (vbd_mlp_timeouts). */
+/* Y [n][3] = MLP(X [n][64]) on the 5th-generation tensor cores (tcgen05.mma: the FP32 weights of
+ * params and the inputs rounded to FP16 in shared memory, FP16 accumulators in tensor memory for
+ * the hidden layers and FP32 for the output; bias + SiLU in f16x2 arithmetic with the hardware
+ * tanh approximation).  w16 is not read (it is the BF16 copy the training kernels use).  X must be
+ * 16-byte aligned.  A wait that gives up is counted (vbd_mlp_timeouts). */
 int vbd_mlp_forward(const float* params, const uint16_t* w16, const float* X, int32_t n, float* Y, void* stream);
 /* The same inference on the previous tensor-core path (mma.sync m16n8k16 fragments, exact SiLU),
  * kept to cross-check the tcgen05 kernel. */
@@ -388,10 +390,13 @@ int vbd_mlp_warm_start(VbdSolver* solver, const float* params, const uint16_t* w
                        void* stream);
 
 /* Learned warm start as a mode of vbd_step: every step becomes forward -> features -> MLP ->
- * start from y + prediction -> `iterations` colour sweeps -> finalize, and the step's correction
- * x_solved - y is kept (solver-owned) as the next step's feature.  params / w16 / mean / inv_std
- * are caller-owned device buffers that must outlive the solver's use of them; params == NULL
- * turns the mode off.  Allocates the solver's correction and workspace buffers on first use. */
+ * start from y + prediction -> `iterations` colour sweeps (or the residual gate's loop) ->
+ * finalize, and the step's correction x_solved - y is kept (solver-owned) as the next step's
+ * feature.  Features, inference and the start run as one tcgen05 kernel (no feature rows in
+ * memory); the results equal vbd_mlp_features -> vbd_mlp_forward -> vbd_mlp_warm_start's bit for
+ * bit.  params / w16 / mean / inv_std are caller-owned device buffers that must outlive the
+ * solver's use of them; params == NULL turns the mode off.  Allocates the solver's correction
+ * buffer on first use. */
 int vbd_set_warm_start(VbdSolver* solver, const float* params, const uint16_t* w16, const float* mean,
                        const float* inv_std, int32_t iterations);
 

@@ -103,21 +103,19 @@ struct VbdModelImpl {
     float soft_ke = 0.f, soft_kd = 0.f, soft_mu = 0.f;
 };
 
-// learned warm start (vbd_mlp.cu): per-vertex features after the forward pass, and the warm-start
-// displacement = network output (in characteristic lengths) * length
-// mode: VBD_FEATURES_CORRECTIONS or VBD_FEATURES_KINEMATIC; dt: the step's (kinematic set)
-// internal: rows in the internal (color-major) vertex order instead of the model's (the step
-// mode's own buffers); corr_prev is in model order either way
+// learned warm start (vbd_mlp.cu): per-vertex features after the forward pass (model-order rows;
+// corr_prev in model order), and the warm-start displacement = network output (in characteristic
+// lengths) * length.  mode: VBD_FEATURES_CORRECTIONS or VBD_FEATURES_KINEMATIC; dt: the step's
+// (kinematic set)
 int mlp_features_launch(const VbdModelImpl& m, const float4* prev, const float4* y, const int* ccount,
                         const float* corr_prev, const float* mean, const float* inv_std, float* out, int mode,
-                        float dt, cudaStream_t st, int internal = 0, uint16_t* out16 = nullptr);
-// the step mode's start from its internal-order predictions (bounded, scaled by L, added to the
-// displacement and the iterate)
-int mlp_apply_launch(const VbdModelImpl& m, const float* pred, const float4* prev, float4* disp, float4* pos,
-                     cudaStream_t st);
-// the tcgen05 inference on BF16 rows (16-byte aligned), as vbd_mlp_forward on FP32 rows
-int mlp_forward_bf16(const float* params, const uint16_t* w16, const uint16_t* X16, int n, float* Y, cudaStream_t st);
-int mlp_scale_launch(const VbdModelImpl& m, const float* pred, float* delta, cudaStream_t st, int internal = 0);
+                        float dt, cudaStream_t st);
+int mlp_scale_launch(const VbdModelImpl& m, const float* pred, float* delta, cudaStream_t st);
+// the step mode's learned start in one tcgen05 launch: features of every internal vertex (corr_prev
+// in the internal order), inference, the bounded start added to disp and pos
+int mlp_step_start(const VbdModelImpl& m, const float* params, const float4* prev, const float4* y, const int* ccount,
+                   const float* corr_prev, const float* mean, const float* inv_std, int mode, float dt, float4* disp,
+                   float4* pos, cudaStream_t st);
 
 }  // namespace vbd
 

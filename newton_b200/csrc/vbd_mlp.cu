@@ -431,10 +431,10 @@ int ensure_tile_smem() {
                                           static_cast<int>(kTileSmem)));
         VBD_CUDA_TRY(cudaFuncSetAttribute(mlp_tile_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           static_cast<int>(kTileSmem)));
-        VBD_CUDA_TRY(cudaFuncSetAttribute(tc::mlp_infer_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          tc::kSmemBytes));
-        VBD_CUDA_TRY(cudaFuncSetAttribute(tc::mlp_infer_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          tc::kSmemBytes));
+        VBD_CUDA_TRY(cudaFuncSetAttribute(tc::mlp_infer_tc_kernel<tc::kInF32>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes));
+        VBD_CUDA_TRY(cudaFuncSetAttribute(tc::mlp_infer_tc_kernel<tc::kInStep>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes));
         g_attr_done[dev] = true;
     }
     return VBD_OK;
@@ -467,12 +467,10 @@ struct FeatArgs {
     const int* nbr8;
     const float4* vfeat;
     const int* ccount;
-    const float* corr_prev;  // [V][3] (model order; internal order when `internal`), may be NULL
+    const float* corr_prev;  // [V][3] model order, may be NULL
     const float* mean;       // [64] or NULL
     const float* inv_std;    // [64] or NULL
-    float* out;              // [V][64]: row = model index, or internal index when `internal`
-    uint16_t* out16;         // instead of out: BF16 rows (rounded to nearest, as the inference rounds)
-    int internal;
+    float* out;              // [V][64], row = model index
     int mode;                // VBD_FEATURES_CORRECTIONS or VBD_FEATURES_KINEMATIC
     float3 g_dt2;            // gravity * dt^2 (kinematic set)
     float inv_dt;            // 1 / dt (kinematic set)
@@ -526,7 +524,7 @@ __global__ void __launch_bounds__(kFeatBlock) features_kernel(FeatArgs a) {
             f[e + 1] = (xn.y - x.y) * invL;
             f[e + 2] = (xn.z - x.z) * invL;
             if (!kin && a.corr_prev) {
-                const int on = a.internal ? nb : a.perm[nb];
+                const int on = a.perm[nb];
                 f[30 + 3 * j] = a.corr_prev[3 * on] * invL;
                 f[31 + 3 * j] = a.corr_prev[3 * on + 1] * invL;
                 f[32 + 3 * j] = a.corr_prev[3 * on + 2] * invL;
@@ -567,7 +565,7 @@ __global__ void __launch_bounds__(kFeatBlock) features_kernel(FeatArgs a) {
             f[1] = off.y * invL;
             f[2] = off.z * invL;
             if (a.corr_prev) {
-                const int o = a.internal ? i : a.perm[i];
+                const int o = a.perm[i];
                 f[3] = a.corr_prev[3 * o] * invL;
                 f[4] = a.corr_prev[3 * o + 1] * invL;
                 f[5] = a.corr_prev[3 * o + 2] * invL;
@@ -584,96 +582,48 @@ __global__ void __launch_bounds__(kFeatBlock) features_kernel(FeatArgs a) {
     }
     __syncwarp();
     if (!valid) return;
-    const int row = a.internal ? i : a.perm[i];
+    const int row = a.perm[i];
     float v[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int c = 8 * j + k;
         v[k] = a.mean ? (f[c] - __ldg(&a.mean[c])) * __ldg(&a.inv_std[c]) : f[c];
     }
-    if (a.out16) {
-        const uint4 w = make_uint4(tc::pack_bf16(v[0], v[1]), tc::pack_bf16(v[2], v[3]), tc::pack_bf16(v[4], v[5]),
-                                   tc::pack_bf16(v[6], v[7]));
-        *reinterpret_cast<uint4*>(a.out16 + static_cast<size_t>(row) * 64 + 8 * j) = w;
-        return;
-    }
     float4* out = reinterpret_cast<float4*>(a.out + static_cast<size_t>(row) * 64 + 8 * j);
     out[0] = make_float4(v[0], v[1], v[2], v[3]);
     out[1] = make_float4(v[4], v[5], v[6], v[7]);
 }
 
-// Largest warm-start move, in characteristic lengths.  Trained corrections are a few hundredths
-// of L; a prediction beyond this bound (an input unlike the training data) is shortened to it, so
-// that the start cannot fold an element over before the sweeps begin.
-constexpr float kMaxPrediction = 0.25f;
-
-// delta = prediction * characteristic length (solvable vertices, 0 elsewhere), in model order (or
-// internal order for the step mode's rows, `internal`): the
-// network predicts the step's correction x - y from the inertia target in units of the vertex's
-// mean rest edge length, |prediction| <= kMaxPrediction (a non-finite prediction gives 0).  A zero
-// network therefore leaves the solve exactly as plain VBD's.
+// delta = the bounded start (bounded_start) of each solvable vertex, 0 elsewhere, in model order.
+// A zero network therefore leaves the solve exactly as plain VBD's.
 __global__ void scale_prediction_kernel(int V, const int* perm, const float4* pinfo, const float4* vfeat,
-                                        const float* pred, float* delta, int internal) {
+                                        const float* pred, float* delta) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= V) return;
-    const int o = internal ? i : perm[i];
+    const int o = perm[i];
     const float4 pi = pinfo[i];
     const bool solvable = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
-    const float p0 = pred[3 * o], p1 = pred[3 * o + 1], p2 = pred[3 * o + 2];
-    const float n2 = p0 * p0 + p1 * p1 + p2 * p2;
-    float s = vfeat[i].w;
-    if (!(n2 <= kMaxPrediction * kMaxPrediction)) s = s * kMaxPrediction * rsqrtf(n2);
-    const bool use = solvable && isfinite(n2);
-    delta[3 * o] = use ? p0 * s : 0.f;
-    delta[3 * o + 1] = use ? p1 * s : 0.f;
-    delta[3 * o + 2] = use ? p2 * s : 0.f;
-}
-
-// The step mode's start, in one pass over the internal rows: the bounded prediction scaled by L
-// (scale_prediction_kernel's arithmetic) added to the displacement and the iterate
-// (warm_start_kernel's), with the same roundings.
-__global__ void apply_prediction_kernel(int V, const float4* pinfo, const float4* vfeat, const float* pred,
-                                        const float4* prev, float4* disp, float4* pos) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= V) return;
-    const float4 pi = pinfo[i];
-    if (!((__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f)) return;
-    const float p0 = pred[3 * i], p1 = pred[3 * i + 1], p2 = pred[3 * i + 2];
-    const float n2 = p0 * p0 + p1 * p1 + p2 * p2;
-    float s = vfeat[i].w;
-    if (!(n2 <= kMaxPrediction * kMaxPrediction)) s = s * kMaxPrediction * rsqrtf(n2);
-    const bool use = isfinite(n2);
-    const float d0 = use ? p0 * s : 0.f, d1 = use ? p1 * s : 0.f, d2 = use ? p2 * s : 0.f;
-    float4 d = disp[i];
-    d = make_float4(d.x + d0, d.y + d1, d.z + d2, 0.f);
-    disp[i] = d;
-    const float4 p = prev[i];
-    pos[i] = make_float4(__fadd_rn(p.x, d.x), __fadd_rn(p.y, d.y), __fadd_rn(p.z, d.z), 0.f);
+    const float3 m = solvable ? bounded_start(pred[3 * o], pred[3 * o + 1], pred[3 * o + 2], vfeat[i].w)
+                              : make_float3(0.f, 0.f, 0.f);
+    delta[3 * o] = m.x;
+    delta[3 * o + 1] = m.y;
+    delta[3 * o + 2] = m.z;
 }
 
 }  // namespace
 
-int mlp_apply_launch(const VbdModelImpl& m, const float* pred, const float4* prev, float4* disp, float4* pos,
-                     cudaStream_t st) {
-    if (m.V == 0) return VBD_OK;
-    apply_prediction_kernel<<<(m.V + 255) / 256, 256, 0, st>>>(m.V, m.pinfo, m.vfeat, pred, prev, disp, pos);
-    VBD_CUDA_TRY(cudaGetLastError());
-    return VBD_OK;
-}
-
 int mlp_features_launch(const VbdModelImpl& m, const float4* prev, const float4* y, const int* ccount,
                         const float* corr_prev, const float* mean, const float* inv_std, float* out, int mode,
-                        float dt, cudaStream_t st, int internal, uint16_t* out16) {
+                        float dt, cudaStream_t st) {
     if (mode != VBD_FEATURES_CORRECTIONS && mode != VBD_FEATURES_KINEMATIC)
         return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_features: unknown feature set");
     if (mode == VBD_FEATURES_KINEMATIC && !(dt > 0.f))
         return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_features: the kinematic set needs the step's dt (run vbd_forward first)");
-    if ((reinterpret_cast<uintptr_t>(out) & 15u) || (reinterpret_cast<uintptr_t>(out16) & 15u))
+    if (reinterpret_cast<uintptr_t>(out) & 15u)
         return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_features: out must be 16-byte aligned");
     if (m.V == 0) return VBD_OK;
     FeatArgs f;
     f.mode = mode;
-    f.internal = internal;
     f.g_dt2 = make_float3(m.gravity[0] * dt * dt, m.gravity[1] * dt * dt, m.gravity[2] * dt * dt);
     f.inv_dt = dt > 0.f ? 1.0f / dt : 0.f;
     f.V = m.V;
@@ -688,16 +638,14 @@ int mlp_features_launch(const VbdModelImpl& m, const float4* prev, const float4*
     f.mean = mean;
     f.inv_std = inv_std;
     f.out = out;
-    f.out16 = out16;
     features_kernel<<<(m.V + kFeatRows - 1) / kFeatRows, kFeatBlock, 0, st>>>(f);
     VBD_CUDA_TRY(cudaGetLastError());
     return VBD_OK;
 }
 
-int mlp_scale_launch(const VbdModelImpl& m, const float* pred, float* delta, cudaStream_t st, int internal) {
+int mlp_scale_launch(const VbdModelImpl& m, const float* pred, float* delta, cudaStream_t st) {
     if (m.V == 0) return VBD_OK;
-    scale_prediction_kernel<<<(m.V + 255) / 256, 256, 0, st>>>(m.V, m.perm, m.pinfo, m.vfeat, pred, delta,
-                                                                internal);
+    scale_prediction_kernel<<<(m.V + 255) / 256, 256, 0, st>>>(m.V, m.perm, m.pinfo, m.vfeat, pred, delta);
     VBD_CUDA_TRY(cudaGetLastError());
     return VBD_OK;
 }
@@ -729,37 +677,76 @@ extern "C" int vbd_mlp_workspace_bytes(int32_t n, int64_t* bytes) {
 }
 
 namespace vbd {
-// the tcgen05 inference on FP32 rows (X) or on BF16 rows (X16)
-static int tc_forward(const float* params, const uint16_t* w16, const float* X, const uint16_t* X16, int32_t n,
-                      float* Y, cudaStream_t st) {
+// the tcgen05 inference on FP32 rows (weights: the FP32 blob, rounded to FP16 in the kernel)
+static int tc_forward(const float* params, const float* X, int32_t n, float* Y, cudaStream_t st) {
     int rc = ensure_tile_smem();
     if (rc) return rc;
     if (n == 0) return VBD_OK;
     tc::TcArgs a;
+    std::memset(&a, 0, sizeof(a));
     a.n = n;
     a.params = params;
-    a.w16 = w16;
     a.X = X;
-    a.X16 = X16;
     a.Y = Y;
     unsigned* counter = nullptr;
     VBD_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&counter), g_mlp_tc_timeouts));
     a.status = counter;
+    a.off_w1 = kOffW1;
     a.off_b1 = kOffB1;
+    a.off_w2 = kOffW2;
     a.off_b2 = kOffB2;
+    a.off_w3 = kOffW3;
     a.off_b3 = kOffB3;
-    if (X16)
-        tc::mlp_infer_tc_kernel<true><<<tc_grid(n), tc::kThreads, tc::kSmemBytes, st>>>(a);
-    else
-        tc::mlp_infer_tc_kernel<false><<<tc_grid(n), tc::kThreads, tc::kSmemBytes, st>>>(a);
+    tc::mlp_infer_tc_kernel<tc::kInF32><<<tc_grid(n), tc::kThreads, tc::kSmemBytes, st>>>(a);
     VBD_CUDA_TRY(cudaGetLastError());
     return VBD_OK;
 }
 
-int mlp_forward_bf16(const float* params, const uint16_t* w16, const uint16_t* X16, int n, float* Y, cudaStream_t st) {
-    if ((reinterpret_cast<uintptr_t>(X16) & 15u) || (reinterpret_cast<uintptr_t>(w16) & 1u))
-        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp: BF16 rows must be 16-byte aligned");
-    return tc_forward(params, w16, nullptr, X16, n, Y, st);
+// The step mode's learned start in one launch: features of every internal vertex computed in the
+// tcgen05 kernel, inference, and the bounded start applied to disp / pos (no feature or prediction
+// rows in HBM).  Equal, bit for bit, to features -> inference -> scaled start of the staged API.
+int mlp_step_start(const VbdModelImpl& m, const float* params, const float4* prev, const float4* y, const int* ccount,
+                   const float* corr_prev, const float* mean, const float* inv_std, int mode, float dt, float4* disp,
+                   float4* pos, cudaStream_t st) {
+    if (mode != VBD_FEATURES_CORRECTIONS && mode != VBD_FEATURES_KINEMATIC)
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd warm start: unknown feature set");
+    if (mode == VBD_FEATURES_KINEMATIC && !(dt > 0.f))
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd warm start: the kinematic set needs the step's dt");
+    if (reinterpret_cast<uintptr_t>(m.nbr8) & 15u)
+        return fail(VBD_ERR_INVALID_ARGUMENT, "vbd warm start: misaligned neighbour table");
+    int rc = ensure_tile_smem();
+    if (rc) return rc;
+    if (m.V == 0) return VBD_OK;
+    tc::TcArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.n = m.V;
+    a.params = params;
+    a.step.pinfo = m.pinfo;
+    a.step.prev = prev;
+    a.step.y = y;
+    a.step.nbr8 = m.nbr8;
+    a.step.vfeat = m.vfeat;
+    a.step.ccount = ccount;
+    a.step.corr_prev = corr_prev;
+    a.step.mean = mean;
+    a.step.inv_std = inv_std;
+    a.step.mode = mode;
+    a.step.g_dt2 = make_float3(m.gravity[0] * dt * dt, m.gravity[1] * dt * dt, m.gravity[2] * dt * dt);
+    a.step.inv_dt = dt > 0.f ? 1.0f / dt : 0.f;
+    a.step.disp = disp;
+    a.step.pos = pos;
+    unsigned* counter = nullptr;
+    VBD_CUDA_TRY(cudaGetSymbolAddress(reinterpret_cast<void**>(&counter), g_mlp_tc_timeouts));
+    a.status = counter;
+    a.off_w1 = kOffW1;
+    a.off_b1 = kOffB1;
+    a.off_w2 = kOffW2;
+    a.off_b2 = kOffB2;
+    a.off_w3 = kOffW3;
+    a.off_b3 = kOffB3;
+    tc::mlp_infer_tc_kernel<tc::kInStep><<<tc_grid(m.V), tc::kThreads, tc::kSmemBytes, st>>>(a);
+    VBD_CUDA_TRY(cudaGetLastError());
+    return VBD_OK;
 }
 }  // namespace vbd
 
@@ -768,7 +755,7 @@ extern "C" int vbd_mlp_forward(const float* params, const uint16_t* w16, const f
     if (!params || !w16 || (n > 0 && (!X || !Y))) return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_forward: NULL argument");
     if ((reinterpret_cast<uintptr_t>(X) & 15u) || (reinterpret_cast<uintptr_t>(w16) & 1u))
         return fail(VBD_ERR_INVALID_ARGUMENT, "vbd_mlp_forward: X must be 16-byte aligned");
-    return tc_forward(params, w16, X, nullptr, n, Y, static_cast<cudaStream_t>(stream));
+    return tc_forward(params, X, n, Y, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int vbd_mlp_forward_mma_sync(const float* params, const uint16_t* w16, const float* X, int32_t n, float* Y,

@@ -110,8 +110,7 @@ struct SolverImpl {
     const float* ws_mean = nullptr;
     const float* ws_inv_std = nullptr;
     int ws_iterations = 0;
-    float* ws_corr = nullptr;        // [V][3] previous step's correction x_solved - y (model order)
-    float* ws_work = nullptr;        // [V][70] features, prediction, displacement
+    float* ws_corr = nullptr;        // [V][3] previous step's correction x_solved - y (internal order)
     int feature_set = VBD_FEATURES_CORRECTIONS;  // vbd_set_feature_set
     float last_dt = 0.f;             // dt of the last vbd_forward (the kinematic features need it)
     // particle self-contact (particle_enable_self_contact)
@@ -1709,8 +1708,6 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
     if (s.ws_params) {
         // learned warm start: features -> MLP -> iterate from y + prediction
         const int V = s.m->V;
-        float* feats = s.ws_work;
-        float* pred = feats + static_cast<size_t>(V) * 64;
         const bool gated = s.gate_tol > 0.f;
         if (gated) {
             VBD_CUDA_TRY(cudaMemsetAsync(s.gate, 0, offsetof(GateState, pad), st));
@@ -1720,17 +1717,13 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
                 gate_ref_kernel<<<1, 32, 0, st>>>(s.gate, s.gate_mean, s.gate_count);
             }
         }
-        // rows in the internal vertex order (coalesced, no model-order scatter), as BF16 (the
-        // inference rounds its inputs to BF16 anyway: half the bytes written and read)
-        uint16_t* feats16 = reinterpret_cast<uint16_t*>(feats);
-        int rc = mlp_features_launch(*s.m, s.prev, s.y, c ? s.ccount : nullptr, s.ws_corr, s.ws_mean, s.ws_inv_std,
-                                     nullptr, s.feature_set, dt, st, 1, feats16);
-        if (!rc) rc = mlp_forward_bf16(s.ws_params, s.ws_w16, feats16, V, pred, st);
-        if (!rc) rc = mlp_apply_launch(*s.m, pred, s.prev, s.disp, s.pos, st);
+        // features, inference and the bounded start in one tcgen05 launch over the internal rows
+        const int rc = mlp_step_start(*s.m, s.ws_params, s.prev, s.y, c ? s.ccount : nullptr, s.ws_corr, s.ws_mean,
+                                      s.ws_inv_std, s.feature_set, dt, s.disp, s.pos, st);
         if (rc) return rc;
         if (gated) {
-            rc = enqueue_gated_iterations(s, c, dt, st, false);
-            if (rc) return rc;
+            const int rg = enqueue_gated_iterations(s, c, dt, st, false);
+            if (rg) return rg;
         } else {
             for (int it = 0; it < s.ws_iterations; ++it)
                 for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st, it == 0);
@@ -1807,8 +1800,7 @@ static void free_solver(SolverImpl& s) {
     s.patch_off = s.patch_ids = nullptr;
     s.tri_loc = s.edge_loc = nullptr;
     if (s.ws_corr) cudaFree(s.ws_corr);
-    if (s.ws_work) cudaFree(s.ws_work);
-    s.ws_corr = s.ws_work = nullptr;
+    s.ws_corr = nullptr;
     for (auto& g : s.graphs) cudaGraphExecDestroy(g.exec);
     s.graphs.clear();
     void* ptrs[] = {s.pos, s.prev, s.y, s.disp, s.ccount, s.cslot, s.ctab, s.status, s.resid_max};
@@ -2190,7 +2182,6 @@ extern "C" int vbd_set_warm_start(VbdSolver* solver, const float* params, const 
     const size_t V = static_cast<size_t>(s.m->V);
     if (!s.ws_corr) {
         VBD_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&s.ws_corr), std::max<size_t>(V, 1) * 3 * sizeof(float)));
-        VBD_CUDA_TRY(cudaMalloc(reinterpret_cast<void**>(&s.ws_work), std::max<size_t>(V, 1) * 70 * sizeof(float)));
     }
     VBD_CUDA_TRY(cudaMemset(s.ws_corr, 0, std::max<size_t>(V, 1) * 3 * sizeof(float)));
     // make the MLP kernel's shared-memory opt-in outside any later stream capture
