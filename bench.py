@@ -829,6 +829,52 @@ def sweep_profile(workload: str, n: int, worlds: int, steps: int) -> dict:
             "algorithmic_bytes_per_iteration": algorithmic_bytes_per_iteration(model)}
 
 
+def learned_start_profile(workload: str, n: int, worlds: int, steps: int) -> dict:
+    """The profile harness of the learned start (the warm-start step mode's fused tcgen05 kernel):
+    the workload's scene, an untrained corrections network, a learned solver and a plain one, both
+    with 0 sweeps; three steps each, then ``steps`` steps of the learned solver inside an NVTX range
+    named ``learned_start`` (for ncu --nvtx-include).  Returns the mean device time of a step of
+    each and their difference, the learned start's cost."""
+    import torch
+
+    from newton_b200 import CollisionPipeline, scenes
+    from newton_b200 import learned as L
+    from newton_b200.solvers import SolverVBD
+
+    dev = torch.device("cuda:0")
+    if workload == "batched-worlds" and worlds:
+        model, q0 = scenes.batched_worlds(worlds, seed=0, device=dev)
+    else:
+        model, q0, _, _ = build_scene(workload, dev, n=n)
+    pipe = CollisionPipeline(model, soft_contact_margin=MARGIN)
+    c = pipe.contacts()
+    mlp = L.WarmStartMLP(dev, seed=0, feature_set="corrections")
+    out = {"workload": workload, "vertices": model.particle_count, "steps": steps}
+    for name, warm in (("plain", False), ("learned", True)):
+        solver = SolverVBD(model, iterations=0)
+        if warm:
+            solver.set_warm_start(mlp, 0)
+        a, b = model.state(), model.state()
+        a.particle_q.copy_(torch.from_numpy(q0).to(dev))
+        pipe.collide(a, c)
+        for _ in range(3):
+            solver.step(a, b, None, c, DT)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if warm:
+            torch.cuda.nvtx.range_push("learned_start")
+        e0.record()
+        for _ in range(steps):
+            solver.step(a, b, None, c, DT)
+        e1.record()
+        if warm:
+            torch.cuda.nvtx.range_pop()
+        e1.synchronize()
+        out[f"{name}_step_us"] = e0.elapsed_time(e1) / steps * 1e3
+    out["learned_start_us"] = out["learned_step_us"] - out["plain_step_us"]
+    return out
+
+
 def mlp_kernels(rows: int, repeats: int) -> dict:
     """Device time of the warm-start MLP kernels on random rows (the profile harness): tcgen05
     inference, the mma.sync inference it replaced, and one training pass (forward + backward +
@@ -897,12 +943,19 @@ def main() -> None:
     ap.add_argument("--workload", default="draped-cloth", choices=sorted(WORKLOADS))
     ap.add_argument("--sweep-profile", action="store_true",
                     help="only run the sweep profile harness (--workload, --n, --worlds, --steps) and print its JSON")
-    ap.add_argument("--worlds", type=int, default=0, help="batched worlds of --sweep-profile (default 512)")
+    ap.add_argument("--learned-start-profile", action="store_true",
+                    help="only run the learned-start profile harness (--workload, --n, --worlds, --steps) and print "
+                         "its JSON")
+    ap.add_argument("--worlds", type=int, default=0,
+                    help="batched worlds of --sweep-profile / --learned-start-profile (default 512)")
     ap.add_argument("--mlp-kernels", type=int, default=0, metavar="ROWS",
                     help="only time the warm-start MLP kernels on ROWS random rows and print their JSON")
     args = ap.parse_args()
     if args.sweep_profile:
         print(json.dumps(sweep_profile(args.workload, args.n, args.worlds, max(args.steps, 1))), flush=True)
+        return
+    if args.learned_start_profile:
+        print(json.dumps(learned_start_profile(args.workload, args.n, args.worlds, max(args.steps, 1))), flush=True)
         return
     if args.mlp_kernels:
         print(json.dumps(mlp_kernels(args.mlp_kernels, max(args.steps, 5))), flush=True)
