@@ -128,6 +128,8 @@ __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // barrier of one group's 128 threads (named barrier 1 + group; 0 is the CTA-wide __syncthreads)
 __device__ __forceinline__ void group_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
 
@@ -485,6 +487,20 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_infer_tc_kernel(TcArgs a) {
         fence_proxy_async();
         fence_before();
         group_sync(bar_id);
+        if (kInput == kInStep) {
+            // the group's next tile: its rows' own data toward L2 while this tile runs (a prefetch
+            // holds no register; measured 4-5% off the launch at 1.89 M rows)
+            const int nxt = (tile + gridDim.x * kGroups) * kRows + r_own;
+            if (nxt < a.n) {
+                prefetch_l2(a.step.prev + nxt);
+                prefetch_l2(a.step.y + nxt);
+                prefetch_l2(a.step.pinfo + nxt);
+                prefetch_l2(a.step.vfeat + nxt);
+                prefetch_l2(a.step.nbr8 + 8 * nxt);
+                prefetch_l2(a.step.disp + nxt);
+                if (a.step.corr_prev) prefetch_l2(a.step.corr_prev + 3 * nxt);
+            }
+        }
         // ---- 2. layer 1 ----
         if (issuer) {
             fence_after();
