@@ -1211,6 +1211,10 @@ __global__ void gather_positions_kernel(const int* perm, const float4* pos, floa
 // every solved vertex; or the Gauss-Seidel residual the last round's sweeps accumulated) decide
 // whether the loop runs another round.  One warp.
 __global__ void gate_check_kernel(GateState* g, cudaGraphConditionalHandle handle, GateParams p) {
+    // launched as a programmatic dependent of the round's last sweep: wait for that grid (its
+    // accumulators), then let the next sweep start its prologue (it waits for this grid in turn)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;");
     if (p.first != 1 && g->stop) return;  // a later round of a loop body that has already decided
     const float r = gate_take_warp(g, p.mean, p.count);
     if (threadIdx.x == 0) gate_decide(g, handle, r, p);
@@ -1218,6 +1222,8 @@ __global__ void gate_check_kernel(GateState* g, cudaGraphConditionalHandle handl
 
 // relative mode with a warm start: the residual at the plain start y becomes the reference
 __global__ void gate_ref_kernel(GateState* g, int mean, int count) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;");
     const float r = gate_take_warp(g, mean, count);
     if (threadIdx.x == 0) g->ref = r;
 }
@@ -1319,6 +1325,23 @@ static void launch_dependent(Kernel kernel, int grid, int block, cudaStream_t st
     cfg.attrs = &attr;
     cfg.numAttrs = a.no_pdl ? 0 : 1;
     cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
+// a one-warp gate kernel as a programmatic dependent of the kernel before it (pdl), so that its
+// launch overlaps that kernel's tail instead of following its completion
+template <typename... Args>
+static void launch_gate(void (*kernel)(Args...), cudaStream_t st, bool pdl, Args... args) {
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(32);
+    cfg.stream = st;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 // the staged instantiations: the same choice between the uncapped (or 72-register gate) kernel
@@ -1684,13 +1707,13 @@ static int enqueue_gated_iterations(SolverImpl& s, const VbdContacts* c, float d
             for (int color = 0; color < s.m->C; ++color)
                 enqueue_color(s, color, c, dt, s.body_stream, false, sweep && last, u > 0);
             if (sweep && last)
-                gate_check_kernel<<<1, 32, 0, s.body_stream>>>(
-                    s.gate, handle, gate_params(s, -1, set_ref ? 1 : 0, s.gate_every));
+                launch_gate(gate_check_kernel, s.body_stream, s.pdl, s.gate, handle,
+                            gate_params(s, -1, set_ref ? 1 : 0, s.gate_every));
         }
     }
     if (!sweep) {
         enqueue_gate_residual(s, c, dt, s.body_stream);
-        gate_check_kernel<<<1, 32, 0, s.body_stream>>>(s.gate, handle, gate_params(s, 0, 0, s.gate_every));
+        launch_gate(gate_check_kernel, s.body_stream, s.pdl, s.gate, handle, gate_params(s, 0, 0, s.gate_every));
     }
     const cudaError_t e1 = cudaGetLastError();
     cudaGraph_t captured = nullptr;
@@ -1714,7 +1737,7 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
             if (s.gate_relative) {
                 // the relative tolerance refers to the plain start y, before the warm start moves it
                 enqueue_gate_residual(s, c, dt, st);
-                gate_ref_kernel<<<1, 32, 0, st>>>(s.gate, s.gate_mean, s.gate_count);
+                launch_gate(gate_ref_kernel, st, s.pdl, s.gate, s.gate_mean, s.gate_count);
             }
         }
         // features, inference and the bounded start in one tcgen05 launch over the internal rows
@@ -1777,7 +1800,7 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
         const bool sweep = s.gate_sweep && s.lanes > 0;
         if (s.gate_relative && sweep) {
             enqueue_gate_residual(s, c, dt, st);
-            gate_ref_kernel<<<1, 32, 0, st>>>(s.gate, s.gate_mean, s.gate_count);
+            launch_gate(gate_ref_kernel, st, s.pdl, s.gate, s.gate_mean, s.gate_count);
         }
         const int rc = enqueue_gated_iterations(s, c, dt, st, !sweep);
         if (rc) return rc;

@@ -149,12 +149,12 @@ def test_zero_network_warm_start_is_plain_vbd():
 
 @pytest.mark.parametrize("feature_set", ["corrections", "kinematic"])
 def test_step_mode_equals_the_staged_learned_path(feature_set):
-    """The warm-start step mode (features in the internal vertex order as BF16 rows, straight into
-    the tcgen05 inference) gives the same bits as the staged path (vbd_mlp_warm_start: FP32
-    features in model order, the same inference) followed by the same sweeps, with a random
-    network: over 12 steps for the kinematic set; for the corrections set over the first step,
-    whose previous correction is zero on both sides (later ones come from each path's own inertia
-    target, rounded differently on the host)."""
+    """The warm-start step mode (one tcgen05 launch: features computed in the kernel, inference,
+    the bounded start applied in its last epilogue) gives the same bits as the staged path
+    (vbd_mlp_warm_start: FP32 features in model order, the inference, the scaled start) followed
+    by the same sweeps, with a random network, over 12 steps.  Both take the previous correction
+    from the staged path (the step mode through set_warm_start_correction), so the corrections
+    set's one-ring gathers of nonzero corrections are compared too."""
     dt = 1.0 / 600.0
     model, q0 = scenes.single_cloth(n=24, side=1.0, seed=7, pin_top_corners=False, ground=0.0,
                                     sphere=((0.0, 0.0, 0.5), 0.4), height=0.95)
@@ -176,8 +176,9 @@ def test_step_mode_equals_the_staged_learned_path(feature_set):
     a2.particle_q.copy_(torch.from_numpy(q0).cuda())
     corr = torch.zeros(model.particle_count, 3, device="cuda:0")
     work = torch.empty(model.particle_count * 70, device="cuda:0")
-    for _ in range(12 if feature_set == "kinematic" else 1):
+    for _ in range(12):
         pipe.collide(a, c)
+        s_mode.set_warm_start_correction(corr)
         s_mode.step(a, b, None, c, dt)
         a, b = b, a
         pipe.collide(a2, c)
