@@ -1,8 +1,6 @@
 // vbd_mlp_tc.cuh -- inference of the warm-start MLP (64 -> 128 -> 128 -> 3, SiLU) on the 5th-
-// generation tensor cores: tcgen05.mma with FP16 operands in shared memory and accumulators in
-// tensor memory (TMEM): FP16 for the two hidden layers (the epilogue reads them as packed pairs,
-// tcgen05.ld .pack::16b, and runs bias + SiLU in f16x2 arithmetic with no conversion), FP32 for
-// the output layer.  Included by vbd_mlp.cu only.
+// generation tensor cores: tcgen05.mma with FP16 operands in shared memory and FP32 accumulators
+// in tensor memory (TMEM); bias + SiLU in f16x2 arithmetic.  Included by vbd_mlp.cu only.
 //
 // Work split.  One persistent CTA of 512 threads per SM runs four independent tile pipelines
 // ("groups" of 4 warps) over one shared copy of the weights.  A group owns one 128-row tile of
@@ -15,8 +13,8 @@
 //      commits to the group's mbarrier; each thread waits, reads its row of D (tcgen05.ld), adds
 //      the bias, applies SiLU and writes the FP16 row into the buffer (X is no longer needed);
 //   3. layer 2 likewise: D = H1 W2 (8 MMAs, D's columns reused), epilogue back into the buffer;
-//   4. layer 3: D[128 x 16] = H2 W3 (8 MMAs, N padded from 3 to 16, FP32 accumulators); the
-//      epilogue adds the bias and stores the 3 outputs (the step mode: applies the start).
+//   4. layer 3: D[128 x 16] = H2 W3 (8 MMAs, N padded from 3 to 16); the epilogue adds the bias
+//      and stores the 3 outputs (the step mode: applies the start).
 // Each step of a tile waits on the previous one (MMA -> epilogue -> MMA); four tiles in flight per
 // SM keep the tensor core busy across those waits.
 //
@@ -27,9 +25,10 @@
 // MMA's K = 16 slice) is (R / 8) * 128 and the stride-dimension byte offset (between 8-row
 // groups) is 128; the slice for MMA step s starts at byte s * 2 * (R / 8) * 128.  B operands are
 // the FP32 weights rounded to FP16 and transposed to [N][K] (K-major), written once per CTA.
-// FP16 (11-bit significand) rather than BF16 (8-bit): the values of this network (standardized
-// features, activations and sums of a few units, weights below 1) are far inside its range, and
-// the epilogue's arithmetic needs no FP32 <-> 16-bit conversion.
+// FP16 (11-bit significand) rather than BF16 (8-bit) operands: the values of this network
+// (standardized features, activations of a few units, weights below 1) are far inside FP16's
+// range, and the rounding of the inputs decides how well the start carries the previous
+// correction (measured: fewer Gauss-Seidel iterations after an FP16 start than after a BF16 one).
 //
 // Every wait on an mbarrier is bounded: after kTcSpinLimit polls the group records a timeout (its
 // four warps decide together), stops taking tiles, waits (bounded again) for the MMAs it has
@@ -147,11 +146,11 @@ __device__ __forceinline__ bool group_all(int id, bool v) {
     return r != 0;
 }
 
-// 128 consecutive FP16 accumulator columns of this thread's TMEM lane as 64 packed pairs (one
-// load, one wait): register j holds columns 2 j (low half) and 2 j + 1 (high half)
-__device__ __forceinline__ void tmem_ld128_f16(uint32_t taddr, uint32_t (&r)[64]) {
+// 64 consecutive FP32 columns of this thread's TMEM lane (one load, one wait)
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float (&v)[64]) {
+    uint32_t r[64];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x64.pack::16b.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
         "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,"
         "%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
         "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];\n\t"
@@ -166,6 +165,8 @@ __device__ __forceinline__ void tmem_ld128_f16(uint32_t taddr, uint32_t (&r)[64]
           "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
         : "r"(taddr)
         : "memory");
+#pragma unroll
+    for (int j = 0; j < 64; ++j) v[j] = __uint_as_float(r[j]);
 }
 
 // two FP32 values rounded to nearest FP16, packed (lo in the low half)
@@ -174,10 +175,13 @@ __device__ __forceinline__ uint32_t pack_f16(float lo, float hi) {
     return *reinterpret_cast<uint32_t*>(&v);
 }
 
-// SiLU(z + b) of a packed pair of FP16 accumulators, in f16x2 arithmetic: bias add, z / 2, tanh
-// (hardware approximation), 1/2 + t / 2 and the product run two lanes per instruction
-__device__ __forceinline__ uint32_t silu2_bias_f16(uint32_t z2, uint32_t bias2) {
+// SiLU(z + b) of two FP32 accumulator columns: z rounded to FP16 once, then bias add, z / 2, tanh
+// (hardware approximation), 1/2 + t / 2 and the product in f16x2 arithmetic, two lanes per
+// instruction (each step rounds to FP16, relative 2^-11, the size of the rounding the activation
+// gets anyway as the next layer's operand)
+__device__ __forceinline__ uint32_t silu2_bias_f16(float z0, float z1, uint32_t bias2) {
     const __half2 half2 = __floats2half2_rn(0.5f, 0.5f);
+    uint32_t z2 = pack_f16(z0, z1);
     const __half2 z = __hadd2(*reinterpret_cast<__half2*>(&z2), *reinterpret_cast<__half2*>(&bias2));
     __half2 h = __hmul2(z, half2);
     uint32_t hu = *reinterpret_cast<uint32_t*>(&h), tu;
@@ -187,20 +191,21 @@ __device__ __forceinline__ uint32_t silu2_bias_f16(uint32_t z2, uint32_t bias2) 
     return *reinterpret_cast<uint32_t*>(&out);
 }
 
-// bias + SiLU of the row's 128 packed accumulator pairs, stored as FP16 into an R = 128 row K-major
-// operand (16 stores of 16 bytes); the bias is read 8 values at a time (a broadcast: every thread
-// of the warp reads the same address)
-__device__ __forceinline__ void store_hidden128(unsigned char* A, int r, const uint32_t (&acc)[64],
-                                                const uint32_t* bias2) {
+// bias + SiLU of 64 accumulator columns [c0, c0 + 64) of row r, stored as FP16 into an R = 128 row
+// K-major operand (8 stores of 16 bytes); the bias is read 8 values at a time (a broadcast: every
+// thread of the warp reads the same address)
+__device__ __forceinline__ void store_hidden64(unsigned char* A, int r, int c0, const float (&acc)[64],
+                                               const uint32_t* bias2) {
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
-        const uint4 b = *reinterpret_cast<const uint4*>(bias2 + 4 * q);  // 8 biases, FP16 pairs
+    for (int q = 0; q < 8; ++q) {
+        const uint4 b = *reinterpret_cast<const uint4*>(bias2 + (c0 + q * 8) / 2);  // 8 biases, FP16 pairs
+        const float* x = acc + q * 8;
         uint4 w;
-        w.x = silu2_bias_f16(acc[4 * q], b.x);
-        w.y = silu2_bias_f16(acc[4 * q + 1], b.y);
-        w.z = silu2_bias_f16(acc[4 * q + 2], b.z);
-        w.w = silu2_bias_f16(acc[4 * q + 3], b.w);
-        *reinterpret_cast<uint4*>(A + kmajor_offset(r, 8 * q, kRows)) = w;
+        w.x = silu2_bias_f16(x[0], x[1], b.x);
+        w.y = silu2_bias_f16(x[2], x[3], b.y);
+        w.z = silu2_bias_f16(x[4], x[5], b.z);
+        w.w = silu2_bias_f16(x[6], x[7], b.w);
+        *reinterpret_cast<uint4*>(A + kmajor_offset(r, c0 + q * 8, kRows)) = w;
     }
 }
 
@@ -443,7 +448,7 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_infer_tc_kernel(TcArgs a) {
     fence_after();
     const uint32_t d = *tmem_slot + static_cast<uint32_t>(group * 128);   // this group's columns
     const uint32_t lane_base = static_cast<uint32_t>(quarter * 32) << 16;  // this warp's TMEM lanes
-    const uint32_t idesc128 = instr_desc(128, 128, false), idesc16 = instr_desc(128, kN3, true);
+    const uint32_t idesc128 = instr_desc(128, 128, true), idesc16 = instr_desc(128, kN3, true);
     const uint32_t ab = smem_u32(buf), w1 = smem_u32(sW1), w2 = smem_u32(sW2), w3 = smem_u32(sW3);
     const bool issuer = gtid == 0;
     const int r_own = quarter * 32 + lane;  // this thread's row of the tile
@@ -514,10 +519,11 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_infer_tc_kernel(TcArgs a) {
         if (!ok) break;
         phase ^= 1u;
         fence_after();
-        {
-            uint32_t acc[64];
-            tmem_ld128_f16(d + lane_base, acc);
-            store_hidden128(buf, r_own, acc, sB1);  // layer 1's MMAs have completed: X is free
+#pragma unroll 1
+        for (int c0 = 0; c0 < 128; c0 += 64) {
+            float acc[64];
+            tmem_ld64(d + lane_base + c0, acc);
+            store_hidden64(buf, r_own, c0, acc, sB1);  // layer 1's MMAs have completed: X is free
         }
         fence_proxy_async();
         fence_before();
@@ -535,10 +541,11 @@ __global__ void __launch_bounds__(kThreads, 1) mlp_infer_tc_kernel(TcArgs a) {
         if (!ok) break;
         phase ^= 1u;
         fence_after();
-        {
-            uint32_t acc[64];
-            tmem_ld128_f16(d + lane_base, acc);
-            store_hidden128(buf, r_own, acc, sB2);  // layer 2's MMAs have completed: H1 is free
+#pragma unroll 1
+        for (int c0 = 0; c0 < 128; c0 += 64) {
+            float acc[64];
+            tmem_ld64(d + lane_base + c0, acc);
+            store_hidden64(buf, r_own, c0, acc, sB2);  // layer 2's MMAs have completed: H1 is free
         }
         fence_proxy_async();
         fence_before();

@@ -80,8 +80,8 @@ def test_tcgen05_inference_matches_the_mma_sync_path_and_fp64(n):
     torch.cuda.synchronize()
     a, b = y_tc.cpu().numpy(), y_ms.cpu().numpy()
     assert np.isfinite(a).all()
-    # FP16 operands and hidden accumulators against BF16 operands with FP32 accumulators; SiLU
-    # differs (hardware tanh vs exact): ~1e-3 relative
+    # FP16 operands against BF16 operands, both with FP32 accumulators; SiLU differs (hardware
+    # tanh vs exact): ~1e-3 relative
     assert _rel(a, b) < 2e-2, _rel(a, b)
     if n <= 4097:
         y_ref, _ = _reference(mlp, X.cpu().numpy(), np.zeros((n, 3)))
