@@ -1,7 +1,8 @@
 """Learned warm start for the VBD step.
 
-A per-vertex MLP (64 -> 128 -> 128 -> 3, SiLU; trained with FP32 master weights and BF16
-mma.sync tiles, run for inference on tcgen05 with FP16 operands) predicts the correction ``x_solved - y`` that the coming step applies to the inertia
+A per-vertex MLP (64 -> 128 -> 128 -> 3, SiLU; trained with FP32 master weights on BF16 mma.sync
+tiles with FP32 accumulation, run for inference on tcgen05 with FP16 operands and FP32
+accumulation) predicts the correction ``x_solved - y`` that the coming step applies to the inertia
 target ``y``, in units of the vertex's characteristic element length, from one-ring features
 (``vbd_mlp_features``).  Two feature sets: ``"corrections"`` (default) -- the inertia offset, the
 previous step's correction of the vertex and of 8 one-ring neighbours, the 8 one-ring edge
