@@ -740,17 +740,13 @@ __device__ __forceinline__ void reduce_residual(const SweepArgs& a, float r, boo
     }
 }
 
-// Block-collective (every thread of the block calls it; blockDim a multiple of 32, at most 256):
-// the same reduction for a sweep whose vertices are held by lanes 0, L, 2L, ... of each warp (the
-// others pass r = 0): the warp's values are combined over those lanes only, the warps' results in
-// shared memory, and one thread adds the block's sum (and max, in max mode) to slot (block mod
-// kGateSlots) -- one atomic per block.
+// Warp-collective (every thread of the warp calls it): the same reduction for a sweep whose
+// vertices are held by lanes 0, L, 2L, ... of each warp (the others pass r = 0): the warp's values
+// are combined over those lanes only and lane 0 adds the warp's sum (and max, in max mode) to slot
+// (global warp index mod kGateSlots).  Integer sums: the result does not depend on the order.
 template <int L>
-__device__ __forceinline__ void reduce_residual_block(const SweepArgs& a, float r, bool counted) {
-    __shared__ unsigned long long s_sum[8];
-    __shared__ unsigned s_max[8];
+__device__ __forceinline__ void reduce_residual_lanes(const SweepArgs& a, float r, bool counted) {
     const unsigned full = 0xffffffffu;
-    const int w = threadIdx.x >> 5;
     const bool want_max = a.gate_max != nullptr;
     unsigned mx = __float_as_uint(r);
     unsigned long long sum = counted ? resid_fixed(r) : 0ull;
@@ -759,21 +755,13 @@ __device__ __forceinline__ void reduce_residual_block(const SweepArgs& a, float 
         sum += __shfl_xor_sync(full, sum, off);
         if (want_max) mx = max(mx, __shfl_xor_sync(full, mx, off));
     }
+    // one atomic per warp, spread over the slots by global warp index: no block barrier at the
+    // end of the sweep (a block-level reduction before one atomic per block cost 0.7 us per
+    // iteration at 65,536 vertices and 8 us at 1.89 M)
     if ((threadIdx.x & 31) == 0) {
-        s_sum[w] = sum;
-        s_max[w] = mx;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long bs = 0ull;
-        unsigned bm = 0u;
-        for (int k = 0; k < static_cast<int>(blockDim.x >> 5); ++k) {
-            bs += s_sum[k];
-            bm = max(bm, s_max[k]);
-        }
-        const int slot = static_cast<int>(blockIdx.x & (kGateSlots - 1));
-        if (want_max) atomicMax(a.gate_max + slot * kMaxStride, bm);
-        if (a.gate_sum && bs) atomicAdd(a.gate_sum + slot * kSumStride, bs);
+        const int slot = static_cast<int>(((blockIdx.x * blockDim.x + threadIdx.x) >> 5) & (kGateSlots - 1));
+        if (want_max) atomicMax(a.gate_max + slot * kMaxStride, mx);
+        if (a.gate_sum && sum) atomicAdd(a.gate_sum + slot * kSumStride, sum);
     }
 }
 
@@ -862,12 +850,16 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a) {
         f.x = warp_sum(f.x, L);
         f.y = warp_sum(f.y, L);
         f.z = warp_sum(f.z, L);
-        h.xx = warp_sum(h.xx, L);
-        h.xy = warp_sum(h.xy, L);
-        h.xz = warp_sum(h.xz, L);
-        h.yy = warp_sum(h.yy, L);
-        h.yz = warp_sum(h.yz, L);
-        h.zz = warp_sum(h.zz, L);
+        if (!kResidual) {
+            // the Jacobi residual reads the force only: without these reductions the compiler
+            // drops the Hessian arithmetic of every element evaluation from that instantiation
+            h.xx = warp_sum(h.xx, L);
+            h.xy = warp_sum(h.xy, L);
+            h.xz = warp_sum(h.xz, L);
+            h.yy = warp_sum(h.yy, L);
+            h.yz = warp_sum(h.yz, L);
+            h.zz = warp_sum(h.zz, L);
+        }
     }
     if (kResidual) {
         // Jacobi residual: lane 0 of each vertex forms r_i, then the warp reduces max, sum and
@@ -905,7 +897,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a) {
                 solve_and_commit(a, i, pv, h, f);
             }
         }
-        reduce_residual_block<L>(a, rg, counted);
+        reduce_residual_lanes<L>(a, rg, counted);
         return;
     }
     if (!valid || lane != 0) return;
