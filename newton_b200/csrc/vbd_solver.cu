@@ -1122,6 +1122,10 @@ struct FinalizeArgs {
     float* q_out;
     float* qd_out;
     int* ccount;
+    // learned warm start: the step's correction x_solved - y, internal order (NULL: not kept)
+    const float4* pinfo;
+    const float4* y;
+    float* corr;
     int V;
     float dt;
 };
@@ -1147,6 +1151,14 @@ __global__ void finalize_kernel(FinalizeArgs a) {
         a.qd_out[3 * o + 2] = (p.z - pv.z) / a.dt;
     }
     if (a.ccount) a.ccount[i] = 0;
+    if (a.corr) {
+        const float4 pi = a.pinfo[i];
+        const bool solvable = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
+        const float4 yy = a.y[i];
+        a.corr[3 * i] = solvable ? p.x - yy.x : 0.f;
+        a.corr[3 * i + 1] = solvable ? p.y - yy.y : 0.f;
+        a.corr[3 * i + 2] = solvable ? p.z - yy.z : 0.f;
+    }
 }
 
 // Warm start: the initial Gauss-Seidel iterate becomes inertia target + delta for every vertex the
@@ -1173,20 +1185,6 @@ __global__ void gather_rows3_kernel(const int* perm, const float* in, float* out
     out[3 * i] = in[3 * o];
     out[3 * i + 1] = in[3 * o + 1];
     out[3 * i + 2] = in[3 * o + 2];
-}
-
-// correction of the finished step, x_solved - y, the next step's warm-start feature
-__global__ void correction_kernel(const int* perm, const float4* pinfo, const float4* pos, const float4* y,
-                                  float* corr, int V) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= V) return;
-    const int o = perm ? perm[i] : i;  // NULL: internal order (the step mode's own buffer)
-    const float4 pi = pinfo[i];
-    const bool solvable = (__float_as_int(pi.w) & VBD_PARTICLE_ACTIVE) && pi.x != 0.0f;
-    const float4 p = pos[i], yy = y[i];
-    corr[3 * o] = solvable ? p.x - yy.x : 0.f;
-    corr[3 * o + 1] = solvable ? p.y - yy.y : 0.f;
-    corr[3 * o + 2] = solvable ? p.z - yy.z : 0.f;
 }
 
 __global__ void gather_positions_kernel(const int* perm, const float4* pos, float* q, int V) {
@@ -1569,10 +1567,14 @@ static void enqueue_color(SolverImpl& s, int color, const VbdContacts* c, float 
     }
 }
 
-static void enqueue_finalize(SolverImpl& s, float* q_in, float* q_out, float* qd_out, float dt, cudaStream_t st) {
+static void enqueue_finalize(SolverImpl& s, float* q_in, float* q_out, float* qd_out, float dt, cudaStream_t st,
+                             float* corr = nullptr) {
     const VbdModelImpl& m = *s.m;
     FinalizeArgs a;
     a.perm = m.perm;
+    a.pinfo = m.pinfo;
+    a.y = s.y;
+    a.corr = corr;
     a.pos = s.pos;
     a.prev = s.prev;
     a.q_in = q_in;
@@ -1722,7 +1724,6 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
     enqueue_forward(s, q_in, qd_in, f_ext, c, dt, st);
     if (s.ws_params) {
         // learned warm start: features -> MLP -> iterate from y + prediction
-        const int V = s.m->V;
         const bool gated = s.gate_tol > 0.f;
         if (gated) {
             VBD_CUDA_TRY(cudaMemsetAsync(s.gate, 0, offsetof(GateState, pad), st));
@@ -1743,8 +1744,7 @@ static int enqueue_step(SolverImpl& s, float* q_in, const float* qd_in, const fl
             for (int it = 0; it < s.ws_iterations; ++it)
                 for (int color = 0; color < s.m->C; ++color) enqueue_color(s, color, c, dt, st, it == 0);
         }
-        correction_kernel<<<(V + 255) / 256, 256, 0, st>>>(nullptr, s.m->pinfo, s.pos, s.y, s.ws_corr, V);
-        enqueue_finalize(s, q_in, q_out, qd_out, dt, st);
+        enqueue_finalize(s, q_in, q_out, qd_out, dt, st, s.ws_corr);  // and the correction kept
         return VBD_OK;
     }
     if (s.resident_on && s.resident.ready && iterations > 0 && !(s.gate_tol > 0.f)) {
