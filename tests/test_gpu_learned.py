@@ -350,7 +350,7 @@ def _ratios(r):
 def test_learned_warm_start_at_equal_residual_on_a_held_out_drape(drape_ab):
     """From the same states (so to the same absolute residual), with the trajectory's own previous
     correction as the history feature, the corrections network needs at most 0.65x the iterations
-    of plain VBD (measured on a B200: 0.55); the kinematic network, which sees no solver history,
+    of plain VBD (measured on a B200: 0.51); the kinematic network, which sees no solver history,
     at most 0.9x (measured 0.82)."""
     ratio = _ratios(drape_ab)
     assert ratio["corrections"] <= 0.65
