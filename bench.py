@@ -717,8 +717,10 @@ def learned_ab(dev, workload: str, plain: dict, start_state, K: int) -> dict:
     plain_tf = L.teacher_forced_steps(model, states, pipe, gate, DT, None, launch, warm=W, timer=tp)
     plain_ms = tp.ms()
     arms = {}
+    nets = {}
     for fs in FEATURE_SETS:
         mlp = L.WarmStartMLP(dev, seed=0, feature_set=fs)
+        nets[fs] = mlp
         mlp.set_standardization(X[fs])
         t1 = time.time()
         hist = mlp.train(mlp.standardize(X[fs]), T, epochs=TRAIN_EPOCHS, batch=16384, lr=2e-3)
@@ -767,6 +769,8 @@ def learned_ab(dev, workload: str, plain: dict, start_state, K: int) -> dict:
         del solver
     head = arms[FEATURE_SETS[0]]
     flops = 2 * (64 * 128 + 128 * 128 + 128 * 3) * model.particle_count
+    plain0_us, learned0_us = _start_cost(model, q_start, pipe, nets[FEATURE_SETS[0]], 20)
+    start_us = learned0_us - plain0_us
     return {
         "tolerance": gate,
         "protocol": "teacher forced: both arms step from the same recorded plain-VBD states (same y, same "
@@ -784,6 +788,9 @@ def learned_ab(dev, workload: str, plain: dict, start_state, K: int) -> dict:
         "feature_sets": arms,
         "training_data": info,
         "mlp_flop_per_step": flops,
+        "learned_start": {"us_per_step": start_us, "mlp_tflops": flops / (start_us * 1e-6) / 1e12,
+                          "note": "features + tcgen05 inference + bounded start, one kernel: a learned step "
+                                  "with 0 sweeps minus a plain one (CUDA events, 20 steps)"},
         "unit": "batch steps/s" if batched else "steps/s",
         "note": "the networks never saw the timed scene",
     }
@@ -829,6 +836,40 @@ def sweep_profile(workload: str, n: int, worlds: int, steps: int) -> dict:
             "algorithmic_bytes_per_iteration": algorithmic_bytes_per_iteration(model)}
 
 
+def _start_cost(model, q0, pipe, mlp, steps: int, nvtx: str | None = None) -> tuple:
+    """Device time per step (us) of a plain and of a learned solver with 0 sweeps from q0 (their
+    difference is the learned start: features + tcgen05 inference + start, one kernel); the
+    learned steps run inside the NVTX range ``nvtx`` when given."""
+    import torch
+
+    from newton_b200.solvers import SolverVBD
+
+    c = pipe.contacts()
+    out = []
+    for warm in (False, True):
+        solver = SolverVBD(model, iterations=0)
+        if warm:
+            solver.set_warm_start(mlp, 0)
+        a, b = model.state(), model.state()
+        a.particle_q.copy_(q0)
+        pipe.collide(a, c)
+        for _ in range(3):
+            solver.step(a, b, None, c, DT)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if warm and nvtx:
+            torch.cuda.nvtx.range_push(nvtx)
+        e0.record()
+        for _ in range(steps):
+            solver.step(a, b, None, c, DT)
+        e1.record()
+        if warm and nvtx:
+            torch.cuda.nvtx.range_pop()
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1) / steps * 1e3)
+    return out[0], out[1]
+
+
 def learned_start_profile(workload: str, n: int, worlds: int, steps: int) -> dict:
     """The profile harness of the learned start (the warm-start step mode's fused tcgen05 kernel):
     the workload's scene, an untrained corrections network, a learned solver and a plain one, both
@@ -839,7 +880,6 @@ def learned_start_profile(workload: str, n: int, worlds: int, steps: int) -> dic
 
     from newton_b200 import CollisionPipeline, scenes
     from newton_b200 import learned as L
-    from newton_b200.solvers import SolverVBD
 
     dev = torch.device("cuda:0")
     if workload == "batched-worlds" and worlds:
@@ -847,32 +887,10 @@ def learned_start_profile(workload: str, n: int, worlds: int, steps: int) -> dic
     else:
         model, q0, _, _ = build_scene(workload, dev, n=n)
     pipe = CollisionPipeline(model, soft_contact_margin=MARGIN)
-    c = pipe.contacts()
     mlp = L.WarmStartMLP(dev, seed=0, feature_set="corrections")
-    out = {"workload": workload, "vertices": model.particle_count, "steps": steps}
-    for name, warm in (("plain", False), ("learned", True)):
-        solver = SolverVBD(model, iterations=0)
-        if warm:
-            solver.set_warm_start(mlp, 0)
-        a, b = model.state(), model.state()
-        a.particle_q.copy_(torch.from_numpy(q0).to(dev))
-        pipe.collide(a, c)
-        for _ in range(3):
-            solver.step(a, b, None, c, DT)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        if warm:
-            torch.cuda.nvtx.range_push("learned_start")
-        e0.record()
-        for _ in range(steps):
-            solver.step(a, b, None, c, DT)
-        e1.record()
-        if warm:
-            torch.cuda.nvtx.range_pop()
-        e1.synchronize()
-        out[f"{name}_step_us"] = e0.elapsed_time(e1) / steps * 1e3
-    out["learned_start_us"] = out["learned_step_us"] - out["plain_step_us"]
-    return out
+    plain_us, learned_us = _start_cost(model, torch.from_numpy(q0).to(dev), pipe, mlp, steps, nvtx="learned_start")
+    return {"workload": workload, "vertices": model.particle_count, "steps": steps, "plain_step_us": plain_us,
+            "learned_step_us": learned_us, "learned_start_us": learned_us - plain_us}
 
 
 def mlp_kernels(rows: int, repeats: int) -> dict:
