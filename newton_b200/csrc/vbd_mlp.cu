@@ -2,10 +2,10 @@
 //
 // A per-vertex MLP 64 -> 128 -> 128 -> 3 with SiLU activations predicts the step's correction
 // to the inertia target (x_solved - y) from one-ring features; the Gauss-Seidel iterations then
-// start from y + prediction instead of y.  Weights are BF16, every product accumulates in FP32
-// on the tensor cores.  Inference (vbd_mlp_forward, the step's warm start) runs on tcgen05.mma
-// with TMEM accumulators (vbd_mlp_tc.cuh).  Training is hand-written too, on mma.sync
-// m16n8k16 tiles:
+// start from y + prediction instead of y.  Every product accumulates in FP32 on the tensor cores.
+// Inference (vbd_mlp_forward; in the step mode also the features and the start, one launch) runs
+// on tcgen05.mma with FP16 operands and TMEM accumulators (vbd_mlp_tc.cuh).  Training is
+// hand-written too, on BF16 mma.sync m16n8k16 tiles with FP32 master weights:
 //   * mlp_tile_kernel: per warp, 16 samples through the three layers with the activations handed
 //     from one layer's accumulator fragments to the next layer's A fragments in registers; in
 //     training mode it continues with the backward pass (dY, dH2 = dY W3^T, dZ2, dH1 = dZ2 W2^T,
