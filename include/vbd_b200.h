@@ -358,8 +358,9 @@ int vbd_mlp_features(VbdSolver* solver, const float* corr_prev, const float* mea
                      void* stream);
 /* Y [n][3] = MLP(X [n][64]) on the 5th-generation tensor cores (tcgen05.mma: the FP32 weights of
  * params and the inputs rounded to FP16 in shared memory, FP32 accumulators in tensor memory;
- * bias + SiLU in f16x2 arithmetic with the hardware tanh approximation).  w16 is not read (it is the BF16 copy the training kernels use).  X must be
- * 16-byte aligned.  A wait that gives up is counted (vbd_mlp_timeouts). */
+ * bias + SiLU in f16x2 arithmetic with the hardware tanh approximation).  w16 is not read (it is
+ * the BF16 copy the training kernels use).  X must be 16-byte aligned.  A wait that gives up is
+ * counted (vbd_mlp_timeouts). */
 int vbd_mlp_forward(const float* params, const uint16_t* w16, const float* X, int32_t n, float* Y, void* stream);
 /* The same inference on the previous tensor-core path (mma.sync m16n8k16 fragments, exact SiLU),
  * kept to cross-check the tcgen05 kernel. */
