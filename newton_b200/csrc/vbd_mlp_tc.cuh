@@ -27,8 +27,9 @@
 // the FP32 weights rounded to FP16 and transposed to [N][K] (K-major), written once per CTA.
 // FP16 (11-bit significand) rather than BF16 (8-bit) operands: the values of this network
 // (standardized features, activations of a few units, weights below 1) are far inside FP16's
-// range, and the rounding of the inputs decides how well the start carries the previous
-// correction (measured: fewer Gauss-Seidel iterations after an FP16 start than after a BF16 one).
+// range, and the rounding of the inputs limits how well the start carries the previous correction
+// (measured on the draped cloth: fewer Gauss-Seidel iterations after an FP16 start than after a
+// BF16 one; on batched worlds the same).
 //
 // Every wait on an mbarrier is bounded: after kTcSpinLimit polls the group records a timeout (its
 // four warps decide together), stops taking tiles, waits (bounded again) for the MMAs it has
