@@ -331,8 +331,9 @@ int vbd_finalize(VbdSolver* solver, float* q_in, float* q_out, float* qd_out, fl
 int vbd_warm_start(VbdSolver* solver, const float* delta, void* stream);
 
 /* ---- learned warm start (no reference counterpart) -----------------------------------------
- * A per-vertex MLP 64 -> 128 -> 128 -> 3 (SiLU) with BF16 weights and FP32 accumulation on the
- * tensor cores predicts the coming step's correction x_solved - y, in units of the vertex's
+ * A per-vertex MLP 64 -> 128 -> 128 -> 3 (SiLU), trained on BF16 tensor-core tiles and run on
+ * FP16 ones (FP32 accumulation in both), predicts the coming step's correction x_solved - y, in
+ * units of the vertex's
  * characteristic element length L; the warm start is y + prediction * L (a zero network leaves
  * the start at y, plain VBD).  Parameters: an FP32 blob of vbd_mlp_sizes()->params floats
  * (W1 [64][128], b1, W2 [128][128], b2, W3 [128][8] with columns 3..7 zero, b3 [8]) and its BF16
