@@ -119,6 +119,23 @@ def test_training_fits_a_smooth_function():
     assert hist[-1] < 0.1 * hist[0]
 
 
+def test_saved_network_restores_the_same_predictions():
+    """state_dict / load_state_dict: a network restored into a new WarmStartMLP (FP32 blob, the
+    BF16 copy re-packed, standardization, feature set) predicts the same bits."""
+    mlp = L.WarmStartMLP("cuda:0", seed=5, feature_set="kinematic")
+    rng = np.random.default_rng(3)
+    X = torch.from_numpy(rng.normal(size=(700, L.IN)).astype(np.float32)).cuda()
+    mlp.set_standardization(X)
+    y0 = mlp.forward(X)
+    other = L.WarmStartMLP("cuda:0", seed=9)
+    other.load_state_dict(mlp.state_dict())
+    y1 = other.forward(X)
+    torch.cuda.synchronize()
+    assert other.feature_set == "kinematic"
+    assert torch.equal(other.w16, mlp.w16) and torch.equal(y0, y1)
+    assert torch.equal(other.mean, mlp.mean) and torch.equal(other.inv_std, mlp.inv_std)
+
+
 def test_zero_network_warm_start_is_plain_vbd():
     """The learned step mode with a network whose output is zero reproduces plain VBD bit for bit
     (same start y, same sweeps), contacts included."""
