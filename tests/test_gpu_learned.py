@@ -136,6 +136,35 @@ def test_saved_network_restores_the_same_predictions():
     assert torch.equal(other.mean, mlp.mean) and torch.equal(other.inv_std, mlp.inv_std)
 
 
+def test_learned_gated_steps_are_deterministic():
+    """The learned step mode under the residual gate (the benchmark's learned arm) gives the same
+    bits, iterations and residuals on two runs from the same state: the fused start kernel and the
+    gate's fixed-point sums are order-independent."""
+    dt = 1.0 / 600.0
+    model, q0 = scenes.draped_cloth(n=64, seed=2, height=0.9)
+    mlp = L.WarmStartMLP("cuda:0", seed=4, feature_set="corrections")
+    mlp.params.mul_(0.3)
+    mlp.pack()
+    pipe = CollisionPipeline(model, soft_contact_margin=5e-3)
+    runs = []
+    for _ in range(2):
+        solver = SolverVBD(model, iterations=10)
+        solver.set_warm_start(mlp, 10)
+        solver.set_residual_gate(0.9, max_iterations=40, relative=True, norm="mean", residual="sweep")
+        c = pipe.contacts()
+        a, b = model.state(), model.state()
+        a.particle_q.copy_(torch.from_numpy(q0).cuda())
+        for _ in range(15):
+            pipe.collide(a, c)
+            solver.step(a, b, None, c, dt)
+            a, b = b, a
+        torch.cuda.synchronize()
+        st = solver.gate_stats()
+        runs.append((a.particle_q.clone(), a.particle_qd.clone(), st["iterations"], st["last_residual"]))
+    assert torch.equal(runs[0][0], runs[1][0]) and torch.equal(runs[0][1], runs[1][1])
+    assert runs[0][2:] == runs[1][2:]
+
+
 def test_zero_network_warm_start_is_plain_vbd():
     """The learned step mode with a network whose output is zero reproduces plain VBD bit for bit
     (same start y, same sweeps), contacts included."""
